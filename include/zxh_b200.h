@@ -1,0 +1,167 @@
+/*
+ * zxh_b200.h -- C ABI of the B200-native ZXH state-vector path.
+ *
+ * This is the drop-in boundary for ZXH-Sim's single-GPU circuit-run path: a gate
+ * list goes in, the state, amplitudes or shot samples come out. Every entry point
+ * takes plain pointers and sizes; no PyTorch or C++ type crosses it. Each call
+ * returns ZXH_OK (0) or an error code; zxh_last_error() gives the message. No
+ * entry point aborts the process (the reference calls std::abort on any error,
+ * src/zxh/src/runtime/runtime_general.cpp:79-89).
+ *
+ * Citations are to the reference project ZXH-Sim (AxEquals-b/ZXH_ADAE), paths
+ * relative to its root. The pybind11 surface these entry points replace is
+ * src/zxh/src/pybind/bindings.cpp:79-118 (class _core.ZXH); the C++ methods behind
+ * it are declared in src/zxh/include/zxhsim/zxh.h:11-53.
+ */
+#ifndef ZXH_B200_H
+#define ZXH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Gate codes. Same numbering as the reference's gate_type_t
+ * (src/zxh/include/zxhsim/defs.h:61-74). CRz is stored as P + CP and Rx as U3,
+ * exactly as the reference records them (src/zxh/src/core/zxh.cpp:246-252,303-310). */
+enum {
+    ZXH_GATE_NONE = 0,
+    ZXH_GATE_BARRIER = 1,
+    ZXH_GATE_Z = 2,
+    ZXH_GATE_RZ = 3,
+    ZXH_GATE_P = 4,
+    ZXH_GATE_CRZ = 5,
+    ZXH_GATE_CP = 6,
+    ZXH_GATE_X = 7,
+    ZXH_GATE_CX = 8,
+    ZXH_GATE_H = 9,
+    ZXH_GATE_U3 = 10,
+    ZXH_GATE_RX = 11 /* accepted by zxh_push_gates, recorded as U3(theta, pi/2, -pi/2) */
+};
+
+/* One gate record. Field meaning follows the reference's gate_t
+ * (src/zxh/include/zxhsim/defs.h:76-84): U3 parameters are (theta, lambda, phi),
+ * the order ZXH::U3 takes them (src/zxh/include/zxhsim/zxh.h:36). 40 bytes. */
+typedef struct zxh_gate {
+    uint32_t type;
+    uint32_t cq;
+    uint32_t q;
+    uint32_t reserved;
+    double theta;
+    double lambda;
+    double phi;
+} zxh_gate;
+
+/* Amplitude storage type of a simulator handle. The reference is complex128 only
+ * (src/zxh/include/zxhsim/types.h:11-12); complex64 is this library's addition. */
+enum { ZXH_C64 = 1, ZXH_C128 = 2 };
+
+/* get_state orderings. ZXH_ORDER_REFERENCE is the reference's get_state order:
+ * virtual index bit-reversed so qubit 0 is the most significant bit, times the
+ * accumulated global phase (src/zxh/src/core/zxh.cpp:627-635). ZXH_ORDER_QUBIT
+ * keeps qubit q at bit q (Qiskit order), also times the global phase. */
+enum { ZXH_ORDER_REFERENCE = 0, ZXH_ORDER_QUBIT = 1 };
+
+/* Status codes. */
+enum {
+    ZXH_OK = 0,
+    ZXH_ERR_ARG = 1,     /* invalid argument (qubit out of range, null pointer, bad size) */
+    ZXH_ERR_STATE = 2,   /* call out of order (e.g. get_state before execute) */
+    ZXH_ERR_CUDA = 3,    /* CUDA runtime error */
+    ZXH_ERR_OOM = 4,     /* device or host allocation failed */
+    ZXH_ERR_LIMIT = 5,   /* size beyond a documented limit (n > 63, too many shots, ...) */
+    ZXH_ERR_TIMEOUT = 6  /* a bounded device-side wait gave up */
+};
+
+typedef struct zxh_sim zxh_sim;
+
+/* Library version string. */
+const char *zxh_version(void);
+
+/* Message of the last failing call on this handle, or of the last failing
+ * zxh_create in this thread when sim is NULL. Never NULL. */
+const char *zxh_last_error(const zxh_sim *sim);
+
+/* Replaces ZXH::ZXH(N, disable_x, eager_expand_all) (zxh.h:14, zxh.cpp:209-212).
+ * dtype is ZXH_C64 or ZXH_C128; device is the CUDA ordinal. n must be 1..63. */
+int zxh_create(zxh_sim **out, size_t n, int disable_x, int eager_expand_all, int dtype, int device);
+int zxh_destroy(zxh_sim *sim);
+
+/* Replace ZXH::set_seed / clear_seed / clear_gates (zxh.cpp:216-232). */
+int zxh_set_seed(zxh_sim *sim, uint64_t seed);
+int zxh_clear_seed(zxh_sim *sim);
+int zxh_clear_gates(zxh_sim *sim);
+
+/* Per-gate recorders; replace ZXH::Barrier..ZXH::Rx (zxh.cpp:234-310). */
+int zxh_barrier(zxh_sim *sim);
+int zxh_rz(zxh_sim *sim, size_t q, double theta);
+int zxh_crz(zxh_sim *sim, size_t cq, size_t q, double theta);
+int zxh_cp(zxh_sim *sim, size_t cq, size_t q, double theta);
+int zxh_p(zxh_sim *sim, size_t q, double theta);
+int zxh_z(zxh_sim *sim, size_t q);
+int zxh_x(zxh_sim *sim, size_t q);
+int zxh_cx(zxh_sim *sim, size_t cq, size_t q);
+int zxh_h(zxh_sim *sim, size_t q);
+int zxh_u3(zxh_sim *sim, size_t q, double theta, double lambda, double phi);
+int zxh_rx(zxh_sim *sim, size_t q, double theta);
+
+/* Batch recorder: appends count records in one call (the reference's Python
+ * loader calls one pybind method per gate, src/zxh/zxhsim/qasm.py:65-133).
+ * Validates every record first; on error nothing is appended. */
+int zxh_push_gates(zxh_sim *sim, const zxh_gate *gates, size_t count);
+
+/* Replaces ZXH::execute (zxh.cpp:312-553): resets the state to |0...0>, runs the
+ * whole recorded gate list on the device, and returns once the device is done. */
+int zxh_execute(zxh_sim *sim);
+
+/* Applies count more gates to the current state, continuing from where the last
+ * zxh_execute / zxh_apply left the state and the affine map, without recording
+ * them. Gates that would enlarge the state beyond the size chosen at the last
+ * zxh_execute return ZXH_ERR_LIMIT. No counterpart in the reference (its
+ * execute() always restarts from |0...0>, zxh.cpp:329-338). */
+int zxh_apply(zxh_sim *sim, const zxh_gate *gates, size_t count);
+
+/* Replaces ZXH::measure (zxh.cpp:555-559, measure_common.cpp:73-92): draws shots
+ * outcomes with the reference GPU sampler's uniform stream
+ * (src/zxh/src/measure/measure_cuda.cu:387-516,642-691) and keeps them on the
+ * device until zxh_get_results. */
+int zxh_measure(zxh_sim *sim, size_t shots);
+
+/* Replaces ZXH::get_results (zxh.cpp:561-564): copies the first shots cached
+ * outcomes to words, ceil(n/64) uint64 per shot, bit q = virtual qubit q
+ * (measure_result_pack.h:24-44 layout). */
+int zxh_get_results(zxh_sim *sim, uint64_t *words, size_t shots);
+
+/* Replaces ZXH::measured_count (zxh.cpp:566-569). */
+int zxh_measured_count(const zxh_sim *sim, size_t *out);
+
+/* Replaces ZXH::get_state (zxh.cpp:579-636). out is a HOST buffer of out_elems
+ * complex values (2^n required) in the handle's dtype, interleaved re/im. */
+int zxh_get_state(zxh_sim *sim, void *out, size_t out_elems, int order);
+
+/* Same as zxh_get_state but writes into a DEVICE buffer of 2^n elements. */
+int zxh_get_state_device(zxh_sim *sim, void *out_device, size_t out_elems, int order);
+
+/* Replace ZXH::required_M / num_qubits (zxh.cpp:638-646). */
+int zxh_required_M(const zxh_sim *sim, size_t *out);
+int zxh_num_qubits(const zxh_sim *sim, size_t *out);
+
+/* Device view of the real-address state after zxh_execute: data pointer, number
+ * of real address bits m (2^m elements), bytes per element, global phase. */
+int zxh_state_view(zxh_sim *sim, void **data, size_t *m_bits, size_t *elem_bytes, double *global_phase_re,
+                   double *global_phase_im);
+
+/* The handle's CUDA stream (cudaStream_t), for callers that time or order work. */
+int zxh_stream(zxh_sim *sim, void **stream);
+
+/* Launch statistics of the last zxh_execute / zxh_apply / zxh_measure: number of
+ * kernels launched and number of full read-modify-write passes over the state. */
+int zxh_last_stats(const zxh_sim *sim, uint64_t *kernels, uint64_t *passes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ZXH_B200_H */

@@ -1,0 +1,38 @@
+"""B200-native ZXH-Sim state-vector path.
+
+Drop-in for the reference's ``zxhsim`` package entry points on the single-GPU
+path (src/zxh/zxhsim/__init__.py of ZXH-Sim): ``ZXH``, ``init``, ``finalize``,
+``active``, ``rank``, ``nprocs``, ``PrintRes`` and ``load_circuit_transpiled``.
+"""
+from __future__ import annotations
+
+from . import _core
+from ._core import (
+    ZXH,
+    PrintRes,
+    active,
+    as_records,
+    finalize,
+    init,
+    library_path,
+    nprocs,
+    rank,
+    version,
+)
+from .loader import load_circuit_transpiled
+
+__version__ = _core.__version__
+
+__all__ = [
+    "ZXH",
+    "PrintRes",
+    "init",
+    "finalize",
+    "active",
+    "rank",
+    "nprocs",
+    "as_records",
+    "library_path",
+    "version",
+    "load_circuit_transpiled",
+]

@@ -1,0 +1,319 @@
+"""ctypes binding of libzxhb200.so (include/zxh_b200.h).
+
+Mirrors the reference's pybind11 module ``zxhsim._core``
+(src/zxh/src/pybind/bindings.cpp:79-118 of ZXH-Sim): the same class ``ZXH(n,
+disable_x=False, eager_expand_all=False)`` with the same method names and
+argument order, plus module functions ``init/finalize/active/rank/nprocs`` and
+``PrintRes``. Where the reference aborts the process on an error
+(src/zxh/src/runtime/runtime_general.cpp:79-89), this binding raises:
+``ValueError`` for bad arguments and limits, ``RuntimeError`` for calls out of
+order, CUDA errors and device-side timeouts, ``MemoryError`` for failed
+allocations.
+
+The library is required: importing this module without the built
+``libzxhb200.so`` raises ImportError; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from collections import Counter
+from pathlib import Path
+
+import numpy as np
+
+__version__ = "0.1.0"
+
+_HERE = Path(__file__).resolve().parent
+_LIB_PATH = Path(os.environ.get("ZXH_B200_LIB", _HERE / "libzxhb200.so"))
+
+if not _LIB_PATH.is_file():
+    raise ImportError(
+        f"{_LIB_PATH} is missing: build it with `make -C zxh_adae_b200/csrc` "
+        "(or __graft_entry__.build()); the B200 path has no CPU fallback"
+    )
+
+_lib = ctypes.CDLL(str(_LIB_PATH))
+
+GATE_DTYPE = np.dtype(
+    [("type", "<u4"), ("cq", "<u4"), ("q", "<u4"), ("reserved", "<u4"),
+     ("theta", "<f8"), ("lam", "<f8"), ("phi", "<f8")]
+)
+
+# gate codes (include/zxh_b200.h)
+BARRIER, Z, RZ, P, CRZ, CP, X, CX, H, U3, RX = 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11
+C64, C128 = 1, 2
+ORDER_REFERENCE, ORDER_QUBIT = 0, 1
+
+_P = ctypes.c_void_p
+_SZ = ctypes.c_size_t
+_D = ctypes.c_double
+_U64 = ctypes.c_uint64
+
+
+def _sig(name, args, res=ctypes.c_int):
+    f = getattr(_lib, name)
+    f.argtypes = args
+    f.restype = res
+    return f
+
+
+_sig("zxh_version", [], ctypes.c_char_p)
+_sig("zxh_last_error", [_P], ctypes.c_char_p)
+_sig("zxh_create", [ctypes.POINTER(_P), _SZ, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int])
+_sig("zxh_destroy", [_P])
+_sig("zxh_set_seed", [_P, _U64])
+_sig("zxh_clear_seed", [_P])
+_sig("zxh_clear_gates", [_P])
+_sig("zxh_barrier", [_P])
+_sig("zxh_rz", [_P, _SZ, _D])
+_sig("zxh_crz", [_P, _SZ, _SZ, _D])
+_sig("zxh_cp", [_P, _SZ, _SZ, _D])
+_sig("zxh_p", [_P, _SZ, _D])
+_sig("zxh_z", [_P, _SZ])
+_sig("zxh_x", [_P, _SZ])
+_sig("zxh_cx", [_P, _SZ, _SZ])
+_sig("zxh_h", [_P, _SZ])
+_sig("zxh_u3", [_P, _SZ, _D, _D, _D])
+_sig("zxh_rx", [_P, _SZ, _D])
+_sig("zxh_push_gates", [_P, _P, _SZ])
+_sig("zxh_execute", [_P])
+_sig("zxh_apply", [_P, _P, _SZ])
+_sig("zxh_measure", [_P, _SZ])
+_sig("zxh_get_results", [_P, _P, _SZ])
+_sig("zxh_measured_count", [_P, ctypes.POINTER(_SZ)])
+_sig("zxh_get_state", [_P, _P, _SZ, ctypes.c_int])
+_sig("zxh_get_state_device", [_P, _P, _SZ, ctypes.c_int])
+_sig("zxh_required_M", [_P, ctypes.POINTER(_SZ)])
+_sig("zxh_num_qubits", [_P, ctypes.POINTER(_SZ)])
+_sig("zxh_state_view", [_P, ctypes.POINTER(_P), ctypes.POINTER(_SZ), ctypes.POINTER(_SZ),
+                        ctypes.POINTER(_D), ctypes.POINTER(_D)])
+_sig("zxh_stream", [_P, ctypes.POINTER(_P)])
+_sig("zxh_last_stats", [_P, ctypes.POINTER(_U64), ctypes.POINTER(_U64)])
+
+_ERRORS = {1: ValueError, 2: RuntimeError, 3: RuntimeError, 4: MemoryError, 5: ValueError, 6: RuntimeError}
+
+
+def library_path() -> str:
+    return str(_LIB_PATH)
+
+
+def version() -> str:
+    return _lib.zxh_version().decode()
+
+
+def _raise(rc: int, handle) -> None:
+    msg = _lib.zxh_last_error(handle).decode(errors="replace")
+    raise _ERRORS.get(rc, RuntimeError)(msg or f"zxh error {rc}")
+
+
+def as_records(gates) -> np.ndarray:
+    """Gate records from a structured array or an iterable of
+    ``(type, cq, q[, theta, lambda, phi])`` tuples."""
+    if isinstance(gates, np.ndarray) and gates.dtype == GATE_DTYPE:
+        return np.ascontiguousarray(gates)
+    rows = list(gates)
+    rec = np.zeros(len(rows), GATE_DTYPE)
+    for i, g in enumerate(rows):
+        t, cq, q, th, la, ph = (list(g) + [0.0] * 6)[:6]
+        rec[i] = (t, cq, q, 0, th, la, ph)
+    return rec
+
+
+# Module-level runtime calls of the reference (bindings.cpp:86-90). One process
+# drives one or more GPUs through independent handles, so these only track state.
+_active = False
+
+
+def init() -> None:
+    global _active
+    _active = True
+
+
+def finalize() -> None:
+    global _active
+    _active = False
+
+
+def active() -> bool:
+    return _active
+
+
+def rank() -> int:
+    return 0
+
+
+def nprocs() -> int:
+    return 1
+
+
+def PrintRes(res, n: int) -> None:
+    """Prints bitstring counts, qubit n-1 first (zxh.cpp:842-871)."""
+    counts: dict = {}
+    for row in res:
+        s = "".join("1" if (i < len(row) and row[i]) else "0" for i in range(n - 1, -1, -1))
+        counts[s] = counts.get(s, 0) + 1
+    for k in sorted(counts):
+        print(f"{k}: {counts[k]}")
+
+
+class ZXH:
+    """One simulator: a gate list, a device state and its sampler results.
+
+    ``dtype`` selects complex128 (the reference's only type) or complex64
+    amplitudes; ``device`` is the CUDA ordinal.
+    """
+
+    def __init__(self, n: int, disable_x: bool = False, eager_expand_all: bool = False, *,
+                 dtype: str = "complex128", device: int = 0):
+        if dtype not in ("complex64", "complex128"):
+            raise ValueError("dtype must be 'complex64' or 'complex128'")
+        h = _P()
+        rc = _lib.zxh_create(ctypes.byref(h), int(n), int(bool(disable_x)), int(bool(eager_expand_all)),
+                             C64 if dtype == "complex64" else C128, int(device))
+        if rc != 0:
+            _raise(rc, None)
+        self._h = h
+        self._n = int(n)
+        self.dtype = np.dtype(dtype)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.zxh_destroy(h)
+            self._h = None
+
+    def close(self) -> None:
+        self.__del__()
+
+    def _ck(self, rc: int) -> None:
+        if rc != 0:
+            _raise(rc, self._h)
+
+    # --- recording (zxh.cpp:216-310) -------------------------------------------------
+    def set_seed(self, seed: int) -> None:
+        self._ck(_lib.zxh_set_seed(self._h, int(seed) & 0xFFFFFFFFFFFFFFFF))
+
+    def clear_seed(self) -> None:
+        self._ck(_lib.zxh_clear_seed(self._h))
+
+    def clear_gates(self) -> None:
+        self._ck(_lib.zxh_clear_gates(self._h))
+
+    def Barrier(self) -> None:
+        self._ck(_lib.zxh_barrier(self._h))
+
+    def Rz(self, q: int, theta: float) -> None:
+        self._ck(_lib.zxh_rz(self._h, q, theta))
+
+    def CRz(self, cq: int, q: int, theta: float) -> None:
+        self._ck(_lib.zxh_crz(self._h, cq, q, theta))
+
+    def CP(self, cq: int, q: int, theta: float) -> None:
+        self._ck(_lib.zxh_cp(self._h, cq, q, theta))
+
+    def P(self, q: int, theta: float) -> None:
+        self._ck(_lib.zxh_p(self._h, q, theta))
+
+    def Z(self, q: int) -> None:
+        self._ck(_lib.zxh_z(self._h, q))
+
+    def X(self, q: int) -> None:
+        self._ck(_lib.zxh_x(self._h, q))
+
+    def CX(self, cq: int, q: int) -> None:
+        self._ck(_lib.zxh_cx(self._h, cq, q))
+
+    def H(self, q: int) -> None:
+        self._ck(_lib.zxh_h(self._h, q))
+
+    def U3(self, q: int, theta: float, lam: float, phi: float) -> None:
+        """U3 with the reference's argument order (theta, lambda, phi) (zxh.h:36)."""
+        self._ck(_lib.zxh_u3(self._h, q, theta, lam, phi))
+
+    def Rx(self, q: int, theta: float) -> None:
+        self._ck(_lib.zxh_rx(self._h, q, theta))
+
+    def push_gates(self, gates) -> None:
+        rec = as_records(gates)
+        self._ck(_lib.zxh_push_gates(self._h, rec.ctypes.data, len(rec)))
+
+    # --- running ---------------------------------------------------------------------
+    def execute(self) -> None:
+        self._ck(_lib.zxh_execute(self._h))
+
+    def apply(self, gates) -> None:
+        """Applies more gates to the current state without recording them."""
+        rec = as_records(gates)
+        self._ck(_lib.zxh_apply(self._h, rec.ctypes.data, len(rec)))
+
+    def measure(self, shots: int) -> None:
+        self._ck(_lib.zxh_measure(self._h, int(shots)))
+
+    def measured_count(self) -> int:
+        out = _SZ(0)
+        self._ck(_lib.zxh_measured_count(self._h, ctypes.byref(out)))
+        return int(out.value)
+
+    def results_words(self, shots: int | None = None) -> np.ndarray:
+        """Cached outcomes as uint64 words (bit q = qubit q), in draw order."""
+        cnt = self.measured_count() if shots is None else int(shots)
+        words = np.zeros(max(cnt, 1), np.uint64)
+        self._ck(_lib.zxh_get_results(self._h, words.ctypes.data, cnt))
+        return words[:cnt]
+
+    def _rows(self, words: np.ndarray) -> list:
+        n = self._n
+        bits = ((words[:, None] >> np.arange(n, dtype=np.uint64)[None, :]) & np.uint64(1)).astype(bool)
+        return [list(map(bool, r)) for r in bits]
+
+    def get_results(self) -> list:
+        """list[list[bool]] with entry q = qubit q (bindings.cpp:61-75)."""
+        return self._rows(self.results_words())
+
+    def Sampling(self, shots: int) -> list:
+        self.measure(shots)
+        return self._rows(self.results_words(shots))
+
+    def sample_counts(self, shots: int) -> dict:
+        """Counts keyed by bitstrings with qubit n-1 first (bindings.cpp:36-54)."""
+        self.measure(shots)
+        words = self.results_words(shots)
+        n = self._n
+        cnt = Counter(words.tolist())
+        return {format(int(k), f"0{n}b"): int(v) for k, v in sorted(cnt.items())}
+
+    def get_state(self, order: int = ORDER_REFERENCE) -> np.ndarray:
+        """2^n amplitudes in the reference's get_state order (zxh.cpp:579-636)."""
+        out = np.zeros(1 << self._n, self.dtype)
+        self._ck(_lib.zxh_get_state(self._h, out.ctypes.data, out.size, int(order)))
+        return out
+
+    def get_state_device(self, ptr: int, elems: int, order: int = ORDER_REFERENCE) -> None:
+        self._ck(_lib.zxh_get_state_device(self._h, ctypes.c_void_p(ptr), int(elems), int(order)))
+
+    def required_M(self) -> int:
+        out = _SZ(0)
+        self._ck(_lib.zxh_required_M(self._h, ctypes.byref(out)))
+        return int(out.value)
+
+    def num_qubits(self) -> int:
+        return self._n
+
+    def state_view(self):
+        """(device pointer, real bits m, bytes per amplitude, global phase)."""
+        p, m, eb = _P(), _SZ(0), _SZ(0)
+        gr, gi = _D(0.0), _D(0.0)
+        self._ck(_lib.zxh_state_view(self._h, ctypes.byref(p), ctypes.byref(m), ctypes.byref(eb),
+                                     ctypes.byref(gr), ctypes.byref(gi)))
+        return int(p.value or 0), int(m.value), int(eb.value), complex(gr.value, gi.value)
+
+    def stream(self) -> int:
+        s = _P()
+        self._ck(_lib.zxh_stream(self._h, ctypes.byref(s)))
+        return int(s.value or 0)
+
+    def last_stats(self) -> tuple:
+        k, p = _U64(0), _U64(0)
+        self._ck(_lib.zxh_last_stats(self._h, ctypes.byref(k), ctypes.byref(p)))
+        return int(k.value), int(p.value)

@@ -1,0 +1,570 @@
+// capi.cpp -- the extern "C" boundary (include/zxh_b200.h) over the host core and
+// the sm_100a kernels. One zxh_sim handle owns its gate list, device state, CUDA
+// stream and scratch; handles are independent (the reference keeps its diagonal
+// buckets and U3 descriptors in process-global statics, kernel_cuda.cu:91-142).
+#include "../../include/zxh_b200.h"
+#include "host.h"
+#include "sampler.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <random>
+#include <string>
+#include <vector>
+
+using zxh::Gate;
+
+struct zxh_sim {
+    size_t n = 0;
+    bool disable_x = false, eager = false;
+    int dtype = ZXH_C128, elem_bytes = 16, device = 0, sms = 148;
+    std::vector<Gate> gates;
+    bool use_seed = false;
+    uint64_t seed = 0;
+    std::string err;
+    cudaStream_t stream = nullptr;
+
+    void *d_state = nullptr;
+    size_t state_cap_bytes = 0;
+    int M = 0;
+    zxh::WalkState ws;
+    bool executed = false;
+
+    uint8_t *d_blob = nullptr;
+    size_t blob_cap = 0;
+    uint8_t *h_stage = nullptr;
+    size_t stage_cap = 0;
+    zxh::DevStatus *d_status = nullptr;
+    zxh::DevStatus *h_status = nullptr;
+
+    uint8_t *d_samp = nullptr;
+    size_t samp_cap = 0;
+    zxh::SamplerScratch sc;
+    size_t measured = 0;
+
+    void *d_out = nullptr;
+    size_t out_cap = 0;
+
+    uint64_t stat_kernels = 0, stat_passes = 0;
+    zxh::PlanParams pp;
+};
+
+namespace {
+
+thread_local std::string g_create_error;
+
+int fail(zxh_sim *s, int code, const std::string &msg)
+{
+    if (s) s->err = msg;
+    else g_create_error = msg;
+    return code;
+}
+
+int cuda_fail(zxh_sim *s, cudaError_t e, const char *what)
+{
+    return fail(s, e == cudaErrorMemoryAllocation ? ZXH_ERR_OOM : ZXH_ERR_CUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(s, call, what)                             \
+    do {                                              \
+        cudaError_t e_ = (call);                      \
+        if (e_ != cudaSuccess) return cuda_fail(s, e_, what); \
+    } while (0)
+
+int use_device(zxh_sim *s)
+{
+    CK(s, cudaSetDevice(s->device), "cudaSetDevice");
+    return ZXH_OK;
+}
+
+int ensure_dev(zxh_sim *s, void **p, size_t &cap, size_t need, const char *what)
+{
+    if (need <= cap && *p) return ZXH_OK;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    cap = 0;
+    CK(s, cudaMalloc(p, need), what);
+    cap = need;
+    return ZXH_OK;
+}
+
+int check_q(zxh_sim *s, size_t q, const char *gate)
+{
+    if (q >= s->n) return fail(s, ZXH_ERR_ARG, std::string(gate) + " target qubit out of range");
+    return ZXH_OK;
+}
+
+int push(zxh_sim *s, uint32_t t, size_t cq, size_t q, double th, double la, double ph)
+{
+    Gate g;
+    g.type = t;
+    g.cq = uint32_t(cq);
+    g.q = uint32_t(q);
+    g.reserved = 0;
+    g.theta = th;
+    g.lambda = la;
+    g.phi = ph;
+    s->gates.push_back(g);
+    return ZXH_OK;
+}
+
+const double kPi = 3.14159265358979323846;
+
+// Lowers one record the way the reference's recorders do (zxh.cpp:234-310).
+int lower(zxh_sim *s, const zxh_gate &g, std::vector<Gate> &out)
+{
+    auto add = [&](uint32_t t, size_t cq, size_t q, double th, double la, double ph) {
+        Gate r;
+        r.type = t;
+        r.cq = uint32_t(cq);
+        r.q = uint32_t(q);
+        r.reserved = 0;
+        r.theta = th;
+        r.lambda = la;
+        r.phi = ph;
+        out.push_back(r);
+    };
+    const bool two = g.type == ZXH_GATE_CRZ || g.type == ZXH_GATE_CP || g.type == ZXH_GATE_CX;
+    if (g.type != ZXH_GATE_BARRIER && g.q >= s->n) return fail(s, ZXH_ERR_ARG, "gate target qubit out of range");
+    if (two && g.cq >= s->n) return fail(s, ZXH_ERR_ARG, "gate control qubit out of range");
+    switch (g.type) {
+    case ZXH_GATE_BARRIER: add(zxh::G_BARRIER, 0, 0, 0, 0, 0); break;
+    case ZXH_GATE_Z: add(zxh::G_Z, 0, g.q, 0, 0, 0); break;
+    case ZXH_GATE_RZ: add(zxh::G_RZ, 0, g.q, g.theta, 0, 0); break;
+    case ZXH_GATE_P: add(zxh::G_P, 0, g.q, g.theta, 0, 0); break;
+    case ZXH_GATE_CRZ:
+        add(zxh::G_P, 0, g.cq, -0.5 * g.theta, 0, 0);
+        add(zxh::G_CP, g.cq, g.q, g.theta, 0, 0);
+        break;
+    case ZXH_GATE_CP: add(zxh::G_CP, g.cq, g.q, g.theta, 0, 0); break;
+    case ZXH_GATE_X: add(zxh::G_X, 0, g.q, 0, 0, 0); break;
+    case ZXH_GATE_CX: add(zxh::G_CX, g.cq, g.q, 0, 0, 0); break;
+    case ZXH_GATE_H: add(zxh::G_H, 0, g.q, 0, 0, 0); break;
+    case ZXH_GATE_U3: add(zxh::G_U3, 0, g.q, g.theta, g.lambda, g.phi); break;
+    case ZXH_GATE_RX: add(zxh::G_U3, 0, g.q, g.theta, kPi / 2.0, -kPi / 2.0); break;
+    default: return fail(s, ZXH_ERR_ARG, "unknown gate type " + std::to_string(g.type));
+    }
+    return ZXH_OK;
+}
+
+// Uploads the plan, runs it and waits for the device.
+int run_plan(zxh_sim *s, const zxh::Plan &pl)
+{
+    const size_t bytes = std::max<size_t>(pl.blob.size(), 16);
+    if (bytes > s->stage_cap) {
+        if (s->h_stage) cudaFreeHost(s->h_stage);
+        s->h_stage = nullptr;
+        s->stage_cap = 0;
+        CK(s, cudaMallocHost(reinterpret_cast<void **>(&s->h_stage), bytes * 2), "cudaMallocHost(program)");
+        s->stage_cap = bytes * 2;
+    }
+    int rc = ensure_dev(s, reinterpret_cast<void **>(&s->d_blob), s->blob_cap, s->stage_cap, "cudaMalloc(program)");
+    if (rc) return rc;
+    std::memcpy(s->h_stage, pl.blob.data(), pl.blob.size());
+    CK(s, cudaMemcpyAsync(s->d_blob, s->h_stage, pl.blob.size(), cudaMemcpyHostToDevice, s->stream), "upload program");
+    CK(s, cudaMemsetAsync(s->d_status, 0, sizeof(zxh::DevStatus), s->stream), "reset status");
+    uint64_t kernels = 0;
+    CK(s, zxh::run_passes(pl.passes, s->d_blob, s->d_state, s->elem_bytes, s->d_status, s->sms, s->stream, kernels),
+       "launch");
+    CK(s, cudaMemcpyAsync(s->h_status, s->d_status, sizeof(zxh::DevStatus), cudaMemcpyDeviceToHost, s->stream),
+       "read status");
+    CK(s, cudaStreamSynchronize(s->stream), "execute");
+    s->stat_kernels = kernels;
+    s->stat_passes = 0;
+    for (const zxh::Pass &p : pl.passes)
+        if (p.kind != zxh::Pass::PRODUCT) s->stat_passes++;
+    if (s->h_status->code != 0)
+        return fail(s, int(s->h_status->code),
+                    "device wait gave up (site " + std::to_string(s->h_status->where) + ")");
+    return ZXH_OK;
+}
+
+void column_tables(const zxh::AffineMap &A, uint64_t tab[8][256])
+{
+    uint64_t col[64] = {0};
+    for (int q = 0; q < A.n(); q++)
+        for (int c = 0; c < A.m(); c++)
+            if ((A.row(q) >> c) & 1) col[c] |= 1ULL << q;
+    for (int k = 0; k < 8; k++)
+        for (int byte = 0; byte < 256; byte++) {
+            uint64_t v = 0;
+            for (int i = 0; i < 8; i++)
+                if ((byte >> i) & 1) v ^= col[8 * k + i];
+            tab[k][byte] = v;
+        }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *zxh_version(void) { return "zxh_b200 0.1.0 (sm_100a)"; }
+
+const char *zxh_last_error(const zxh_sim *sim)
+{
+    if (!sim) return g_create_error.c_str();
+    return sim->err.c_str();
+}
+
+int zxh_create(zxh_sim **out, size_t n, int disable_x, int eager_expand_all, int dtype, int device)
+{
+    if (!out) return fail(nullptr, ZXH_ERR_ARG, "out is null");
+    *out = nullptr;
+    if (n < 1 || n > 63) return fail(nullptr, ZXH_ERR_LIMIT, "n must be in 1..63");
+    if (dtype != ZXH_C64 && dtype != ZXH_C128) return fail(nullptr, ZXH_ERR_ARG, "dtype must be ZXH_C64 or ZXH_C128");
+    zxh_sim *s = new (std::nothrow) zxh_sim();
+    if (!s) return fail(nullptr, ZXH_ERR_OOM, "out of host memory");
+    s->n = n;
+    s->disable_x = disable_x != 0;
+    s->eager = eager_expand_all != 0;
+    s->dtype = dtype;
+    s->elem_bytes = dtype == ZXH_C64 ? 8 : 16;
+    s->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void **>(&s->d_status), sizeof(zxh::DevStatus));
+    if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void **>(&s->h_status), sizeof(zxh::DevStatus));
+    if (e != cudaSuccess) {
+        const std::string msg = std::string("CUDA init: ") + cudaGetErrorString(e);
+        zxh_destroy(s);
+        return fail(nullptr, ZXH_ERR_CUDA, msg);
+    }
+    s->ws.map.reset(int(n));
+    *out = s;
+    return ZXH_OK;
+}
+
+int zxh_destroy(zxh_sim *s)
+{
+    if (!s) return ZXH_OK;
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->d_state) cudaFree(s->d_state);
+    if (s->d_blob) cudaFree(s->d_blob);
+    if (s->h_stage) cudaFreeHost(s->h_stage);
+    if (s->d_status) cudaFree(s->d_status);
+    if (s->h_status) cudaFreeHost(s->h_status);
+    if (s->d_samp) cudaFree(s->d_samp);
+    if (s->d_out) cudaFree(s->d_out);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return ZXH_OK;
+}
+
+int zxh_set_seed(zxh_sim *s, uint64_t seed)
+{
+    if (!s) return ZXH_ERR_ARG;
+    s->use_seed = true;
+    s->seed = seed;
+    return ZXH_OK;
+}
+
+int zxh_clear_seed(zxh_sim *s)
+{
+    if (!s) return ZXH_ERR_ARG;
+    s->use_seed = false;
+    s->seed = 0;
+    return ZXH_OK;
+}
+
+int zxh_clear_gates(zxh_sim *s)
+{
+    if (!s) return ZXH_ERR_ARG;
+    s->gates.clear();
+    s->ws.gphase = zxh::cd(1.0, 0.0);  // zxh.cpp:228-232
+    return ZXH_OK;
+}
+
+int zxh_barrier(zxh_sim *s) { return s ? push(s, zxh::G_BARRIER, 0, 0, 0, 0, 0) : ZXH_ERR_ARG; }
+
+int zxh_rz(zxh_sim *s, size_t q, double theta)
+{
+    if (!s) return ZXH_ERR_ARG;
+    if (int rc = check_q(s, q, "Rz")) return rc;
+    return push(s, zxh::G_RZ, 0, q, theta, 0, 0);
+}
+
+int zxh_crz(zxh_sim *s, size_t cq, size_t q, double theta)
+{
+    if (!s) return ZXH_ERR_ARG;
+    if (cq >= s->n || q >= s->n) return fail(s, ZXH_ERR_ARG, "CRz qubit out of range");
+    push(s, zxh::G_P, 0, cq, -0.5 * theta, 0, 0);  // zxh.cpp:246-252
+    return push(s, zxh::G_CP, cq, q, theta, 0, 0);
+}
+
+int zxh_cp(zxh_sim *s, size_t cq, size_t q, double theta)
+{
+    if (!s) return ZXH_ERR_ARG;
+    if (cq >= s->n || q >= s->n) return fail(s, ZXH_ERR_ARG, "CP qubit out of range");
+    return push(s, zxh::G_CP, cq, q, theta, 0, 0);
+}
+
+int zxh_p(zxh_sim *s, size_t q, double theta)
+{
+    if (!s) return ZXH_ERR_ARG;
+    if (int rc = check_q(s, q, "P")) return rc;
+    return push(s, zxh::G_P, 0, q, theta, 0, 0);
+}
+
+int zxh_z(zxh_sim *s, size_t q)
+{
+    if (!s) return ZXH_ERR_ARG;
+    if (int rc = check_q(s, q, "Z")) return rc;
+    return push(s, zxh::G_Z, 0, q, 0, 0, 0);
+}
+
+int zxh_x(zxh_sim *s, size_t q)
+{
+    if (!s) return ZXH_ERR_ARG;
+    if (int rc = check_q(s, q, "X")) return rc;
+    return push(s, zxh::G_X, 0, q, 0, 0, 0);
+}
+
+int zxh_cx(zxh_sim *s, size_t cq, size_t q)
+{
+    if (!s) return ZXH_ERR_ARG;
+    if (cq >= s->n || q >= s->n) return fail(s, ZXH_ERR_ARG, "CX qubit out of range");
+    return push(s, zxh::G_CX, cq, q, 0, 0, 0);
+}
+
+int zxh_h(zxh_sim *s, size_t q)
+{
+    if (!s) return ZXH_ERR_ARG;
+    if (int rc = check_q(s, q, "H")) return rc;
+    return push(s, zxh::G_H, 0, q, 0, 0, 0);
+}
+
+int zxh_u3(zxh_sim *s, size_t q, double theta, double lambda, double phi)
+{
+    if (!s) return ZXH_ERR_ARG;
+    if (int rc = check_q(s, q, "U3")) return rc;
+    return push(s, zxh::G_U3, 0, q, theta, lambda, phi);
+}
+
+int zxh_rx(zxh_sim *s, size_t q, double theta)
+{
+    if (!s) return ZXH_ERR_ARG;
+    if (int rc = check_q(s, q, "Rx")) return rc;
+    return push(s, zxh::G_U3, 0, q, theta, kPi / 2.0, -kPi / 2.0);  // zxh.cpp:303-310
+}
+
+int zxh_push_gates(zxh_sim *s, const zxh_gate *gates, size_t count)
+{
+    if (!s) return ZXH_ERR_ARG;
+    if (count && !gates) return fail(s, ZXH_ERR_ARG, "gates is null");
+    std::vector<Gate> tmp;
+    tmp.reserve(count + count / 8);
+    for (size_t i = 0; i < count; i++)
+        if (int rc = lower(s, gates[i], tmp)) return rc;
+    s->gates.insert(s->gates.end(), tmp.begin(), tmp.end());
+    return ZXH_OK;
+}
+
+int zxh_execute(zxh_sim *s)
+{
+    if (!s) return ZXH_ERR_ARG;
+    if (int rc = use_device(s)) return rc;
+    const int M = s->eager ? int(s->n) : zxh::calc_mem(s->gates.data(), s->gates.size(), int(s->n), s->disable_x);
+    const size_t need = size_t(s->elem_bytes) << M;
+    if (int rc = ensure_dev(s, &s->d_state, s->state_cap_bytes, std::max<size_t>(need, 256), "cudaMalloc(state)"))
+        return rc;
+    s->M = M;
+    s->executed = false;
+    s->measured = 0;
+    zxh::WalkState &ws = s->ws;
+    ws.map.reset(int(s->n));
+    ws.m = 0;
+    ws.gphase = zxh::cd(1.0, 0.0);
+    ws.fresh = true;
+    ws.init_bits = 0;
+    if (s->eager) {  // expand_all, zxh.cpp:721-729
+        for (size_t q = 0; q < s->n; q++) ws.map.append_col(int(q));
+        ws.m = int(s->n);
+        ws.init_bits = int(s->n);
+    }
+    zxh::WalkState start = ws;
+    std::vector<zxh::Op> ops;
+    std::string err;
+    if (int rc = zxh::walk(s->gates.data(), s->gates.size(), s->disable_x, M, ws, ops, err)) return fail(s, rc, err);
+    zxh::Plan pl;
+    if (int rc = zxh::plan(ops, s->elem_bytes, s->pp, start, pl, err)) return fail(s, rc, err);
+    if (int rc = run_plan(s, pl)) return rc;
+    ws.fresh = false;
+    s->executed = true;
+    return ZXH_OK;
+}
+
+int zxh_apply(zxh_sim *s, const zxh_gate *gates, size_t count)
+{
+    if (!s) return ZXH_ERR_ARG;
+    if (!s->executed) return fail(s, ZXH_ERR_STATE, "zxh_apply requires zxh_execute first");
+    if (count && !gates) return fail(s, ZXH_ERR_ARG, "gates is null");
+    if (int rc = use_device(s)) return rc;
+    std::vector<Gate> tmp;
+    for (size_t i = 0; i < count; i++)
+        if (int rc = lower(s, gates[i], tmp)) return rc;
+    zxh::WalkState start = s->ws;
+    zxh::WalkState ws = s->ws;
+    std::vector<zxh::Op> ops;
+    std::string err;
+    if (int rc = zxh::walk(tmp.data(), tmp.size(), s->disable_x, s->M, ws, ops, err)) return fail(s, rc, err);
+    zxh::Plan pl;
+    if (int rc = zxh::plan(ops, s->elem_bytes, s->pp, start, pl, err)) return fail(s, rc, err);
+    if (int rc = run_plan(s, pl)) return rc;
+    s->ws = ws;
+    s->measured = 0;
+    return ZXH_OK;
+}
+
+int zxh_measure(zxh_sim *s, size_t shots)
+{
+    if (!s) return ZXH_ERR_ARG;
+    if (shots == 0) {
+        s->measured = 0;
+        return ZXH_OK;
+    }
+    if (!s->executed) return fail(s, ZXH_ERR_STATE, "measure requires execute() to be called first");
+    if (shots > (size_t(1) << 40)) return fail(s, ZXH_ERR_LIMIT, "too many shots");
+    if (int rc = use_device(s)) return rc;
+    const uint64_t base = s->use_seed ? s->seed : uint64_t(std::random_device{}());  // measure_cuda.cu:111-116
+    const uint64_t stream_seed = zxh::mix_seed_host(base, 0);                        // measure_cuda.cu:1033
+    const int m = s->ws.m;
+    const uint64_t local = 1ULL << m;
+    const uint64_t seglen = std::min<uint64_t>(4096, local);
+    const uint64_t nseg = local / seglen;
+    const size_t need = zxh::SamplerScratch::need_bytes(nseg, shots);
+    if (int rc = ensure_dev(s, reinterpret_cast<void **>(&s->d_samp), s->samp_cap, need, "cudaMalloc(sampler)"))
+        return rc;
+    s->sc.carve(s->d_samp, nseg, shots);
+    static thread_local uint64_t tab[8][256];
+    column_tables(s->ws.map, tab);
+    CK(s, cudaMemsetAsync(s->d_status, 0, sizeof(zxh::DevStatus), s->stream), "reset status");
+    uint64_t kernels = 0;
+    CK(s, zxh::run_sampler(s->d_state, s->elem_bytes, m, shots, stream_seed, &tab[0][0], s->ws.map.b(), s->sc,
+                           s->d_status, s->sms, s->stream, kernels),
+       "sampler launch");
+    CK(s, cudaMemcpyAsync(s->h_status, s->d_status, sizeof(zxh::DevStatus), cudaMemcpyDeviceToHost, s->stream),
+       "read status");
+    CK(s, cudaStreamSynchronize(s->stream), "sampler");
+    s->stat_kernels = kernels;
+    s->stat_passes = 2;
+    if (s->h_status->code != 0) return fail(s, int(s->h_status->code), "sampler device wait gave up");
+    s->measured = shots;
+    return ZXH_OK;
+}
+
+int zxh_get_results(zxh_sim *s, uint64_t *words, size_t shots)
+{
+    if (!s) return ZXH_ERR_ARG;
+    if (shots == 0) return ZXH_OK;
+    if (!words) return fail(s, ZXH_ERR_ARG, "get_results results is null");
+    if (shots > s->measured) return fail(s, ZXH_ERR_ARG, "get_results count exceeds cached result count");
+    if (int rc = use_device(s)) return rc;
+    CK(s, cudaMemcpyAsync(words, s->sc.words, shots * sizeof(uint64_t), cudaMemcpyDeviceToHost, s->stream),
+       "copy results");
+    CK(s, cudaStreamSynchronize(s->stream), "copy results");
+    return ZXH_OK;
+}
+
+int zxh_measured_count(const zxh_sim *s, size_t *out)
+{
+    if (!s || !out) return ZXH_ERR_ARG;
+    *out = s->measured;
+    return ZXH_OK;
+}
+
+static int state_to_device(zxh_sim *s, void *dst, int order)
+{
+    const int N = int(s->n);
+    const uint64_t nv = 1ULL << N;
+    if (s->ws.m < N) CK(s, cudaMemsetAsync(dst, 0, size_t(nv) * size_t(s->elem_bytes), s->stream), "zero state");
+    static thread_local uint64_t tab[8][256];
+    column_tables(s->ws.map, tab);
+    void *dtab = nullptr;
+    CK(s, cudaMallocAsync(&dtab, sizeof(tab), s->stream), "cudaMallocAsync(table)");
+    CK(s, cudaMemcpyAsync(dtab, tab, sizeof(tab), cudaMemcpyHostToDevice, s->stream), "upload table");
+    CK(s, zxh::run_scatter(s->d_state, 1ULL << s->ws.m, static_cast<uint64_t *>(dtab), s->ws.map.b(), N, order,
+                           s->ws.gphase.real(), s->ws.gphase.imag(), dst, s->elem_bytes, s->sms, s->stream),
+       "scatter");
+    CK(s, cudaFreeAsync(dtab, s->stream), "cudaFreeAsync(table)");
+    return ZXH_OK;
+}
+
+int zxh_get_state(zxh_sim *s, void *out, size_t out_elems, int order)
+{
+    if (!s) return ZXH_ERR_ARG;
+    if (!s->executed) return fail(s, ZXH_ERR_STATE, "get_state requires execute() to be called first");
+    if (!out) return fail(s, ZXH_ERR_ARG, "out is null");
+    if (s->n > 40) return fail(s, ZXH_ERR_LIMIT, "get_state export needs fewer than 41 qubits");
+    const uint64_t nv = 1ULL << s->n;
+    if (out_elems < nv) return fail(s, ZXH_ERR_ARG, "output buffer holds fewer than 2^n amplitudes");
+    if (int rc = use_device(s)) return rc;
+    const size_t bytes = size_t(nv) * size_t(s->elem_bytes);
+    if (int rc = ensure_dev(s, &s->d_out, s->out_cap, bytes, "cudaMalloc(get_state)")) return rc;
+    if (int rc = state_to_device(s, s->d_out, order)) return rc;
+    CK(s, cudaMemcpyAsync(out, s->d_out, bytes, cudaMemcpyDeviceToHost, s->stream), "copy state");
+    CK(s, cudaStreamSynchronize(s->stream), "get_state");
+    return ZXH_OK;
+}
+
+int zxh_get_state_device(zxh_sim *s, void *out_device, size_t out_elems, int order)
+{
+    if (!s) return ZXH_ERR_ARG;
+    if (!s->executed) return fail(s, ZXH_ERR_STATE, "get_state requires execute() to be called first");
+    if (!out_device) return fail(s, ZXH_ERR_ARG, "out is null");
+    if (s->n > 40) return fail(s, ZXH_ERR_LIMIT, "get_state export needs fewer than 41 qubits");
+    if (out_elems < (1ULL << s->n)) return fail(s, ZXH_ERR_ARG, "output buffer holds fewer than 2^n amplitudes");
+    if (int rc = use_device(s)) return rc;
+    if (int rc = state_to_device(s, out_device, order)) return rc;
+    CK(s, cudaStreamSynchronize(s->stream), "get_state");
+    return ZXH_OK;
+}
+
+int zxh_required_M(const zxh_sim *s, size_t *out)
+{
+    if (!s || !out) return ZXH_ERR_ARG;
+    *out = size_t(zxh::calc_mem(s->gates.data(), s->gates.size(), int(s->n), s->disable_x));
+    return ZXH_OK;
+}
+
+int zxh_num_qubits(const zxh_sim *s, size_t *out)
+{
+    if (!s || !out) return ZXH_ERR_ARG;
+    *out = s->n;
+    return ZXH_OK;
+}
+
+int zxh_state_view(zxh_sim *s, void **data, size_t *m_bits, size_t *elem_bytes, double *gre, double *gim)
+{
+    if (!s) return ZXH_ERR_ARG;
+    if (!s->executed) return fail(s, ZXH_ERR_STATE, "state_view requires execute() first");
+    if (data) *data = s->d_state;
+    if (m_bits) *m_bits = size_t(s->ws.m);
+    if (elem_bytes) *elem_bytes = size_t(s->elem_bytes);
+    if (gre) *gre = s->ws.gphase.real();
+    if (gim) *gim = s->ws.gphase.imag();
+    return ZXH_OK;
+}
+
+int zxh_stream(zxh_sim *s, void **stream)
+{
+    if (!s || !stream) return ZXH_ERR_ARG;
+    *stream = s->stream;
+    return ZXH_OK;
+}
+
+int zxh_last_stats(const zxh_sim *s, uint64_t *kernels, uint64_t *passes)
+{
+    if (!s) return ZXH_ERR_ARG;
+    if (kernels) *kernels = s->stat_kernels;
+    if (passes) *passes = s->stat_passes;
+    return ZXH_OK;
+}
+
+}  // extern "C"

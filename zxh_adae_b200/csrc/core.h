@@ -1,0 +1,195 @@
+// core.h -- host-side types of the B200-native ZXH path: gate records, the GF(2)
+// affine address map, the operation list produced by the execute() walk, and the
+// per-pass programs handed to the device kernels.
+//
+// Reference: ZXH-Sim (AxEquals-b/ZXH_ADAE), src/zxh/. The affine map follows
+// src/core/bitmat.cpp:34-161 and selector.cpp:20-49; the walk follows
+// src/core/zxh.cpp:312-553.
+#pragma once
+
+#include <complex>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace zxh {
+
+using cd = std::complex<double>;
+
+enum GateType : uint32_t {
+    G_NONE = 0,
+    G_BARRIER = 1,
+    G_Z = 2,
+    G_RZ = 3,
+    G_P = 4,
+    G_CRZ = 5,
+    G_CP = 6,
+    G_X = 7,
+    G_CX = 8,
+    G_H = 9,
+    G_U3 = 10,
+    G_RX = 11,
+};
+
+struct Gate {
+    uint32_t type;
+    uint32_t cq;
+    uint32_t q;
+    uint32_t reserved;
+    double theta;
+    double lambda;
+    double phi;
+};
+static_assert(sizeof(Gate) == 40, "gate record is 40 bytes");
+
+// A selector S(x) = parity(alpha & x) xor beta over real addresses
+// (src/zxh/include/zxhsim/defs.h:23-37).
+struct Sel {
+    uint64_t alpha = 0;
+    int beta = 0;
+};
+
+inline int parity64(uint64_t x) { return __builtin_popcountll(x) & 1; }
+inline uint64_t low_mask(int bits) { return bits >= 64 ? ~0ULL : ((1ULL << bits) - 1ULL); }
+
+// GF(2) affine map x_virtual = A x_real xor b. rows[q] is row q of A (m bits).
+// Columns are linearly independent, so A x = e_q has at most one solution. All
+// solutions are computed at once by one elimination of [A | I] and cached until the
+// map changes (the reference re-runs a full elimination for every U3 probe,
+// bitmat.cpp:46-122).
+class AffineMap {
+  public:
+    void reset(int n);
+    int n() const { return n_; }
+    int m() const { return m_; }
+    uint64_t row(int q) const { return rows_[q]; }
+    uint64_t b() const { return b_; }
+    Sel selector(int q) const { return Sel{rows_[q], int((b_ >> q) & 1)}; }
+    // delta with A delta = e_q; false if e_q is outside the column span.
+    bool solve(int q, uint64_t &delta);
+    void append_col(int q);          // append e_q as a new column
+    void row_xor(int dst, int src);  // CX transport
+    void flip_b(int q) { b_ ^= 1ULL << q; }
+    void b_xor(int dst, int src) { if ((b_ >> src) & 1) b_ ^= 1ULL << dst; }
+    // virtual index of a real index
+    uint64_t virt(uint64_t real) const;
+
+  private:
+    void refresh();
+    int n_ = 0;
+    int m_ = 0;
+    uint64_t rows_[64] = {0};
+    uint64_t b_ = 0;
+    bool dirty_ = true;
+    uint64_t sol_[64] = {0};
+    uint64_t solvable_ = 0;
+};
+
+// ---------------------------------------------------------------------------
+// Operation list: what the reference's execute() would launch, in order, with
+// real-address selectors and deltas already resolved.
+
+struct U3Op {
+    uint64_t delta = 0;
+    Sel sel;            // pair (i, i^delta) with S(i) == 0 is "even"
+    cd u[4];            // u00, u01, u10, u11
+    bool has_ctrl = false;
+    Sel ctrl;           // explicit CX: act only where ctrl(i) == 1
+};
+
+struct DiagTerm {
+    Sel s0, s1;
+    bool two = false;   // CP (s0 && s1) vs P (s0)
+    double theta = 0.0;
+};
+
+struct Op {
+    enum Kind { EXPAND, U3BATCH, DIAG } kind;
+    // EXPAND: state grows from m to m+1 bits then one pair op with delta 2^m.
+    // U3BATCH: pair ops applied in order on the current 2^m block.
+    // DIAG: one diagonal window.
+    int m = 0;                   // state bits when the op runs (after growth for EXPAND)
+    std::vector<U3Op> u3;
+    std::vector<DiagTerm> diag;
+};
+
+// ---------------------------------------------------------------------------
+// Device programs (plain-old-data, uploaded once per execute()).
+
+constexpr int kMaxTileBits = 16;
+
+struct LinTerm { uint32_t bit; uint32_t pad; int64_t coef; };
+struct QuadTerm { uint32_t i; uint32_t j; int64_t coef; };
+struct GenTerm {
+    uint64_t a1_t, a1_out, a2_t, a2_out;  // selector masks split into tile coords / out-of-tile real bits
+    uint32_t b1, b2;
+    int64_t coef;                         // added where S1 && S2 (P: S2 == 1 always)
+};
+
+// One diagonal window compiled for a tile geometry. Phases are int64 fixed-point
+// turns: coef / 2^64 of a full turn, so sums wrap exactly modulo 2*pi.
+struct DiagDev {
+    int64_t c0;
+    int64_t lin_in[kMaxTileBits];   // linear coefficient of each tile coordinate
+    uint32_t n_out_lin, n_out_quad, n_in_quad, n_cross, n_gen, pad;
+    uint64_t off_out_lin, off_out_quad, off_in_quad, off_cross, off_gen;  // byte offsets in the blob
+};
+
+struct U3Dev {
+    uint64_t delta_t;   // delta in tile coordinates
+    uint64_t alpha_t;   // selector alpha restricted to tile coordinates
+    uint64_t alpha_out; // selector alpha on out-of-tile real bits
+    uint32_t beta;
+    uint32_t pivot;     // a set bit of delta_t
+    uint64_t ctrl_t, ctrl_out;
+    uint32_t ctrl_beta, has_ctrl;
+    double u[8];        // u00 re,im, u01, u10, u11
+};
+
+struct StepDev { uint32_t kind; uint32_t pad; uint64_t off; };  // kind 0 = DIAG, 1 = U3
+enum { STEP_DIAG = 0, STEP_U3 = 1 };
+
+// Tile geometry: tile coordinate k maps to real bit pos[k]. Coordinates [0, c) are
+// the c low contiguous bits; coordinates [c, T) are single high bits.
+struct TileDev {
+    uint32_t T, c, h, m;
+    uint64_t tile_mask;   // real bits inside the tile
+    uint64_t free_mask;   // real bits < m outside the tile (tile index deposits here)
+    uint64_t ntiles;
+    uint8_t pos[kMaxTileBits];
+    uint32_t nsteps, pad;
+    uint64_t off_steps;
+};
+
+struct ExpandDev {
+    uint32_t m_old;      // doubling from 2^m_old to 2^(m_old+1)
+    uint32_t has_ctrl;
+    uint64_t alpha;      // selector of the pair op restricted to old bits
+    uint32_t beta, ctrl_beta;
+    uint64_t ctrl_alpha;
+    double u[8];
+};
+
+// A pair op applied straight in global memory (deltas spanning more high bits
+// than a tile holds).
+struct PairDev {
+    uint32_t m, pivot;
+    uint64_t delta, alpha;
+    uint32_t beta, has_ctrl;
+    uint64_t ctrl_alpha;
+    uint32_t ctrl_beta, pad;
+    double u[8];
+};
+
+struct ProductDev {
+    uint32_t m;          // output bits
+    uint32_t c;          // low bits covered by the lookup table
+    double a0[2];        // initial amplitude
+    double v[64][4];     // per-bit factor: amplitude multiplier when the bit is 0 / 1 (complex)
+};
+
+// Status word shared with the device (bounded waits report here).
+struct DevStatus { uint32_t code; uint32_t where; uint64_t info; };
+
+}  // namespace zxh

@@ -1,0 +1,152 @@
+// dev.cuh -- device helpers shared by the sm_100a kernels: element traits, parity,
+// phase application from fixed-point turns, bounded mbarrier waits, and the TMA
+// bulk-copy PTX (cp.async.bulk, no multicast).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace zxh {
+
+constexpr int kThreads = 256;
+constexpr uint32_t kErrTimeout = 6;  // ZXH_ERR_TIMEOUT
+
+template <typename E>
+struct ET;
+template <>
+struct ET<float2> {
+    using R = float;
+    static constexpr int V = 2;  // elements per 16-byte vector
+};
+template <>
+struct ET<double2> {
+    using R = double;
+    static constexpr int V = 1;
+};
+
+__device__ __forceinline__ int par64(uint64_t x) { return __popcll(x) & 1; }
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+// Multiplies a by exp(i * 2 pi * th / 2^64). th is a signed fixed-point number of
+// turns, so the angle is pi * x with x = th / 2^63 in [-1, 1).
+__device__ __forceinline__ float2 apply_phase(float2 a, int64_t th)
+{
+    // x = xh + xl: xh has the top 24 bits (exact in float), xl < 2^-23 the rest.
+    const int32_t hi = static_cast<int32_t>(th >> 40);
+    const float xh = static_cast<float>(hi) * 0x1p-23f;
+    const float xl = static_cast<float>(static_cast<uint64_t>(th) & ((1ULL << 40) - 1ULL)) * 0x1p-63f;
+    float s, c;
+    sincospif(xh, &s, &c);
+    // first-order correction for xl (second-order term below 1e-13)
+    const float d = 3.14159265358979f * xl;
+    const float s2 = fmaf(d, c, s), c2 = fmaf(-d, s, c);
+    float2 o;
+    o.x = a.x * c2 - a.y * s2;
+    o.y = a.x * s2 + a.y * c2;
+    return o;
+}
+
+__device__ __forceinline__ double2 apply_phase(double2 a, int64_t th)
+{
+    const double x = static_cast<double>(th) * 0x1p-63;
+    double s, c;
+    sincospi(x, &s, &c);
+    double2 o;
+    o.x = a.x * c - a.y * s;
+    o.y = a.x * s + a.y * c;
+    return o;
+}
+
+__device__ __forceinline__ int64_t warp_sum_i64(int64_t v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ double warp_sum_f64(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+struct DevStatusView { uint32_t code; uint32_t where; uint64_t info; };
+
+__device__ __forceinline__ void report(void *status, uint32_t code, uint32_t where, uint64_t info)
+{
+    DevStatusView *s = static_cast<DevStatusView *>(status);
+    if (atomicCAS(&s->code, 0u, code) == 0u) {
+        s->where = where;
+        s->info = info;
+    }
+}
+
+// ---- mbarrier ----
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Waits for the phase with the given parity; gives up after about 2^31 SM clocks
+// (around a second) and returns false.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity))
+        if (clock64() - t0 > (1LL << 31)) return false;
+    return true;
+}
+
+// ---- TMA bulk copies (1-D, no tensor map, no multicast) ----
+
+__device__ __forceinline__ void bulk_g2s(void *smem_dst, const void *gsrc, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(smem_dst)),
+                 "l"(gsrc), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_s2g(void *gdst, const void *smem_src, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst), "r"(smem_u32(smem_src)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+
+__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+
+__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+}  // namespace zxh

@@ -1,0 +1,810 @@
+// host.cpp -- host side of the B200-native ZXH path:
+//   * AffineMap: the GF(2) address map with cached solutions.
+//   * walk():    the reference execute() schedule (src/zxh/src/core/zxh.cpp:312-553)
+//                turned into an operation list with real-address selectors.
+//   * plan():    the operation list compiled into device passes (product init,
+//                doubling, TMA-tiled passes with fused diagonal windows).
+#include "host.h"
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <stdexcept>
+
+namespace zxh {
+
+// ---------------------------------------------------------------------------
+// AffineMap
+
+void AffineMap::reset(int n)
+{
+    n_ = n;
+    m_ = 0;
+    std::memset(rows_, 0, sizeof(rows_));
+    b_ = 0;
+    dirty_ = true;
+}
+
+void AffineMap::append_col(int q)
+{
+    rows_[q] |= 1ULL << m_;  // bitmat_t::append_col(e_q), bitmat.cpp:139-145
+    m_++;
+    dirty_ = true;
+}
+
+void AffineMap::row_xor(int dst, int src)
+{
+    rows_[dst] ^= rows_[src];  // bitmat_t::row_xor, bitmat.cpp:34-44
+    dirty_ = true;
+}
+
+// One elimination of [A | I_n]: the reduced pivot row of column c carries, in its
+// right half, which original rows sum to it. The solution of A x = e_q is then
+// x_c = bit q of that combination, and e_q is in the span iff no zero row of the
+// reduced left half has bit q set in its combination.
+void AffineMap::refresh()
+{
+    uint64_t left[64], right[64];
+    for (int i = 0; i < n_; i++) {
+        left[i] = rows_[i];
+        right[i] = 1ULL << i;
+    }
+    int pivot_of_col[64];
+    int row = 0;
+    for (int col = 0; col < m_; col++) {
+        pivot_of_col[col] = -1;
+        int piv = row;
+        while (piv < n_ && !((left[piv] >> col) & 1)) piv++;
+        if (piv >= n_) continue;
+        std::swap(left[piv], left[row]);
+        std::swap(right[piv], right[row]);
+        for (int i = 0; i < n_; i++)
+            if (i != row && ((left[i] >> col) & 1)) {
+                left[i] ^= left[row];
+                right[i] ^= right[row];
+            }
+        pivot_of_col[col] = row;
+        row++;
+    }
+    uint64_t null_union = 0;
+    for (int i = 0; i < n_; i++)
+        if (left[i] == 0) null_union |= right[i];
+    solvable_ = 0;
+    for (int q = 0; q < n_; q++) {
+        if ((null_union >> q) & 1) {
+            sol_[q] = 0;
+            continue;
+        }
+        uint64_t x = 0;
+        for (int col = 0; col < m_; col++)
+            if (pivot_of_col[col] >= 0 && ((right[pivot_of_col[col]] >> q) & 1)) x |= 1ULL << col;
+        sol_[q] = x;
+        solvable_ |= 1ULL << q;
+    }
+    dirty_ = false;
+}
+
+bool AffineMap::solve(int q, uint64_t &delta)
+{
+    if (dirty_) refresh();
+    if (!((solvable_ >> q) & 1)) return false;
+    delta = sol_[q];
+    return true;
+}
+
+uint64_t AffineMap::virt(uint64_t real) const
+{
+    uint64_t v = 0;
+    for (int q = 0; q < n_; q++)
+        if (parity64(real & rows_[q]) ^ int((b_ >> q) & 1)) v |= 1ULL << q;
+    return v;
+}
+
+// ---------------------------------------------------------------------------
+// The execute() walk.
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+const double kU3BatchEps = double(1e-5f);  // zxh.cpp:29 (a float literal promoted to double)
+
+cd phase(double a) { return std::exp(cd(0.0, a)); }
+
+void build_u3(double th, double la, double ph, cd u[4])
+{
+    // build_u3_matrix, zxh.cpp:101-113
+    const double c = std::cos(th / 2.0), s = std::sin(th / 2.0);
+    const cd el = phase(la), ep = phase(ph), epl = phase(ph + la);
+    u[0] = cd(c, 0.0);
+    u[1] = -el * s;
+    u[2] = ep * s;
+    u[3] = epl * c;
+}
+
+struct Acc {
+    bool active = false;
+    cd u[4] = {cd(1, 0), cd(0, 0), cd(0, 0), cd(1, 0)};
+};
+
+bool close_val(cd a, cd b) { return std::abs(a - b) <= kU3BatchEps; }
+
+bool is_identity(const Acc &a)
+{
+    return close_val(a.u[0], cd(1, 0)) && close_val(a.u[1], cd(0, 0)) && close_val(a.u[2], cd(0, 0)) &&
+           close_val(a.u[3], cd(1, 0));
+}
+
+void acc_reset(Acc &a)
+{
+    a.active = false;
+    a.u[0] = cd(1, 0);
+    a.u[1] = cd(0, 0);
+    a.u[2] = cd(0, 0);
+    a.u[3] = cd(1, 0);
+}
+
+void left_mul(Acc &a, const cd n[4])
+{
+    // left_multiply_u3, zxh.cpp:144-156
+    const cd o00 = a.u[0], o01 = a.u[1], o10 = a.u[2], o11 = a.u[3];
+    a.u[0] = n[0] * o00 + n[1] * o10;
+    a.u[1] = n[0] * o01 + n[1] * o11;
+    a.u[2] = n[2] * o00 + n[3] * o10;
+    a.u[3] = n[2] * o01 + n[3] * o11;
+    a.active = !is_identity(a);
+}
+
+}  // namespace
+
+int walk(const Gate *gates, size_t count, bool disable_x, int M, WalkState &ws, std::vector<Op> &ops, std::string &err)
+{
+    AffineMap &A = ws.map;
+    const int N = A.n();
+    std::vector<DiagTerm> window;
+    Acc pend[64];
+    int pend_count = 0;
+
+    auto flush_window = [&]() {
+        if (window.empty()) return;
+        Op op;
+        op.kind = Op::DIAG;
+        op.m = ws.m;
+        op.diag.swap(window);
+        ops.push_back(std::move(op));
+        window.clear();
+    };
+
+    auto flush_u3_batch = [&]() {
+        if (pend_count == 0) return;
+        Op op;
+        op.kind = Op::U3BATCH;
+        op.m = ws.m;
+        for (int q = 0; q < N; q++) {
+            if (!pend[q].active) continue;
+            U3Op u;
+            A.solve(q, u.delta);
+            u.delta &= low_mask(ws.m);
+            u.sel = A.selector(q);
+            for (int k = 0; k < 4; k++) u.u[k] = pend[q].u[k];
+            op.u3.push_back(u);
+        }
+        for (int q = 0; q < N; q++) acc_reset(pend[q]);
+        pend_count = 0;
+        if (!op.u3.empty()) ops.push_back(std::move(op));
+    };
+
+    // solve_expand (zxh.cpp:701-719): returns whether the state grew.
+    auto solve_expand = [&](int q, uint64_t &delta) -> int {
+        if (A.solve(q, delta)) return 0;
+        if (ws.m + 1 > M) return -1;
+        ws.m++;
+        A.append_col(q);
+        delta = 1ULL << (A.m() - 1);
+        return 1;
+    };
+
+    // One pair op, after a possible expansion (apply_u3 / apply_x_explicit /
+    // apply_cx_explicit, zxh.cpp:742-825).
+    auto pair_op = [&](int q, const cd u[4], int ctrl_q) -> int {
+        uint64_t d = 0;
+        const int grew = solve_expand(q, d);
+        if (grew < 0) return -1;
+        U3Op op;
+        op.delta = d & low_mask(ws.m);
+        op.sel = A.selector(q);
+        for (int k = 0; k < 4; k++) op.u[k] = u[k];
+        if (ctrl_q >= 0) {
+            op.has_ctrl = true;
+            op.ctrl = A.selector(ctrl_q);
+        }
+        Op o;
+        o.kind = grew ? Op::EXPAND : Op::U3BATCH;
+        o.m = ws.m;
+        o.u3.push_back(op);
+        ops.push_back(std::move(o));
+        return 0;
+    };
+
+    for (size_t gi = 0; gi < count;) {
+        const Gate &g = gates[gi];
+        if (g.type == G_H || g.type == G_U3) {
+            flush_window();
+            while (gi < count && (gates[gi].type == G_H || gates[gi].type == G_U3)) {
+                const Gate &u = gates[gi];
+                const bool isH = u.type == G_H;
+                cd mat[4];
+                build_u3(isH ? kPi / 2.0 : u.theta, isH ? kPi : u.lambda, isH ? 0.0 : u.phi, mat);
+                uint64_t d;
+                if (!A.solve(int(u.q), d)) {
+                    flush_u3_batch();
+                    if (pair_op(int(u.q), mat, -1) < 0) {
+                        err = "gate needs a state larger than the size chosen at execute()";
+                        return 5;
+                    }
+                    gi++;
+                    continue;
+                }
+                Acc &a = pend[u.q];
+                const bool was = a.active;
+                if (!was) acc_reset(a), a.active = true;
+                left_mul(a, mat);
+                if (!was && a.active) pend_count++;
+                else if (was && !a.active) pend_count--;
+                gi++;
+            }
+            flush_u3_batch();
+            continue;
+        }
+        switch (g.type) {
+        case G_BARRIER:
+            flush_window();
+            break;
+        case G_Z:
+        case G_RZ: {
+            const double th = g.type == G_Z ? kPi : g.theta;
+            DiagTerm t;
+            t.s0 = A.selector(int(g.q));
+            t.theta = th;
+            window.push_back(t);
+            ws.gphase *= phase(-0.5 * th);  // zxh.cpp:477-493
+            break;
+        }
+        case G_P: {
+            DiagTerm t;
+            t.s0 = A.selector(int(g.q));
+            t.theta = g.theta;
+            window.push_back(t);
+            break;
+        }
+        case G_CP: {
+            // All CP gates stay in the window: a CP whose selector straddles the
+            // reference's 8-bit lane split is applied by the same pass (the
+            // reference flushes and launches cp_kernel, zxh.cpp:526-541; the
+            // product of diagonal factors is the same).
+            DiagTerm t;
+            t.s0 = A.selector(int(g.cq));
+            t.s1 = A.selector(int(g.q));
+            t.two = true;
+            t.theta = g.theta;
+            window.push_back(t);
+            break;
+        }
+        case G_X:
+            if (disable_x) {
+                flush_window();
+                const cd X[4] = {cd(0, 0), cd(1, 0), cd(1, 0), cd(0, 0)};
+                if (pair_op(int(g.q), X, -1) < 0) {
+                    err = "gate needs a state larger than the size chosen at execute()";
+                    return 5;
+                }
+            } else {
+                A.flip_b(int(g.q));
+            }
+            break;
+        case G_CX:
+            if (disable_x) {
+                flush_window();
+                const cd X[4] = {cd(0, 0), cd(1, 0), cd(1, 0), cd(0, 0)};
+                if (pair_op(int(g.q), X, int(g.cq)) < 0) {
+                    err = "gate needs a state larger than the size chosen at execute()";
+                    return 5;
+                }
+            } else {
+                A.row_xor(int(g.q), int(g.cq));
+                A.b_xor(int(g.q), int(g.cq));
+            }
+            break;
+        default:
+            break;
+        }
+        gi++;
+    }
+    flush_window();
+    return 0;
+}
+
+int calc_mem(const Gate *gates, size_t count, int n, bool disable_x)
+{
+    // zxh.cpp:648-681
+    AffineMap A;
+    A.reset(n);
+    for (size_t i = 0; i < count; i++) {
+        const Gate &g = gates[i];
+        bool probe = false;
+        if (g.type == G_X || g.type == G_CX) {
+            if (!disable_x) {
+                if (g.type == G_CX) A.row_xor(int(g.q), int(g.cq));
+            } else {
+                probe = true;
+            }
+        } else if (g.type == G_H || g.type == G_U3) {
+            probe = true;
+        }
+        if (probe) {
+            uint64_t d;
+            if (!A.solve(int(g.q), d)) A.append_col(int(g.q));
+        }
+    }
+    return A.m();
+}
+
+// ---------------------------------------------------------------------------
+// Planner
+
+namespace {
+
+int64_t turns(double theta)
+{
+    // theta / (2 pi) as a 64-bit fixed-point fraction of a turn, wrapping mod 2^64.
+    long double f = (long double)theta / (2.0L * 3.141592653589793238462643383279502884L);
+    f -= floorl(f);
+    long double s = f * 18446744073709551616.0L;  // 2^64
+    if (s >= 18446744073709551616.0L) s -= 18446744073709551616.0L;
+    return (int64_t)(uint64_t)s;
+}
+
+bool single_bit_or_zero(uint64_t a) { return (a & (a - 1)) == 0; }
+
+int bit_index(uint64_t a) { return __builtin_ctzll(a); }
+
+struct Poly {
+    int64_t c0 = 0;
+    std::map<int, int64_t> lin;
+    std::map<std::pair<int, int>, int64_t> quad;
+    std::vector<DiagTerm> general;
+
+    void add_lin(int i, int64_t c) { lin[i] += c; }
+    void add_quad(int i, int j, int64_t c)
+    {
+        if (i == j) { lin[i] += c; return; }
+        if (i > j) std::swap(i, j);
+        quad[{i, j}] += c;
+    }
+};
+
+// Expands a window into a polynomial over real address bits where every selector
+// is a single bit (or constant), and keeps the rest as general terms.
+Poly to_poly(const std::vector<DiagTerm> &terms)
+{
+    Poly p;
+    for (const DiagTerm &t : terms) {
+        const bool simple = single_bit_or_zero(t.s0.alpha) && (!t.two || single_bit_or_zero(t.s1.alpha));
+        if (!simple) {
+            p.general.push_back(t);
+            continue;
+        }
+        const int64_t th = turns(t.theta);
+        // [S] = c + s*x_i with (c, s) = (beta, 1 - 2 beta); constant selector: s = 0.
+        const int64_t c0 = t.s0.beta, s0 = t.s0.alpha ? (t.s0.beta ? -1 : 1) : 0;
+        const int i0 = t.s0.alpha ? bit_index(t.s0.alpha) : -1;
+        if (!t.two) {
+            p.c0 += th * c0;
+            if (s0) p.add_lin(i0, th * s0);
+            continue;
+        }
+        const int64_t c1 = t.s1.beta, s1 = t.s1.alpha ? (t.s1.beta ? -1 : 1) : 0;
+        const int i1 = t.s1.alpha ? bit_index(t.s1.alpha) : -1;
+        p.c0 += th * c0 * c1;
+        if (s1) p.add_lin(i1, th * c0 * s1);
+        if (s0) p.add_lin(i0, th * c1 * s0);
+        if (s0 && s1) p.add_quad(i0, i1, th * s0 * s1);
+    }
+    return p;
+}
+
+template <typename T>
+uint64_t put(std::vector<uint8_t> &blob, const T &v)
+{
+    uint64_t off = (blob.size() + 15) & ~uint64_t(15);
+    blob.resize(off + sizeof(T));
+    std::memcpy(blob.data() + off, &v, sizeof(T));
+    return off;
+}
+
+template <typename T>
+uint64_t put_vec(std::vector<uint8_t> &blob, const std::vector<T> &v)
+{
+    uint64_t off = (blob.size() + 15) & ~uint64_t(15);
+    blob.resize(off + sizeof(T) * v.size() + 16);
+    if (!v.empty()) std::memcpy(blob.data() + off, v.data(), sizeof(T) * v.size());
+    return off;
+}
+
+uint64_t pext_pos(uint64_t x, const uint8_t *pos, int T)
+{
+    uint64_t r = 0;
+    for (int k = 0; k < T; k++)
+        if ((x >> pos[k]) & 1) r |= 1ULL << k;
+    return r;
+}
+
+// Compiles one window for a tile geometry; returns its blob offset.
+uint64_t compile_diag(std::vector<uint8_t> &blob, const std::vector<DiagTerm> &terms, const TileDev &g)
+{
+    const Poly p = to_poly(terms);
+    int coord_of_bit[64];
+    for (int i = 0; i < 64; i++) coord_of_bit[i] = -1;
+    for (uint32_t k = 0; k < g.T; k++) coord_of_bit[g.pos[k]] = int(k);
+
+    DiagDev d;
+    std::memset(&d, 0, sizeof(d));
+    d.c0 = p.c0;
+    std::vector<LinTerm> out_lin;
+    std::vector<QuadTerm> out_quad, in_quad, cross;
+    for (const auto &kv : p.lin) {
+        if (kv.second == 0) continue;
+        const int k = coord_of_bit[kv.first];
+        if (k >= 0) d.lin_in[k] += kv.second;
+        else out_lin.push_back(LinTerm{uint32_t(kv.first), 0, kv.second});
+    }
+    for (const auto &kv : p.quad) {
+        if (kv.second == 0) continue;
+        const int i = kv.first.first, j = kv.first.second;
+        const int ki = coord_of_bit[i], kj = coord_of_bit[j];
+        if (ki >= 0 && kj >= 0) in_quad.push_back(QuadTerm{uint32_t(std::min(ki, kj)), uint32_t(std::max(ki, kj)), kv.second});
+        else if (ki >= 0) cross.push_back(QuadTerm{uint32_t(ki), uint32_t(j), kv.second});
+        else if (kj >= 0) cross.push_back(QuadTerm{uint32_t(kj), uint32_t(i), kv.second});
+        else out_quad.push_back(QuadTerm{uint32_t(i), uint32_t(j), kv.second});
+    }
+    std::vector<GenTerm> gen;
+    for (const DiagTerm &t : p.general) {
+        GenTerm gt;
+        gt.a1_t = pext_pos(t.s0.alpha, g.pos, int(g.T));
+        gt.a1_out = t.s0.alpha & ~g.tile_mask;
+        gt.b1 = uint32_t(t.s0.beta);
+        if (t.two) {
+            gt.a2_t = pext_pos(t.s1.alpha, g.pos, int(g.T));
+            gt.a2_out = t.s1.alpha & ~g.tile_mask;
+            gt.b2 = uint32_t(t.s1.beta);
+        } else {
+            gt.a2_t = 0;
+            gt.a2_out = 0;
+            gt.b2 = 1;  // constant-true second selector
+        }
+        gt.coef = turns(t.theta);
+        gen.push_back(gt);
+    }
+    d.n_out_lin = uint32_t(out_lin.size());
+    d.n_out_quad = uint32_t(out_quad.size());
+    d.n_in_quad = uint32_t(in_quad.size());
+    d.n_cross = uint32_t(cross.size());
+    d.n_gen = uint32_t(gen.size());
+    d.off_out_lin = put_vec(blob, out_lin);
+    d.off_out_quad = put_vec(blob, out_quad);
+    d.off_in_quad = put_vec(blob, in_quad);
+    d.off_cross = put_vec(blob, cross);
+    d.off_gen = put_vec(blob, gen);
+    return put(blob, d);
+}
+
+U3Dev compile_u3(const U3Op &u, const TileDev &g)
+{
+    U3Dev d;
+    std::memset(&d, 0, sizeof(d));
+    d.delta_t = pext_pos(u.delta, g.pos, int(g.T));
+    d.alpha_t = pext_pos(u.sel.alpha, g.pos, int(g.T));
+    d.alpha_out = u.sel.alpha & ~g.tile_mask;
+    d.beta = uint32_t(u.sel.beta);
+    d.pivot = uint32_t(__builtin_ctzll(d.delta_t));
+    if (u.has_ctrl) {
+        d.has_ctrl = 1;
+        d.ctrl_t = pext_pos(u.ctrl.alpha, g.pos, int(g.T));
+        d.ctrl_out = u.ctrl.alpha & ~g.tile_mask;
+        d.ctrl_beta = uint32_t(u.ctrl.beta);
+    }
+    for (int k = 0; k < 4; k++) {
+        d.u[2 * k] = u.u[k].real();
+        d.u[2 * k + 1] = u.u[k].imag();
+    }
+    return d;
+}
+
+TileDev make_geom(int m, int c, const std::vector<int> &dirs)
+{
+    TileDev g;
+    std::memset(&g, 0, sizeof(g));
+    g.m = uint32_t(m);
+    g.c = uint32_t(c);
+    g.h = uint32_t(dirs.size());
+    g.T = g.c + g.h;
+    uint64_t mask = low_mask(c);
+    for (int k = 0; k < c; k++) g.pos[k] = uint8_t(k);
+    for (size_t j = 0; j < dirs.size(); j++) {
+        g.pos[c + j] = uint8_t(dirs[j]);
+        mask |= 1ULL << dirs[j];
+    }
+    g.tile_mask = mask;
+    g.free_mask = low_mask(m) & ~mask;
+    g.ntiles = 1ULL << (m - int(g.T));
+    return g;
+}
+
+}  // namespace
+
+void Plan::clear()
+{
+    blob.clear();
+    passes.clear();
+}
+
+int plan(const std::vector<Op> &ops, int elem_bytes, const PlanParams &pp, const WalkState &start, Plan &out,
+         std::string &err)
+{
+    out.clear();
+    size_t i = 0;
+    int m = start.m;
+
+    // 1. Product-state prefix: expansions whose selector is constant on the old
+    //    bits, starting from |0...0>, and diagonal windows made only of P phases on
+    //    existing bits / constant selectors. The prefix is written in one pass.
+    if (start.fresh) {
+        ProductDev pd;
+        std::memset(&pd, 0, sizeof(pd));
+        cd a0(1.0, 0.0);
+        cd v[64][2];
+        int pm = start.init_bits;
+        for (int b = 0; b < pm; b++) {
+            v[b][0] = cd(1.0, 0.0);
+            v[b][1] = cd(0.0, 0.0);
+        }
+        size_t j = 0;
+        for (; j < ops.size(); j++) {
+            const Op &op = ops[j];
+            if (op.kind == Op::EXPAND) {
+                const U3Op &u = op.u3[0];
+                const uint64_t old_alpha = u.sel.alpha & low_mask(pm);
+                const bool ctrl_const = !u.has_ctrl || (u.ctrl.alpha & low_mask(pm + 1)) == 0;
+                if (old_alpha != 0 || !ctrl_const || op.m != pm + 1) break;
+                if (u.has_ctrl && !u.ctrl.beta) {
+                    // control constantly false: identity on old bits, new half zero
+                    v[pm][0] = cd(1, 0);
+                    v[pm][1] = cd(0, 0);
+                } else if (u.sel.beta == 0) {
+                    v[pm][0] = u.u[0];
+                    v[pm][1] = u.u[2];
+                } else {
+                    v[pm][0] = u.u[3];
+                    v[pm][1] = u.u[1];
+                }
+                pm++;
+                continue;
+            }
+            if (op.kind == Op::DIAG) {
+                bool ok = true;
+                for (const DiagTerm &t : op.diag)
+                    if (t.two && t.s0.alpha && t.s1.alpha) ok = false;
+                    else if (!single_bit_or_zero(t.s0.alpha) || (t.two && !single_bit_or_zero(t.s1.alpha))) ok = false;
+                if (!ok) break;
+                // linear phases factor over bits
+                for (const DiagTerm &t : op.diag) {
+                    const Sel *var = nullptr;
+                    bool cst = true;
+                    if (t.s0.alpha) var = &t.s0;
+                    else cst = cst && t.s0.beta;
+                    if (t.two) {
+                        if (t.s1.alpha) var = &t.s1;
+                        else cst = cst && t.s1.beta;
+                    }
+                    if (!cst) continue;
+                    const cd ph = std::exp(cd(0.0, t.theta));
+                    if (!var) { a0 *= ph; continue; }
+                    const int b = bit_index(var->alpha);
+                    v[b][var->beta ? 0 : 1] *= ph;
+                }
+                continue;
+            }
+            break;
+        }
+        i = j;
+        pd.m = uint32_t(pm);
+        pd.c = uint32_t(std::min(pm, pp.product_table_bits));
+        pd.a0[0] = a0.real();
+        pd.a0[1] = a0.imag();
+        for (int b = 0; b < pm; b++) {
+            pd.v[b][0] = v[b][0].real();
+            pd.v[b][1] = v[b][0].imag();
+            pd.v[b][2] = v[b][1].real();
+            pd.v[b][3] = v[b][1].imag();
+        }
+        // lookup table over the low c bits, computed in double
+        std::vector<double> tab(size_t(2) << pd.c);
+        for (uint64_t y = 0; y < (1ULL << pd.c); y++) {
+            cd acc(1.0, 0.0);
+            for (uint32_t b = 0; b < pd.c; b++) acc *= ((y >> b) & 1) ? v[b][1] : v[b][0];
+            tab[2 * y] = acc.real();
+            tab[2 * y + 1] = acc.imag();
+        }
+        Pass ps;
+        ps.kind = Pass::PRODUCT;
+        ps.m = pm;
+        ps.off = put(out.blob, pd);
+        if (elem_bytes == 8) {
+            std::vector<float> tf(tab.begin(), tab.end());
+            ps.off2 = put_vec(out.blob, tf);
+        } else {
+            ps.off2 = put_vec(out.blob, tab);
+        }
+        out.passes.push_back(ps);
+        m = pm;
+    }
+
+    const int tmax = elem_bytes == 8 ? pp.tile_bits_c64 : pp.tile_bits_c128;
+    int last_tile_pass = -1;          // index of a tile pass that can take an epilogue
+    const std::vector<DiagTerm> *held = nullptr;  // window waiting for the next tile pass
+
+    auto emit_tile = [&](int mm, int c, const std::vector<int> &dirs, const std::vector<const U3Op *> &u3s,
+                         const std::vector<DiagTerm> *pro) {
+        TileDev g = make_geom(mm, c, dirs);
+        std::vector<StepDev> steps;
+        if (pro) steps.push_back(StepDev{STEP_DIAG, 0, compile_diag(out.blob, *pro, g)});
+        for (const U3Op *u : u3s) steps.push_back(StepDev{STEP_U3, 0, put(out.blob, compile_u3(*u, g))});
+        Pass ps;
+        ps.kind = Pass::TILE;
+        ps.m = mm;
+        ps.geom = g;
+        ps.steps = steps;
+        out.passes.push_back(ps);
+        return int(out.passes.size()) - 1;
+    };
+
+    auto attach_epilogue = [&](int pidx, const std::vector<DiagTerm> &w) {
+        Pass &ps = out.passes[pidx];
+        ps.steps.push_back(StepDev{STEP_DIAG, 0, compile_diag(out.blob, w, ps.geom)});
+    };
+
+    auto standalone_diag = [&](int mm, const std::vector<DiagTerm> &w) {
+        const int T = std::min(mm, pp.diag_tile_bits);
+        std::vector<const U3Op *> none;
+        emit_tile(mm, T, std::vector<int>(), none, &w);
+    };
+
+    for (; i < ops.size(); i++) {
+        const Op &op = ops[i];
+        if (op.kind == Op::DIAG) {
+            if (held) standalone_diag(m, *held), held = nullptr;
+            if (last_tile_pass >= 0 && out.passes[last_tile_pass].m == op.m &&
+                out.passes[last_tile_pass].steps.size() < size_t(pp.max_steps)) {
+                attach_epilogue(last_tile_pass, op.diag);
+                last_tile_pass = -1;  // keep one epilogue window per pass
+            } else if (i + 1 < ops.size() && ops[i + 1].kind == Op::U3BATCH && ops[i + 1].m == op.m) {
+                held = &op.diag;
+            } else {
+                standalone_diag(op.m, op.diag);
+                last_tile_pass = -1;
+            }
+            continue;
+        }
+        if (op.kind == Op::EXPAND) {
+            if (held) standalone_diag(m, *held), held = nullptr;
+            const U3Op &u = op.u3[0];
+            ExpandDev e;
+            std::memset(&e, 0, sizeof(e));
+            e.m_old = uint32_t(op.m - 1);
+            e.alpha = u.sel.alpha & low_mask(op.m - 1);
+            e.beta = uint32_t(u.sel.beta);
+            e.has_ctrl = u.has_ctrl ? 1 : 0;
+            e.ctrl_alpha = u.ctrl.alpha & low_mask(op.m - 1);
+            e.ctrl_beta = uint32_t(u.ctrl.beta);
+            for (int k = 0; k < 4; k++) {
+                e.u[2 * k] = u.u[k].real();
+                e.u[2 * k + 1] = u.u[k].imag();
+            }
+            Pass ps;
+            ps.kind = Pass::EXPAND;
+            ps.m = op.m;
+            ps.off = put(out.blob, e);
+            out.passes.push_back(ps);
+            m = op.m;
+            last_tile_pass = -1;
+            continue;
+        }
+        // U3BATCH: group pair ops into tiles.
+        const int mm = op.m;
+        const int cfull = std::min(mm, tmax);
+        std::vector<const U3Op *> low, high;
+        for (const U3Op &u : op.u3) ((u.delta >> cfull) == 0 ? low : high).push_back(&u);
+        std::vector<std::pair<std::vector<int>, std::vector<const U3Op *>>> groups;  // (dirs, ops) ; dirs empty = low
+        for (size_t k = 0; k < low.size(); k += size_t(pp.max_gates)) {
+            std::vector<const U3Op *> gvec(low.begin() + k, low.begin() + std::min(low.size(), k + size_t(pp.max_gates)));
+            groups.push_back({std::vector<int>(), gvec});
+        }
+        const int clo = std::min(cfull, pp.contig_bits);
+        const int maxdirs = tmax - clo;
+        std::vector<int> dirs;
+        std::vector<const U3Op *> cur;
+        std::vector<const U3Op *> direct;  // ops too wide for any tile
+        auto close_high = [&]() {
+            if (cur.empty()) return;
+            std::sort(dirs.begin(), dirs.end());
+            groups.push_back({dirs, cur});
+            dirs.clear();
+            cur.clear();
+        };
+        for (const U3Op *u : high) {
+            std::vector<int> need;
+            for (int b = clo; b < mm; b++)
+                if ((u->delta >> b) & 1) need.push_back(b);
+            if (int(need.size()) > maxdirs) {
+                direct.push_back(u);
+                continue;
+            }
+            std::vector<int> uni = dirs;
+            for (int b : need)
+                if (std::find(uni.begin(), uni.end(), b) == uni.end()) uni.push_back(b);
+            if (int(uni.size()) > maxdirs || int(cur.size()) >= pp.max_gates) {
+                close_high();
+                uni = need;
+            }
+            dirs = uni;
+            cur.push_back(u);
+        }
+        close_high();
+        if (!direct.empty()) {
+            // pair ops of one batch commute, so the wide ones go first; a held
+            // window must still precede them.
+            if (held) standalone_diag(mm, *held), held = nullptr;
+            for (const U3Op *u : direct) {
+                PairDev pd;
+                std::memset(&pd, 0, sizeof(pd));
+                pd.m = uint32_t(mm);
+                pd.pivot = uint32_t(63 - __builtin_clzll(u->delta));
+                pd.delta = u->delta;
+                pd.alpha = u->sel.alpha;
+                pd.beta = uint32_t(u->sel.beta);
+                pd.has_ctrl = u->has_ctrl ? 1 : 0;
+                pd.ctrl_alpha = u->ctrl.alpha;
+                pd.ctrl_beta = uint32_t(u->ctrl.beta);
+                for (int k = 0; k < 4; k++) {
+                    pd.u[2 * k] = u->u[k].real();
+                    pd.u[2 * k + 1] = u->u[k].imag();
+                }
+                Pass ps;
+                ps.kind = Pass::PAIR;
+                ps.m = mm;
+                ps.off = put(out.blob, pd);
+                out.passes.push_back(ps);
+            }
+            last_tile_pass = -1;
+        }
+        for (size_t k = 0; k < groups.size(); k++) {
+            const bool lowgrp = groups[k].first.empty();
+            const int c = lowgrp ? cfull : clo;
+            const std::vector<DiagTerm> *pro = (k == 0) ? held : nullptr;
+            last_tile_pass = emit_tile(mm, c, groups[k].first, groups[k].second, pro);
+        }
+        held = nullptr;
+        m = mm;
+    }
+    if (held) standalone_diag(m, *held);
+
+    // finalize step arrays
+    for (Pass &ps : out.passes) {
+        if (ps.kind != Pass::TILE) continue;
+        ps.geom.nsteps = uint32_t(ps.steps.size());
+        ps.geom.off_steps = put_vec(out.blob, ps.steps);
+        ps.off = put(out.blob, ps.geom);
+    }
+    return 0;
+}
+
+}  // namespace zxh

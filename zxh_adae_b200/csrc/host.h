@@ -1,0 +1,53 @@
+// host.h -- walk and planner interfaces (implemented in host.cpp).
+#pragma once
+
+#include "core.h"
+
+namespace zxh {
+
+struct WalkState {
+    AffineMap map;
+    int m = 0;                 // current real address bits of the state
+    cd gphase = cd(1.0, 0.0);  // accumulated Z/Rz global phase (zxh.cpp:477-493)
+    bool fresh = true;         // state is |0...0> and no device work has been done yet
+    int init_bits = 0;         // bits of the fresh |0...0> state (n under eager_expand_all, else 0)
+};
+
+// Runs the reference execute() schedule over gates, updating ws (affine map, m,
+// global phase) and appending the operations the reference would launch.
+// M bounds the state size. Returns 0 or a status code with err set.
+int walk(const Gate *gates, size_t count, bool disable_x, int M, WalkState &ws, std::vector<Op> &ops,
+         std::string &err);
+
+// calc_mem (zxh.cpp:648-681): real address bits the gate list needs.
+int calc_mem(const Gate *gates, size_t count, int n, bool disable_x);
+
+struct PlanParams {
+    int tile_bits_c64 = 12;     // log2 amplitudes per TMA tile, complex64
+    int tile_bits_c128 = 11;    // same for complex128
+    int contig_bits = 6;        // contiguous low bits of a tile that also spans high bits
+    int max_gates = 12;         // pair ops per tile pass
+    int max_steps = 16;
+    int diag_tile_bits = 12;    // tile size of a standalone diagonal pass
+    int product_table_bits = 12;
+};
+
+struct Pass {
+    enum Kind { PRODUCT, EXPAND, TILE, PAIR } kind;
+    int m = 0;
+    uint64_t off = 0;    // blob offset of the pass descriptor
+    uint64_t off2 = 0;   // PRODUCT: lookup table
+    TileDev geom;        // TILE
+    std::vector<StepDev> steps;
+};
+
+struct Plan {
+    std::vector<uint8_t> blob;
+    std::vector<Pass> passes;
+    void clear();
+};
+
+int plan(const std::vector<Op> &ops, int elem_bytes, const PlanParams &pp, const WalkState &start, Plan &out,
+         std::string &err);
+
+}  // namespace zxh

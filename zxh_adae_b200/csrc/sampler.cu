@@ -1,0 +1,522 @@
+// sampler.cu -- multinomial sampler of the B200-native ZXH path (sm_100a).
+//
+// Draws the same outcomes as the reference GPU sampler when fed the same seed: it
+// consumes the reference's uniform stream (splitmix64 of seed-mixed shot and output
+// indices, src/zxh/src/measure/measure_cuda.cu:387-443,493-515) with the same two-
+// level structure (segments of 2^12 amplitudes, then an offset inside the segment),
+// and returns shots grouped by segment in the reference's output order. The
+// machinery is new:
+//   seg_scan_kernel      one read of the state: per-segment FP64 |amp|^2 mass and a
+//                        single-pass decoupled-lookback inclusive scan over segments
+//                        (the reference runs segment_mass_kernel + a CUB scan).
+//   count_kernel         shot -> segment by binary search, warp-aggregated atomics.
+//   offsets (3 kernels)  exclusive scan of the per-segment counts.
+//   resolve_warp_kernel  segments hit by <= 32 shots: one warp streams the segment
+//                        once, lane-scans it and places each shot with a warp-
+//                        cooperative search (ballot over lane prefixes, then over
+//                        4-amplitude sub-ranges).
+//   resolve_cta_kernel   heavier segments: the CTA builds the segment CDF in shared
+//                        memory and binary-searches it, split over CTAs by shot chunk.
+//   map_kernel           real index -> packed virtual bits (measure_cuda.cu:315-338).
+// Every spin on a predecessor flag is bounded and reports ZXH_ERR_TIMEOUT.
+#include "core.h"
+#include "dev.cuh"
+#include "sampler.h"
+
+#include <algorithm>
+#include <cuda_runtime.h>
+
+namespace zxh {
+
+namespace {
+
+constexpr uint64_t kSeedShot = 0x510e527fade682d1ULL;    // measure_cuda.cu:427
+constexpr uint64_t kSeedOffset = 0x9b05688c2b3e6c1fULL;  // measure_cuda.cu:499
+constexpr int kSegsPerChunk = 8;
+constexpr int kWarpMax = 32;
+constexpr uint32_t kCtaShots = 16384;
+constexpr int kScanBlock = 4096;
+
+__device__ __forceinline__ uint64_t splitmix64(uint64_t x)
+{
+    uint64_t z = x + 0x9e3779b97f4a7c15ULL;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+
+// (mant + 1) / (2^53 + 1) evaluated in double; 2^53 + 1 rounds to 2^53 as on the
+// reference device (measure_cuda.cu:395-410).
+__device__ __forceinline__ double uniform_open01(uint64_t seed)
+{
+    const uint64_t mant = splitmix64(seed) >> 11;
+    return (static_cast<double>(mant) + 1.0) / (static_cast<double>(1ULL << 53) + 1.0);
+}
+
+template <typename E>
+__device__ __forceinline__ double prob(const E &a)
+{
+    const double re = double(a.x), im = double(a.y);
+    return re * re + im * im;
+}
+
+__device__ __forceinline__ uint32_t ld_flag(const uint32_t *p)
+{
+    return *reinterpret_cast<const volatile uint32_t *>(p);
+}
+
+__device__ __forceinline__ double ld_val(const double *p) { return *reinterpret_cast<const volatile double *>(p); }
+
+// ---------------------------------------------------------------------------
+
+template <typename E>
+__global__ void __launch_bounds__(kThreads) seg_scan_kernel(const E *__restrict__ state, uint64_t nseg, uint32_t seglen,
+                                                            double *__restrict__ segcdf, double *agg_val,
+                                                            uint32_t *agg_flag, double *inc_val, uint32_t *inc_flag,
+                                                            uint32_t *ticket, DevStatus *status)
+{
+    __shared__ uint32_t s_chunk;
+    __shared__ double s_mass[kSegsPerChunk];
+    __shared__ double s_prefix;
+    __shared__ int s_abort;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint64_t nchunks = (nseg + kSegsPerChunk - 1) / kSegsPerChunk;
+    if (tid == 0) s_abort = 0;
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) s_chunk = atomicAdd(ticket, 1u);
+        __syncthreads();
+        const uint64_t chunk = s_chunk;
+        if (chunk >= nchunks || s_abort) break;
+        const uint64_t base = chunk * kSegsPerChunk;
+        const int nloc = int((nseg - base < uint64_t(kSegsPerChunk) ? nseg - base : uint64_t(kSegsPerChunk)));
+        for (int sl = warp; sl < nloc; sl += kThreads / 32) {
+            const E *seg = state + (base + uint64_t(sl)) * seglen;
+            double acc = 0.0;
+            for (uint32_t k = uint32_t(lane); k < seglen; k += 32) acc += prob(seg[k]);
+            acc = warp_sum_f64(acc);
+            if (lane == 0) s_mass[sl] = acc;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double run = 0.0;
+            for (int i = 0; i < nloc; i++) {
+                run += s_mass[i];
+                s_mass[i] = run;
+            }
+            const double agg = run;
+            double excl = 0.0;
+            if (chunk == 0) {
+                inc_val[0] = agg;
+                __threadfence();
+                atomicExch(&inc_flag[0], 1u);
+            } else {
+                agg_val[chunk] = agg;
+                __threadfence();
+                atomicExch(&agg_flag[chunk], 1u);
+                int64_t p = int64_t(chunk) - 1;
+                const long long t0 = clock64();
+                while (p >= 0) {
+                    if (ld_flag(&inc_flag[p])) {
+                        __threadfence();
+                        excl += ld_val(&inc_val[p]);
+                        break;
+                    }
+                    if (ld_flag(&agg_flag[p])) {
+                        __threadfence();
+                        excl += ld_val(&agg_val[p]);
+                        p--;
+                        continue;
+                    }
+                    if (clock64() - t0 > (1LL << 31)) {
+                        report(status, kErrTimeout, 2, chunk);
+                        s_abort = 1;
+                        break;
+                    }
+                }
+                inc_val[chunk] = excl + agg;
+                __threadfence();
+                atomicExch(&inc_flag[chunk], 1u);
+            }
+            s_prefix = excl;
+        }
+        __syncthreads();
+        if (tid < nloc) segcdf[base + uint64_t(tid)] = s_prefix + s_mass[tid];
+    }
+}
+
+__device__ __forceinline__ uint64_t upper_index(const double *cdf, uint64_t n, double tau)
+{
+    uint64_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint64_t mid = lo + (hi - lo) / 2;
+        if (cdf[mid] <= tau) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo >= n ? n - 1 : lo;
+}
+
+__global__ void __launch_bounds__(kThreads) count_kernel(const double *__restrict__ segcdf, uint64_t nseg,
+                                                         uint64_t stream_seed, uint64_t shots,
+                                                         unsigned long long *__restrict__ counts)
+{
+    const double total = segcdf[nseg - 1];
+    for (uint64_t base = uint64_t(blockIdx.x) * kThreads; base < shots; base += uint64_t(gridDim.x) * kThreads) {
+        const uint64_t idx = base + threadIdx.x;
+        const bool live = idx < shots && total > 0.0;
+        uint64_t seg = ~0ULL;
+        if (live) {
+            const double u = uniform_open01(stream_seed ^ (kSeedShot + idx));
+            seg = upper_index(segcdf, nseg, u * total);
+        }
+        // one atomic per distinct segment in the warp
+        const unsigned peers = __match_any_sync(0xffffffffu, seg);
+        const int leader = __ffs(peers) - 1;
+        if (live && int(threadIdx.x & 31) == leader) atomicAdd(&counts[seg], static_cast<unsigned long long>(__popc(peers)));
+    }
+}
+
+// exclusive scan of counts: block sums, scan of block sums, block scans
+__global__ void __launch_bounds__(kThreads) block_sum_kernel(const unsigned long long *__restrict__ counts, uint64_t n,
+                                                             unsigned long long *__restrict__ bsum)
+{
+    __shared__ unsigned long long sh[kThreads / 32];
+    const uint64_t b0 = uint64_t(blockIdx.x) * kScanBlock;
+    unsigned long long acc = 0;
+    for (uint64_t i = b0 + threadIdx.x; i < (n < b0 + kScanBlock ? n : b0 + kScanBlock); i += kThreads) acc += counts[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int w = 0; w < kThreads / 32; w++) t += sh[w];
+        bsum[blockIdx.x] = t;
+    }
+}
+
+__global__ void scan_small_kernel(unsigned long long *v, uint64_t n)
+{
+    // single thread; n is at most a few thousand block sums
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    unsigned long long run = 0;
+    for (uint64_t i = 0; i < n; i++) {
+        const unsigned long long x = v[i];
+        v[i] = run;
+        run += x;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) block_scan_kernel(const unsigned long long *__restrict__ counts, uint64_t n,
+                                                              const unsigned long long *__restrict__ boff,
+                                                              unsigned long long *__restrict__ offsets)
+{
+    constexpr int PER = kScanBlock / kThreads;  // 16 consecutive counts per thread
+    __shared__ unsigned long long sh[kThreads];
+    const uint64_t b0 = uint64_t(blockIdx.x) * kScanBlock + uint64_t(threadIdx.x) * PER;
+    unsigned long long loc[PER];
+    unsigned long long acc = 0;
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+        loc[k] = (b0 + k < n) ? counts[b0 + k] : 0ULL;
+        acc += loc[k];
+    }
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = 1; o < kThreads; o <<= 1) {
+        const unsigned long long v = threadIdx.x >= unsigned(o) ? sh[threadIdx.x - o] : 0ULL;
+        __syncthreads();
+        sh[threadIdx.x] += v;
+        __syncthreads();
+    }
+    unsigned long long run = boff[blockIdx.x] + sh[threadIdx.x] - acc;
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+        if (b0 + k < n) offsets[b0 + k] = run;
+        run += loc[k];
+    }
+}
+
+// segments hit by at most kWarpMax shots
+template <typename E>
+__global__ void __launch_bounds__(kThreads) resolve_warp_kernel(const E *__restrict__ state, uint64_t nseg,
+                                                                uint32_t seglen, const unsigned long long *counts,
+                                                                const unsigned long long *offsets, uint64_t stream2,
+                                                                uint64_t *__restrict__ real_out,
+                                                                uint32_t *heavy_list, uint32_t *heavy_count)
+{
+    const int lane = threadIdx.x & 31;
+    const uint64_t gwarp = (uint64_t(blockIdx.x) * kThreads + threadIdx.x) >> 5;
+    const uint64_t nwarps = (uint64_t(gridDim.x) * kThreads) >> 5;
+    const uint32_t per_lane = (seglen + 31) / 32;  // amplitudes owned by a lane
+    for (uint64_t g0 = gwarp * 32; g0 < nseg; g0 += nwarps * 32) {
+        const uint64_t gl = g0 + uint64_t(lane);
+        const unsigned long long cl = gl < nseg ? counts[gl] : 0ULL;
+        unsigned todo = __ballot_sync(0xffffffffu, cl != 0);
+        if (cl > kWarpMax) heavy_list[atomicAdd(heavy_count, 1u)] = uint32_t(gl);
+        todo &= __ballot_sync(0xffffffffu, cl <= kWarpMax);
+        while (todo) {
+            const int src = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const uint64_t g = g0 + uint64_t(src);
+            const unsigned long long cnt = __shfl_sync(0xffffffffu, cl, src);
+            const unsigned long long off = offsets[g];
+            const E *seg = state + g * seglen;
+            // lane range [lane*per_lane, (lane+1)*per_lane)
+            const uint32_t lo = uint32_t(lane) * per_lane;
+            const uint32_t hi = min(seglen, lo + per_lane);
+            double part = 0.0;
+            for (uint32_t k = lo; k < hi; k++) part += prob(seg[k]);
+            double incl = part;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const double v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const double total = __shfl_sync(0xffffffffu, incl, 31);
+            const double excl = incl - part;
+            // this lane's shot
+            double tau = 0.0;
+            if (uint64_t(lane) < cnt) tau = uniform_open01(stream2 ^ (kSeedOffset + off + uint64_t(lane))) * total;
+            for (int j = 0; j < int(cnt); j++) {
+                const double t = __shfl_sync(0xffffffffu, tau, j);
+                // owner lane: first lane whose inclusive prefix exceeds t
+                const unsigned le = __ballot_sync(0xffffffffu, incl <= t);
+                int owner = __popc(le);
+                uint64_t hit;
+                if (owner >= 32) {
+                    hit = seglen - 1;
+                } else {
+                    // cooperative search in the owner's range: each lane takes a sub-range
+                    const double obase = __shfl_sync(0xffffffffu, excl, owner);
+                    const uint32_t olo = uint32_t(owner) * per_lane;
+                    const uint32_t ohi = min(seglen, olo + per_lane);
+                    const uint32_t sub = (per_lane + 31) / 32;
+                    const uint32_t slo = min(ohi, olo + uint32_t(lane) * sub);
+                    const uint32_t shi = min(ohi, slo + sub);
+                    double sp = 0.0;
+                    for (uint32_t k = slo; k < shi; k++) sp += prob(seg[k]);
+                    double sincl = sp;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const double v = __shfl_up_sync(0xffffffffu, sincl, o);
+                        if (lane >= o) sincl += v;
+                    }
+                    const unsigned le2 = __ballot_sync(0xffffffffu, obase + sincl <= t);
+                    const int sl = __popc(le2);
+                    uint32_t found = ohi;  // none below the end of the owner's range
+                    if (sl < 32 && lane == sl) {
+                        double run = obase + sincl - sp;
+                        found = shi;
+                        for (uint32_t k = slo; k < shi; k++) {
+                            run += prob(seg[k]);
+                            if (run > t) {
+                                found = k;
+                                break;
+                            }
+                        }
+                    }
+                    const uint32_t fs = __shfl_sync(0xffffffffu, found, sl < 32 ? sl : 0);
+                    hit = (sl < 32) ? fs : ohi;
+                    if (hit >= seglen) hit = seglen - 1;
+                }
+                if (lane == 0) real_out[off + uint64_t(j)] = g * seglen + hit;
+            }
+        }
+    }
+}
+
+template <typename E>
+__global__ void __launch_bounds__(kThreads) resolve_cta_kernel(const E *__restrict__ state, uint32_t seglen,
+                                                               const unsigned long long *counts,
+                                                               const unsigned long long *offsets, uint64_t stream2,
+                                                               uint64_t *__restrict__ real_out,
+                                                               const uint32_t *heavy_list,
+                                                               const uint32_t *heavy_count)
+{
+    extern __shared__ double cdf[];
+    __shared__ double s_tot[kThreads];
+    const uint32_t nh = *heavy_count;
+    uint64_t item = 0;
+    for (uint32_t h = 0; h < nh; h++) {
+        const uint64_t g = heavy_list[h];
+        const unsigned long long cnt = counts[g], off = offsets[g];
+        const uint64_t nchunks = (cnt + kCtaShots - 1) / kCtaShots;
+        const uint64_t first = item;
+        item += nchunks;
+        // this CTA's chunks of segment g
+        uint64_t c0 = first % gridDim.x == 0 ? 0 : gridDim.x - first % gridDim.x;
+        c0 = (c0 + blockIdx.x) % gridDim.x;
+        if (c0 >= nchunks) continue;
+        // build the segment CDF once for all of this CTA's chunks
+        const E *seg = state + g * seglen;
+        const uint32_t per = (seglen + kThreads - 1) / kThreads;
+        const uint32_t lo = threadIdx.x * per, hi = min(seglen, lo + per);
+        double run = 0.0;
+        for (uint32_t k = lo; k < hi; k++) {
+            run += prob(seg[k]);
+            cdf[k] = run;
+        }
+        s_tot[threadIdx.x] = run;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double acc = 0.0;
+            for (int t = 0; t < kThreads; t++) {
+                const double v = s_tot[t];
+                s_tot[t] = acc;
+                acc += v;
+            }
+        }
+        __syncthreads();
+        const double add = s_tot[threadIdx.x];
+        for (uint32_t k = lo; k < hi; k++) cdf[k] += add;
+        __syncthreads();
+        const double total = cdf[seglen - 1];
+        for (uint64_t c = c0; c < nchunks; c += gridDim.x) {
+            const uint64_t j0 = c * kCtaShots, j1 = (cnt < j0 + kCtaShots ? cnt : j0 + kCtaShots);
+            for (uint64_t j = j0 + threadIdx.x; j < j1; j += kThreads) {
+                const double tau = uniform_open01(stream2 ^ (kSeedOffset + off + j)) * total;
+                real_out[off + j] = g * seglen + upper_index(cdf, seglen, tau);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) map_kernel(const uint64_t *__restrict__ real, uint64_t shots,
+                                                       const uint64_t *__restrict__ coltab, uint64_t b,
+                                                       uint64_t *__restrict__ words)
+{
+    __shared__ uint64_t tab[8][256];
+    for (int i = threadIdx.x; i < 8 * 256; i += kThreads) tab[i >> 8][i & 255] = coltab[i];
+    __syncthreads();
+    for (uint64_t i = uint64_t(blockIdx.x) * kThreads + threadIdx.x; i < shots; i += uint64_t(gridDim.x) * kThreads) {
+        const uint64_t r = real[i];
+        uint64_t v = b;
+#pragma unroll
+        for (int k = 0; k < 8; k++) v ^= tab[k][(r >> (8 * k)) & 255];
+        words[i] = v;
+    }
+}
+
+}  // namespace
+
+// One layout routine serves both the size query and the carving, so the two can
+// never disagree.
+static size_t layout(SamplerScratch *sc, uint8_t *base, uint64_t nseg, uint64_t shots)
+{
+    const uint64_t nchunks = (nseg + kSegsPerChunk - 1) / kSegsPerChunk;
+    const uint64_t nblk = (nseg + kScanBlock - 1) / kScanBlock;
+    size_t b = 0;
+    auto take = [&](size_t x) {
+        uint8_t *p = base ? base + b : nullptr;
+        b += (x + 255) & ~size_t(255);
+        return p;
+    };
+    uint8_t *segcdf = take(nseg * 8);
+    uint8_t *fb = base ? base + b : nullptr;
+    uint8_t *agg_val = take(nchunks * 8);
+    uint8_t *inc_val = take(nchunks * 8);
+    uint8_t *agg_flag = take(nchunks * 4);
+    uint8_t *inc_flag = take(nchunks * 4);
+    uint8_t *ticket = take(16);
+    uint8_t *fe = base ? base + b : nullptr;
+    uint8_t *counts = take(nseg * 8);
+    uint8_t *offsets = take(nseg * 8);
+    uint8_t *bsum = take(nblk * 8);
+    uint8_t *heavy = take(nseg * 4);
+    uint8_t *real = take(shots * 8);
+    uint8_t *words = take(shots * 8);
+    uint8_t *coltab = take(8 * 256 * 8);
+    if (sc) {
+        sc->segcdf = reinterpret_cast<double *>(segcdf);
+        sc->flags_begin = fb;
+        sc->agg_val = reinterpret_cast<double *>(agg_val);
+        sc->inc_val = reinterpret_cast<double *>(inc_val);
+        sc->agg_flag = reinterpret_cast<uint32_t *>(agg_flag);
+        sc->inc_flag = reinterpret_cast<uint32_t *>(inc_flag);
+        sc->ticket = reinterpret_cast<uint32_t *>(ticket);
+        sc->heavy_count = sc->ticket + 1;
+        sc->flags_end = fe;
+        sc->counts = reinterpret_cast<unsigned long long *>(counts);
+        sc->offsets = reinterpret_cast<unsigned long long *>(offsets);
+        sc->bsum = reinterpret_cast<unsigned long long *>(bsum);
+        sc->heavy_list = reinterpret_cast<uint32_t *>(heavy);
+        sc->real = reinterpret_cast<uint64_t *>(real);
+        sc->words = reinterpret_cast<uint64_t *>(words);
+        sc->coltab = reinterpret_cast<uint64_t *>(coltab);
+    }
+    return b;
+}
+
+size_t SamplerScratch::need_bytes(uint64_t nseg, uint64_t shots) { return layout(nullptr, nullptr, nseg, shots); }
+
+void SamplerScratch::carve(uint8_t *base, uint64_t nseg, uint64_t shots) { layout(this, base, nseg, shots); }
+
+cudaError_t run_sampler(const void *state, int elem_bytes, int m, uint64_t shots, uint64_t stream_seed,
+                        const uint64_t *host_coltab, uint64_t b, SamplerScratch &sc, DevStatus *status, int sms,
+                        cudaStream_t st, uint64_t &kernels)
+{
+    const uint64_t local = 1ULL << m;
+    const uint32_t seglen = uint32_t(std::min<uint64_t>(4096, local));
+    const uint64_t nseg = local / seglen;
+    const uint64_t nchunks = (nseg + kSegsPerChunk - 1) / kSegsPerChunk;
+    const uint64_t nblk = (nseg + kScanBlock - 1) / kScanBlock;
+    const uint64_t stream2 = mix_seed_host(stream_seed, 1);
+    cudaError_t e;
+    e = cudaMemsetAsync(sc.flags_begin, 0, size_t(static_cast<uint8_t *>(sc.flags_end) - static_cast<uint8_t *>(sc.flags_begin)), st);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(sc.counts, 0, nseg * 8, st);
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyAsync(sc.coltab, host_coltab, 8 * 256 * 8, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return e;
+    const unsigned gs = unsigned(std::max<uint64_t>(1, std::min<uint64_t>(nchunks, uint64_t(sms) * 4)));
+    if (elem_bytes == 8)
+        seg_scan_kernel<float2><<<gs, kThreads, 0, st>>>(static_cast<const float2 *>(state), nseg, seglen, sc.segcdf,
+                                                        sc.agg_val, sc.agg_flag, sc.inc_val, sc.inc_flag, sc.ticket,
+                                                        status);
+    else
+        seg_scan_kernel<double2><<<gs, kThreads, 0, st>>>(static_cast<const double2 *>(state), nseg, seglen, sc.segcdf,
+                                                         sc.agg_val, sc.agg_flag, sc.inc_val, sc.inc_flag, sc.ticket,
+                                                         status);
+    const unsigned gc = unsigned(std::max<uint64_t>(1, std::min<uint64_t>((shots + kThreads - 1) / kThreads, uint64_t(sms) * 8)));
+    count_kernel<<<gc, kThreads, 0, st>>>(sc.segcdf, nseg, stream_seed, shots, sc.counts);
+    block_sum_kernel<<<unsigned(nblk), kThreads, 0, st>>>(sc.counts, nseg, sc.bsum);
+    scan_small_kernel<<<1, 32, 0, st>>>(sc.bsum, nblk);
+    block_scan_kernel<<<unsigned(nblk), kThreads, 0, st>>>(sc.counts, nseg, sc.bsum, sc.offsets);
+    const uint64_t warps_needed = (nseg + 31) / 32;
+    const unsigned gw = unsigned(std::max<uint64_t>(1, std::min<uint64_t>((warps_needed * 32 + kThreads - 1) / kThreads,
+                                                                          uint64_t(sms) * 8)));
+    if (elem_bytes == 8)
+        resolve_warp_kernel<float2><<<gw, kThreads, 0, st>>>(static_cast<const float2 *>(state), nseg, seglen, sc.counts,
+                                                            sc.offsets, stream2, sc.real, sc.heavy_list, sc.heavy_count);
+    else
+        resolve_warp_kernel<double2><<<gw, kThreads, 0, st>>>(static_cast<const double2 *>(state), nseg, seglen,
+                                                             sc.counts, sc.offsets, stream2, sc.real, sc.heavy_list,
+                                                             sc.heavy_count);
+    const size_t smem = size_t(seglen) * 8;
+    const unsigned gh = unsigned(sms) * 2;
+    if (elem_bytes == 8)
+        resolve_cta_kernel<float2><<<gh, kThreads, smem, st>>>(static_cast<const float2 *>(state), seglen, sc.counts,
+                                                              sc.offsets, stream2, sc.real, sc.heavy_list,
+                                                              sc.heavy_count);
+    else
+        resolve_cta_kernel<double2><<<gh, kThreads, smem, st>>>(static_cast<const double2 *>(state), seglen, sc.counts,
+                                                               sc.offsets, stream2, sc.real, sc.heavy_list,
+                                                               sc.heavy_count);
+    const unsigned gm = unsigned(std::max<uint64_t>(1, std::min<uint64_t>((shots + kThreads - 1) / kThreads, uint64_t(sms) * 8)));
+    map_kernel<<<gm, kThreads, 0, st>>>(sc.real, shots, sc.coltab, b, sc.words);
+    kernels += 8;
+    return cudaGetLastError();
+}
+
+uint64_t mix_seed_host(uint64_t base, uint64_t salt)
+{
+    // mix_seed, measure_cuda.cu:103-109
+    uint64_t z = base + 0x9e3779b97f4a7c15ULL + salt;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+
+}  // namespace zxh

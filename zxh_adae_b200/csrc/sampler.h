@@ -1,0 +1,40 @@
+// sampler.h -- device scratch layout and launcher of the multinomial sampler.
+#pragma once
+
+#include "core.h"
+
+#include <cuda_runtime.h>
+
+namespace zxh {
+
+struct SamplerScratch {
+    double *segcdf = nullptr;
+    double *agg_val = nullptr, *inc_val = nullptr;
+    uint32_t *agg_flag = nullptr, *inc_flag = nullptr;
+    uint32_t *ticket = nullptr, *heavy_count = nullptr;
+    void *flags_begin = nullptr, *flags_end = nullptr;  // region zeroed before every draw
+    unsigned long long *counts = nullptr, *offsets = nullptr, *bsum = nullptr;
+    uint32_t *heavy_list = nullptr;
+    uint64_t *real = nullptr, *words = nullptr;
+    uint64_t *coltab = nullptr;
+
+    static size_t need_bytes(uint64_t nseg, uint64_t shots);
+    void carve(uint8_t *base, uint64_t nseg, uint64_t shots);
+};
+
+uint64_t mix_seed_host(uint64_t base, uint64_t salt);
+
+// Draws shots outcomes from the 2^m-amplitude state into sc.real (real indices,
+// grouped by segment) and sc.words (virtual bits, one word per shot for n <= 63).
+cudaError_t run_sampler(const void *state, int elem_bytes, int m, uint64_t shots, uint64_t stream_seed,
+                        const uint64_t *host_coltab, uint64_t b, SamplerScratch &sc, DevStatus *status, int sms,
+                        cudaStream_t st, uint64_t &kernels);
+
+// Pass runner and get_state scatter (kernels.cu).
+struct Pass;
+cudaError_t run_passes(const std::vector<Pass> &passes, const uint8_t *dblob, void *state, int elem_bytes,
+                       DevStatus *status, int sms, cudaStream_t st, uint64_t &kernels);
+cudaError_t run_scatter(const void *state, uint64_t n_real, const uint64_t *dcoltab, uint64_t b, int N, int order,
+                        double gre, double gim, void *out, int elem_bytes, int sms, cudaStream_t st);
+
+}  // namespace zxh

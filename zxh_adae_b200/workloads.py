@@ -1,0 +1,127 @@
+"""Seeded synthetic circuits of the benchmark configurations.
+
+The reference quotes its results on MQT-Bench circuits (not used here); these
+generators stand in for them with the shapes, sizes and angle distributions of
+the five configurations this path is measured on. Every generator takes one
+integer seed and draws from ``numpy.random.default_rng(seed)`` in a fixed order,
+so any run (ours, the oracle's, the reference's) sees the same gate list.
+
+Records use the 40-byte layout of include/zxh_b200.h; U3 records carry
+(theta, lambda, phi) in ZXH's argument order.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from ._core import BARRIER, CP, CX, H, P, RZ, U3, X, as_records
+
+TWO_PI = 2.0 * math.pi
+
+
+def plain_layers(n: int, layers: int, seed: int) -> np.ndarray:
+    """H on every qubit, then `layers` x [U3 on every qubit; cp(alpha) on (i, i+1)].
+
+    Draw order per layer: for each qubit (theta, phi, lambda), then the n-1 alphas.
+    Configuration 1 is plain_layers(20, 10, seed) followed by 1024 shots.
+    """
+    rng = np.random.default_rng(seed)
+    recs = [(H, 0, q) for q in range(n)]
+    for _ in range(layers):
+        ang = rng.uniform(0.0, TWO_PI, size=(n, 3))
+        alpha = rng.uniform(0.0, TWO_PI, size=n - 1)
+        for q in range(n):
+            th, ph, la = ang[q]
+            recs.append((U3, 0, q, th, la, ph))
+        for i in range(n - 1):
+            recs.append((CP, i, i + 1, alpha[i]))
+    return as_records(recs)
+
+
+def h_all(n: int) -> np.ndarray:
+    return as_records([(H, 0, q) for q in range(n)])
+
+
+def diag_batch(n: int, batch: int, seed: int) -> np.ndarray:
+    """B gates: p on a uniform qubit or cp on a uniform ordered pair (50/50),
+    angle uniform [0, 2 pi) (configuration 2, without the H header)."""
+    rng = np.random.default_rng(seed)
+    recs = []
+    for _ in range(batch):
+        kind = rng.integers(2)
+        th = rng.uniform(0.0, TWO_PI)
+        if kind == 0:
+            recs.append((P, 0, int(rng.integers(n)), th))
+        else:
+            c = int(rng.integers(n))
+            t = int(rng.integers(n - 1))
+            t = t + 1 if t >= c else t
+            recs.append((CP, c, t, th))
+    return as_records(recs)
+
+
+def cp_cascade(n: int) -> np.ndarray:
+    """Controlled-phase cascade over all pairs j > i with angle pi / 2^(j - i)."""
+    recs = []
+    for i in range(n):
+        for j in range(i + 1, n):
+            recs.append((CP, i, j, math.pi / float(2 ** (j - i))))
+    return as_records(recs)
+
+
+def u3_matching_layers(n: int, layers: int, seed: int) -> np.ndarray:
+    """`layers` x [U3 on every qubit (angles uniform [0, 2 pi)); cz on a random
+    perfect matching] after H on every qubit (configuration 3, first part).
+    cz is recorded as CP(pi). Draw order per layer: angles (n x 3), then a
+    permutation of the qubits whose consecutive pairs are matched."""
+    rng = np.random.default_rng(seed)
+    recs = [(H, 0, q) for q in range(n)]
+    for _ in range(layers):
+        ang = rng.uniform(0.0, TWO_PI, size=(n, 3))
+        perm = rng.permutation(n)
+        for q in range(n):
+            th, ph, la = ang[q]
+            recs.append((U3, 0, q, th, la, ph))
+        for k in range(0, n - 1, 2):
+            recs.append((CP, int(perm[k]), int(perm[k + 1]), math.pi))
+    return as_records(recs)
+
+
+def hidden_string(n_data: int, seed: int):
+    """Hidden-string circuit on n_data + 1 qubits (ancilla = qubit n_data): H on
+    every data qubit, X then H on the ancilla (preparing |->), CX from every data
+    qubit whose secret bit is 1 onto the ancilla, H on the data qubits. The data
+    register then reads the secret with certainty. (An H on the ancilla before
+    its X would make H X H = Z act on |0>, cancel the phase kickback and lose the
+    deterministic answer, so the ancilla gets X then H only.)
+    Returns (records, secret)."""
+    rng = np.random.default_rng(seed)
+    secret = int(rng.integers(1, 1 << n_data))
+    anc = n_data
+    recs = [(H, 0, q) for q in range(n_data)]
+    recs += [(X, 0, anc), (H, 0, anc)]
+    for i in range(n_data):
+        if (secret >> i) & 1:
+            recs.append((CX, i, anc))
+    recs += [(H, 0, q) for q in range(n_data)]
+    return as_records(recs), secret
+
+
+def random_circuit(n: int, count: int, seed: int, kinds=None) -> np.ndarray:
+    """Random gate list over the whole native set (test workload)."""
+    rng = np.random.default_rng(seed)
+    kinds = kinds or [BARRIER, 2, RZ, P, 5, CP, X, CX, H, U3, 11]
+    if n == 1:  # two-qubit gates need two distinct qubits
+        kinds = [k for k in kinds if k not in (5, CP, CX)]
+    recs = []
+    for _ in range(count):
+        t = int(kinds[rng.integers(len(kinds))])
+        q = int(rng.integers(n))
+        cq = int(rng.integers(n))
+        if n > 1:
+            while cq == q:
+                cq = int(rng.integers(n))
+        a = rng.uniform(0.0, TWO_PI, size=3)
+        recs.append((t, cq, q, a[0], a[1], a[2]))
+    return as_records(recs)
