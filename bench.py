@@ -1,0 +1,342 @@
+"""Benchmark of the B200-native ZXH path (one JSON line on stdout, rank 0).
+
+Workload (configuration 2, the diagonal-batch microbenchmark): a 30-qubit
+complex64 state (8 GiB) prepared with H on every qubit; one step applies one
+batch of B = 4096 seeded random p/cp gates (50/50, angles uniform [0, 2 pi)) as
+one read-modify-write pass of the state. The state (8 GiB) is larger than L2
+(126 MB), so no flush is needed between steps.
+
+* value        whole-job GB/s from the device time of the pass kernels
+               (algorithmic bytes 2 * 2^30 * 8 per step), inputs resident.
+* e2e          the same metric through the C ABI (zxh_apply with host gate
+               records: host planning, program upload, launch, status read-back),
+               timed on the host around K calls.
+* roofline     the dominant kernel (the diagonal pass) against the measured HBM
+               copy bandwidth in MEASURED_PEAKS.json.
+* cpu_baseline the reference ZXH-Sim OpenMP backend (compiled from its own sources
+               into oracle/_ref) on a bounded sample: the same B = 4096 batch
+               distribution on a 20-qubit complex128 state, timed with the
+               reference's header-subtraction method, GB/s at 16 B/amplitude.
+
+``--impl reference`` runs that reference CPU backend alone and prints its line.
+Multi-GPU (``torchrun``): the path does not shard, each rank runs an independent
+replica; value is the sum over ranks, times are the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "30q GB/s vs HBM peak; adjoint vs param-shift grads/s at <=1e-5 err, 1 GPU"
+UNIT = "GB/s"
+N_QUBITS = 30
+BATCH = 4096
+REF_SAMPLE_QUBITS = 18
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--qubits", type=int, default=N_QUBITS)
+    ap.add_argument("--batch", type=int, default=BATCH)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    return world, rank, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def max_over_ranks(pg, x: float, local: int) -> float:
+    if pg is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"zxh_clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in self.path.read_text().strip().splitlines() if r.strip()]
+        except Exception:
+            return None
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows]
+        mx = float(rows[0][2])
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip().lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.is_file():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(name: str):
+    """DRAM bytes per launch of a kernel from a committed ncu summary, if any."""
+    p = ROOT / "profiles" / name
+    if not p.is_file():
+        return None
+    for line in p.read_text().splitlines():
+        if line.strip().startswith("traffic_bytes_per_launch"):
+            try:
+                return float(line.split("=")[1].split()[0])
+            except Exception:
+                return None
+    return None
+
+
+# --------------------------------------------------------------------------- reference CPU
+
+
+def ref_cpu_sample(steps: int, warmup: int, batch: int):
+    """Reference OpenMP backend, diag batch on a REF_SAMPLE_QUBITS-qubit state,
+    header-subtracted as the reference's diag microbenchmark does
+    (benchmarks/runners/diag_batch_microbench.py:209-231), 16 B/amplitude."""
+    from oracle.bridge import Reference, ref_available
+    from zxh_adae_b200 import workloads as wl
+
+    if not ref_available("omp"):
+        return None
+    n = REF_SAMPLE_QUBITS
+    header = wl.h_all(n)
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    os.environ["OMP_NUM_THREADS"] = str(cores)
+    bytes_step = 2 * (1 << n) * 16
+    times = []
+    for k in range(warmup + steps):
+        full = np.concatenate([header, wl.diag_batch(n, batch, seed=1000 + k)])
+        hs = Reference(n, backend="omp")
+        hs.push(header)
+        fs = Reference(n, backend="omp")
+        fs.push(full)
+
+        def ex(sim):
+            t0 = time.perf_counter()
+            sim.execute()
+            return time.perf_counter() - t0
+
+        h1 = ex(hs)
+        f1 = ex(fs)
+        f2 = ex(fs)
+        h2 = ex(hs)
+        d = max(1e-9, 0.5 * ((f1 - h1) + (f2 - h2)))
+        if k >= warmup:
+            times.append(d)
+    t = sum(times) / len(times)
+    return {
+        "value": bytes_step / t / 1e9,
+        "unit": UNIT,
+        "cores": cores,
+        "kind": "reference",
+        "sample": f"reference omp backend, {n}-qubit complex128 state, H header + B={batch} random p/cp "
+                  f"(50/50), header-subtracted execute(), mean of {len(times)} steps "
+                  f"({1e3 * t:.1f} ms/step), GB/s at 2*2^{n}*16 B",
+        "ms_per_step": 1e3 * t,
+    }
+
+
+def run_reference(args):
+    world, rank, local, pg = dist_setup(args)
+    if rank != 0:
+        return
+    steps = min(args.steps, 10)
+    cb = ref_cpu_sample(steps, min(args.warmup, 1), args.batch)
+    if cb is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference OpenMP backend not built (oracle/_ref)"}))
+        return
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": cb["value"],
+        "unit": UNIT,
+        "n_gpus": args.gpus,
+        "steps": steps,
+        "warmup": min(args.warmup, 1),
+        "ms_per_step": cb["ms_per_step"],
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "c128",
+        "data": "synthetic",
+        "config": {"workload": f"diag-batch {REF_SAMPLE_QUBITS}q complex128 B={args.batch} random p/cp "
+                               "(bounded CPU sample of the 30q workload)",
+                   "qubits": REF_SAMPLE_QUBITS, "batch": args.batch},
+        "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# --------------------------------------------------------------------------- ours
+
+
+def run_ours(args):
+    world, rank, local, pg = dist_setup(args)
+    import zxh_adae_b200 as zx
+    from zxh_adae_b200 import workloads as wl
+
+    n, B = args.qubits, args.batch
+    dtype = "complex64"
+    eb = 8
+    bytes_step = 2 * (1 << n) * eb
+    sim = zx.ZXH(n, dtype=dtype, device=local)
+    sim.push_gates(wl.h_all(n))
+    sim.execute()
+    batches = [wl.diag_batch(n, B, seed=rank * 100000 + k) for k in range(args.warmup + args.steps)]
+    for k in range(args.warmup):
+        sim.apply(batches[k])
+
+    # device-timed: kernel time of each step
+    barrier(pg)
+    dev_ms = []
+    launches = 0
+    with Clocks(local) as clk:
+        t0 = time.perf_counter()
+        for k in range(args.steps):
+            sim.apply(batches[args.warmup + k])
+            kk, _, ms = sim.last_stats()
+            dev_ms.append(ms)
+            launches += kk
+        wall = time.perf_counter() - t0
+    barrier(pg)
+    dev_total_ms = max_over_ranks(pg, sum(dev_ms), local)
+    wall = max_over_ranks(pg, wall, local)
+    value = world * args.steps * bytes_step / (dev_total_ms / 1e3) / 1e9
+    e2e_value = world * args.steps * bytes_step / wall / 1e9
+    peak, peak_kind = peaks()
+    achieved = bytes_step / (statistics.mean(dev_ms) / 1e3) / 1e9
+    traffic = profile_traffic(f"diag_pass_{n}q_c64.md")
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = ref_cpu_sample(3, 1, B)
+        if cpu is not None:
+            cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    clocks = clk.summary()
+    sim.close()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": dev_total_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "c64",
+        "data": "synthetic",
+        "config": {
+            "workload": f"diag-batch {n}q complex64, H-prepared, B={B} random p/cp (50/50) per step",
+            "qubits": n,
+            "batch": B,
+            "state_bytes": (1 << n) * eb,
+            "l2": "state larger than L2, no flush",
+            "parallelism": f"replicas x{world}",
+        },
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(B * 40), "d2h_bytes_per_step": 16},
+        "roofline": {
+            "bound": "hbm",
+            "achieved": achieved,
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": achieved / peak,
+            "peak_kind": peak_kind,
+            "traffic": traffic,
+        },
+        "cpu_baseline": cpu,
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

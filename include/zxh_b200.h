@@ -157,8 +157,10 @@ int zxh_state_view(zxh_sim *sim, void **data, size_t *m_bits, size_t *elem_bytes
 int zxh_stream(zxh_sim *sim, void **stream);
 
 /* Launch statistics of the last zxh_execute / zxh_apply / zxh_measure: number of
- * kernels launched and number of full read-modify-write passes over the state. */
-int zxh_last_stats(const zxh_sim *sim, uint64_t *kernels, uint64_t *passes);
+ * kernels launched, number of full read-modify-write passes over the state, and
+ * the device time of those kernels in milliseconds (CUDA events recorded on the
+ * handle's stream around the launches). Any pointer may be NULL. */
+int zxh_last_stats(const zxh_sim *sim, uint64_t *kernels, uint64_t *passes, double *device_ms);
 
 #ifdef __cplusplus
 }

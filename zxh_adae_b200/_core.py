@@ -89,7 +89,7 @@ _sig("zxh_num_qubits", [_P, ctypes.POINTER(_SZ)])
 _sig("zxh_state_view", [_P, ctypes.POINTER(_P), ctypes.POINTER(_SZ), ctypes.POINTER(_SZ),
                         ctypes.POINTER(_D), ctypes.POINTER(_D)])
 _sig("zxh_stream", [_P, ctypes.POINTER(_P)])
-_sig("zxh_last_stats", [_P, ctypes.POINTER(_U64), ctypes.POINTER(_U64)])
+_sig("zxh_last_stats", [_P, ctypes.POINTER(_U64), ctypes.POINTER(_U64), ctypes.POINTER(_D)])
 
 _ERRORS = {1: ValueError, 2: RuntimeError, 3: RuntimeError, 4: MemoryError, 5: ValueError, 6: RuntimeError}
 
@@ -314,6 +314,7 @@ class ZXH:
         return int(s.value or 0)
 
     def last_stats(self) -> tuple:
-        k, p = _U64(0), _U64(0)
-        self._ck(_lib.zxh_last_stats(self._h, ctypes.byref(k), ctypes.byref(p)))
-        return int(k.value), int(p.value)
+        """(kernels launched, state passes, device ms) of the last execute/apply/measure."""
+        k, p, ms = _U64(0), _U64(0), _D(0.0)
+        self._ck(_lib.zxh_last_stats(self._h, ctypes.byref(k), ctypes.byref(p), ctypes.byref(ms)))
+        return int(k.value), int(p.value), float(ms.value)

@@ -50,6 +50,8 @@ struct zxh_sim {
     size_t out_cap = 0;
 
     uint64_t stat_kernels = 0, stat_passes = 0;
+    float last_ms = 0.0f;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     zxh::PlanParams pp;
 };
 
@@ -169,11 +171,14 @@ int run_plan(zxh_sim *s, const zxh::Plan &pl)
     CK(s, cudaMemcpyAsync(s->d_blob, s->h_stage, pl.blob.size(), cudaMemcpyHostToDevice, s->stream), "upload program");
     CK(s, cudaMemsetAsync(s->d_status, 0, sizeof(zxh::DevStatus), s->stream), "reset status");
     uint64_t kernels = 0;
+    CK(s, cudaEventRecord(s->ev0, s->stream), "event");
     CK(s, zxh::run_passes(pl.passes, s->d_blob, s->d_state, s->elem_bytes, s->d_status, s->sms, s->stream, kernels),
        "launch");
+    CK(s, cudaEventRecord(s->ev1, s->stream), "event");
     CK(s, cudaMemcpyAsync(s->h_status, s->d_status, sizeof(zxh::DevStatus), cudaMemcpyDeviceToHost, s->stream),
        "read status");
     CK(s, cudaStreamSynchronize(s->stream), "execute");
+    CK(s, cudaEventElapsedTime(&s->last_ms, s->ev0, s->ev1), "event time");
     s->stat_kernels = kernels;
     s->stat_passes = 0;
     for (const zxh::Pass &p : pl.passes)
@@ -230,6 +235,8 @@ int zxh_create(zxh_sim **out, size_t n, int disable_x, int eager_expand_all, int
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void **>(&s->d_status), sizeof(zxh::DevStatus));
     if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void **>(&s->h_status), sizeof(zxh::DevStatus));
+    if (e == cudaSuccess) e = cudaEventCreate(&s->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->ev1);
     if (e != cudaSuccess) {
         const std::string msg = std::string("CUDA init: ") + cudaGetErrorString(e);
         zxh_destroy(s);
@@ -252,6 +259,8 @@ int zxh_destroy(zxh_sim *s)
     if (s->h_status) cudaFreeHost(s->h_status);
     if (s->d_samp) cudaFree(s->d_samp);
     if (s->d_out) cudaFree(s->d_out);
+    if (s->ev0) cudaEventDestroy(s->ev0);
+    if (s->ev1) cudaEventDestroy(s->ev1);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return ZXH_OK;
@@ -446,12 +455,15 @@ int zxh_measure(zxh_sim *s, size_t shots)
     column_tables(s->ws.map, tab);
     CK(s, cudaMemsetAsync(s->d_status, 0, sizeof(zxh::DevStatus), s->stream), "reset status");
     uint64_t kernels = 0;
+    CK(s, cudaEventRecord(s->ev0, s->stream), "event");
     CK(s, zxh::run_sampler(s->d_state, s->elem_bytes, m, shots, stream_seed, &tab[0][0], s->ws.map.b(), s->sc,
                            s->d_status, s->sms, s->stream, kernels),
        "sampler launch");
+    CK(s, cudaEventRecord(s->ev1, s->stream), "event");
     CK(s, cudaMemcpyAsync(s->h_status, s->d_status, sizeof(zxh::DevStatus), cudaMemcpyDeviceToHost, s->stream),
        "read status");
     CK(s, cudaStreamSynchronize(s->stream), "sampler");
+    CK(s, cudaEventElapsedTime(&s->last_ms, s->ev0, s->ev1), "event time");
     s->stat_kernels = kernels;
     s->stat_passes = 2;
     if (s->h_status->code != 0) return fail(s, int(s->h_status->code), "sampler device wait gave up");
@@ -559,11 +571,12 @@ int zxh_stream(zxh_sim *s, void **stream)
     return ZXH_OK;
 }
 
-int zxh_last_stats(const zxh_sim *s, uint64_t *kernels, uint64_t *passes)
+int zxh_last_stats(const zxh_sim *s, uint64_t *kernels, uint64_t *passes, double *device_ms)
 {
     if (!s) return ZXH_ERR_ARG;
     if (kernels) *kernels = s->stat_kernels;
     if (passes) *passes = s->stat_passes;
+    if (device_ms) *device_ms = double(s->last_ms);
     return ZXH_OK;
 }
 
