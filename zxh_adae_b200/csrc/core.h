@@ -134,7 +134,12 @@ struct DiagDev {
     int64_t lin_in[kMaxTileBits];   // linear coefficient of each tile coordinate
     uint32_t n_out_lin, n_out_quad, n_in_quad, n_cross, n_gen, pad;
     uint64_t off_out_lin, off_out_quad, off_in_quad, off_cross, off_gen;  // byte offsets in the blob
+    uint64_t off_kidx;  // uint32[kMaxTileBits + 1]: cross terms are sorted by tile coordinate i,
+                        // those of coordinate k are [kidx[k], kidx[k+1])
 };
+
+// exp(2 pi i j / 1024), j = 0..1023: the coarse factor of a phase given in turns.
+constexpr int kExpTableBits = 10;
 
 struct U3Dev {
     uint64_t delta_t;   // delta in tile coordinates
@@ -182,11 +187,11 @@ struct PairDev {
     double u[8];
 };
 
+// Product state written in one pass: amplitude(y) = L[y low c0 bits] *
+// M[next c1 bits] * H[remaining c2 bits] (the initial amplitude folded into H).
+// The three tables follow each other in the blob at off2.
 struct ProductDev {
-    uint32_t m;          // output bits
-    uint32_t c;          // low bits covered by the lookup table
-    double a0[2];        // initial amplitude
-    double v[64][4];     // per-bit factor: amplitude multiplier when the bit is 0 / 1 (complex)
+    uint32_t m, c0, c1, c2;
 };
 
 // Status word shared with the device (bounded waits report here).

@@ -494,6 +494,13 @@ uint64_t compile_diag(std::vector<uint8_t> &blob, const std::vector<DiagTerm> &t
     d.off_in_quad = put_vec(blob, in_quad);
     d.off_cross = put_vec(blob, cross);
     d.off_gen = put_vec(blob, gen);
+    // cross terms grouped by tile coordinate for the lane-parallel per-tile sums
+    std::stable_sort(cross.begin(), cross.end(), [](const QuadTerm &a, const QuadTerm &b) { return a.i < b.i; });
+    std::vector<uint32_t> kidx(kMaxTileBits + 1, 0);
+    for (const QuadTerm &t : cross) kidx[t.i + 1]++;
+    for (int k = 0; k < kMaxTileBits; k++) kidx[k + 1] += kidx[k];
+    d.off_cross = put_vec(blob, cross);
+    d.off_kidx = put_vec(blob, kidx);
     return put(blob, d);
 }
 
@@ -547,10 +554,41 @@ void Plan::clear()
     passes.clear();
 }
 
-int plan(const std::vector<Op> &ops, int elem_bytes, const PlanParams &pp, const WalkState &start, Plan &out,
+// Splits windows whose multi-bit-selector terms exceed what one diagonal step
+// evaluates per amplitude; the pieces commute, so their order is free.
+std::vector<Op> split_windows(const std::vector<Op> &ops, size_t max_general)
+{
+    std::vector<Op> out;
+    out.reserve(ops.size());
+    for (const Op &op : ops) {
+        if (op.kind != Op::DIAG) {
+            out.push_back(op);
+            continue;
+        }
+        Op cur;
+        cur.kind = Op::DIAG;
+        cur.m = op.m;
+        size_t ngen = 0;
+        for (const DiagTerm &t : op.diag) {
+            const bool simple = single_bit_or_zero(t.s0.alpha) && (!t.two || single_bit_or_zero(t.s1.alpha));
+            if (!simple && ngen == max_general) {
+                out.push_back(cur);
+                cur.diag.clear();
+                ngen = 0;
+            }
+            if (!simple) ngen++;
+            cur.diag.push_back(t);
+        }
+        if (!cur.diag.empty()) out.push_back(cur);
+    }
+    return out;
+}
+
+int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, const WalkState &start, Plan &out,
          std::string &err)
 {
     out.clear();
+    const std::vector<Op> ops = split_windows(ops_in, 32);
     size_t i = 0;
     int m = start.m;
 
@@ -617,23 +655,26 @@ int plan(const std::vector<Op> &ops, int elem_bytes, const PlanParams &pp, const
         }
         i = j;
         pd.m = uint32_t(pm);
-        pd.c = uint32_t(std::min(pm, pp.product_table_bits));
-        pd.a0[0] = a0.real();
-        pd.a0[1] = a0.imag();
-        for (int b = 0; b < pm; b++) {
-            pd.v[b][0] = v[b][0].real();
-            pd.v[b][1] = v[b][0].imag();
-            pd.v[b][2] = v[b][1].real();
-            pd.v[b][3] = v[b][1].imag();
+        pd.c0 = uint32_t(std::min(pm, pp.product_table_bits));
+        pd.c1 = uint32_t(std::min(pm - int(pd.c0), pp.product_table_bits));
+        pd.c2 = uint32_t(pm - int(pd.c0) - int(pd.c1));
+        if (pd.c2 > 16) {
+            err = "product state larger than 2^(2*table bits + 16) amplitudes";
+            return 5;
         }
-        // lookup table over the low c bits, computed in double
-        std::vector<double> tab(size_t(2) << pd.c);
-        for (uint64_t y = 0; y < (1ULL << pd.c); y++) {
-            cd acc(1.0, 0.0);
-            for (uint32_t b = 0; b < pd.c; b++) acc *= ((y >> b) & 1) ? v[b][1] : v[b][0];
-            tab[2 * y] = acc.real();
-            tab[2 * y + 1] = acc.imag();
-        }
+        // three factor tables over consecutive bit ranges, computed in double
+        std::vector<double> tab;
+        auto add_table = [&](int lo, int bits, cd scale) {
+            for (uint64_t y = 0; y < (1ULL << bits); y++) {
+                cd acc = scale;
+                for (int b = 0; b < bits; b++) acc *= ((y >> b) & 1) ? v[lo + b][1] : v[lo + b][0];
+                tab.push_back(acc.real());
+                tab.push_back(acc.imag());
+            }
+        };
+        add_table(0, int(pd.c0), cd(1.0, 0.0));
+        add_table(int(pd.c0), int(pd.c1), cd(1.0, 0.0));
+        add_table(int(pd.c0 + pd.c1), int(pd.c2), a0);
         Pass ps;
         ps.kind = Pass::PRODUCT;
         ps.m = pm;
@@ -672,10 +713,29 @@ int plan(const std::vector<Op> &ops, int elem_bytes, const PlanParams &pp, const
         ps.steps.push_back(StepDev{STEP_DIAG, 0, compile_diag(out.blob, w, ps.geom)});
     };
 
+    uint64_t exp_off = 0;
     auto standalone_diag = [&](int mm, const std::vector<DiagTerm> &w) {
-        const int T = std::min(mm, pp.diag_tile_bits);
-        std::vector<const U3Op *> none;
-        emit_tile(mm, T, std::vector<int>(), none, &w);
+        if (!exp_off) {
+            // exp(2 pi i j / 1024) rounded from long double
+            const int nt = 1 << kExpTableBits;
+            std::vector<double> t(2 * nt);
+            for (int j = 0; j < nt; j++) {
+                const long double a = 2.0L * 3.141592653589793238462643383279502884L * j / nt;
+                t[2 * j] = double(cosl(a));
+                t[2 * j + 1] = double(sinl(a));
+            }
+            if (elem_bytes == 8) exp_off = put_vec(out.blob, std::vector<float>(t.begin(), t.end()));
+            else exp_off = put_vec(out.blob, t);
+        }
+        const int T = std::min(mm, diag_tile_bits(elem_bytes));
+        TileDev g = make_geom(mm, T, std::vector<int>());
+        Pass ps;
+        ps.kind = Pass::DIAG;
+        ps.m = mm;
+        ps.geom = g;
+        ps.off = compile_diag(out.blob, w, g);
+        ps.off2 = exp_off;
+        out.passes.push_back(ps);
     };
 
     for (; i < ops.size(); i++) {

@@ -33,10 +33,10 @@ struct PlanParams {
 };
 
 struct Pass {
-    enum Kind { PRODUCT, EXPAND, TILE, PAIR } kind;
+    enum Kind { PRODUCT, EXPAND, TILE, PAIR, DIAG } kind;
     int m = 0;
     uint64_t off = 0;    // blob offset of the pass descriptor
-    uint64_t off2 = 0;   // PRODUCT: lookup table
+    uint64_t off2 = 0;   // PRODUCT: lookup table; DIAG: exp table
     TileDev geom;        // TILE
     std::vector<StepDev> steps;
 };
@@ -46,6 +46,9 @@ struct Plan {
     std::vector<Pass> passes;
     void clear();
 };
+
+// Tile bits of the standalone diagonal pass (diag.cu).
+int diag_tile_bits(int elem_bytes);
 
 int plan(const std::vector<Op> &ops, int elem_bytes, const PlanParams &pp, const WalkState &start, Plan &out,
          std::string &err);

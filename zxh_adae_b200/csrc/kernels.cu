@@ -32,37 +32,28 @@ template <typename E>
 __global__ void __launch_bounds__(kThreads) product_kernel(const uint8_t *__restrict__ blob, uint64_t off,
                                                            uint64_t tab_off, E *__restrict__ state)
 {
-    using R = typename ET<E>::R;
-    const ProductDev *p = reinterpret_cast<const ProductDev *>(blob + off);
-    const R *tab = reinterpret_cast<const R *>(blob + tab_off);
-    const uint32_t m = p->m, c = p->c;
-    const uint64_t tile = 1ULL << c;
-    const uint64_t ntiles = 1ULL << (m - c);
-    __shared__ R s_h[2];
-    for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double hr = p->a0[0], hi = p->a0[1];
-            for (uint32_t b = c; b < m; b++) {
-                const int bit = int((t >> (b - c)) & 1);
-                const double vr = p->v[b][2 * bit], vi = p->v[b][2 * bit + 1];
-                const double nr = hr * vr - hi * vi, ni = hr * vi + hi * vr;
-                hr = nr;
-                hi = ni;
-            }
-            s_h[0] = R(hr);
-            s_h[1] = R(hi);
+    using VT = typename ET<E>::VT;
+    constexpr int V = ET<E>::V;
+    const ProductDev p = *reinterpret_cast<const ProductDev *>(blob + off);
+    const E *L = reinterpret_cast<const E *>(blob + tab_off);
+    const E *M = L + (1u << p.c0);
+    const E *H = M + (1u << p.c1);
+    const uint64_t n = 1ULL << p.m;
+    const uint64_t m0 = (1ULL << p.c0) - 1, m1 = (1ULL << p.c1) - 1;
+    const uint32_t s1 = p.c0, s2 = p.c0 + p.c1;
+    if (n < uint64_t(V)) {  // a single complex64 amplitude
+        if (blockIdx.x == 0 && threadIdx.x == 0) state[0] = cmul(cmul(L[0], M[0]), H[0]);
+        return;
+    }
+    const uint64_t nv = n / V;
+    for (uint64_t i = uint64_t(blockIdx.x) * kThreads + threadIdx.x; i < nv; i += uint64_t(gridDim.x) * kThreads) {
+        VT x;
+#pragma unroll
+        for (int v = 0; v < V; v++) {
+            const uint64_t y = i * V + v;
+            vset(x, v, cmul(cmul(__ldg(&L[y & m0]), __ldg(&M[(y >> s1) & m1])), __ldg(&H[y >> s2])));
         }
-        __syncthreads();
-        const R hr = s_h[0], hi = s_h[1];
-        E *dst = state + t * tile;
-        for (uint64_t y = threadIdx.x; y < tile; y += kThreads) {
-            const R ar = tab[2 * y], ai = tab[2 * y + 1];
-            E o;
-            o.x = ar * hr - ai * hi;
-            o.y = ar * hi + ai * hr;
-            dst[y] = o;
-        }
+        __stcs(reinterpret_cast<VT *>(state) + i, x);
     }
 }
 
@@ -514,9 +505,9 @@ cudaError_t run_passes(const std::vector<Pass> &passes, const uint8_t *dblob, vo
     for (const Pass &ps : passes) {
         cudaError_t e = cudaSuccess;
         if (ps.kind == Pass::PRODUCT) {
-            const uint64_t c = std::min<uint64_t>(uint64_t(ps.m), 12);
-            const uint64_t ntiles = 1ULL << (uint64_t(ps.m) - c);
-            const unsigned grid = unsigned(std::min<uint64_t>(ntiles, uint64_t(sms) * 8));
+            const uint64_t nvec = std::max<uint64_t>(1, (1ULL << ps.m) / (16 / elem_bytes));
+            const unsigned grid = unsigned(std::max<uint64_t>(1, std::min<uint64_t>((nvec + kThreads - 1) / kThreads,
+                                                                                    uint64_t(sms) * 8)));
             if (elem_bytes == 8)
                 product_kernel<float2><<<grid, kThreads, 0, st>>>(dblob, ps.off, ps.off2, static_cast<float2 *>(state));
             else
@@ -531,6 +522,8 @@ cudaError_t run_passes(const std::vector<Pass> &passes, const uint8_t *dblob, vo
             else
                 expand_kernel<double2><<<grid, kThreads, 0, st>>>(dblob, ps.off, static_cast<double2 *>(state));
             e = cudaGetLastError();
+        } else if (ps.kind == Pass::DIAG) {
+            e = run_diag(dblob, ps.off, ps.off2, ps.m, elem_bytes, state, sms, st);
         } else if (ps.kind == Pass::PAIR) {
             const uint64_t np = 1ULL << (ps.m - 1);
             const unsigned grid = unsigned(std::max<uint64_t>(1, std::min<uint64_t>((np + kThreads - 1) / kThreads,

@@ -34,6 +34,9 @@ cudaError_t run_sampler(const void *state, int elem_bytes, int m, uint64_t shots
 struct Pass;
 cudaError_t run_passes(const std::vector<Pass> &passes, const uint8_t *dblob, void *state, int elem_bytes,
                        DevStatus *status, int sms, cudaStream_t st, uint64_t &kernels);
+cudaError_t run_diag(const uint8_t *dblob, uint64_t doff, uint64_t toff, int m, int elem_bytes, void *state, int sms,
+                     cudaStream_t st);
+int diag_tile_bits(int elem_bytes);
 cudaError_t run_scatter(const void *state, uint64_t n_real, const uint64_t *dcoltab, uint64_t b, int N, int order,
                         double gre, double gim, void *out, int elem_bytes, int sms, cudaStream_t st);
 
