@@ -162,6 +162,12 @@ int zxh_stream(zxh_sim *sim, void **stream);
  * handle's stream around the launches). Any pointer may be NULL. */
 int zxh_last_stats(const zxh_sim *sim, uint64_t *kernels, uint64_t *passes, double *device_ms);
 
+/* Pass-planner tuning (used by the autotuner): tile_bits_c64, tile_bits_c128,
+ * contig_bits, max_gates (generic tile pass), fast_gates (gates per fast U3
+ * pass), fast_fuse_quad, fast_contig_c64, fast_contig_c128. Takes effect at the
+ * next zxh_execute / zxh_apply. No counterpart in the reference. */
+int zxh_set_param(zxh_sim *sim, const char *name, int value);
+
 #ifdef __cplusplus
 }
 #endif

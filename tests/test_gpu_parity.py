@@ -164,3 +164,30 @@ def test_errors_raise_instead_of_abort():
     s.execute()
     with pytest.raises(ValueError):
         s.get_results() if False else s.results_words(5)
+
+
+def _layers_with_x(n, layers, seed):
+    """U3 layers with X gates and big cp cascades in between (exercises flipped
+    selectors, fused and unfused windows in the fast U3 pass)."""
+    rng = np.random.default_rng(seed)
+    recs = [(zx._core.H, 0, q) for q in range(n)]
+    for layer in range(layers):
+        for q in rng.choice(n, size=n // 3, replace=False):
+            recs.append((zx._core.X, 0, int(q)))
+        for q in range(n):
+            recs.append((zx._core.U3, 0, q, *rng.uniform(0, 2 * np.pi, 3)))
+        if layer % 2:
+            recs.extend((int(g["type"]), int(g["cq"]), int(g["q"]), float(g["theta"])) for g in wl.cp_cascade(n))
+        else:
+            for i in range(n - 1):
+                recs.append((zx._core.CP, i, i + 1, rng.uniform(0, 2 * np.pi)))
+        recs.append((zx._core.RZ, 0, int(rng.integers(n)), rng.uniform(0, 2 * np.pi)))
+    return zx.as_records(recs)
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+@pytest.mark.parametrize("n", [11, 12, 13, 18])
+def test_fast_u3_pass_edges(dtype, n):
+    gates = _layers_with_x(n, 4, seed=n)
+    o, s = run_pair(n, gates, dtype)
+    assert max_err(s, o) <= TOL[dtype]

@@ -89,6 +89,7 @@ _sig("zxh_num_qubits", [_P, ctypes.POINTER(_SZ)])
 _sig("zxh_state_view", [_P, ctypes.POINTER(_P), ctypes.POINTER(_SZ), ctypes.POINTER(_SZ),
                         ctypes.POINTER(_D), ctypes.POINTER(_D)])
 _sig("zxh_stream", [_P, ctypes.POINTER(_P)])
+_sig("zxh_set_param", [_P, ctypes.c_char_p, ctypes.c_int])
 _sig("zxh_last_stats", [_P, ctypes.POINTER(_U64), ctypes.POINTER(_U64), ctypes.POINTER(_D)])
 
 _ERRORS = {1: ValueError, 2: RuntimeError, 3: RuntimeError, 4: MemoryError, 5: ValueError, 6: RuntimeError}
@@ -312,6 +313,10 @@ class ZXH:
         s = _P()
         self._ck(_lib.zxh_stream(self._h, ctypes.byref(s)))
         return int(s.value or 0)
+
+    def set_param(self, name: str, value: int) -> None:
+        """Pass-planner tuning knob (see zxh_set_param in include/zxh_b200.h)."""
+        self._ck(_lib.zxh_set_param(self._h, name.encode(), int(value)))
 
     def last_stats(self) -> tuple:
         """(kernels launched, state passes, device ms) of the last execute/apply/measure."""

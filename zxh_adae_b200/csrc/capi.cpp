@@ -571,6 +571,32 @@ int zxh_stream(zxh_sim *s, void **stream)
     return ZXH_OK;
 }
 
+int zxh_set_param(zxh_sim *s, const char *name, int value)
+{
+    if (!s || !name) return ZXH_ERR_ARG;
+    struct Entry { const char *key; int *field; int lo, hi; };
+    const Entry table[] = {
+        {"tile_bits_c64", &s->pp.tile_bits_c64, 1, 13},
+        {"tile_bits_c128", &s->pp.tile_bits_c128, 1, 12},
+        {"contig_bits", &s->pp.contig_bits, 1, 12},
+        {"max_gates", &s->pp.max_gates, 1, 16},
+        {"fast_gates", &s->pp.fast_gates, 1, 16},
+        {"fast_fuse_quad", &s->pp.fast_fuse_quad, 0, 64},
+        {"fast_contig_c64", &s->pp.fast_contig_c64, 1, 11},
+        {"fast_contig_c128", &s->pp.fast_contig_c128, 0, 10},
+        {"row_wide", &s->pp.row_wide, 0, 1},
+    };
+    for (const Entry &e : table)
+        if (std::strcmp(e.key, name) == 0) {
+            if (value < e.lo || value > e.hi)
+                return fail(s, ZXH_ERR_ARG, std::string(name) + " must be in [" + std::to_string(e.lo) + ", " +
+                                                std::to_string(e.hi) + "]");
+            *e.field = value;
+            return ZXH_OK;
+        }
+    return fail(s, ZXH_ERR_ARG, std::string("unknown parameter ") + name);
+}
+
 int zxh_last_stats(const zxh_sim *s, uint64_t *kernels, uint64_t *passes, double *device_ms)
 {
     if (!s) return ZXH_ERR_ARG;

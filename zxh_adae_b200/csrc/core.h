@@ -194,6 +194,49 @@ struct ProductDev {
     uint32_t m, c0, c1, c2;
 };
 
+// Fast tile pass (u3pass.cu): every pair op has a single-bit delta equal to its
+// selector bit (the X-transported map is a permutation on those bits) and no
+// control. Tile coordinates 0..4 are the lanes of a warp; per shared-memory round
+// R coordinates are held in registers and 3 more select the warp.
+constexpr int kFastMaxGates = 16;
+constexpr int kFastMaxRounds = 4;
+
+struct FastGateDev {
+    uint32_t coord;      // tile coordinate of the gate's bit
+    uint32_t round;      // register round the gate runs in (lane gates: round 0)
+    uint64_t alpha_out;  // selector bits outside the tile (tile parity flips beta)
+    uint32_t beta, pad;
+    double u[8];
+};
+
+struct RoundDev {
+    uint8_t rc[4];  // register coordinates
+    uint8_t oc[3];  // warp coordinates
+    uint8_t pad;
+};
+
+struct FastDev {
+    TileDev g;
+    uint32_t R, nrounds, ngates, pad;
+    RoundDev rounds[kFastMaxRounds];
+    uint64_t off_gates;
+    uint64_t off_pre, off_post;  // DiagDev offsets of the fused windows, 0 if none
+};
+
+// Strided high-qubit pass (u3pass.cu): real bits [0, F) are a thread's 16-byte
+// vector and the lanes of its warp (F = 6 for complex64, 5 for complex128); R more
+// bits (the gates' bits, any positions) are a thread's registers; every other bit
+// enumerates work items. Each register row of a warp is 512 contiguous bytes and
+// the warps of a CTA take consecutive items.
+struct RowPassDev {
+    uint32_t m, F, R, ngates;
+    uint8_t rb[8];        // real bits of the register coordinates, ascending
+    uint64_t tile_mask;   // bits [0, F) and rb
+    uint64_t nitems;      // 2^(m - F - R)
+    uint64_t off_gates;   // FastGateDev[ngates] (coord = tile coordinate, round unused)
+    uint64_t off_pre, off_post;
+};
+
 // Status word shared with the device (bounded waits report here).
 struct DevStatus { uint32_t code; uint32_t where; uint64_t info; };
 

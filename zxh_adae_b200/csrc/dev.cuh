@@ -32,6 +32,8 @@ __device__ __forceinline__ void vset(float4 &x, int v, float2 a)
 {
     if (v) { x.z = a.x; x.w = a.y; } else { x.x = a.x; x.y = a.y; }
 }
+__device__ __forceinline__ float2 vget(const float2 &x, int) { return x; }
+__device__ __forceinline__ void vset(float2 &x, int, float2 a) { x = a; }
 __device__ __forceinline__ double2 vget(const double2 &x, int) { return x; }
 __device__ __forceinline__ void vset(double2 &x, int, double2 a) { x = a; }
 

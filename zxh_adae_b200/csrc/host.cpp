@@ -714,7 +714,7 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
     };
 
     uint64_t exp_off = 0;
-    auto standalone_diag = [&](int mm, const std::vector<DiagTerm> &w) {
+    auto ensure_exp = [&]() {
         if (!exp_off) {
             // exp(2 pi i j / 1024) rounded from long double
             const int nt = 1 << kExpTableBits;
@@ -727,6 +727,9 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
             if (elem_bytes == 8) exp_off = put_vec(out.blob, std::vector<float>(t.begin(), t.end()));
             else exp_off = put_vec(out.blob, t);
         }
+    };
+    auto standalone_diag = [&](int mm, const std::vector<DiagTerm> &w) {
+        ensure_exp();
         const int T = std::min(mm, diag_tile_bits(elem_bytes));
         TileDev g = make_geom(mm, T, std::vector<int>());
         Pass ps;
@@ -738,12 +741,179 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
         out.passes.push_back(ps);
     };
 
+    // Fuses a window into a fast pass as prologue (pre) or epilogue when it is
+    // small enough for per-thread evaluation; returns false otherwise.
+    auto fuse_fast = [&](Pass &ps, const std::vector<DiagTerm> &w, bool pre) -> bool {
+        uint64_t &slot = ps.kind == Pass::ROW ? (pre ? ps.row.off_pre : ps.row.off_post)
+                                              : (pre ? ps.fast.off_pre : ps.fast.off_post);
+        if (slot) return false;
+        const size_t mark = out.blob.size();
+        const uint64_t off = compile_diag(out.blob, w, ps.geom);
+        const DiagDev *d = reinterpret_cast<const DiagDev *>(out.blob.data() + off);
+        if (d->n_gen != 0 || d->n_in_quad > uint32_t(pp.fast_fuse_quad)) {
+            out.blob.resize(mark);
+            return false;
+        }
+        ensure_exp();
+        slot = off;
+        ps.off2 = exp_off;
+        return true;
+    };
+
+    const int tfast = fast_tile_bits(elem_bytes);
+    const int rfast = fast_reg_bits(elem_bytes);
+    const int clo_fast = std::max(elem_bytes == 8 ? 1 : 0,
+                                  std::min(tfast - 1, elem_bytes == 8 ? pp.fast_contig_c64 : pp.fast_contig_c128));
+    auto fast_ok = [&](const Op &op) {
+        if (op.m < tfast) return false;
+        for (const U3Op &u : op.u3)
+            if (u.has_ctrl || !u.delta || (u.delta & (u.delta - 1)) || u.sel.alpha != u.delta) return false;
+        return true;
+    };
+
+    // One fast pass over the gates (each with a single bit) in a tile made of
+    // `c` contiguous bits plus `dirs`.
+    auto emit_fast = [&](int mm, int c, std::vector<int> dirs, const std::vector<const U3Op *> &gs) {
+        // pad the high directions so the tile has exactly tfast coordinates
+        for (int b = c; int(dirs.size()) < tfast - c && b < mm; b++)
+            if (std::find(dirs.begin(), dirs.end(), b) == dirs.end()) dirs.push_back(b);
+        std::sort(dirs.begin(), dirs.end());
+        Pass ps;
+        ps.kind = Pass::FAST;
+        ps.m = mm;
+        ps.geom = make_geom(mm, c, dirs);
+        std::memset(&ps.fast, 0, sizeof(ps.fast));
+        int coord_of_bit[64];
+        for (int b = 0; b < 64; b++) coord_of_bit[b] = -1;
+        for (uint32_t k = 0; k < ps.geom.T; k++) coord_of_bit[ps.geom.pos[k]] = int(k);
+        std::vector<int> regc;  // coordinates >= 5 carrying gates
+        for (const U3Op *u : gs) {
+            const int k = coord_of_bit[__builtin_ctzll(u->delta)];
+            if (k >= 5) regc.push_back(k);
+        }
+        std::sort(regc.begin(), regc.end());
+        const int nr = std::max<int>(1, (int(regc.size()) + rfast - 1) / rfast);
+        ps.fast.R = uint32_t(rfast);
+        ps.fast.nrounds = uint32_t(nr);
+        for (int r = 0; r < nr; r++) {
+            std::vector<int> rc(regc.begin() + std::min<size_t>(regc.size(), size_t(r) * rfast),
+                                regc.begin() + std::min<size_t>(regc.size(), size_t(r + 1) * rfast));
+            for (int k = 5; int(rc.size()) < rfast; k++)
+                if (std::find(rc.begin(), rc.end(), k) == rc.end()) rc.push_back(k);
+            std::vector<int> oc;
+            for (int k = 5; k < tfast; k++)
+                if (std::find(rc.begin(), rc.end(), k) == rc.end()) oc.push_back(k);
+            for (int j = 0; j < rfast; j++) ps.fast.rounds[r].rc[j] = uint8_t(rc[j]);
+            for (int j = 0; j < 3; j++) ps.fast.rounds[r].oc[j] = uint8_t(oc[j]);
+        }
+        for (const U3Op *u : gs) {
+            FastGateDev fg;
+            std::memset(&fg, 0, sizeof(fg));
+            const int k = coord_of_bit[__builtin_ctzll(u->delta)];
+            fg.coord = uint32_t(k);
+            fg.round = 0;
+            if (k >= 5) {
+                const int idx = int(std::find(regc.begin(), regc.end(), k) - regc.begin());
+                fg.round = uint32_t(idx / rfast);
+            }
+            fg.alpha_out = u->sel.alpha & ~ps.geom.tile_mask;
+            fg.beta = uint32_t(u->sel.beta);
+            for (int q = 0; q < 4; q++) {
+                fg.u[2 * q] = u->u[q].real();
+                fg.u[2 * q + 1] = u->u[q].imag();
+            }
+            ps.fgates.push_back(fg);
+        }
+        ps.fast.ngates = uint32_t(ps.fgates.size());
+        out.passes.push_back(ps);
+        return int(out.passes.size()) - 1;
+    };
+
     for (; i < ops.size(); i++) {
         const Op &op = ops[i];
+        if (op.kind == Op::U3BATCH && fast_ok(op)) {
+            const int mm = op.m;
+            std::vector<const U3Op *> gs;
+            for (const U3Op &u : op.u3) gs.push_back(&u);
+            std::sort(gs.begin(), gs.end(), [](const U3Op *a, const U3Op *b) { return a->delta < b->delta; });
+            const int G = std::max(pp.fast_gates, row_fixed_bits(elem_bytes, pp.row_wide));
+            std::vector<std::pair<std::vector<int>, std::vector<const U3Op *>>> groups;
+            size_t k = 0;
+            {
+                std::vector<const U3Op *> first;
+                while (k < gs.size() && int(first.size()) < G && (gs[k]->delta >> tfast) == 0) first.push_back(gs[k++]);
+                if (!first.empty()) groups.push_back({std::vector<int>(), first});
+            }
+            const int first_pass = int(out.passes.size());
+            for (size_t gidx = 0; gidx < groups.size(); gidx++)
+                last_tile_pass = emit_fast(mm, tfast, groups[gidx].first, groups[gidx].second);
+            // the rest: strided register passes over the high bits
+            const int frow = row_fixed_bits(elem_bytes, pp.row_wide), rrow = row_reg_bits(elem_bytes, pp.row_wide);
+            while (k < gs.size()) {
+                std::vector<const U3Op *> grp;
+                while (k < gs.size() && int(grp.size()) < rrow) grp.push_back(gs[k++]);
+                std::vector<int> rb;
+                for (const U3Op *u : grp) rb.push_back(__builtin_ctzll(u->delta));
+                // pad with the lowest free bits so every thread keeps 2^R rows in flight
+                for (int b = frow; int(rb.size()) < rrow && b < mm; b++)
+                    if (std::find(rb.begin(), rb.end(), b) == rb.end()) rb.push_back(b);
+                std::sort(rb.begin(), rb.end());
+                std::vector<int> coord_of(grp.size());
+                for (size_t r = 0; r < grp.size(); r++)
+                    coord_of[r] = frow + int(std::find(rb.begin(), rb.end(), __builtin_ctzll(grp[r]->delta)) - rb.begin());
+                Pass ps;
+                ps.kind = Pass::ROW;
+                ps.m = mm;
+                ps.geom = make_geom(mm, frow, rb);
+                std::memset(&ps.row, 0, sizeof(ps.row));
+                ps.row.m = uint32_t(mm);
+                ps.row.F = uint32_t(frow);
+                ps.row.R = uint32_t(rb.size());
+                ps.row.ngates = uint32_t(grp.size());
+                for (size_t r = 0; r < rb.size(); r++) ps.row.rb[r] = uint8_t(rb[r]);
+                ps.row.tile_mask = ps.geom.tile_mask;
+                ps.row.nitems = 1ULL << (mm - frow - int(rb.size()));
+                ps.wide = pp.row_wide;
+                for (size_t r = 0; r < grp.size(); r++) {
+                    FastGateDev fg;
+                    std::memset(&fg, 0, sizeof(fg));
+                    fg.coord = uint32_t(coord_of[r]);
+                    fg.alpha_out = grp[r]->sel.alpha & ~ps.geom.tile_mask;
+                    fg.beta = uint32_t(grp[r]->sel.beta);
+                    for (int q = 0; q < 4; q++) {
+                        fg.u[2 * q] = grp[r]->u[q].real();
+                        fg.u[2 * q + 1] = grp[r]->u[q].imag();
+                    }
+                    ps.fgates.push_back(fg);
+                }
+                out.passes.push_back(ps);
+                last_tile_pass = int(out.passes.size()) - 1;
+            }
+            if (held) {
+                if (!fuse_fast(out.passes[first_pass], *held, true)) {
+                    // not fusable: run it on its own, before the batch
+                    const std::vector<DiagTerm> w = *held;
+                    Pass keep_last;
+                    std::vector<Pass> batch(out.passes.begin() + first_pass, out.passes.end());
+                    out.passes.resize(first_pass);
+                    standalone_diag(mm, w);
+                    for (Pass &p : batch) out.passes.push_back(p);
+                    last_tile_pass = int(out.passes.size()) - 1;
+                }
+                held = nullptr;
+            }
+            m = mm;
+            continue;
+        }
         if (op.kind == Op::DIAG) {
             if (held) standalone_diag(m, *held), held = nullptr;
-            if (last_tile_pass >= 0 && out.passes[last_tile_pass].m == op.m &&
-                out.passes[last_tile_pass].steps.size() < size_t(pp.max_steps)) {
+            if (last_tile_pass >= 0 &&
+                (out.passes[last_tile_pass].kind == Pass::FAST || out.passes[last_tile_pass].kind == Pass::ROW) &&
+                out.passes[last_tile_pass].m == op.m && fuse_fast(out.passes[last_tile_pass], op.diag, false)) {
+                last_tile_pass = -1;
+            } else if (last_tile_pass >= 0 && out.passes[last_tile_pass].kind == Pass::TILE &&
+                       out.passes[last_tile_pass].m == op.m &&
+                       out.passes[last_tile_pass].steps.size() < size_t(pp.max_steps)) {
                 attach_epilogue(last_tile_pass, op.diag);
                 last_tile_pass = -1;  // keep one epilogue window per pass
             } else if (i + 1 < ops.size() && ops[i + 1].kind == Op::U3BATCH && ops[i + 1].m == op.m) {
@@ -859,6 +1029,17 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
 
     // finalize step arrays
     for (Pass &ps : out.passes) {
+        if (ps.kind == Pass::ROW) {
+            ps.row.off_gates = put_vec(out.blob, ps.fgates);
+            ps.off = put(out.blob, ps.row);
+            continue;
+        }
+        if (ps.kind == Pass::FAST) {
+            ps.fast.g = ps.geom;
+            ps.fast.off_gates = put_vec(out.blob, ps.fgates);
+            ps.off = put(out.blob, ps.fast);
+            continue;
+        }
         if (ps.kind != Pass::TILE) continue;
         ps.geom.nsteps = uint32_t(ps.steps.size());
         ps.geom.off_steps = put_vec(out.blob, ps.steps);

@@ -26,19 +26,28 @@ struct PlanParams {
     int tile_bits_c64 = 12;     // log2 amplitudes per TMA tile, complex64
     int tile_bits_c128 = 11;    // same for complex128
     int contig_bits = 6;        // contiguous low bits of a tile that also spans high bits
-    int max_gates = 12;         // pair ops per tile pass
+    int max_gates = 12;         // pair ops per generic tile pass
+    int fast_gates = 8;         // fused gates per fast U3 pass (bounded by the FMA budget per byte)
+    int fast_fuse_quad = 32;    // largest in-tile quadratic term count of a window fused into a fast pass
+    int fast_contig_c64 = 4;    // contiguous low bits of a fast tile that also spans high bits (complex64)
+    int fast_contig_c128 = 3;   // same for complex128
+    int row_wide = 0;           // strided high-qubit pass shape: 0 = 16-byte lanes, 1 = more register bits
     int max_steps = 16;
     int diag_tile_bits = 12;    // tile size of a standalone diagonal pass
     int product_table_bits = 12;
 };
 
 struct Pass {
-    enum Kind { PRODUCT, EXPAND, TILE, PAIR, DIAG } kind;
+    enum Kind { PRODUCT, EXPAND, TILE, PAIR, DIAG, FAST, ROW } kind;
     int m = 0;
     uint64_t off = 0;    // blob offset of the pass descriptor
     uint64_t off2 = 0;   // PRODUCT: lookup table; DIAG: exp table
     TileDev geom;        // TILE
     std::vector<StepDev> steps;
+    FastDev fast;                        // FAST
+    RowPassDev row;                      // ROW
+    int wide = 0;                        // ROW: kernel shape
+    std::vector<FastGateDev> fgates;     // FAST
 };
 
 struct Plan {
@@ -47,8 +56,13 @@ struct Plan {
     void clear();
 };
 
-// Tile bits of the standalone diagonal pass (diag.cu).
+// Tile bits of the standalone diagonal pass (diag.cu) and of the fast U3 pass
+// (u3pass.cu), and the register bits of one fast-pass round.
 int diag_tile_bits(int elem_bytes);
+int fast_tile_bits(int elem_bytes);
+int fast_reg_bits(int elem_bytes);
+int row_reg_bits(int elem_bytes, int wide);
+int row_fixed_bits(int elem_bytes, int wide);
 
 int plan(const std::vector<Op> &ops, int elem_bytes, const PlanParams &pp, const WalkState &start, Plan &out,
          std::string &err);

@@ -522,6 +522,10 @@ cudaError_t run_passes(const std::vector<Pass> &passes, const uint8_t *dblob, vo
             else
                 expand_kernel<double2><<<grid, kThreads, 0, st>>>(dblob, ps.off, static_cast<double2 *>(state));
             e = cudaGetLastError();
+        } else if (ps.kind == Pass::ROW) {
+            e = run_row_pass(dblob, ps.off, ps.off2, ps.row.nitems, elem_bytes, ps.wide, state, sms, st);
+        } else if (ps.kind == Pass::FAST) {
+            e = run_fast_tile(dblob, ps.off, ps.off2, ps.geom.ntiles, elem_bytes, state, status, sms, st);
         } else if (ps.kind == Pass::DIAG) {
             e = run_diag(dblob, ps.off, ps.off2, ps.m, elem_bytes, state, sms, st);
         } else if (ps.kind == Pass::PAIR) {

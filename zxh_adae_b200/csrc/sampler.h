@@ -37,6 +37,10 @@ cudaError_t run_passes(const std::vector<Pass> &passes, const uint8_t *dblob, vo
 cudaError_t run_diag(const uint8_t *dblob, uint64_t doff, uint64_t toff, int m, int elem_bytes, void *state, int sms,
                      cudaStream_t st);
 int diag_tile_bits(int elem_bytes);
+cudaError_t run_fast_tile(const uint8_t *dblob, uint64_t foff, uint64_t toff, uint64_t ntiles, int elem_bytes,
+                          void *state, DevStatus *status, int sms, cudaStream_t st);
+cudaError_t run_row_pass(const uint8_t *dblob, uint64_t poff, uint64_t toff, uint64_t nitems, int elem_bytes,
+                         int wide, void *state, int sms, cudaStream_t st);
 cudaError_t run_scatter(const void *state, uint64_t n_real, const uint64_t *dcoltab, uint64_t b, int N, int order,
                         double gre, double gim, void *out, int elem_bytes, int sms, cudaStream_t st);
 

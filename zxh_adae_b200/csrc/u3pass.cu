@@ -1,0 +1,742 @@
+// u3pass.cu -- the U3-batch pass (sm_100a), fast form.
+//
+// One pass applies up to 8 fused single-qubit gates (and, fused around them, small
+// diagonal windows) to the whole state with one read and one write of every
+// amplitude. The reference runs one full grid sweep per fused gate with a
+// cooperative grid.sync() between them (u3_block_batch_kernel_cuda,
+// src/zxh/src/kernel/kernel_cuda.cu:390-423).
+//
+// A tile is 2^T amplitudes: 2^c contiguous ones times 2^h strided chunks, moved
+// global <-> shared by TMA bulk copies (cp.async.bulk, double-buffered, mbarrier
+// completion, bounded waits). Inside the tile the amplitudes are worked on in
+// registers: tile coordinates 0..4 are the lanes of a warp (gates there exchange
+// partners with shfl.xor), in each shared-memory round R further coordinates are
+// a thread's registers (gates there are register-local 2x2 updates) and 3 select
+// the warp. Diagonal windows fused into the pass are evaluated per amplitude as a
+// polynomial in 64-bit fixed-point turns (Gray-code walk over the register bits)
+// and one table-plus-Taylor exp.
+#include "core.h"
+#include "dev.cuh"
+#include "host.h"
+#include "sampler.h"
+
+#include <algorithm>
+#include <cuda_runtime.h>
+
+namespace zxh {
+
+namespace {
+
+template <typename E>
+struct FastCfg;
+template <>
+struct FastCfg<float2> {
+    static constexpr int R = 4;  // register coordinates per round: T = 5 + 3 + 4 = 12
+};
+template <>
+struct FastCfg<double2> {
+    static constexpr int R = 3;  // T = 11
+};
+
+__device__ __forceinline__ uint64_t pdep_bits(uint64_t x, uint64_t mask)
+{
+    uint64_t r = 0;
+    for (uint64_t bb = 1; mask; bb += bb) {
+        const uint64_t low = mask & (0 - mask);
+        if (x & bb) r |= low;
+        mask &= mask - 1;
+    }
+    return r;
+}
+
+__device__ __forceinline__ uint64_t fchunk_base(const TileDev &g, uint64_t r, uint32_t j)
+{
+    uint64_t a = r;
+    for (uint32_t b = 0; b < g.h; b++)
+        if ((j >> b) & 1) a |= 1ULL << g.pos[g.c + b];
+    return a;
+}
+
+// Bulk copies of one tile, spread over all threads: thread t moves chunks t,
+// t + 256, ...; each warp announces its own byte count on the stage's mbarrier
+// (initialised with one arrival per warp), so no cross-warp ordering is needed.
+template <typename E>
+__device__ __forceinline__ void fload(const TileDev &g, const E *state, E *buf, uint64_t r, uint64_t *bar, int tid)
+{
+    const uint32_t nchunk = 1u << g.h;
+    const uint32_t cbytes = uint32_t(sizeof(E)) << g.c;
+    const int warp = tid >> 5, lane = tid & 31;
+    uint32_t mine = 0;  // chunks of this warp
+    for (uint32_t j0 = uint32_t(warp) * 32; j0 < nchunk; j0 += kThreads) mine += min(32u, nchunk - j0);
+    if (lane == 0) mbar_arrive_expect_tx(bar, mine * cbytes);
+    __syncwarp();
+    for (uint32_t j = uint32_t(tid); j < nchunk; j += kThreads)
+        bulk_g2s(buf + (size_t(j) << g.c), state + fchunk_base(g, r, j), cbytes, bar);
+}
+
+template <typename E>
+__device__ __forceinline__ void fstore(const TileDev &g, E *state, const E *buf, uint64_t r, int tid)
+{
+    const uint32_t nchunk = 1u << g.h;
+    const uint32_t cbytes = uint32_t(sizeof(E)) << g.c;
+    for (uint32_t j = uint32_t(tid); j < nchunk; j += kThreads)
+        bulk_s2g(state + fchunk_base(g, r, j), buf + (size_t(j) << g.c), cbytes);
+    bulk_commit();
+}
+
+// Per-tile coefficients of a fused window, computed by one warp: lane k < T sums
+// the cross terms of tile coordinate k, all lanes share the out-of-tile constant.
+__device__ __forceinline__ void window_tile_params(const uint8_t *blob, const DiagDev &d, uint64_t r, uint32_t T,
+                                                   int lane, int64_t *da, int64_t *K)
+{
+    const QuadTerm *cr = reinterpret_cast<const QuadTerm *>(blob + d.off_cross);
+    const LinTerm *ol = reinterpret_cast<const LinTerm *>(blob + d.off_out_lin);
+    const QuadTerm *oq = reinterpret_cast<const QuadTerm *>(blob + d.off_out_quad);
+    const uint32_t *kidx = reinterpret_cast<const uint32_t *>(blob + d.off_kidx);
+    int64_t a = 0;
+    if (lane < int(T)) {
+        a = d.lin_in[lane];
+        for (uint32_t q = kidx[lane]; q < kidx[lane + 1]; q++) {
+            const QuadTerm t = cr[q];
+            if ((r >> t.j) & 1) a += t.coef;
+        }
+        da[lane] = a;
+    }
+    int64_t kp = 0;
+    for (uint32_t q = uint32_t(lane); q < d.n_out_lin; q += 32)
+        if ((r >> ol[q].bit) & 1) kp += ol[q].coef;
+    for (uint32_t q = uint32_t(lane); q < d.n_out_quad; q += 32) {
+        const QuadTerm t = oq[q];
+        if (((r >> t.i) & 1) && ((r >> t.j) & 1)) kp += t.coef;
+    }
+    kp = warp_sum_i64(kp);
+    if (lane == 0) *K = kp + d.c0;
+}
+
+}  // namespace
+
+namespace {
+
+template <typename E, int R>
+__device__ __forceinline__ void apply_window(E (&x)[1 << R], const E *s_exp, int64_t A, const int64_t (&w)[R],
+                                             const int64_t *qreg)
+{
+    int64_t acc = A;
+#pragma unroll
+    for (int jj = 0; jj < (1 << R); jj++) {
+        const int gj = jj ^ (jj >> 1);
+        if (jj > 0) {
+            int fb = 0;
+            while (!((jj >> fb) & 1)) fb++;
+            acc += ((gj >> fb) & 1) ? w[fb] : -w[fb];
+        }
+        x[gj] = cmul(x[gj], phase_factor(s_exp, acc + qreg[gj]));
+    }
+}
+
+template <typename E>
+__device__ __forceinline__ E shfl_xor_e(E v, int m);
+template <>
+__device__ __forceinline__ float2 shfl_xor_e(float2 v, int m)
+{
+    return make_float2(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
+}
+template <>
+__device__ __forceinline__ double2 shfl_xor_e(double2 v, int m)
+{
+    return make_double2(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
+}
+
+// a*x + b*y for complex a, b given as (re, im) pairs
+template <typename E, typename RT>
+__device__ __forceinline__ E cmad2(RT ar, RT ai, E x, RT br, RT bi, E y)
+{
+    E o;
+    o.x = ar * x.x - ai * x.y + br * y.x - bi * y.y;
+    o.y = ar * x.y + ai * x.x + br * y.y + bi * y.x;
+    return o;
+}
+
+template <typename E>
+__global__ void __launch_bounds__(kThreads) fast_tile_kernel(const uint8_t *__restrict__ blob, uint64_t foff,
+                                                             uint64_t toff, E *__restrict__ state, DevStatus *status)
+{
+    using RT = typename ET<E>::R;
+    constexpr int R = FastCfg<E>::R;
+    constexpr int NR = 1 << R;
+    const FastDev &f = *reinterpret_cast<const FastDev *>(blob + foff);
+    const TileDev g = f.g;
+    const uint32_t T = g.T;
+    const uint32_t tile_elems = 1u << T;
+    extern __shared__ __align__(128) unsigned char dsm[];
+    E *bufs[2] = {reinterpret_cast<E *>(dsm), reinterpret_cast<E *>(dsm) + tile_elems};
+    E *s_exp = reinterpret_cast<E *>(dsm) + 2 * tile_elems;
+    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ uint64_t s_r[2];
+    __shared__ int64_t s_da[2][kMaxTileBits];
+    __shared__ int64_t s_K[2];
+    __shared__ int64_t s_qreg[2][NR];
+    __shared__ RT s_u[kFastMaxGates][8];
+    __shared__ uint32_t s_gc[kFastMaxGates];
+
+    const int tid = int(threadIdx.x), lane = tid & 31, warp = tid >> 5;
+    const uint32_t ngates = f.ngates, nrounds = f.nrounds;
+    const uint64_t offw[2] = {f.off_pre, f.off_post};
+    const FastGateDev *gates = reinterpret_cast<const FastGateDev *>(blob + f.off_gates);
+
+    if (offw[0] || offw[1]) {
+        const E *tab = reinterpret_cast<const E *>(blob + toff);
+        for (int i = tid; i < (1 << kExpTableBits); i += kThreads) s_exp[i] = tab[i];
+    }
+    if (tid < int(ngates)) s_gc[tid] = gates[tid].coord | (gates[tid].round << 8);
+
+    // tile-independent parts of the fused windows for the round each one runs in
+    int64_t qfix[2] = {0, 0};
+    int64_t rho[2][R];
+#pragma unroll
+    for (int d = 0; d < 2; d++) {
+#pragma unroll
+        for (int r = 0; r < R; r++) rho[d][r] = 0;
+        if (!offw[d]) continue;
+        const DiagDev &dd = *reinterpret_cast<const DiagDev *>(blob + offw[d]);
+        const QuadTerm *iq = reinterpret_cast<const QuadTerm *>(blob + dd.off_in_quad);
+        const RoundDev rd = f.rounds[d == 0 ? 0 : nrounds - 1];
+        // class of a coordinate: 0..R-1 = register index, -1 = fixed bit 0, -2 = fixed bit 1
+        auto cls = [&](uint32_t k) -> int {
+            if (k < 5) return ((lane >> k) & 1) ? -2 : -1;
+            for (int i = 0; i < 3; i++)
+                if (k == rd.oc[i]) return ((warp >> i) & 1) ? -2 : -1;
+            for (int r = 0; r < R; r++)
+                if (k == rd.rc[r]) return r;
+            return -1;
+        };
+        for (uint32_t q = 0; q < dd.n_in_quad; q++) {
+            const QuadTerm t = iq[q];
+            const int a = cls(t.i), b = cls(t.j);
+            if (a == -2 && b == -2) qfix[d] += t.coef;
+            else if (a == -2 && b >= 0) {
+#pragma unroll
+                for (int r = 0; r < R; r++)
+                    if (r == b) rho[d][r] += t.coef;
+            } else if (b == -2 && a >= 0) {
+#pragma unroll
+                for (int r = 0; r < R; r++)
+                    if (r == a) rho[d][r] += t.coef;
+            }
+        }
+        if (tid < NR) {
+            int64_t acc = 0;
+            for (uint32_t q = 0; q < dd.n_in_quad; q++) {
+                const QuadTerm t = iq[q];
+                int a = -1, b = -1;
+                for (int r = 0; r < R; r++) {
+                    if (t.i == rd.rc[r]) a = r;
+                    if (t.j == rd.rc[r]) b = r;
+                }
+                if (a >= 0 && b >= 0 && ((tid >> a) & 1) && ((tid >> b) & 1)) acc += t.coef;
+            }
+            s_qreg[d][tid] = acc;
+        }
+    }
+
+    if (tid == 0) {
+        mbar_init(&mbar[0], kThreads / 32);
+        mbar_init(&mbar[1], kThreads / 32);
+        s_r[0] = pdep_bits(blockIdx.x, g.free_mask);
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    uint64_t tidx = blockIdx.x;
+    if (tidx >= g.ntiles) return;
+    fload(g, state, bufs[0], s_r[0], &mbar[0], tid);
+
+    for (uint32_t k = 0;; k++, tidx += gridDim.x) {
+        if (tidx >= g.ntiles) break;
+        const int s = int(k & 1);
+        const uint64_t nxt = tidx + gridDim.x;
+        if (!mbar_wait_bounded(&mbar[s], (k >> 1) & 1)) {
+            if (tid == 0) report(status, kErrTimeout, 3, tidx);
+            bulk_wait0();
+            return;
+        }
+        bulk_wait_read0();  // this thread's stores of the previous tile (other stage) have read it
+        if (tid == 0 && nxt < g.ntiles) s_r[s ^ 1] = pdep_bits(nxt, g.free_mask);
+        E *buf = bufs[s];
+        const uint64_t r = s_r[s];
+
+        // per-tile parameters: warp 0 / 1 the fused windows, warp 2 the gate selectors
+        if (warp < 2 && offw[warp])
+            window_tile_params(blob, *reinterpret_cast<const DiagDev *>(blob + offw[warp]), r, T, lane, s_da[warp],
+                               &s_K[warp]);
+        if (warp == 2 && lane < int(ngates)) {
+            const FastGateDev &gg = gates[lane];
+            const int beta = int(gg.beta) ^ par64(gg.alpha_out & r);
+            // with beta = 1 the odd partner sits at bit value 0: swap the roles
+            const int p[8] = {0, 1, 2, 3, 4, 5, 6, 7};
+            const int q[8] = {6, 7, 4, 5, 2, 3, 0, 1};
+#pragma unroll
+            for (int i = 0; i < 8; i++) s_u[lane][i] = RT(gg.u[beta ? q[i] : p[i]]);
+        }
+        __syncthreads();
+        if (nxt < g.ntiles) fload(g, state, bufs[s ^ 1], s_r[s ^ 1], &mbar[s ^ 1], tid);
+
+        for (uint32_t rnd = 0; rnd < nrounds; rnd++) {
+            const RoundDev rd = f.rounds[rnd];
+            const uint32_t ebase = uint32_t(lane) | (uint32_t(warp & 1) << rd.oc[0]) |
+                                   (uint32_t((warp >> 1) & 1) << rd.oc[1]) | (uint32_t((warp >> 2) & 1) << rd.oc[2]);
+            uint32_t off[NR];
+#pragma unroll
+            for (int j = 0; j < NR; j++) {
+                uint32_t o = 0;
+#pragma unroll
+                for (int rr = 0; rr < R; rr++)
+                    if ((j >> rr) & 1) o |= 1u << rd.rc[rr];
+                off[j] = ebase | o;
+            }
+            E x[NR];
+#pragma unroll
+            for (int j = 0; j < NR; j++) x[j] = buf[off[j]];
+
+#pragma unroll
+            for (int d = 0; d < 2; d++) {
+                if (!offw[d]) continue;
+                if (d == 0 && rnd != 0) continue;
+                if (d == 1) break;  // the epilogue runs after the gates
+                int64_t A = s_K[d] + qfix[d];
+#pragma unroll
+                for (int kk = 0; kk < 5; kk++)
+                    if ((lane >> kk) & 1) A += s_da[d][kk];
+#pragma unroll
+                for (int i = 0; i < 3; i++)
+                    if ((warp >> i) & 1) A += s_da[d][rd.oc[i]];
+                int64_t w[R];
+#pragma unroll
+                for (int rr = 0; rr < R; rr++) w[rr] = s_da[d][rd.rc[rr]] + rho[d][rr];
+                apply_window<E, R>(x, s_exp, A, w, s_qreg[d]);
+            }
+
+            for (uint32_t gi = 0; gi < ngates; gi++) {
+                const uint32_t gc = s_gc[gi];
+                if ((gc >> 8) != rnd) continue;
+                const uint32_t c = gc & 255u;
+                const RT m00r = s_u[gi][0], m00i = s_u[gi][1], m01r = s_u[gi][2], m01i = s_u[gi][3];
+                const RT m10r = s_u[gi][4], m10i = s_u[gi][5], m11r = s_u[gi][6], m11i = s_u[gi][7];
+                if (c < 5) {
+                    const bool hi = (lane >> c) & 1;
+                    const RT ar = hi ? m11r : m00r, ai = hi ? m11i : m00i;  // own amplitude
+                    const RT br = hi ? m10r : m01r, bi = hi ? m10i : m01i;  // partner's
+#pragma unroll
+                    for (int j = 0; j < NR; j++) {
+                        const E p = shfl_xor_e(x[j], 1 << c);
+                        x[j] = cmad2(ar, ai, x[j], br, bi, p);
+                    }
+                } else {
+#pragma unroll
+                    for (int rr = 0; rr < R; rr++) {
+                        if (rd.rc[rr] != c) continue;
+#pragma unroll
+                        for (int j = 0; j < NR; j++) {
+                            if ((j >> rr) & 1) continue;
+                            const E lo = x[j], hiv = x[j | (1 << rr)];
+                            x[j] = cmad2(m00r, m00i, lo, m01r, m01i, hiv);
+                            x[j | (1 << rr)] = cmad2(m10r, m10i, lo, m11r, m11i, hiv);
+                        }
+                    }
+                }
+            }
+
+            if (offw[1] && rnd == nrounds - 1) {
+                int64_t A = s_K[1] + qfix[1];
+#pragma unroll
+                for (int kk = 0; kk < 5; kk++)
+                    if ((lane >> kk) & 1) A += s_da[1][kk];
+#pragma unroll
+                for (int i = 0; i < 3; i++)
+                    if ((warp >> i) & 1) A += s_da[1][rd.oc[i]];
+                int64_t w[R];
+#pragma unroll
+                for (int rr = 0; rr < R; rr++) w[rr] = s_da[1][rd.rc[rr]] + rho[1][rr];
+                apply_window<E, R>(x, s_exp, A, w, s_qreg[1]);
+            }
+#pragma unroll
+            for (int j = 0; j < NR; j++) buf[off[j]] = x[j];
+            __syncthreads();
+        }
+
+        fence_proxy_async();
+        __syncthreads();
+        fstore(g, state, buf, r, tid);
+    }
+    bulk_wait0();
+}
+
+}  // namespace
+
+int fast_tile_bits(int elem_bytes) { return 8 + (elem_bytes == 8 ? FastCfg<float2>::R : FastCfg<double2>::R); }
+
+int fast_reg_bits(int elem_bytes) { return elem_bytes == 8 ? FastCfg<float2>::R : FastCfg<double2>::R; }
+
+cudaError_t run_fast_tile(const uint8_t *dblob, uint64_t foff, uint64_t toff, uint64_t ntiles, int elem_bytes,
+                          void *state, DevStatus *status, int sms, cudaStream_t st)
+{
+    const int T = fast_tile_bits(elem_bytes);
+    const size_t smem = 2 * (size_t(elem_bytes) << T) + size_t(elem_bytes) * (1u << kExpTableBits);
+    int per_sm = 1;
+    cudaError_t e;
+    if (elem_bytes == 8) {
+        e = cudaFuncSetAttribute(fast_tile_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        if (e != cudaSuccess) return e;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fast_tile_kernel<float2>, kThreads, smem);
+    } else {
+        e = cudaFuncSetAttribute(fast_tile_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        if (e != cudaSuccess) return e;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fast_tile_kernel<double2>, kThreads, smem);
+    }
+    if (per_sm < 1) per_sm = 1;
+    const unsigned grid = unsigned(std::max<uint64_t>(1, std::min<uint64_t>(ntiles, uint64_t(sms) * uint64_t(per_sm))));
+    if (elem_bytes == 8)
+        fast_tile_kernel<float2><<<grid, kThreads, smem, st>>>(dblob, foff, toff, static_cast<float2 *>(state), status);
+    else
+        fast_tile_kernel<double2><<<grid, kThreads, smem, st>>>(dblob, foff, toff, static_cast<double2 *>(state), status);
+    return cudaGetLastError();
+}
+
+}  // namespace zxh
+
+// ---------------------------------------------------------------------------
+// Strided high-qubit pass: no shared-memory staging; a thread's registers span R
+// arbitrary (high) bits, so one pass applies up to R gates on any bits with each
+// amplitude read and written once.
+
+namespace zxh {
+
+namespace {
+
+// Row-pass shapes: VT is what one lane loads per row (V amplitudes), R the register
+// bits. Variant 0 / 1 of each type are picked by the planner's row_wide knob.
+template <typename E, int W>
+struct RowCfg;
+template <>
+struct RowCfg<float2, 0> {
+    using VT = float4;
+    static constexpr int V = 2, R = 4;  // 16 rows of 512 bytes per warp
+};
+template <>
+struct RowCfg<float2, 1> {
+    using VT = float2;
+    static constexpr int V = 1, R = 5;  // 32 rows of 256 bytes per warp
+};
+template <>
+struct RowCfg<double2, 0> {
+    using VT = double2;
+    static constexpr int V = 1, R = 3;  // 8 rows of 512 bytes per warp
+};
+template <>
+struct RowCfg<double2, 1> {
+    using VT = double2;
+    static constexpr int V = 1, R = 4;
+};
+
+template <typename E, int W>
+__global__ void __launch_bounds__(kThreads) row_pass_kernel(const uint8_t *__restrict__ blob, uint64_t poff,
+                                                            uint64_t toff, E *__restrict__ state)
+{
+    using VT = typename RowCfg<E, W>::VT;
+    using RT = typename ET<E>::R;
+    constexpr int V = RowCfg<E, W>::V;
+    constexpr int LV = (V == 2) ? 1 : 0;
+    constexpr int F = 5 + LV;
+    constexpr int R = RowCfg<E, W>::R;
+    constexpr int NR = 1 << R;
+    constexpr int WARPS = kThreads / 32;
+
+    const RowPassDev p = *reinterpret_cast<const RowPassDev *>(blob + poff);
+    const FastGateDev *gates = reinterpret_cast<const FastGateDev *>(blob + p.off_gates);
+    const uint64_t offw[2] = {p.off_pre, p.off_post};
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t ngates = p.ngates;
+    const uint32_t Rn = p.R;  // register bits in use (<= R)
+
+    __shared__ E s_exp[1 << kExpTableBits];
+    __shared__ RT s_u[kFastMaxGates][2][8];
+    __shared__ uint32_t s_gc[kFastMaxGates];
+    __shared__ int64_t s_qreg[2][NR];
+    __shared__ uint64_t s_off[NR];
+
+    if (offw[0] || offw[1]) {
+        const E *tab = reinterpret_cast<const E *>(blob + toff);
+        for (int i = tid; i < (1 << kExpTableBits); i += kThreads) s_exp[i] = tab[i];
+    }
+    if (tid < int(ngates)) {
+        const FastGateDev &gg = gates[tid];
+        const int sw[8] = {6, 7, 4, 5, 2, 3, 0, 1};  // odd partner at bit value 0: swap roles
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            s_u[tid][0][i] = RT(gg.u[i]);
+            s_u[tid][1][i] = RT(gg.u[sw[i]]);
+        }
+        s_gc[tid] = gg.coord;
+    }
+    if (tid < NR) {
+        uint64_t o = 0;
+        for (uint32_t r = 0; r < Rn; r++)
+            if ((tid >> r) & 1) o |= 1ULL << p.rb[r];
+        s_off[tid] = (uint32_t(tid) >> Rn) ? ~0ULL : o;  // rows beyond 2^Rn are unused
+    }
+
+    // tile-independent parts of the windows: tile coordinates are [0, F) = vector and
+    // lane bits, then F + r = register bit r
+    int64_t qfix[2][V], rho[2][R][V];
+#pragma unroll
+    for (int d = 0; d < 2; d++) {
+#pragma unroll
+        for (int v = 0; v < V; v++) {
+            qfix[d][v] = 0;
+#pragma unroll
+            for (int r = 0; r < R; r++) rho[d][r][v] = 0;
+        }
+        if (!offw[d]) continue;
+        const DiagDev &dd = *reinterpret_cast<const DiagDev *>(blob + offw[d]);
+        const QuadTerm *iq = reinterpret_cast<const QuadTerm *>(blob + dd.off_in_quad);
+        for (uint32_t q = 0; q < dd.n_in_quad; q++) {
+            const QuadTerm t = iq[q];  // t.i < t.j
+#pragma unroll
+            for (int v = 0; v < V; v++) {
+                const uint32_t e = uint32_t(v) | (uint32_t(lane) << LV);
+                if (int(t.i) >= F || !((e >> t.i) & 1)) continue;
+                if (int(t.j) < F) {
+                    if ((e >> t.j) & 1) qfix[d][v] += t.coef;
+                } else {
+#pragma unroll
+                    for (int r = 0; r < R; r++)
+                        if (int(t.j) - F == r) rho[d][r][v] += t.coef;
+                }
+            }
+        }
+        if (tid < NR) {
+            int64_t acc = 0;
+            for (uint32_t q = 0; q < dd.n_in_quad; q++) {
+                const QuadTerm t = iq[q];
+                if (int(t.i) >= F && ((tid >> (t.i - F)) & 1) && ((tid >> (t.j - F)) & 1)) acc += t.coef;
+            }
+            s_qreg[d][tid] = acc;
+        }
+    }
+    __syncthreads();
+
+    const int nrows = 1 << Rn;
+    const uint64_t stride = uint64_t(gridDim.x) * WARPS;
+    for (uint64_t item = uint64_t(blockIdx.x) * WARPS + uint64_t(warp); item < p.nitems; item += stride) {
+        // item bits go to every real bit outside [0, F) and the register bits
+        uint64_t base = item << F;
+        for (uint32_t r = 0; r < Rn; r++) {
+            const uint32_t b = p.rb[r];
+            base = ((base >> b) << (b + 1)) | (base & ((1ULL << b) - 1ULL));
+        }
+        E *rowp = state + base + (uint64_t(lane) << LV);
+        VT x[NR];
+#pragma unroll
+        for (int j = 0; j < NR; j++)
+            if (j < nrows) x[j] = __ldcs(reinterpret_cast<const VT *>(rowp + s_off[j]));
+
+        // per-item selector orientation of every gate
+        int ob = 0;
+        if (lane < int(ngates)) {
+            const FastGateDev &gg = gates[lane];
+            ob = int(gg.beta) ^ par64(gg.alpha_out & base);
+        }
+        const uint32_t omask = __ballot_sync(0xffffffffu, ob);
+
+#pragma unroll
+        for (int d = 0; d < 2; d++) {
+            if (!offw[d]) continue;
+            if (d == 1) {
+                // gates run between the prologue and the epilogue
+                for (uint32_t gi = 0; gi < ngates; gi++) {
+                    const uint32_t c = s_gc[gi];
+                    const RT *u = s_u[gi][(omask >> gi) & 1];
+                    const RT m00r = u[0], m00i = u[1], m01r = u[2], m01i = u[3];
+                    const RT m10r = u[4], m10i = u[5], m11r = u[6], m11i = u[7];
+                    if (int(c) < LV) {
+#pragma unroll
+                        for (int j = 0; j < NR; j++) {
+                            const E lo = vget(x[j], 0), hi = vget(x[j], V - 1);
+                            vset(x[j], 0, cmad2(m00r, m00i, lo, m01r, m01i, hi));
+                            vset(x[j], V - 1, cmad2(m10r, m10i, lo, m11r, m11i, hi));
+                        }
+                    } else if (int(c) < F) {
+                        const int lb = int(c) - LV;
+                        const bool hb = (lane >> lb) & 1;
+                        const RT ar = hb ? m11r : m00r, ai = hb ? m11i : m00i;
+                        const RT br = hb ? m10r : m01r, bi = hb ? m10i : m01i;
+#pragma unroll
+                        for (int j = 0; j < NR; j++)
+#pragma unroll
+                            for (int v = 0; v < V; v++) {
+                                const E mine = vget(x[j], v);
+                                const E pt = shfl_xor_e(mine, 1 << lb);
+                                vset(x[j], v, cmad2(ar, ai, mine, br, bi, pt));
+                            }
+                    } else {
+#pragma unroll
+                        for (int rr = 0; rr < R; rr++) {
+                            if (int(c) - F != rr) continue;
+#pragma unroll
+                            for (int j = 0; j < NR; j++) {
+                                if ((j >> rr) & 1) continue;
+#pragma unroll
+                                for (int v = 0; v < V; v++) {
+                                    const E lo = vget(x[j], v), hi = vget(x[j | (1 << rr)], v);
+                                    vset(x[j], v, cmad2(m00r, m00i, lo, m01r, m01i, hi));
+                                    vset(x[j | (1 << rr)], v, cmad2(m10r, m10i, lo, m11r, m11i, hi));
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+            const DiagDev &dd = *reinterpret_cast<const DiagDev *>(blob + offw[d]);
+            const int T = F + int(Rn);
+            int64_t da = 0, K = 0;
+            {
+                const QuadTerm *cr = reinterpret_cast<const QuadTerm *>(blob + dd.off_cross);
+                const LinTerm *ol = reinterpret_cast<const LinTerm *>(blob + dd.off_out_lin);
+                const QuadTerm *oq = reinterpret_cast<const QuadTerm *>(blob + dd.off_out_quad);
+                const uint32_t *kidx = reinterpret_cast<const uint32_t *>(blob + dd.off_kidx);
+                if (lane < T) {
+                    da = dd.lin_in[lane];
+                    for (uint32_t q = kidx[lane]; q < kidx[lane + 1]; q++) {
+                        const QuadTerm t = cr[q];
+                        if ((base >> t.j) & 1) da += t.coef;
+                    }
+                }
+                for (uint32_t q = uint32_t(lane); q < dd.n_out_lin; q += 32)
+                    if ((base >> ol[q].bit) & 1) K += ol[q].coef;
+                for (uint32_t q = uint32_t(lane); q < dd.n_out_quad; q += 32) {
+                    const QuadTerm t = oq[q];
+                    if (((base >> t.i) & 1) && ((base >> t.j) & 1)) K += t.coef;
+                }
+                K = warp_sum_i64(K) + dd.c0;
+            }
+            int64_t acc[V], w[R][V];
+#pragma unroll
+            for (int v = 0; v < V; v++) acc[v] = K + qfix[d][v];
+#pragma unroll
+            for (int k = 0; k < F; k++) {
+                const int64_t dk = __shfl_sync(0xffffffffu, da, k);
+#pragma unroll
+                for (int v = 0; v < V; v++)
+                    if (((uint32_t(v) | (uint32_t(lane) << LV)) >> k) & 1) acc[v] += dk;
+            }
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                const int64_t dk = __shfl_sync(0xffffffffu, da, (F + r) & 31);
+#pragma unroll
+                for (int v = 0; v < V; v++) w[r][v] = (r < int(Rn)) ? dk + rho[d][r][v] : 0;
+            }
+#pragma unroll
+            for (int jj = 0; jj < NR; jj++) {
+                const int gj = jj ^ (jj >> 1);
+                if (jj > 0) {
+                    int fb = 0;
+                    while (!((jj >> fb) & 1)) fb++;
+#pragma unroll
+                    for (int v = 0; v < V; v++) acc[v] += ((gj >> fb) & 1) ? w[fb][v] : -w[fb][v];
+                }
+                if (gj >= nrows) continue;
+                const int64_t qr = s_qreg[d][gj];
+#pragma unroll
+                for (int v = 0; v < V; v++) vset(x[gj], v, cmul(vget(x[gj], v), phase_factor(s_exp, acc[v] + qr)));
+            }
+        }
+        if (!offw[1]) {
+            // no epilogue: the gates have not run yet
+            for (uint32_t gi = 0; gi < ngates; gi++) {
+                const uint32_t c = s_gc[gi];
+                const RT *u = s_u[gi][(omask >> gi) & 1];
+                const RT m00r = u[0], m00i = u[1], m01r = u[2], m01i = u[3];
+                const RT m10r = u[4], m10i = u[5], m11r = u[6], m11i = u[7];
+                if (int(c) < LV) {
+#pragma unroll
+                    for (int j = 0; j < NR; j++) {
+                        const E lo = vget(x[j], 0), hi = vget(x[j], V - 1);
+                        vset(x[j], 0, cmad2(m00r, m00i, lo, m01r, m01i, hi));
+                        vset(x[j], V - 1, cmad2(m10r, m10i, lo, m11r, m11i, hi));
+                    }
+                } else if (int(c) < F) {
+                    const int lb = int(c) - LV;
+                    const bool hb = (lane >> lb) & 1;
+                    const RT ar = hb ? m11r : m00r, ai = hb ? m11i : m00i;
+                    const RT br = hb ? m10r : m01r, bi = hb ? m10i : m01i;
+#pragma unroll
+                    for (int j = 0; j < NR; j++)
+#pragma unroll
+                        for (int v = 0; v < V; v++) {
+                            const E mine = vget(x[j], v);
+                            const E pt = shfl_xor_e(mine, 1 << lb);
+                            vset(x[j], v, cmad2(ar, ai, mine, br, bi, pt));
+                        }
+                } else {
+#pragma unroll
+                    for (int rr = 0; rr < R; rr++) {
+                        if (int(c) - F != rr) continue;
+#pragma unroll
+                        for (int j = 0; j < NR; j++) {
+                            if ((j >> rr) & 1) continue;
+#pragma unroll
+                            for (int v = 0; v < V; v++) {
+                                const E lo = vget(x[j], v), hi = vget(x[j | (1 << rr)], v);
+                                vset(x[j], v, cmad2(m00r, m00i, lo, m01r, m01i, hi));
+                                vset(x[j | (1 << rr)], v, cmad2(m10r, m10i, lo, m11r, m11i, hi));
+                            }
+                        }
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < NR; j++)
+            if (j < nrows) __stcs(reinterpret_cast<VT *>(rowp + s_off[j]), x[j]);
+    }
+}
+
+}  // namespace
+
+int row_reg_bits(int elem_bytes, int wide)
+{
+    if (elem_bytes == 8) return wide ? RowCfg<float2, 1>::R : RowCfg<float2, 0>::R;
+    return wide ? RowCfg<double2, 1>::R : RowCfg<double2, 0>::R;
+}
+
+int row_fixed_bits(int elem_bytes, int wide)
+{
+    const int v = elem_bytes == 8 ? (wide ? RowCfg<float2, 1>::V : RowCfg<float2, 0>::V)
+                                  : (wide ? RowCfg<double2, 1>::V : RowCfg<double2, 0>::V);
+    return 5 + (v == 2 ? 1 : 0);
+}
+
+template <typename E, int W>
+static cudaError_t launch_row(const uint8_t *dblob, uint64_t poff, uint64_t toff, uint64_t nitems, void *state,
+                              int sms, cudaStream_t st)
+{
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, row_pass_kernel<E, W>, kThreads, 0);
+    if (per_sm < 1) per_sm = 1;
+    const uint64_t ctas = (nitems + kThreads / 32 - 1) / (kThreads / 32);
+    const unsigned grid = unsigned(std::max<uint64_t>(1, std::min<uint64_t>(ctas, uint64_t(sms) * uint64_t(per_sm))));
+    row_pass_kernel<E, W><<<grid, kThreads, 0, st>>>(dblob, poff, toff, static_cast<E *>(state));
+    return cudaGetLastError();
+}
+
+cudaError_t run_row_pass(const uint8_t *dblob, uint64_t poff, uint64_t toff, uint64_t nitems, int elem_bytes,
+                         int wide, void *state, int sms, cudaStream_t st)
+{
+    if (elem_bytes == 8)
+        return wide ? launch_row<float2, 1>(dblob, poff, toff, nitems, state, sms, st)
+                    : launch_row<float2, 0>(dblob, poff, toff, nitems, state, sms, st);
+    return wide ? launch_row<double2, 1>(dblob, poff, toff, nitems, state, sms, st)
+                : launch_row<double2, 0>(dblob, poff, toff, nitems, state, sms, st);
+}
+
+}  // namespace zxh
