@@ -164,7 +164,8 @@ int zxh_last_stats(const zxh_sim *sim, uint64_t *kernels, uint64_t *passes, doub
 
 /* Pass-planner tuning (used by the autotuner): tile_bits_c64, tile_bits_c128,
  * contig_bits, max_gates (generic tile pass), fast_gates (gates per fast U3
- * pass), fast_fuse_quad, fast_contig_c64, fast_contig_c128. Takes effect at the
+ * pass), fast_fuse_quad, fast_contig_c64, fast_contig_c128, row_wide_c64,
+ * row_wide_c128 (shape of the strided high-qubit pass). Takes effect at the
  * next zxh_execute / zxh_apply. No counterpart in the reference. */
 int zxh_set_param(zxh_sim *sim, const char *name, int value);
 

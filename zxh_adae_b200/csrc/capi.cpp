@@ -584,7 +584,8 @@ int zxh_set_param(zxh_sim *s, const char *name, int value)
         {"fast_fuse_quad", &s->pp.fast_fuse_quad, 0, 64},
         {"fast_contig_c64", &s->pp.fast_contig_c64, 1, 11},
         {"fast_contig_c128", &s->pp.fast_contig_c128, 0, 10},
-        {"row_wide", &s->pp.row_wide, 0, 1},
+        {"row_wide_c64", &s->pp.row_wide_c64, 0, 1},
+        {"row_wide_c128", &s->pp.row_wide_c128, 0, 1},
     };
     for (const Entry &e : table)
         if (std::strcmp(e.key, name) == 0) {

@@ -71,6 +71,9 @@ __device__ __forceinline__ E cmul(E a, E b)
     return o;
 }
 
+// Trailing zeros of a compile-time constant (index arithmetic in unrolled loops).
+__host__ __device__ constexpr int ctz_const(int x) { return (x & 1) ? 0 : 1 + ctz_const(x >> 1); }
+
 __device__ __forceinline__ int par64(uint64_t x) { return __popcll(x) & 1; }
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }

@@ -178,8 +178,7 @@ __global__ void __launch_bounds__(kThreads) diag_kernel(const uint8_t *__restric
         for (int it = 0; it < ROWS; it++) {
             const uint32_t gi = uint32_t(it ^ (it >> 1));
             if (it > 0) {
-                int fb = 0;
-                while (!((it >> fb) & 1)) fb++;
+                const int fb = ctz_const(it);
                 const bool up = (gi >> fb) & 1;
 #pragma unroll
                 for (int v = 0; v < V; v++) acc[v] += up ? w[fb][v] : -w[fb][v];

@@ -836,7 +836,7 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
             std::vector<const U3Op *> gs;
             for (const U3Op &u : op.u3) gs.push_back(&u);
             std::sort(gs.begin(), gs.end(), [](const U3Op *a, const U3Op *b) { return a->delta < b->delta; });
-            const int G = std::max(pp.fast_gates, row_fixed_bits(elem_bytes, pp.row_wide));
+            const int G = std::max(pp.fast_gates, row_fixed_bits(elem_bytes, (elem_bytes == 8 ? pp.row_wide_c64 : pp.row_wide_c128)));
             std::vector<std::pair<std::vector<int>, std::vector<const U3Op *>>> groups;
             size_t k = 0;
             {
@@ -848,7 +848,7 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
             for (size_t gidx = 0; gidx < groups.size(); gidx++)
                 last_tile_pass = emit_fast(mm, tfast, groups[gidx].first, groups[gidx].second);
             // the rest: strided register passes over the high bits
-            const int frow = row_fixed_bits(elem_bytes, pp.row_wide), rrow = row_reg_bits(elem_bytes, pp.row_wide);
+            const int frow = row_fixed_bits(elem_bytes, (elem_bytes == 8 ? pp.row_wide_c64 : pp.row_wide_c128)), rrow = row_reg_bits(elem_bytes, (elem_bytes == 8 ? pp.row_wide_c64 : pp.row_wide_c128));
             while (k < gs.size()) {
                 std::vector<const U3Op *> grp;
                 while (k < gs.size() && int(grp.size()) < rrow) grp.push_back(gs[k++]);
@@ -873,7 +873,7 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
                 for (size_t r = 0; r < rb.size(); r++) ps.row.rb[r] = uint8_t(rb[r]);
                 ps.row.tile_mask = ps.geom.tile_mask;
                 ps.row.nitems = 1ULL << (mm - frow - int(rb.size()));
-                ps.wide = pp.row_wide;
+                ps.wide = (elem_bytes == 8 ? pp.row_wide_c64 : pp.row_wide_c128);
                 for (size_t r = 0; r < grp.size(); r++) {
                     FastGateDev fg;
                     std::memset(&fg, 0, sizeof(fg));

@@ -27,11 +27,12 @@ struct PlanParams {
     int tile_bits_c128 = 11;    // same for complex128
     int contig_bits = 6;        // contiguous low bits of a tile that also spans high bits
     int max_gates = 12;         // pair ops per generic tile pass
-    int fast_gates = 8;         // fused gates per fast U3 pass (bounded by the FMA budget per byte)
+    int fast_gates = 6;         // fused gates per TMA low-qubit pass (bounded by the FMA budget per byte)
     int fast_fuse_quad = 32;    // largest in-tile quadratic term count of a window fused into a fast pass
     int fast_contig_c64 = 4;    // contiguous low bits of a fast tile that also spans high bits (complex64)
     int fast_contig_c128 = 3;   // same for complex128
-    int row_wide = 0;           // strided high-qubit pass shape: 0 = 16-byte lanes, 1 = more register bits
+    int row_wide_c64 = 0;       // strided high-qubit pass shape, complex64: 0 = 16-byte lanes x 16 rows, 1 = 8-byte x 32
+    int row_wide_c128 = 1;      // complex128: 0 = 8 rows, 1 = 16 rows
     int max_steps = 16;
     int diag_tile_bits = 12;    // tile size of a standalone diagonal pass
     int product_table_bits = 12;

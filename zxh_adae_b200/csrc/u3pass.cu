@@ -126,8 +126,7 @@ __device__ __forceinline__ void apply_window(E (&x)[1 << R], const E *s_exp, int
     for (int jj = 0; jj < (1 << R); jj++) {
         const int gj = jj ^ (jj >> 1);
         if (jj > 0) {
-            int fb = 0;
-            while (!((jj >> fb) & 1)) fb++;
+            const int fb = ctz_const(jj);
             acc += ((gj >> fb) & 1) ? w[fb] : -w[fb];
         }
         x[gj] = cmul(x[gj], phase_factor(s_exp, acc + qreg[gj]));
@@ -157,8 +156,69 @@ __device__ __forceinline__ E cmad2(RT ar, RT ai, E x, RT br, RT bi, E y)
     return o;
 }
 
+// 2x2 gate on register bit RR of every row pair: compile-time positions keep the
+// amplitudes in registers.
+template <int RR, int NR, int V, typename VT, typename RT>
+__device__ __forceinline__ void reg_gate(VT (&x)[NR], const RT *u)
+{
+    using E = decltype(vget(x[0], 0));
+    const RT m00r = u[0], m00i = u[1], m01r = u[2], m01i = u[3];
+    const RT m10r = u[4], m10i = u[5], m11r = u[6], m11i = u[7];
+#pragma unroll
+    for (int j = 0; j < NR; j++) {
+        if ((j >> RR) & 1) continue;
+#pragma unroll
+        for (int v = 0; v < V; v++) {
+            const E lo = vget(x[j], v), hi = vget(x[j | (1 << RR)], v);
+            vset(x[j], v, cmad2(m00r, m00i, lo, m01r, m01i, hi));
+            vset(x[j | (1 << RR)], v, cmad2(m10r, m10i, lo, m11r, m11i, hi));
+        }
+    }
+}
+
+// One gate on tile coordinate c of a row-pass thread's amplitudes: c < LV is the
+// vector bit, c < F a lane bit (partner by shfl.xor), otherwise register bit c - F.
+template <int R, int V, int LV, int F, typename VT, typename RT>
+__device__ __forceinline__ void row_gate(VT (&x)[1 << R], uint32_t c, const RT *u, int lane)
+{
+    using E = decltype(vget(x[0], 0));
+    constexpr int NR = 1 << R;
+    if (int(c) < LV) {
+        const RT m00r = u[0], m00i = u[1], m01r = u[2], m01i = u[3];
+        const RT m10r = u[4], m10i = u[5], m11r = u[6], m11i = u[7];
+#pragma unroll
+        for (int j = 0; j < NR; j++) {
+            const E lo = vget(x[j], 0), hi = vget(x[j], V - 1);
+            vset(x[j], 0, cmad2(m00r, m00i, lo, m01r, m01i, hi));
+            vset(x[j], V - 1, cmad2(m10r, m10i, lo, m11r, m11i, hi));
+        }
+    } else if (int(c) < F) {
+        const int lb = int(c) - LV;
+        const bool hb = (lane >> lb) & 1;
+        const RT ar = hb ? u[6] : u[0], ai = hb ? u[7] : u[1];
+        const RT br = hb ? u[4] : u[2], bi = hb ? u[5] : u[3];
+#pragma unroll
+        for (int j = 0; j < NR; j++)
+#pragma unroll
+            for (int v = 0; v < V; v++) {
+                const E mine = vget(x[j], v);
+                const E pt = shfl_xor_e(mine, 1 << lb);
+                vset(x[j], v, cmad2(ar, ai, mine, br, bi, pt));
+            }
+    } else {
+        switch (int(c) - F) {
+        case 0: reg_gate<0, NR, V>(x, u); break;
+        case 1: if constexpr (R > 1) reg_gate<(R > 1 ? 1 : 0), NR, V>(x, u); break;
+        case 2: if constexpr (R > 2) reg_gate<(R > 2 ? 2 : 0), NR, V>(x, u); break;
+        case 3: if constexpr (R > 3) reg_gate<(R > 3 ? 3 : 0), NR, V>(x, u); break;
+        case 4: if constexpr (R > 4) reg_gate<(R > 4 ? 4 : 0), NR, V>(x, u); break;
+        default: break;
+        }
+    }
+}
+
 template <typename E>
-__global__ void __launch_bounds__(kThreads) fast_tile_kernel(const uint8_t *__restrict__ blob, uint64_t foff,
+__global__ void __launch_bounds__(kThreads, 2) fast_tile_kernel(const uint8_t *__restrict__ blob, uint64_t foff,
                                                              uint64_t toff, E *__restrict__ state, DevStatus *status)
 {
     using RT = typename ET<E>::R;
@@ -181,62 +241,34 @@ __global__ void __launch_bounds__(kThreads) fast_tile_kernel(const uint8_t *__re
 
     const int tid = int(threadIdx.x), lane = tid & 31, warp = tid >> 5;
     const uint32_t ngates = f.ngates, nrounds = f.nrounds;
-    const uint64_t offw[2] = {f.off_pre, f.off_post};
+    const uint64_t offw0 = f.off_pre, offw1 = f.off_post;
     const FastGateDev *gates = reinterpret_cast<const FastGateDev *>(blob + f.off_gates);
 
-    if (offw[0] || offw[1]) {
+    if (offw0 || offw1) {
         const E *tab = reinterpret_cast<const E *>(blob + toff);
         for (int i = tid; i < (1 << kExpTableBits); i += kThreads) s_exp[i] = tab[i];
     }
     if (tid < int(ngates)) s_gc[tid] = gates[tid].coord | (gates[tid].round << 8);
 
-    // tile-independent parts of the fused windows for the round each one runs in
-    int64_t qfix[2] = {0, 0};
-    int64_t rho[2][R];
+    // register x register quadratic part of each window, for the round it runs in
 #pragma unroll
     for (int d = 0; d < 2; d++) {
-#pragma unroll
-        for (int r = 0; r < R; r++) rho[d][r] = 0;
-        if (!offw[d]) continue;
-        const DiagDev &dd = *reinterpret_cast<const DiagDev *>(blob + offw[d]);
+        const uint64_t ow = d ? offw1 : offw0;
+        if (!ow || tid >= NR) continue;
+        const DiagDev &dd = *reinterpret_cast<const DiagDev *>(blob + ow);
         const QuadTerm *iq = reinterpret_cast<const QuadTerm *>(blob + dd.off_in_quad);
         const RoundDev rd = f.rounds[d == 0 ? 0 : nrounds - 1];
-        // class of a coordinate: 0..R-1 = register index, -1 = fixed bit 0, -2 = fixed bit 1
-        auto cls = [&](uint32_t k) -> int {
-            if (k < 5) return ((lane >> k) & 1) ? -2 : -1;
-            for (int i = 0; i < 3; i++)
-                if (k == rd.oc[i]) return ((warp >> i) & 1) ? -2 : -1;
-            for (int r = 0; r < R; r++)
-                if (k == rd.rc[r]) return r;
-            return -1;
-        };
+        int64_t acc = 0;
         for (uint32_t q = 0; q < dd.n_in_quad; q++) {
             const QuadTerm t = iq[q];
-            const int a = cls(t.i), b = cls(t.j);
-            if (a == -2 && b == -2) qfix[d] += t.coef;
-            else if (a == -2 && b >= 0) {
-#pragma unroll
-                for (int r = 0; r < R; r++)
-                    if (r == b) rho[d][r] += t.coef;
-            } else if (b == -2 && a >= 0) {
-#pragma unroll
-                for (int r = 0; r < R; r++)
-                    if (r == a) rho[d][r] += t.coef;
+            int a = -1, b = -1;
+            for (int r = 0; r < R; r++) {
+                if (t.i == rd.rc[r]) a = r;
+                if (t.j == rd.rc[r]) b = r;
             }
+            if (a >= 0 && b >= 0 && ((tid >> a) & 1) && ((tid >> b) & 1)) acc += t.coef;
         }
-        if (tid < NR) {
-            int64_t acc = 0;
-            for (uint32_t q = 0; q < dd.n_in_quad; q++) {
-                const QuadTerm t = iq[q];
-                int a = -1, b = -1;
-                for (int r = 0; r < R; r++) {
-                    if (t.i == rd.rc[r]) a = r;
-                    if (t.j == rd.rc[r]) b = r;
-                }
-                if (a >= 0 && b >= 0 && ((tid >> a) & 1) && ((tid >> b) & 1)) acc += t.coef;
-            }
-            s_qreg[d][tid] = acc;
-        }
+        s_qreg[d][tid] = acc;
     }
 
     if (tid == 0) {
@@ -266,9 +298,10 @@ __global__ void __launch_bounds__(kThreads) fast_tile_kernel(const uint8_t *__re
         const uint64_t r = s_r[s];
 
         // per-tile parameters: warp 0 / 1 the fused windows, warp 2 the gate selectors
-        if (warp < 2 && offw[warp])
-            window_tile_params(blob, *reinterpret_cast<const DiagDev *>(blob + offw[warp]), r, T, lane, s_da[warp],
-                               &s_K[warp]);
+        if (warp == 0 && offw0)
+            window_tile_params(blob, *reinterpret_cast<const DiagDev *>(blob + offw0), r, T, lane, s_da[0], &s_K[0]);
+        if (warp == 1 && offw1)
+            window_tile_params(blob, *reinterpret_cast<const DiagDev *>(blob + offw1), r, T, lane, s_da[1], &s_K[1]);
         if (warp == 2 && lane < int(ngates)) {
             const FastGateDev &gg = gates[lane];
             const int beta = int(gg.beta) ^ par64(gg.alpha_out & r);
@@ -298,67 +331,68 @@ __global__ void __launch_bounds__(kThreads) fast_tile_kernel(const uint8_t *__re
 #pragma unroll
             for (int j = 0; j < NR; j++) x[j] = buf[off[j]];
 
-#pragma unroll
-            for (int d = 0; d < 2; d++) {
-                if (!offw[d]) continue;
-                if (d == 0 && rnd != 0) continue;
-                if (d == 1) break;  // the epilogue runs after the gates
-                int64_t A = s_K[d] + qfix[d];
+            // fused window d for this thread's amplitudes (fixed bits: lane and warp
+            // coordinates; register bits: rd.rc)
+            auto window = [&](int d, uint64_t ow) {
+                const DiagDev &dd = *reinterpret_cast<const DiagDev *>(blob + ow);
+                const QuadTerm *iq = reinterpret_cast<const QuadTerm *>(blob + dd.off_in_quad);
+                int64_t A = s_K[d];
+                int64_t w[R];
 #pragma unroll
                 for (int kk = 0; kk < 5; kk++)
                     if ((lane >> kk) & 1) A += s_da[d][kk];
 #pragma unroll
                 for (int i = 0; i < 3; i++)
                     if ((warp >> i) & 1) A += s_da[d][rd.oc[i]];
-                int64_t w[R];
 #pragma unroll
-                for (int rr = 0; rr < R; rr++) w[rr] = s_da[d][rd.rc[rr]] + rho[d][rr];
+                for (int rr = 0; rr < R; rr++) w[rr] = s_da[d][rd.rc[rr]];
+                // quadratic terms with a fixed bit set: fixed x fixed -> A, fixed x register -> w
+                for (uint32_t q = 0; q < dd.n_in_quad; q++) {
+                    const QuadTerm t = iq[q];
+                    int bi = -1, bj = -1, ri = -1, rj = -1;  // bit value of a fixed coordinate, or register slot
+                    if (t.i < 5) bi = (lane >> t.i) & 1;
+                    if (t.j < 5) bj = (lane >> t.j) & 1;
+#pragma unroll
+                    for (int i = 0; i < 3; i++) {
+                        if (t.i == rd.oc[i]) bi = (warp >> i) & 1;
+                        if (t.j == rd.oc[i]) bj = (warp >> i) & 1;
+                    }
+#pragma unroll
+                    for (int rr = 0; rr < R; rr++) {
+                        if (t.i == rd.rc[rr]) ri = rr;
+                        if (t.j == rd.rc[rr]) rj = rr;
+                    }
+                    if (bi == 1 && bj == 1) A += t.coef;
+                    else if (bi == 1 && rj >= 0) {
+#pragma unroll
+                        for (int rr = 0; rr < R; rr++)
+                            if (rr == rj) w[rr] += t.coef;
+                    } else if (bj == 1 && ri >= 0) {
+#pragma unroll
+                        for (int rr = 0; rr < R; rr++)
+                            if (rr == ri) w[rr] += t.coef;
+                    }
+                }
                 apply_window<E, R>(x, s_exp, A, w, s_qreg[d]);
-            }
+            };
+            if (offw0 && rnd == 0) window(0, offw0);
 
             for (uint32_t gi = 0; gi < ngates; gi++) {
                 const uint32_t gc = s_gc[gi];
                 if ((gc >> 8) != rnd) continue;
                 const uint32_t c = gc & 255u;
-                const RT m00r = s_u[gi][0], m00i = s_u[gi][1], m01r = s_u[gi][2], m01i = s_u[gi][3];
-                const RT m10r = s_u[gi][4], m10i = s_u[gi][5], m11r = s_u[gi][6], m11i = s_u[gi][7];
-                if (c < 5) {
-                    const bool hi = (lane >> c) & 1;
-                    const RT ar = hi ? m11r : m00r, ai = hi ? m11i : m00i;  // own amplitude
-                    const RT br = hi ? m10r : m01r, bi = hi ? m10i : m01i;  // partner's
+                // lane coordinates 0..4 stay; a register coordinate maps to its slot
+                uint32_t cc = c;
+                if (c >= 5) {
+                    cc = 5 + R;  // not in this round (cannot happen for a planned gate)
 #pragma unroll
-                    for (int j = 0; j < NR; j++) {
-                        const E p = shfl_xor_e(x[j], 1 << c);
-                        x[j] = cmad2(ar, ai, x[j], br, bi, p);
-                    }
-                } else {
-#pragma unroll
-                    for (int rr = 0; rr < R; rr++) {
-                        if (rd.rc[rr] != c) continue;
-#pragma unroll
-                        for (int j = 0; j < NR; j++) {
-                            if ((j >> rr) & 1) continue;
-                            const E lo = x[j], hiv = x[j | (1 << rr)];
-                            x[j] = cmad2(m00r, m00i, lo, m01r, m01i, hiv);
-                            x[j | (1 << rr)] = cmad2(m10r, m10i, lo, m11r, m11i, hiv);
-                        }
-                    }
+                    for (int rr = 0; rr < R; rr++)
+                        if (rd.rc[rr] == c) cc = 5 + uint32_t(rr);
                 }
+                row_gate<R, 1, 0, 5>(x, cc, &s_u[gi][0], lane);
             }
 
-            if (offw[1] && rnd == nrounds - 1) {
-                int64_t A = s_K[1] + qfix[1];
-#pragma unroll
-                for (int kk = 0; kk < 5; kk++)
-                    if ((lane >> kk) & 1) A += s_da[1][kk];
-#pragma unroll
-                for (int i = 0; i < 3; i++)
-                    if ((warp >> i) & 1) A += s_da[1][rd.oc[i]];
-                int64_t w[R];
-#pragma unroll
-                for (int rr = 0; rr < R; rr++) w[rr] = s_da[1][rd.rc[rr]] + rho[1][rr];
-                apply_window<E, R>(x, s_exp, A, w, s_qreg[1]);
-            }
+            if (offw1 && rnd == nrounds - 1) window(1, offw1);
 #pragma unroll
             for (int j = 0; j < NR; j++) buf[off[j]] = x[j];
             __syncthreads();
@@ -438,8 +472,9 @@ struct RowCfg<double2, 1> {
     static constexpr int V = 1, R = 4;
 };
 
+
 template <typename E, int W>
-__global__ void __launch_bounds__(kThreads) row_pass_kernel(const uint8_t *__restrict__ blob, uint64_t poff,
+__global__ void __launch_bounds__(kThreads, 2) row_pass_kernel(const uint8_t *__restrict__ blob, uint64_t poff,
                                                             uint64_t toff, E *__restrict__ state)
 {
     using VT = typename RowCfg<E, W>::VT;
@@ -451,12 +486,15 @@ __global__ void __launch_bounds__(kThreads) row_pass_kernel(const uint8_t *__res
     constexpr int NR = 1 << R;
     constexpr int WARPS = kThreads / 32;
 
-    const RowPassDev p = *reinterpret_cast<const RowPassDev *>(blob + poff);
+    const RowPassDev &p = *reinterpret_cast<const RowPassDev *>(blob + poff);
     const FastGateDev *gates = reinterpret_cast<const FastGateDev *>(blob + p.off_gates);
-    const uint64_t offw[2] = {p.off_pre, p.off_post};
+    const uint64_t offw0 = p.off_pre, offw1 = p.off_post;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t ngates = p.ngates;
-    const uint32_t Rn = p.R;  // register bits in use (<= R)
+    constexpr uint32_t Rn = R;  // the planner pads the register bits to exactly R
+    const uint64_t nitems = p.nitems;
+    __shared__ uint32_t s_rb[8];
+    if (tid < 8) s_rb[tid] = p.rb[tid];
 
     __shared__ E s_exp[1 << kExpTableBits];
     __shared__ RT s_u[kFastMaxGates][2][8];
@@ -464,81 +502,57 @@ __global__ void __launch_bounds__(kThreads) row_pass_kernel(const uint8_t *__res
     __shared__ int64_t s_qreg[2][NR];
     __shared__ uint64_t s_off[NR];
 
-    if (offw[0] || offw[1]) {
+    if (offw0 || offw1) {
         const E *tab = reinterpret_cast<const E *>(blob + toff);
         for (int i = tid; i < (1 << kExpTableBits); i += kThreads) s_exp[i] = tab[i];
     }
     if (tid < int(ngates)) {
         const FastGateDev &gg = gates[tid];
-        const int sw[8] = {6, 7, 4, 5, 2, 3, 0, 1};  // odd partner at bit value 0: swap roles
 #pragma unroll
         for (int i = 0; i < 8; i++) {
             s_u[tid][0][i] = RT(gg.u[i]);
-            s_u[tid][1][i] = RT(gg.u[sw[i]]);
+            s_u[tid][1][i] = RT(gg.u[i ^ 6]);  // odd partner at bit value 0: [[u11,u10],[u01,u00]]
         }
         s_gc[tid] = gg.coord;
     }
     if (tid < NR) {
         uint64_t o = 0;
         for (uint32_t r = 0; r < Rn; r++)
-            if ((tid >> r) & 1) o |= 1ULL << p.rb[r];
-        s_off[tid] = (uint32_t(tid) >> Rn) ? ~0ULL : o;  // rows beyond 2^Rn are unused
+            if ((tid >> r) & 1) o |= 1ULL << p.rb[r];  // read once per CTA
+        s_off[tid] = o;
     }
 
     // tile-independent parts of the windows: tile coordinates are [0, F) = vector and
     // lane bits, then F + r = register bit r
-    int64_t qfix[2][V], rho[2][R][V];
+    // row-only quadratic part of each window (reg x reg coordinates): per CTA
 #pragma unroll
     for (int d = 0; d < 2; d++) {
-#pragma unroll
-        for (int v = 0; v < V; v++) {
-            qfix[d][v] = 0;
-#pragma unroll
-            for (int r = 0; r < R; r++) rho[d][r][v] = 0;
-        }
-        if (!offw[d]) continue;
-        const DiagDev &dd = *reinterpret_cast<const DiagDev *>(blob + offw[d]);
+        const uint64_t ow = d ? offw1 : offw0;
+        if (!ow || tid >= NR) continue;
+        const DiagDev &dd = *reinterpret_cast<const DiagDev *>(blob + ow);
         const QuadTerm *iq = reinterpret_cast<const QuadTerm *>(blob + dd.off_in_quad);
+        int64_t acc = 0;
         for (uint32_t q = 0; q < dd.n_in_quad; q++) {
-            const QuadTerm t = iq[q];  // t.i < t.j
-#pragma unroll
-            for (int v = 0; v < V; v++) {
-                const uint32_t e = uint32_t(v) | (uint32_t(lane) << LV);
-                if (int(t.i) >= F || !((e >> t.i) & 1)) continue;
-                if (int(t.j) < F) {
-                    if ((e >> t.j) & 1) qfix[d][v] += t.coef;
-                } else {
-#pragma unroll
-                    for (int r = 0; r < R; r++)
-                        if (int(t.j) - F == r) rho[d][r][v] += t.coef;
-                }
-            }
+            const QuadTerm t = iq[q];
+            if (int(t.i) >= F && ((tid >> (t.i - F)) & 1) && ((tid >> (t.j - F)) & 1)) acc += t.coef;
         }
-        if (tid < NR) {
-            int64_t acc = 0;
-            for (uint32_t q = 0; q < dd.n_in_quad; q++) {
-                const QuadTerm t = iq[q];
-                if (int(t.i) >= F && ((tid >> (t.i - F)) & 1) && ((tid >> (t.j - F)) & 1)) acc += t.coef;
-            }
-            s_qreg[d][tid] = acc;
-        }
+        s_qreg[d][tid] = acc;
     }
     __syncthreads();
 
-    const int nrows = 1 << Rn;
     const uint64_t stride = uint64_t(gridDim.x) * WARPS;
-    for (uint64_t item = uint64_t(blockIdx.x) * WARPS + uint64_t(warp); item < p.nitems; item += stride) {
+    for (uint64_t item = uint64_t(blockIdx.x) * WARPS + uint64_t(warp); item < nitems; item += stride) {
         // item bits go to every real bit outside [0, F) and the register bits
         uint64_t base = item << F;
         for (uint32_t r = 0; r < Rn; r++) {
-            const uint32_t b = p.rb[r];
+            const uint32_t b = s_rb[r];
             base = ((base >> b) << (b + 1)) | (base & ((1ULL << b) - 1ULL));
         }
         E *rowp = state + base + (uint64_t(lane) << LV);
         VT x[NR];
 #pragma unroll
         for (int j = 0; j < NR; j++)
-            if (j < nrows) x[j] = __ldcs(reinterpret_cast<const VT *>(rowp + s_off[j]));
+            x[j] = __ldcs(reinterpret_cast<const VT *>(rowp + s_off[j]));
 
         // per-item selector orientation of every gate
         int ob = 0;
@@ -548,80 +562,52 @@ __global__ void __launch_bounds__(kThreads) row_pass_kernel(const uint8_t *__res
         }
         const uint32_t omask = __ballot_sync(0xffffffffu, ob);
 
-#pragma unroll
-        for (int d = 0; d < 2; d++) {
-            if (!offw[d]) continue;
-            if (d == 1) {
-                // gates run between the prologue and the epilogue
-                for (uint32_t gi = 0; gi < ngates; gi++) {
-                    const uint32_t c = s_gc[gi];
-                    const RT *u = s_u[gi][(omask >> gi) & 1];
-                    const RT m00r = u[0], m00i = u[1], m01r = u[2], m01i = u[3];
-                    const RT m10r = u[4], m10i = u[5], m11r = u[6], m11i = u[7];
-                    if (int(c) < LV) {
-#pragma unroll
-                        for (int j = 0; j < NR; j++) {
-                            const E lo = vget(x[j], 0), hi = vget(x[j], V - 1);
-                            vset(x[j], 0, cmad2(m00r, m00i, lo, m01r, m01i, hi));
-                            vset(x[j], V - 1, cmad2(m10r, m10i, lo, m11r, m11i, hi));
-                        }
-                    } else if (int(c) < F) {
-                        const int lb = int(c) - LV;
-                        const bool hb = (lane >> lb) & 1;
-                        const RT ar = hb ? m11r : m00r, ai = hb ? m11i : m00i;
-                        const RT br = hb ? m10r : m01r, bi = hb ? m10i : m01i;
-#pragma unroll
-                        for (int j = 0; j < NR; j++)
-#pragma unroll
-                            for (int v = 0; v < V; v++) {
-                                const E mine = vget(x[j], v);
-                                const E pt = shfl_xor_e(mine, 1 << lb);
-                                vset(x[j], v, cmad2(ar, ai, mine, br, bi, pt));
-                            }
-                    } else {
-#pragma unroll
-                        for (int rr = 0; rr < R; rr++) {
-                            if (int(c) - F != rr) continue;
-#pragma unroll
-                            for (int j = 0; j < NR; j++) {
-                                if ((j >> rr) & 1) continue;
-#pragma unroll
-                                for (int v = 0; v < V; v++) {
-                                    const E lo = vget(x[j], v), hi = vget(x[j | (1 << rr)], v);
-                                    vset(x[j], v, cmad2(m00r, m00i, lo, m01r, m01i, hi));
-                                    vset(x[j | (1 << rr)], v, cmad2(m10r, m10i, lo, m11r, m11i, hi));
-                                }
-                            }
-                        }
-                    }
-                }
-            }
-            const DiagDev &dd = *reinterpret_cast<const DiagDev *>(blob + offw[d]);
-            const int T = F + int(Rn);
+        auto window = [&](const DiagDev &dd, const int64_t *qreg) {
+            constexpr int T = F + R;
             int64_t da = 0, K = 0;
-            {
-                const QuadTerm *cr = reinterpret_cast<const QuadTerm *>(blob + dd.off_cross);
-                const LinTerm *ol = reinterpret_cast<const LinTerm *>(blob + dd.off_out_lin);
-                const QuadTerm *oq = reinterpret_cast<const QuadTerm *>(blob + dd.off_out_quad);
-                const uint32_t *kidx = reinterpret_cast<const uint32_t *>(blob + dd.off_kidx);
-                if (lane < T) {
-                    da = dd.lin_in[lane];
-                    for (uint32_t q = kidx[lane]; q < kidx[lane + 1]; q++) {
-                        const QuadTerm t = cr[q];
-                        if ((base >> t.j) & 1) da += t.coef;
-                    }
+            const QuadTerm *cr = reinterpret_cast<const QuadTerm *>(blob + dd.off_cross);
+            const LinTerm *ol = reinterpret_cast<const LinTerm *>(blob + dd.off_out_lin);
+            const QuadTerm *oq = reinterpret_cast<const QuadTerm *>(blob + dd.off_out_quad);
+            const uint32_t *kidx = reinterpret_cast<const uint32_t *>(blob + dd.off_kidx);
+            if (lane < T) {
+                da = dd.lin_in[lane];
+                for (uint32_t q = kidx[lane]; q < kidx[lane + 1]; q++) {
+                    const QuadTerm t = cr[q];
+                    if ((base >> t.j) & 1) da += t.coef;
                 }
-                for (uint32_t q = uint32_t(lane); q < dd.n_out_lin; q += 32)
-                    if ((base >> ol[q].bit) & 1) K += ol[q].coef;
-                for (uint32_t q = uint32_t(lane); q < dd.n_out_quad; q += 32) {
-                    const QuadTerm t = oq[q];
-                    if (((base >> t.i) & 1) && ((base >> t.j) & 1)) K += t.coef;
-                }
-                K = warp_sum_i64(K) + dd.c0;
             }
+            for (uint32_t q = uint32_t(lane); q < dd.n_out_lin; q += 32)
+                if ((base >> ol[q].bit) & 1) K += ol[q].coef;
+            for (uint32_t q = uint32_t(lane); q < dd.n_out_quad; q += 32) {
+                const QuadTerm t = oq[q];
+                if (((base >> t.i) & 1) && ((base >> t.j) & 1)) K += t.coef;
+            }
+            K = warp_sum_i64(K) + dd.c0;
             int64_t acc[V], w[R][V];
 #pragma unroll
-            for (int v = 0; v < V; v++) acc[v] = K + qfix[d][v];
+            for (int v = 0; v < V; v++) {
+                acc[v] = K;
+#pragma unroll
+                for (int r = 0; r < R; r++) w[r][v] = 0;
+            }
+            // in-tile quadratic terms touching this thread's fixed (vector / lane) bits
+            const QuadTerm *iq = reinterpret_cast<const QuadTerm *>(blob + dd.off_in_quad);
+            for (uint32_t q = 0; q < dd.n_in_quad; q++) {
+                const QuadTerm t = iq[q];  // t.i < t.j
+                if (int(t.i) >= F) continue;
+#pragma unroll
+                for (int v = 0; v < V; v++) {
+                    const uint32_t e = uint32_t(v) | (uint32_t(lane) << LV);
+                    if (!((e >> t.i) & 1)) continue;
+                    if (int(t.j) < F) {
+                        if ((e >> t.j) & 1) acc[v] += t.coef;
+                    } else {
+#pragma unroll
+                        for (int r = 0; r < R; r++)
+                            if (int(t.j) - F == r) w[r][v] += t.coef;
+                    }
+                }
+            }
 #pragma unroll
             for (int k = 0; k < F; k++) {
                 const int64_t dk = __shfl_sync(0xffffffffu, da, k);
@@ -631,73 +617,30 @@ __global__ void __launch_bounds__(kThreads) row_pass_kernel(const uint8_t *__res
             }
 #pragma unroll
             for (int r = 0; r < R; r++) {
-                const int64_t dk = __shfl_sync(0xffffffffu, da, (F + r) & 31);
+                const int64_t dk = __shfl_sync(0xffffffffu, da, F + r);
 #pragma unroll
-                for (int v = 0; v < V; v++) w[r][v] = (r < int(Rn)) ? dk + rho[d][r][v] : 0;
+                for (int v = 0; v < V; v++) w[r][v] += dk;
             }
 #pragma unroll
             for (int jj = 0; jj < NR; jj++) {
                 const int gj = jj ^ (jj >> 1);
                 if (jj > 0) {
-                    int fb = 0;
-                    while (!((jj >> fb) & 1)) fb++;
+                    const int fb = ctz_const(jj);
 #pragma unroll
                     for (int v = 0; v < V; v++) acc[v] += ((gj >> fb) & 1) ? w[fb][v] : -w[fb][v];
                 }
-                if (gj >= nrows) continue;
-                const int64_t qr = s_qreg[d][gj];
+                const int64_t qr = qreg[gj];
 #pragma unroll
                 for (int v = 0; v < V; v++) vset(x[gj], v, cmul(vget(x[gj], v), phase_factor(s_exp, acc[v] + qr)));
             }
-        }
-        if (!offw[1]) {
-            // no epilogue: the gates have not run yet
-            for (uint32_t gi = 0; gi < ngates; gi++) {
-                const uint32_t c = s_gc[gi];
-                const RT *u = s_u[gi][(omask >> gi) & 1];
-                const RT m00r = u[0], m00i = u[1], m01r = u[2], m01i = u[3];
-                const RT m10r = u[4], m10i = u[5], m11r = u[6], m11i = u[7];
-                if (int(c) < LV) {
-#pragma unroll
-                    for (int j = 0; j < NR; j++) {
-                        const E lo = vget(x[j], 0), hi = vget(x[j], V - 1);
-                        vset(x[j], 0, cmad2(m00r, m00i, lo, m01r, m01i, hi));
-                        vset(x[j], V - 1, cmad2(m10r, m10i, lo, m11r, m11i, hi));
-                    }
-                } else if (int(c) < F) {
-                    const int lb = int(c) - LV;
-                    const bool hb = (lane >> lb) & 1;
-                    const RT ar = hb ? m11r : m00r, ai = hb ? m11i : m00i;
-                    const RT br = hb ? m10r : m01r, bi = hb ? m10i : m01i;
-#pragma unroll
-                    for (int j = 0; j < NR; j++)
-#pragma unroll
-                        for (int v = 0; v < V; v++) {
-                            const E mine = vget(x[j], v);
-                            const E pt = shfl_xor_e(mine, 1 << lb);
-                            vset(x[j], v, cmad2(ar, ai, mine, br, bi, pt));
-                        }
-                } else {
-#pragma unroll
-                    for (int rr = 0; rr < R; rr++) {
-                        if (int(c) - F != rr) continue;
-#pragma unroll
-                        for (int j = 0; j < NR; j++) {
-                            if ((j >> rr) & 1) continue;
-#pragma unroll
-                            for (int v = 0; v < V; v++) {
-                                const E lo = vget(x[j], v), hi = vget(x[j | (1 << rr)], v);
-                                vset(x[j], v, cmad2(m00r, m00i, lo, m01r, m01i, hi));
-                                vset(x[j | (1 << rr)], v, cmad2(m10r, m10i, lo, m11r, m11i, hi));
-                            }
-                        }
-                    }
-                }
-            }
-        }
+        };
+        if (offw0) window(*reinterpret_cast<const DiagDev *>(blob + offw0), s_qreg[0]);
+        for (uint32_t gi = 0; gi < ngates; gi++)
+            row_gate<R, V, LV, F>(x, s_gc[gi], &s_u[gi][(omask >> gi) & 1][0], lane);
+        if (offw1) window(*reinterpret_cast<const DiagDev *>(blob + offw1), s_qreg[1]);
 #pragma unroll
         for (int j = 0; j < NR; j++)
-            if (j < nrows) __stcs(reinterpret_cast<VT *>(rowp + s_off[j]), x[j]);
+            __stcs(reinterpret_cast<VT *>(rowp + s_off[j]), x[j]);
     }
 }
 
