@@ -162,6 +162,25 @@ int zxh_stream(zxh_sim *sim, void **stream);
  * handle's stream around the launches). Any pointer may be NULL. */
 int zxh_last_stats(const zxh_sim *sim, uint64_t *kernels, uint64_t *passes, double *device_ms);
 
+/* Multinomial sampler that allocates nothing, for callers that cannot call
+ * cudaMalloc (inside a CUDA graph capture region, in a process whose device
+ * memory is reserved once up front, or on a latency path that must not take the
+ * allocator's locks). No counterpart in the reference. It draws shots outcomes
+ * from the 2^m_bits-amplitude device state `state` (dtype ZXH_C64 or ZXH_C128,
+ * interleaved re/im, real-address order) with the same uniform stream and the
+ * same output order as zxh_measure after zxh_set_seed(seed), and writes the
+ * real index of each shot to the caller's DEVICE buffer real_out (shots
+ * uint64). Work is enqueued on `stream` (a cudaStream_t, NULL = default stream)
+ * and the call returns once it is done.
+ * Limits: m_bits <= 28 (ZXH_ERR_LIMIT otherwise, before any GPU work). Its
+ * working memory is one 2.25 MiB file-scope device array that every GPU loading
+ * the library holds until exit and that all calls on a device share: calls that
+ * overlap on the GPU race and must be serialised by the caller. The first call on
+ * a device resolves that array's address (cudaGetSymbolAddress); make it before
+ * any stream capture. Errors are reported through zxh_last_error(NULL). */
+int zxh_sample_noalloc(const void *state, int dtype, size_t m_bits, uint64_t seed, size_t shots, uint64_t *real_out,
+                       void *stream);
+
 /* Pass-planner tuning (used by the autotuner): tile_bits_c64, tile_bits_c128,
  * contig_bits, max_gates (generic tile pass), fast_gates (gates per fast U3
  * pass), fast_fuse_quad, fast_contig_c64, fast_contig_c128, row_wide_c64,

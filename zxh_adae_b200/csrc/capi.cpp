@@ -206,6 +206,10 @@ void column_tables(const zxh::AffineMap &A, uint64_t tab[8][256])
 
 }  // namespace
 
+namespace zxh {
+void set_thread_error(const std::string &msg) { g_create_error = msg; }
+}  // namespace zxh
+
 extern "C" {
 
 const char *zxh_version(void) { return "zxh_b200 0.1.0 (sm_100a)"; }

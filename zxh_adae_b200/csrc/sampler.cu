@@ -510,6 +510,55 @@ cudaError_t run_sampler(const void *state, int elem_bytes, int m, uint64_t shots
     return cudaGetLastError();
 }
 
+// The same draw as run_sampler up to the real indices, written to a caller buffer;
+// used by the allocation-free entry point (noalloc.cu). Scratch comes from sc,
+// whose flag region, counts and heavy count the caller has cleared.
+cudaError_t run_sampler_real(const void *state, int elem_bytes, int m, uint64_t shots, uint64_t stream_seed,
+                             uint64_t *real_out, SamplerScratch &sc, DevStatus *status, int sms, cudaStream_t st)
+{
+    const uint64_t local = 1ULL << m;
+    const uint32_t seglen = uint32_t(std::min<uint64_t>(4096, local));
+    const uint64_t nseg = local / seglen;
+    const uint64_t nchunks = (nseg + kSegsPerChunk - 1) / kSegsPerChunk;
+    const uint64_t nblk = (nseg + kScanBlock - 1) / kScanBlock;
+    const uint64_t stream2 = mix_seed_host(stream_seed, 1);
+    const unsigned gs = unsigned(std::max<uint64_t>(1, std::min<uint64_t>(nchunks, uint64_t(sms) * 4)));
+    if (elem_bytes == 8)
+        seg_scan_kernel<float2><<<gs, kThreads, 0, st>>>(static_cast<const float2 *>(state), nseg, seglen, sc.segcdf,
+                                                        sc.agg_val, sc.agg_flag, sc.inc_val, sc.inc_flag, sc.ticket,
+                                                        status);
+    else
+        seg_scan_kernel<double2><<<gs, kThreads, 0, st>>>(static_cast<const double2 *>(state), nseg, seglen, sc.segcdf,
+                                                         sc.agg_val, sc.agg_flag, sc.inc_val, sc.inc_flag, sc.ticket,
+                                                         status);
+    const unsigned gc = unsigned(std::max<uint64_t>(1, std::min<uint64_t>((shots + kThreads - 1) / kThreads, uint64_t(sms) * 8)));
+    count_kernel<<<gc, kThreads, 0, st>>>(sc.segcdf, nseg, stream_seed, shots, sc.counts);
+    block_sum_kernel<<<unsigned(nblk), kThreads, 0, st>>>(sc.counts, nseg, sc.bsum);
+    scan_small_kernel<<<1, 32, 0, st>>>(sc.bsum, nblk);
+    block_scan_kernel<<<unsigned(nblk), kThreads, 0, st>>>(sc.counts, nseg, sc.bsum, sc.offsets);
+    const uint64_t warps_needed = (nseg + 31) / 32;
+    const unsigned gw = unsigned(std::max<uint64_t>(1, std::min<uint64_t>((warps_needed * 32 + kThreads - 1) / kThreads,
+                                                                          uint64_t(sms) * 8)));
+    if (elem_bytes == 8)
+        resolve_warp_kernel<float2><<<gw, kThreads, 0, st>>>(static_cast<const float2 *>(state), nseg, seglen, sc.counts,
+                                                            sc.offsets, stream2, real_out, sc.heavy_list, sc.heavy_count);
+    else
+        resolve_warp_kernel<double2><<<gw, kThreads, 0, st>>>(static_cast<const double2 *>(state), nseg, seglen,
+                                                             sc.counts, sc.offsets, stream2, real_out, sc.heavy_list,
+                                                             sc.heavy_count);
+    const size_t smem = size_t(seglen) * 8;
+    const unsigned gh = unsigned(sms) * 2;
+    if (elem_bytes == 8)
+        resolve_cta_kernel<float2><<<gh, kThreads, smem, st>>>(static_cast<const float2 *>(state), seglen, sc.counts,
+                                                              sc.offsets, stream2, real_out, sc.heavy_list,
+                                                              sc.heavy_count);
+    else
+        resolve_cta_kernel<double2><<<gh, kThreads, smem, st>>>(static_cast<const double2 *>(state), seglen, sc.counts,
+                                                               sc.offsets, stream2, real_out, sc.heavy_list,
+                                                               sc.heavy_count);
+    return cudaGetLastError();
+}
+
 uint64_t mix_seed_host(uint64_t base, uint64_t salt)
 {
     // mix_seed, measure_cuda.cu:103-109

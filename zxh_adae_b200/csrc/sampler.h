@@ -30,6 +30,10 @@ cudaError_t run_sampler(const void *state, int elem_bytes, int m, uint64_t shots
                         const uint64_t *host_coltab, uint64_t b, SamplerScratch &sc, DevStatus *status, int sms,
                         cudaStream_t st, uint64_t &kernels);
 
+// run_sampler's draw up to real indices, into a caller buffer (noalloc.cu).
+cudaError_t run_sampler_real(const void *state, int elem_bytes, int m, uint64_t shots, uint64_t stream_seed,
+                             uint64_t *real_out, SamplerScratch &sc, DevStatus *status, int sms, cudaStream_t st);
+
 // Pass runner and get_state scatter (kernels.cu).
 struct Pass;
 cudaError_t run_passes(const std::vector<Pass> &passes, const uint8_t *dblob, void *state, int elem_bytes,
