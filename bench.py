@@ -85,7 +85,8 @@ def max_over_ranks(pg, x: float, local: int) -> float:
         return x
     import torch
 
-    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+    # local < 0: CPU tensor (gloo process groups, as in the CPU tests)
+    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}" if local >= 0 else "cpu")
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 

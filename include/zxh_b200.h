@@ -181,6 +181,15 @@ int zxh_last_stats(const zxh_sim *sim, uint64_t *kernels, uint64_t *passes, doub
 int zxh_sample_noalloc(const void *state, int dtype, size_t m_bits, uint64_t seed, size_t shots, uint64_t *real_out,
                        void *stream);
 
+/* Host-only dry run of execute(): lowers the records, runs calc_mem, the
+ * reference's execute() schedule and the pass planner, and launches nothing
+ * (no CUDA call is made). out[10]: [0] M, [1] final real bits, [2..8] passes
+ * per kind (product, expand, tile, pair, diagonal, fast low-qubit, strided
+ * high-qubit), [9] state passes (all but product). No counterpart in the
+ * reference. */
+int zxh_plan_stats(size_t n, int disable_x, int eager_expand_all, int dtype, const zxh_gate *gates, size_t count,
+                   uint64_t *out);
+
 /* Pass-planner tuning (used by the autotuner): tile_bits_c64, tile_bits_c128,
  * contig_bits, max_gates (generic tile pass), fast_gates (gates per fast U3
  * pass), fast_fuse_quad, fast_contig_c64, fast_contig_c128, row_wide_c64,

@@ -90,6 +90,7 @@ _sig("zxh_state_view", [_P, ctypes.POINTER(_P), ctypes.POINTER(_SZ), ctypes.POIN
                         ctypes.POINTER(_D), ctypes.POINTER(_D)])
 _sig("zxh_stream", [_P, ctypes.POINTER(_P)])
 _sig("zxh_set_param", [_P, ctypes.c_char_p, ctypes.c_int])
+_sig("zxh_plan_stats", [_SZ, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _SZ, _P])
 _sig("zxh_last_stats", [_P, ctypes.POINTER(_U64), ctypes.POINTER(_U64), ctypes.POINTER(_D)])
 
 _ERRORS = {1: ValueError, 2: RuntimeError, 3: RuntimeError, 4: MemoryError, 5: ValueError, 6: RuntimeError}
@@ -119,6 +120,23 @@ def as_records(gates) -> np.ndarray:
         t, cq, q, th, la, ph = (list(g) + [0.0] * 6)[:6]
         rec[i] = (t, cq, q, 0, th, la, ph)
     return rec
+
+
+PASS_KINDS = ("product", "expand", "tile", "pair", "diagonal", "fast", "row")
+
+
+def plan_stats(n: int, gates, dtype: str = "complex64", disable_x: bool = False,
+               eager_expand_all: bool = False) -> dict:
+    """Host-only dry run of execute() (no GPU needed): state bits and pass counts."""
+    rec = as_records(gates)
+    out = np.zeros(10, np.uint64)
+    rc = _lib.zxh_plan_stats(int(n), int(bool(disable_x)), int(bool(eager_expand_all)),
+                             C64 if dtype == "complex64" else C128, rec.ctypes.data, len(rec), out.ctypes.data)
+    if rc != 0:
+        _raise(rc, None)
+    d = {"M": int(out[0]), "m": int(out[1]), "passes": int(out[9])}
+    d.update({k: int(out[2 + i]) for i, k in enumerate(PASS_KINDS)})
+    return d
 
 
 # Module-level runtime calls of the reference (bindings.cpp:86-90). One process
@@ -180,7 +198,7 @@ class ZXH:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and _lib is not None:  # the module may already be torn down at interpreter exit
             _lib.zxh_destroy(h)
             self._h = None
 

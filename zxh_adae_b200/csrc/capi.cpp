@@ -575,6 +575,42 @@ int zxh_stream(zxh_sim *s, void **stream)
     return ZXH_OK;
 }
 
+int zxh_plan_stats(size_t n, int disable_x, int eager_expand_all, int dtype, const zxh_gate *gates, size_t count,
+                   uint64_t *out)
+{
+    if (!out || (count && !gates)) return fail(nullptr, ZXH_ERR_ARG, "null argument");
+    if (n < 1 || n > 63) return fail(nullptr, ZXH_ERR_LIMIT, "n must be in 1..63");
+    if (dtype != ZXH_C64 && dtype != ZXH_C128) return fail(nullptr, ZXH_ERR_ARG, "dtype must be ZXH_C64 or ZXH_C128");
+    zxh_sim tmp;  // host fields only; no CUDA call is made
+    tmp.n = n;
+    std::vector<Gate> gl;
+    for (size_t i = 0; i < count; i++)
+        if (int rc = lower(&tmp, gates[i], gl)) return fail(nullptr, rc, tmp.err);
+    const int eb = dtype == ZXH_C64 ? 8 : 16;
+    const int M = eager_expand_all ? int(n) : zxh::calc_mem(gl.data(), gl.size(), int(n), disable_x != 0);
+    zxh::WalkState ws;
+    ws.map.reset(int(n));
+    if (eager_expand_all) {
+        for (size_t q = 0; q < n; q++) ws.map.append_col(int(q));
+        ws.m = int(n);
+        ws.init_bits = int(n);
+    }
+    const zxh::WalkState start = ws;
+    std::vector<zxh::Op> ops;
+    std::string err;
+    if (int rc = zxh::walk(gl.data(), gl.size(), disable_x != 0, M, ws, ops, err)) return fail(nullptr, rc, err);
+    zxh::Plan pl;
+    if (int rc = zxh::plan(ops, eb, tmp.pp, start, pl, err)) return fail(nullptr, rc, err);
+    for (int k = 0; k < 10; k++) out[k] = 0;
+    out[0] = uint64_t(M);
+    out[1] = uint64_t(ws.m);
+    for (const zxh::Pass &p : pl.passes) {
+        out[2 + int(p.kind)]++;
+        if (p.kind != zxh::Pass::PRODUCT) out[9]++;
+    }
+    return ZXH_OK;
+}
+
 int zxh_set_param(zxh_sim *s, const char *name, int value)
 {
     if (!s || !name) return ZXH_ERR_ARG;
