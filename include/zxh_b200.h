@@ -181,6 +181,40 @@ int zxh_last_stats(const zxh_sim *sim, uint64_t *kernels, uint64_t *passes, doub
 int zxh_sample_noalloc(const void *state, int dtype, size_t m_bits, uint64_t seed, size_t shots, uint64_t *real_out,
                        void *stream);
 
+/* ---- Expectation values and adjoint gradients (no counterpart in the
+ * reference, which has no observables) ---------------------------------------- */
+
+/* One Pauli term of an observable: kind ZXH_TERM_Z (coef * Z_q0),
+ * ZXH_TERM_ZZ (coef * Z_q0 Z_q1) or ZXH_TERM_X (coef * X_q0). At most 256 terms. */
+enum { ZXH_TERM_Z = 1, ZXH_TERM_ZZ = 2, ZXH_TERM_X = 3 };
+typedef struct zxh_term {
+    uint32_t kind;
+    uint32_t q0;
+    uint32_t q1;
+    uint32_t reserved;
+    double coef;
+} zxh_term;
+
+/* <psi|H|psi> of the state left by the last zxh_execute / zxh_apply, reduced in
+ * FP64 on the device. */
+int zxh_expectation(zxh_sim *sim, const zxh_term *terms, size_t nterms, double *value);
+
+/* Runs the recorded gate list forward (like zxh_execute, saving a copy of the
+ * state after every `checkpoint_every` parameterised gates, 0 = no checkpoints),
+ * then one reverse sweep over the state and lambda = H|psi>, and writes
+ * value = <H> and grads[i] = d<H>/d(theta of recorded gate i) for every recorded
+ * gate (0 for gates without a parameter). Parameterised gates: RZ, P, CP, RX and
+ * U3 records with lambda = phi = 0 (RY). grads holds the recorded gate count
+ * (CRz records count as two: P then CP). The reverse sweep uncomputes with the
+ * inverse gates; at each checkpoint the uncomputed state is replaced by the
+ * saved forward state, which bounds the drift. The sweep holds 2^n amplitudes
+ * per state (n <= 40). After the call the state is the forward output again. */
+int zxh_adjoint_gradient(zxh_sim *sim, const zxh_term *terms, size_t nterms, size_t checkpoint_every, double *value,
+                         double *grads, size_t ngrads);
+
+/* Number of recorded gates (after CRz / Rx lowering). */
+int zxh_gate_count(const zxh_sim *sim, size_t *out);
+
 /* Host-only dry run of execute(): lowers the records, runs calc_mem, the
  * reference's execute() schedule and the pass planner, and launches nothing
  * (no CUDA call is made). out[10]: [0] M, [1] final real bits, [2..8] passes

@@ -92,6 +92,9 @@ _sig("zxh_stream", [_P, ctypes.POINTER(_P)])
 _sig("zxh_set_param", [_P, ctypes.c_char_p, ctypes.c_int])
 _sig("zxh_plan_stats", [_SZ, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _SZ, _P])
 _sig("zxh_last_stats", [_P, ctypes.POINTER(_U64), ctypes.POINTER(_U64), ctypes.POINTER(_D)])
+_sig("zxh_expectation", [_P, _P, _SZ, ctypes.POINTER(_D)])
+_sig("zxh_adjoint_gradient", [_P, _P, _SZ, _SZ, ctypes.POINTER(_D), _P, _SZ])
+_sig("zxh_gate_count", [_P, ctypes.POINTER(_SZ)])
 
 _ERRORS = {1: ValueError, 2: RuntimeError, 3: RuntimeError, 4: MemoryError, 5: ValueError, 6: RuntimeError}
 
@@ -120,6 +123,22 @@ def as_records(gates) -> np.ndarray:
         t, cq, q, th, la, ph = (list(g) + [0.0] * 6)[:6]
         rec[i] = (t, cq, q, 0, th, la, ph)
     return rec
+
+
+# observable terms (include/zxh_b200.h zxh_term)
+TERM_DTYPE = np.dtype([("kind", "<u4"), ("q0", "<u4"), ("q1", "<u4"), ("reserved", "<u4"), ("coef", "<f8")])
+TERM_Z, TERM_ZZ, TERM_X = 1, 2, 3
+
+
+def as_terms(terms) -> np.ndarray:
+    """Observable terms from a structured array or ``(kind, q0, q1, coef)`` tuples."""
+    if isinstance(terms, np.ndarray) and terms.dtype == TERM_DTYPE:
+        return np.ascontiguousarray(terms)
+    rows = list(terms)
+    out = np.zeros(len(rows), TERM_DTYPE)
+    for i, (k, q0, q1, c) in enumerate(rows):
+        out[i] = (k, q0, q1, 0, c)
+    return out
 
 
 PASS_KINDS = ("product", "expand", "tile", "pair", "diagonal", "fast", "row")
@@ -341,3 +360,28 @@ class ZXH:
         k, p, ms = _U64(0), _U64(0), _D(0.0)
         self._ck(_lib.zxh_last_stats(self._h, ctypes.byref(k), ctypes.byref(p), ctypes.byref(ms)))
         return int(k.value), int(p.value), float(ms.value)
+
+    # --- observables and gradients (no counterpart in the reference) -----------------
+    def gate_count(self) -> int:
+        """Recorded gates after lowering (CRz counts as P + CP)."""
+        out = _SZ(0)
+        self._ck(_lib.zxh_gate_count(self._h, ctypes.byref(out)))
+        return int(out.value)
+
+    def expectation(self, terms) -> float:
+        """<psi|H|psi> of the current state for Z / ZZ / X terms, FP64-reduced on the GPU."""
+        t = as_terms(terms)
+        v = _D(0.0)
+        self._ck(_lib.zxh_expectation(self._h, t.ctypes.data, len(t), ctypes.byref(v)))
+        return float(v.value)
+
+    def adjoint_gradient(self, terms, checkpoint_every: int = 0) -> tuple:
+        """(<H>, d<H>/d theta per recorded gate) from one forward and one reverse
+        sweep over the recorded gates; leaves the forward output as the state."""
+        t = as_terms(terms)
+        cnt = self.gate_count()
+        g = np.zeros(max(cnt, 1), np.float64)
+        v = _D(0.0)
+        self._ck(_lib.zxh_adjoint_gradient(self._h, t.ctypes.data, len(t), int(checkpoint_every), ctypes.byref(v),
+                                           g.ctypes.data, g.size))
+        return float(v.value), g[:cnt]

@@ -1,0 +1,411 @@
+// adjoint_api.cpp -- zxh_expectation, zxh_adjoint_gradient and zxh_gate_count.
+//
+// No counterpart in the reference: ZXH-Sim has no observables or gradients. The
+// sweep reuses the execute() walk and planner for the forward pass and works in
+// the real-address space of the affine map throughout.
+//
+// Forward: the recorded gates run with every qubit expanded from the start
+// (eager_expand_all, zxh.cpp:721-729) and X/CX transported through the map, in
+// segments that end after every `checkpoint_every` parameterised gates; the state
+// after each segment is copied aside. With all qubits expanded the map never
+// gains a column, so undoing X/CX on the map while walking the gates backwards
+// gives back, at every gate boundary, exactly the map the forward pass had there,
+// and a checkpoint is a plain copy into the reverse state.
+//
+// Reverse: psi (a copy of the forward output) and lambda = H psi walk back over
+// the gates. A 2x2 gate is one adj_pair pass that reduces its gradient and
+// uncomputes both states with U^dagger; a run of diagonal gates (RZ, P, CP, Z,
+// with X/CX relabelings between them) is one adj_diag pass that reduces every
+// gradient of the run at once, which is exact because the run's gates commute.
+//
+// Global phase: Z/RZ records carry a global phase that the walk keeps outside the
+// state (zxh.cpp:477-493). psi and lambda carry the same untracked factor, so
+// Im<lambda|G|psi> does not see it, and a checkpoint's factor differs from the
+// reverse state's only by rounding of the accumulated phase.
+#include "adjoint.h"
+#include "sim.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace zxh::api;
+
+namespace {
+
+using zxh::AdjDiagGate;
+using zxh::AdjPairDev;
+using zxh::AffineMap;
+using zxh::TermDev;
+
+// gradient generator of a lowered 2x2 record: RY = U3(theta, 0, 0), RX =
+// U3(theta, pi/2, -pi/2) (the lowering of zxh_rx and ZXH_GATE_RX)
+uint32_t pair_generator(const Gate &g)
+{
+    if (g.type != zxh::G_U3) return 0;
+    if (g.lambda == 0.0 && g.phi == 0.0) return 1;
+    if (g.lambda == kPi / 2.0 && g.phi == -kPi / 2.0) return 2;
+    return 0;
+}
+
+bool parameterised(const Gate &g)
+{
+    switch (g.type) {
+    case zxh::G_RZ:
+    case zxh::G_P:
+    case zxh::G_CP: return true;
+    case zxh::G_U3: return pair_generator(g) != 0;
+    default: return false;
+    }
+}
+
+// Terms in the real-address form of map A over m bits. X terms on a qubit whose
+// flip leaves the map's image are dropped when drop_unreachable is set (their
+// expectation is exactly zero) and rejected otherwise.
+int compile_terms(zxh_sim *s, const zxh_term *terms, size_t nterms, AffineMap &A, int m, bool drop_unreachable,
+                  std::vector<TermDev> &out)
+{
+    out.clear();
+    if (nterms && !terms) return fail(s, ZXH_ERR_ARG, "terms is null");
+    if (nterms > zxh::kMaxTerms)
+        return fail(s, ZXH_ERR_LIMIT, "at most " + std::to_string(zxh::kMaxTerms) + " observable terms");
+    for (size_t i = 0; i < nterms; i++) {
+        const zxh_term &t = terms[i];
+        TermDev d;
+        std::memset(&d, 0, sizeof(d));
+        d.kind = t.kind;
+        d.coef = t.coef;
+        if (t.q0 >= s->n || (t.kind == ZXH_TERM_ZZ && t.q1 >= s->n))
+            return fail(s, ZXH_ERR_ARG, "observable term qubit out of range");
+        switch (t.kind) {
+        case ZXH_TERM_ZZ: {
+            const zxh::Sel s1 = A.selector(int(t.q1));
+            d.a1 = s1.alpha;
+            d.b1 = uint32_t(s1.beta);
+        }
+            // fall through
+        case ZXH_TERM_Z: {
+            const zxh::Sel s0 = A.selector(int(t.q0));
+            d.a0 = s0.alpha;
+            d.b0 = uint32_t(s0.beta);
+            break;
+        }
+        case ZXH_TERM_X: {
+            uint64_t delta = 0;
+            if (!A.solve(int(t.q0), delta)) {
+                if (drop_unreachable) continue;
+                return fail(s, ZXH_ERR_STATE, "X term on a qubit the state does not span");
+            }
+            d.delta = delta & zxh::low_mask(m);
+            break;
+        }
+        default: return fail(s, ZXH_ERR_ARG, "unknown observable term kind " + std::to_string(t.kind));
+        }
+        out.push_back(d);
+    }
+    return ZXH_OK;
+}
+
+struct RevStep {
+    enum Kind { PAIR, DIAG, RESTORE } kind;
+    AdjPairDev pair;
+    size_t slot = 0;   // PAIR: gradient slot
+    size_t first = 0;  // DIAG: first gate in the uploaded group array
+    uint32_t ng = 0;   // DIAG: gates in the group
+    size_t ckpt = 0;   // RESTORE: checkpoint index
+};
+
+// Region layout of d_adj: grads | energy | terms | diag gates | diag slots.
+struct AdjLayout {
+    size_t grads, energy, terms, gates, slots, total;
+    AdjLayout(size_t ngrads, size_t nterms, size_t ndiag)
+    {
+        auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
+        grads = 0;
+        energy = up(ngrads * sizeof(double));
+        terms = energy + 256;
+        gates = up(terms + nterms * sizeof(TermDev));
+        slots = up(gates + ndiag * sizeof(AdjDiagGate));
+        total = up(slots + ndiag * sizeof(uint32_t)) + 256;
+    }
+};
+
+// Forward pass in segments [0, ends[0]), [ends[0], ends[1]), ... with every qubit
+// expanded; the state after segment k < ends.size() - 1 is saved as checkpoint k.
+int forward_segments(zxh_sim *s, const std::vector<size_t> &ends, double &ms, uint64_t &kernels)
+{
+    const int N = int(s->n);
+    const size_t bytes = size_t(s->elem_bytes) << N;
+    if (int rc = ensure_dev(s, &s->d_state, s->state_cap_bytes, std::max<size_t>(bytes, 256), "cudaMalloc(state)"))
+        return rc;
+    const size_t nck = ends.empty() ? 0 : ends.size() - 1;
+    if (nck)
+        if (int rc = ensure_dev(s, &s->d_ckpt, s->ckpt_cap, nck * bytes, "cudaMalloc(checkpoints)")) return rc;
+    s->M = N;
+    s->executed = false;
+    s->measured = 0;
+    zxh::WalkState &ws = s->ws;
+    ws.map.reset(N);
+    for (int q = 0; q < N; q++) ws.map.append_col(q);
+    ws.m = N;
+    ws.gphase = zxh::cd(1.0, 0.0);
+    ws.fresh = true;
+    ws.init_bits = N;
+    ms = 0.0;
+    kernels = 0;
+    size_t a = 0;
+    for (size_t k = 0; k < ends.size(); k++) {
+        const zxh::WalkState start = ws;
+        std::vector<zxh::Op> ops;
+        std::string err;
+        if (int rc = zxh::walk(s->gates.data() + a, ends[k] - a, false, N, ws, ops, err)) return fail(s, rc, err);
+        zxh::Plan pl;
+        if (int rc = zxh::plan(ops, s->elem_bytes, s->pp, start, pl, err)) return fail(s, rc, err);
+        if (int rc = run_plan(s, pl)) return rc;
+        ws.fresh = false;
+        ms += double(s->last_ms);
+        kernels += s->stat_kernels;
+        if (k < nck)
+            CK(s, cudaMemcpyAsync(static_cast<uint8_t *>(s->d_ckpt) + k * bytes, s->d_state, bytes,
+                                  cudaMemcpyDeviceToDevice, s->stream),
+               "save checkpoint");
+        a = ends[k];
+    }
+    s->executed = true;
+    return ZXH_OK;
+}
+
+// The reverse program: gates walked backwards from the forward output's map.
+int reverse_program(zxh_sim *s, const std::vector<size_t> &ends, AffineMap A, std::vector<RevStep> &steps,
+                    std::vector<AdjDiagGate> &dgates, std::vector<uint32_t> &dslots)
+{
+    const int N = int(s->n);
+    const size_t count = s->gates.size();
+    long open = -1;                    // diagonal group being filled
+    size_t next_ck = ends.size() - 1;  // checkpoints are restored from the last one down
+    for (size_t gi = count; gi-- > 0;) {
+        if (next_ck > 0 && ends[next_ck - 1] == gi + 1) {
+            next_ck--;
+            RevStep r;
+            r.kind = RevStep::RESTORE;
+            r.ckpt = next_ck;
+            steps.push_back(r);
+            open = -1;
+        }
+        const Gate &g = s->gates[gi];
+        switch (g.type) {
+        case zxh::G_X: A.flip_b(int(g.q)); break;
+        case zxh::G_CX:
+            A.row_xor(int(g.q), int(g.cq));
+            A.b_xor(int(g.q), int(g.cq));
+            break;
+        case zxh::G_Z:
+        case zxh::G_RZ:
+        case zxh::G_P:
+        case zxh::G_CP: {
+            if (open < 0 || steps[size_t(open)].ng == uint32_t(zxh::kAdjDiagMax)) {
+                RevStep r;
+                r.kind = RevStep::DIAG;
+                r.first = dgates.size();
+                steps.push_back(r);
+                open = long(steps.size()) - 1;
+            }
+            AdjDiagGate d;
+            std::memset(&d, 0, sizeof(d));
+            const zxh::Sel s0 = A.selector(int(g.type == zxh::G_CP ? g.cq : g.q));
+            d.a0 = s0.alpha;
+            d.b0 = uint32_t(s0.beta);
+            if (g.type == zxh::G_CP) {
+                const zxh::Sel s1 = A.selector(int(g.q));
+                d.a1 = s1.alpha;
+                d.b1 = uint32_t(s1.beta);
+                d.two = 1;
+            }
+            d.kind = g.type == zxh::G_Z ? 0 : g.type == zxh::G_RZ ? 1 : 2;
+            d.theta = g.type == zxh::G_Z ? kPi : g.theta;
+            dgates.push_back(d);
+            dslots.push_back(uint32_t(gi));
+            steps[size_t(open)].ng++;
+            break;
+        }
+        case zxh::G_H:
+        case zxh::G_U3: {
+            open = -1;
+            RevStep r;
+            r.kind = RevStep::PAIR;
+            std::memset(&r.pair, 0, sizeof(r.pair));
+            uint64_t delta = 0;
+            if (!A.solve(int(g.q), delta)) return fail(s, ZXH_ERR_STATE, "adjoint sweep: qubit outside the map");
+            delta &= zxh::low_mask(N);
+            const zxh::Sel sl = A.selector(int(g.q));
+            r.pair.m = uint32_t(N);
+            r.pair.pivot = uint32_t(__builtin_ctzll(delta));
+            r.pair.delta = delta;
+            r.pair.alpha = sl.alpha;
+            r.pair.beta = uint32_t(sl.beta);
+            r.pair.gen = pair_generator(g);
+            zxh::cd u[4];
+            if (g.type == zxh::G_H) zxh::u3_matrix(kPi / 2.0, kPi, 0.0, u);
+            else zxh::u3_matrix(g.theta, g.lambda, g.phi, u);
+            for (int k = 0; k < 4; k++) {
+                r.pair.u[2 * k] = u[k].real();
+                r.pair.u[2 * k + 1] = u[k].imag();
+            }
+            r.slot = gi;
+            steps.push_back(r);
+            break;
+        }
+        default: break;
+        }
+    }
+    return ZXH_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int zxh_gate_count(const zxh_sim *s, size_t *out)
+{
+    if (!s || !out) return ZXH_ERR_ARG;
+    *out = s->gates.size();
+    return ZXH_OK;
+}
+
+int zxh_expectation(zxh_sim *s, const zxh_term *terms, size_t nterms, double *value)
+{
+    if (!s) return ZXH_ERR_ARG;
+    if (!value) return fail(s, ZXH_ERR_ARG, "value is null");
+    if (!s->executed) return fail(s, ZXH_ERR_STATE, "expectation requires execute() first");
+    if (int rc = use_device(s)) return rc;
+    std::vector<TermDev> dt;
+    if (int rc = compile_terms(s, terms, nterms, s->ws.map, s->ws.m, true, dt)) return rc;
+    const AdjLayout L(0, dt.size(), 0);
+    if (int rc = ensure_dev(s, reinterpret_cast<void **>(&s->d_adj), s->adj_cap, L.total, "cudaMalloc(adjoint)"))
+        return rc;
+    double *d_energy = reinterpret_cast<double *>(s->d_adj + L.energy);
+    auto *d_terms = reinterpret_cast<TermDev *>(s->d_adj + L.terms);
+    CK(s, cudaMemsetAsync(d_energy, 0, sizeof(double), s->stream), "reset energy");
+    if (!dt.empty())
+        CK(s, cudaMemcpyAsync(d_terms, dt.data(), dt.size() * sizeof(TermDev), cudaMemcpyHostToDevice, s->stream),
+           "upload terms");
+    CK(s, cudaEventRecord(s->ev0, s->stream), "event");
+    CK(s, zxh::run_lambda(s->d_state, nullptr, s->ws.m, s->elem_bytes, d_terms, uint32_t(dt.size()), d_energy, s->sms,
+                          s->stream),
+       "expectation launch");
+    CK(s, cudaEventRecord(s->ev1, s->stream), "event");
+    CK(s, cudaMemcpyAsync(value, d_energy, sizeof(double), cudaMemcpyDeviceToHost, s->stream), "read energy");
+    CK(s, cudaStreamSynchronize(s->stream), "expectation");
+    CK(s, cudaEventElapsedTime(&s->last_ms, s->ev0, s->ev1), "event time");
+    s->stat_kernels = 1;
+    s->stat_passes = 1;
+    return ZXH_OK;
+}
+
+int zxh_adjoint_gradient(zxh_sim *s, const zxh_term *terms, size_t nterms, size_t checkpoint_every, double *value,
+                         double *grads, size_t ngrads)
+{
+    if (!s) return ZXH_ERR_ARG;
+    const size_t count = s->gates.size();
+    if (!value) return fail(s, ZXH_ERR_ARG, "value is null");
+    if (count && !grads) return fail(s, ZXH_ERR_ARG, "grads is null");
+    if (ngrads < count) return fail(s, ZXH_ERR_ARG, "grads holds fewer entries than recorded gates");
+    if (s->n > 40) return fail(s, ZXH_ERR_LIMIT, "the adjoint sweep holds 2^n amplitudes: n must be at most 40");
+    for (size_t i = 0; i < nterms && terms; i++)
+        if (terms[i].kind < ZXH_TERM_Z || terms[i].kind > ZXH_TERM_X)
+            return fail(s, ZXH_ERR_ARG, "unknown observable term kind " + std::to_string(terms[i].kind));
+    if (nterms > zxh::kMaxTerms)
+        return fail(s, ZXH_ERR_LIMIT, "at most " + std::to_string(zxh::kMaxTerms) + " observable terms");
+    if (int rc = use_device(s)) return rc;
+    const int N = int(s->n);
+
+    // forward segments
+    std::vector<size_t> ends;
+    size_t np = 0;
+    for (size_t i = 0; i < count; i++)
+        if (parameterised(s->gates[i]) && checkpoint_every && ++np % checkpoint_every == 0 && i + 1 < count)
+            ends.push_back(i + 1);
+    ends.push_back(count);
+    double fwd_ms = 0.0;
+    uint64_t kernels = 0;
+    if (int rc = forward_segments(s, ends, fwd_ms, kernels)) return rc;
+
+    // reverse program
+    AffineMap A = s->ws.map;
+    std::vector<TermDev> dt;
+    if (int rc = compile_terms(s, terms, nterms, A, N, false, dt)) return rc;
+    std::vector<RevStep> steps;
+    std::vector<AdjDiagGate> dgates;
+    std::vector<uint32_t> dslots;
+    if (int rc = reverse_program(s, ends, A, steps, dgates, dslots)) return rc;
+
+    // device buffers
+    const size_t bytes = size_t(s->elem_bytes) << N;
+    if (int rc = ensure_dev(s, &s->d_psi, s->psi_cap, bytes, "cudaMalloc(adjoint psi)")) return rc;
+    if (int rc = ensure_dev(s, &s->d_lam, s->lam_cap, bytes, "cudaMalloc(adjoint lambda)")) return rc;
+    const AdjLayout L(count, dt.size(), dgates.size());
+    if (int rc = ensure_dev(s, reinterpret_cast<void **>(&s->d_adj), s->adj_cap, L.total, "cudaMalloc(adjoint)"))
+        return rc;
+    double *d_grads = reinterpret_cast<double *>(s->d_adj + L.grads);
+    double *d_energy = reinterpret_cast<double *>(s->d_adj + L.energy);
+    auto *d_terms = reinterpret_cast<TermDev *>(s->d_adj + L.terms);
+    auto *d_gates = reinterpret_cast<AdjDiagGate *>(s->d_adj + L.gates);
+    auto *d_slots = reinterpret_cast<uint32_t *>(s->d_adj + L.slots);
+    CK(s, cudaMemsetAsync(s->d_adj, 0, L.terms, s->stream), "reset gradients");
+    if (!dt.empty())
+        CK(s, cudaMemcpyAsync(d_terms, dt.data(), dt.size() * sizeof(TermDev), cudaMemcpyHostToDevice, s->stream),
+           "upload terms");
+    if (!dgates.empty()) {
+        CK(s, cudaMemcpyAsync(d_gates, dgates.data(), dgates.size() * sizeof(AdjDiagGate), cudaMemcpyHostToDevice,
+                              s->stream),
+           "upload diagonal groups");
+        CK(s, cudaMemcpyAsync(d_slots, dslots.data(), dslots.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                              s->stream),
+           "upload diagonal slots");
+    }
+
+    // reverse sweep
+    CK(s, cudaEventRecord(s->ev0, s->stream), "event");
+    CK(s, cudaMemcpyAsync(s->d_psi, s->d_state, bytes, cudaMemcpyDeviceToDevice, s->stream), "copy state");
+    CK(s, zxh::run_lambda(s->d_psi, s->d_lam, N, s->elem_bytes, d_terms, uint32_t(dt.size()), d_energy, s->sms,
+                          s->stream),
+       "lambda launch");
+    kernels++;
+    for (const RevStep &r : steps) {
+        switch (r.kind) {
+        case RevStep::RESTORE:
+            CK(s, cudaMemcpyAsync(s->d_psi, static_cast<uint8_t *>(s->d_ckpt) + r.ckpt * bytes, bytes,
+                                  cudaMemcpyDeviceToDevice, s->stream),
+               "restore checkpoint");
+            break;
+        case RevStep::PAIR:
+            CK(s, zxh::run_adj_pair(s->d_psi, s->d_lam, s->elem_bytes, r.pair, d_grads + r.slot, s->sms, s->stream),
+               "adjoint pair launch");
+            kernels++;
+            break;
+        case RevStep::DIAG:
+            CK(s, zxh::run_adj_diag(s->d_psi, s->d_lam, N, s->elem_bytes, d_gates + r.first, r.ng, d_grads,
+                                    d_slots + r.first, s->sms, s->stream),
+               "adjoint diagonal launch");
+            kernels++;
+            break;
+        }
+    }
+    CK(s, cudaEventRecord(s->ev1, s->stream), "event");
+    CK(s, cudaMemcpyAsync(value, d_energy, sizeof(double), cudaMemcpyDeviceToHost, s->stream), "read energy");
+    if (count)
+        CK(s, cudaMemcpyAsync(grads, d_grads, count * sizeof(double), cudaMemcpyDeviceToHost, s->stream),
+           "read gradients");
+    CK(s, cudaStreamSynchronize(s->stream), "adjoint sweep");
+    float rev_ms = 0.0f;
+    CK(s, cudaEventElapsedTime(&rev_ms, s->ev0, s->ev1), "event time");
+    s->last_ms = float(fwd_ms + double(rev_ms));
+    s->stat_kernels = kernels;
+    s->stat_passes = steps.size() + 1;
+    return ZXH_OK;
+}
+
+}  // extern "C"

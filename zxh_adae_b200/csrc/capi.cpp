@@ -3,8 +3,7 @@
 // stream and scratch; handles are independent (the reference keeps its diagonal
 // buckets and U3 descriptors in process-global statics, kernel_cuda.cu:91-142).
 #include "../../include/zxh_b200.h"
-#include "host.h"
-#include "sampler.h"
+#include "sim.h"
 
 #include <cuda_runtime.h>
 
@@ -18,46 +17,13 @@
 
 using zxh::Gate;
 
-struct zxh_sim {
-    size_t n = 0;
-    bool disable_x = false, eager = false;
-    int dtype = ZXH_C128, elem_bytes = 16, device = 0, sms = 148;
-    std::vector<Gate> gates;
-    bool use_seed = false;
-    uint64_t seed = 0;
-    std::string err;
-    cudaStream_t stream = nullptr;
-
-    void *d_state = nullptr;
-    size_t state_cap_bytes = 0;
-    int M = 0;
-    zxh::WalkState ws;
-    bool executed = false;
-
-    uint8_t *d_blob = nullptr;
-    size_t blob_cap = 0;
-    uint8_t *h_stage = nullptr;
-    size_t stage_cap = 0;
-    zxh::DevStatus *d_status = nullptr;
-    zxh::DevStatus *h_status = nullptr;
-
-    uint8_t *d_samp = nullptr;
-    size_t samp_cap = 0;
-    zxh::SamplerScratch sc;
-    size_t measured = 0;
-
-    void *d_out = nullptr;
-    size_t out_cap = 0;
-
-    uint64_t stat_kernels = 0, stat_passes = 0;
-    float last_ms = 0.0f;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    zxh::PlanParams pp;
-};
 
 namespace {
-
 thread_local std::string g_create_error;
+}  // namespace
+
+namespace zxh {
+namespace api {
 
 int fail(zxh_sim *s, int code, const std::string &msg)
 {
@@ -71,12 +37,6 @@ int cuda_fail(zxh_sim *s, cudaError_t e, const char *what)
     return fail(s, e == cudaErrorMemoryAllocation ? ZXH_ERR_OOM : ZXH_ERR_CUDA,
                 std::string(what) + ": " + cudaGetErrorString(e));
 }
-
-#define CK(s, call, what)                             \
-    do {                                              \
-        cudaError_t e_ = (call);                      \
-        if (e_ != cudaSuccess) return cuda_fail(s, e_, what); \
-    } while (0)
 
 int use_device(zxh_sim *s)
 {
@@ -115,7 +75,6 @@ int push(zxh_sim *s, uint32_t t, size_t cq, size_t q, double th, double la, doub
     return ZXH_OK;
 }
 
-const double kPi = 3.14159265358979323846;
 
 // Lowers one record the way the reference's recorders do (zxh.cpp:234-310).
 int lower(zxh_sim *s, const zxh_gate &g, std::vector<Gate> &out)
@@ -204,11 +163,12 @@ void column_tables(const zxh::AffineMap &A, uint64_t tab[8][256])
         }
 }
 
-}  // namespace
+}  // namespace api
 
-namespace zxh {
 void set_thread_error(const std::string &msg) { g_create_error = msg; }
 }  // namespace zxh
+
+using namespace zxh::api;
 
 extern "C" {
 
@@ -263,6 +223,10 @@ int zxh_destroy(zxh_sim *s)
     if (s->h_status) cudaFreeHost(s->h_status);
     if (s->d_samp) cudaFree(s->d_samp);
     if (s->d_out) cudaFree(s->d_out);
+    if (s->d_psi) cudaFree(s->d_psi);
+    if (s->d_lam) cudaFree(s->d_lam);
+    if (s->d_ckpt) cudaFree(s->d_ckpt);
+    if (s->d_adj) cudaFree(s->d_adj);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     if (s->stream) cudaStreamDestroy(s->stream);

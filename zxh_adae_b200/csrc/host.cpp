@@ -156,6 +156,8 @@ void left_mul(Acc &a, const cd n[4])
 
 }  // namespace
 
+void u3_matrix(double theta, double lambda, double phi, cd u[4]) { build_u3(theta, lambda, phi, u); }
+
 int walk(const Gate *gates, size_t count, bool disable_x, int M, WalkState &ws, std::vector<Op> &ops, std::string &err)
 {
     AffineMap &A = ws.map;

@@ -19,6 +19,10 @@ struct WalkState {
 int walk(const Gate *gates, size_t count, bool disable_x, int M, WalkState &ws, std::vector<Op> &ops,
          std::string &err);
 
+// U3(theta, lambda, phi) as the walk builds it (build_u3_matrix, zxh.cpp:101-113):
+// u00, u01, u10, u11.
+void u3_matrix(double theta, double lambda, double phi, cd u[4]);
+
 // calc_mem (zxh.cpp:648-681): real address bits the gate list needs.
 int calc_mem(const Gate *gates, size_t count, int n, bool disable_x);
 
