@@ -18,6 +18,16 @@ one read-modify-write pass of the state. The state (8 GiB) is larger than L2
                distribution on a 20-qubit complex128 state, timed with the
                reference's header-subtraction method, GB/s at 16 B/amplitude.
 
+* adjoint      the second half of the metric, on the 24-qubit, 432-parameter
+               hardware-efficient ansatz (8 x [RY, RZ on every qubit; CX chain] +
+               final RY/RZ, parameters uniform [-pi, pi)) with the TFIM observable
+               sum Z_i Z_{i+1} + sum X_i: gradients/s of one adjoint sweep
+               (complex64 state, FP64 reductions, checkpoint every 48 parameters)
+               against gradients/s of parameter shift (864 energies on the plain
+               forward path, complex64), both timed on the host through the public
+               API, and the max |error| of both against FP64 central differences
+               (step 1e-6) on the complex128 forward path. Rank 0 at N = 1 only.
+
 ``--impl reference`` runs that reference CPU backend alone and prints its line.
 Multi-GPU (``torchrun``): the path does not shard, each rank runs an independent
 replica; value is the sum over ranks, times are the max over ranks.
@@ -54,6 +64,7 @@ def parse():
     ap.add_argument("--qubits", type=int, default=N_QUBITS)
     ap.add_argument("--batch", type=int, default=BATCH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     return ap.parse_args()
 
 
@@ -242,6 +253,52 @@ def run_reference(args):
 # --------------------------------------------------------------------------- ours
 
 
+def adjoint_leg(local: int, n: int = 24, reps: int = 8, checkpoint_every: int = 48) -> dict:
+    """Adjoint gradients/s vs parameter-shift gradients/s on the same GPU."""
+    import zxh_adae_b200 as zx
+    from zxh_adae_b200 import adjoint as ad
+
+    circ = ad.hardware_efficient_ansatz(n, reps)
+    terms = ad.tfim_terms(n)
+    p = np.random.default_rng(2024).uniform(-np.pi, np.pi, circ.nparams)
+    s64 = zx.ZXH(n, dtype="complex64", device=local)
+    ad.adjoint(s64, circ, p, terms, checkpoint_every)  # warm-up
+    reps_t = 5
+    t0 = time.perf_counter()
+    for _ in range(reps_t):
+        e, g = ad.adjoint(s64, circ, p, terms, checkpoint_every)
+    t_adj = (time.perf_counter() - t0) / reps_t
+    kernels, passes, dev_ms = s64.last_stats()
+    ad.energy(s64, circ, p, terms)  # warm-up of the forward path
+    t0 = time.perf_counter()
+    g_ps = ad.parameter_shift(s64, circ, p, terms)
+    t_ps = time.perf_counter() - t0
+    s64.close()
+    s128 = zx.ZXH(n, dtype="complex128", device=local)
+    e128 = ad.energy(s128, circ, p, terms)
+    fd = ad.finite_difference(s128, circ, p, terms, 1e-6)
+    s128.close()
+    return {
+        "workload": f"{n}q complex64 hardware-efficient ansatz L={reps} (RY, RZ all + CX chain, final RY/RZ), "
+                    f"{circ.nparams} params, TFIM sum ZZ + 1.0 sum X (open)",
+        "params": circ.nparams,
+        "adjoint_ms": 1e3 * t_adj,
+        "adjoint_device_ms": dev_ms,
+        "adjoint_kernels": kernels,
+        "adjoint_grads_per_s": circ.nparams / t_adj,
+        "param_shift_s": t_ps,
+        "param_shift_grads_per_s": circ.nparams / t_ps,
+        "speedup": t_ps / t_adj,
+        "energy": e,
+        "energy_err_vs_c128": abs(e - e128),
+        "max_abs_err_vs_fp64_fd": float(np.max(np.abs(g - fd))),
+        "param_shift_max_abs_err_vs_fp64_fd": float(np.max(np.abs(g_ps - fd))),
+        "checkpoint_every": checkpoint_every,
+        "fd": "central differences, step 1e-6, complex128 forward path",
+    }
+
+
+
 def run_ours(args):
     world, rank, local, pg = dist_setup(args)
     import zxh_adae_b200 as zx
@@ -287,6 +344,9 @@ def run_ours(args):
 
     clocks = clk.summary()
     sim.close()
+    adj = None
+    if rank == 0 and world == 1 and not args.no_adjoint:
+        adj = adjoint_leg(local)
     if rank != 0:
         return
     line = {
@@ -323,6 +383,7 @@ def run_ours(args):
         "cpu_baseline": cpu,
         "gpu_launches": launches,
         "clocks": clocks,
+        "adjoint": adj,
     }
     print(json.dumps(line))
 

@@ -227,7 +227,10 @@ int zxh_plan_stats(size_t n, int disable_x, int eager_expand_all, int dtype, con
 /* Pass-planner tuning (used by the autotuner): tile_bits_c64, tile_bits_c128,
  * contig_bits, max_gates (generic tile pass), fast_gates (gates per fast U3
  * pass), fast_fuse_quad, fast_contig_c64, fast_contig_c128, row_wide_c64,
- * row_wide_c128 (shape of the strided high-qubit pass). Takes effect at the
+ * row_wide_c128 (shape of the strided high-qubit pass), diag_chunk_bits (log2
+ * tiles a warp of the diagonal pass walks in Gray-code order; -1 = automatic),
+ * diag_row_bits_c64, diag_row_bits_c128 (log2 rows of its warp tile).
+ * Takes effect at the
  * next zxh_execute / zxh_apply. No counterpart in the reference. */
 int zxh_set_param(zxh_sim *sim, const char *name, int value);
 

@@ -76,6 +76,23 @@ def test_diag_batch_and_cascade_16q(dtype):
 
 
 @pytest.mark.parametrize("dtype", DTYPES)
+@pytest.mark.parametrize("chunk_bits", [0, 1, 3, 6])
+def test_diag_pass_gray_code_chunks(dtype, chunk_bits):
+    # the diagonal pass walks chunks of 2^chunk_bits tiles in Gray-code order,
+    # updating the out-of-tile coefficients one flipped bit at a time
+    n = 17
+    gates = np.concatenate([wl.h_all(n), wl.diag_batch(n, 900, 8), wl.cp_cascade(n)])
+    o = Oracle(n)
+    o.push(gates)
+    o.execute()
+    s = zx.ZXH(n, dtype=dtype)
+    s.set_param("diag_chunk_bits", chunk_bits)
+    s.push_gates(gates)
+    s.execute()
+    assert max_err(s, o) <= TOL[dtype]
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
 def test_u3_matching_layers(dtype):
     gates = wl.u3_matching_layers(16, 6, seed=3)
     o, s = run_pair(16, gates, dtype)

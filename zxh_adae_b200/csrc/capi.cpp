@@ -590,6 +590,9 @@ int zxh_set_param(zxh_sim *s, const char *name, int value)
         {"fast_contig_c128", &s->pp.fast_contig_c128, 0, 10},
         {"row_wide_c64", &s->pp.row_wide_c64, 0, 1},
         {"row_wide_c128", &s->pp.row_wide_c128, 0, 1},
+        {"diag_chunk_bits", &s->pp.diag_chunk_bits, -1, 8},
+        {"diag_row_bits_c64", &s->pp.diag_row_bits_c64, 2, 4},
+        {"diag_row_bits_c128", &s->pp.diag_row_bits_c128, 2, 4},
     };
     for (const Entry &e : table)
         if (std::strcmp(e.key, name) == 0) {

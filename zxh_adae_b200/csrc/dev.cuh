@@ -51,6 +51,28 @@ __device__ __forceinline__ float2 phase_factor(const float2 *tab, int64_t th)
     return make_float2(t.x * c - t.y * s, t.x * s + t.y * c);
 }
 
+// exp(2 pi i th / 2^32) for complex64 amplitudes: the same 1024-entry table for
+// the top 10 bits of a 32-bit turn count, and a third-order Taylor step for the
+// low 22 bits (angle below 2 pi / 1024; truncation error below 1e-12). The low
+// bits become a float without a conversion instruction: they are placed in the
+// mantissa of 1.0f.
+__device__ __forceinline__ float2 phase_factor32(const float2 *tab, uint32_t th)
+{
+    const float2 t = tab[th >> 22];
+    const float f = __uint_as_float(0x3F800000u | ((th << 1) & 0x007FFFFEu));  // 1 + low22 / 2^22
+    const float eps = fmaf(f, 6.1359231515425650e-3f, -6.1359231515425650e-3f);  // low22 * 2 pi / 2^32
+    const float e2 = eps * eps;
+    const float s = fmaf(-eps * e2, 0.16666667f, eps);
+    const float c = fmaf(-0.5f, e2, 1.0f);
+    return make_float2(t.x * c - t.y * s, t.x * s + t.y * c);
+}
+
+// Nearest 32-bit turn count of a 64-bit one (both modulo a full turn).
+__device__ __forceinline__ uint32_t turns32(int64_t th)
+{
+    return static_cast<uint32_t>((static_cast<uint64_t>(th) + 0x80000000ULL) >> 32);
+}
+
 __device__ __forceinline__ double2 phase_factor(const double2 *tab, int64_t th)
 {
     const uint64_t u = static_cast<uint64_t>(th);

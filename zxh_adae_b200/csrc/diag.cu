@@ -9,14 +9,19 @@
 // fixed-point turns, so sums wrap exactly modulo 2 pi; multi-bit selectors stay as
 // general terms evaluated with parity bit tests on packed masks.
 //
-// Work split: each WARP owns tiles of 2^T contiguous amplitudes (T = 10 for
-// complex64: 16 rows of 64 amplitudes; T = 8 for complex128: 8 rows of 32). A lane
-// holds one 16-byte vector per row, all rows loaded before any is used, so every
-// warp keeps 4 KB (complex64) in flight with no block-level barrier in the loop.
-// Per tile the warp evaluates the tile-dependent coefficients lane-parallel (lane
-// k sums the cross terms of tile bit k) and shares them by shuffles; per amplitude
-// the phase is two int64 adds (Gray-code walk over rows + a row table) and one
-// table-plus-Taylor exp.
+// Work split: each WARP owns tiles of 2^T contiguous amplitudes: 2^ROWB rows of 64
+// amplitudes (complex64) or 32 (complex128); ROWB is a planner knob, 3 and 2 by
+// default (T = 9 and 7), the fastest on B200 at 30 qubits. A lane holds one 16-byte
+// vector per row, all rows loaded before any is used, with no block-level barrier
+// in the loop.
+// A warp takes chunks of 2^cb consecutive tiles and walks each chunk in Gray-code
+// order, so from one tile to the next a single out-of-tile bit o flips: the
+// tile-dependent coefficients (lane k: the cross sum of tile bit k; the out-of-tile
+// constant) move by one entry of dense cross / quadratic tables kept in shared
+// memory, and lane l keeps the gradient g_l of the constant with respect to
+// out-of-tile bit l. The per-tile cost is then independent of the window's size.
+// Per amplitude the phase is two adds (Gray-code walk over rows + a row table) and
+// one table-plus-Taylor exp; complex64 does that part in 32-bit turns.
 #include "core.h"
 #include "dev.cuh"
 #include "host.h"
@@ -30,27 +35,17 @@ namespace zxh {
 namespace {
 
 constexpr int kDiagGen = 32;  // general terms handled per window (more are split by the planner)
+constexpr int kDiagOut = 32;  // out-of-tile bits of the incremental walk (2^(32 + T) amplitudes at most)
+constexpr int kDiagTileMax = 10;
 
-template <typename E>
-struct DiagCfg;
-template <>
-struct DiagCfg<float2> {
-    static constexpr int ROWB = 4;  // log2 rows per warp tile
-};
-template <>
-struct DiagCfg<double2> {
-    static constexpr int ROWB = 3;
-};
-
-template <typename E>
+template <typename E, int ROWB>
 __global__ void __launch_bounds__(kThreads) diag_kernel(const uint8_t *__restrict__ blob, uint64_t doff, uint64_t toff,
-                                                        uint32_t T, uint64_t ntiles, E *__restrict__ state)
+                                                        uint32_t T, uint32_t nout, uint32_t cb, E *__restrict__ state)
 {
     using VT = typename ET<E>::VT;
     constexpr int V = ET<E>::V;
     constexpr int LV = (V == 2) ? 1 : 0;
     constexpr int F = 5 + LV;  // lane bits + vector bit
-    constexpr int ROWB = DiagCfg<E>::ROWB;
     constexpr int ROWS = 1 << ROWB;
     constexpr int WARPS = kThreads / 32;
 
@@ -60,15 +55,29 @@ __global__ void __launch_bounds__(kThreads) diag_kernel(const uint8_t *__restric
     const LinTerm *ol = reinterpret_cast<const LinTerm *>(blob + d.off_out_lin);
     const QuadTerm *oq = reinterpret_cast<const QuadTerm *>(blob + d.off_out_quad);
     const GenTerm *gt = reinterpret_cast<const GenTerm *>(blob + d.off_gen);
-    const uint32_t *kidx = reinterpret_cast<const uint32_t *>(blob + d.off_kidx);
 
     __shared__ E s_exp[1 << kExpTableBits];
     __shared__ int64_t s_qi[ROWS];
     __shared__ uint32_t s_gb[WARPS][kDiagGen];
+    __shared__ int64_t s_cross[kDiagTileMax][kDiagOut];  // [tile bit][out bit]
+    __shared__ int64_t s_quad[kDiagOut][kDiagOut];       // symmetric, zero diagonal
+    __shared__ int64_t s_lin[kDiagOut];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const E *tab = reinterpret_cast<const E *>(blob + toff);
     for (int i = tid; i < (1 << kExpTableBits); i += kThreads) s_exp[i] = tab[i];
+    for (int i = tid; i < kDiagOut * kDiagOut; i += kThreads) (&s_quad[0][0])[i] = 0;
+    for (int i = tid; i < kDiagTileMax * kDiagOut; i += kThreads) (&s_cross[0][0])[i] = 0;
+    if (tid < kDiagOut) s_lin[tid] = 0;
+    __syncthreads();
+    // every (tile bit, out bit), (out bit, out bit) and out bit occurs at most once
+    for (uint32_t q = uint32_t(tid); q < d.n_cross; q += kThreads) s_cross[cr[q].i][cr[q].j - T] = cr[q].coef;
+    for (uint32_t q = uint32_t(tid); q < d.n_out_quad; q += kThreads) {
+        const QuadTerm t = oq[q];
+        s_quad[t.i - T][t.j - T] = t.coef;
+        s_quad[t.j - T][t.i - T] = t.coef;
+    }
+    for (uint32_t q = uint32_t(tid); q < d.n_out_lin; q += kThreads) s_lin[ol[q].bit - T] = ol[q].coef;
 
     const int IB = int(T) > F ? int(T) - F : 0;
     const int NI = 1 << IB;
@@ -117,8 +126,28 @@ __global__ void __launch_bounds__(kThreads) diag_kernel(const uint8_t *__restric
     }
     __syncthreads();
 
+    const uint64_t nchunks = 1ULL << (nout - cb);
     const uint64_t stride = uint64_t(gridDim.x) * WARPS;
-    for (uint64_t tile = uint64_t(blockIdx.x) * WARPS + uint64_t(warp); tile < ntiles; tile += stride) {
+    for (uint64_t chunk = uint64_t(blockIdx.x) * WARPS + uint64_t(warp); chunk < nchunks; chunk += stride) {
+        const uint64_t t0 = chunk << cb;
+        // coefficients of the chunk's first tile, from the dense tables
+        int64_t da = 0, g = 0, h = 0;
+        if (lane < int(T))
+            for (uint32_t o = 0; o < nout; o++)
+                if ((t0 >> o) & 1) da += s_cross[lane][o];
+        if (lane < int(nout)) {
+            g = s_lin[lane];
+            for (uint32_t o = 0; o < nout; o++)
+                if ((t0 >> o) & 1) {
+                    g += s_quad[lane][o];
+                    if (int(o) < lane) h += s_quad[lane][o];
+                }
+            h = ((t0 >> lane) & 1) ? h + s_lin[lane] : 0;
+        }
+        int64_t kp = warp_sum_i64(h) + d.c0;
+
+    for (uint32_t it_t = 0; it_t < (1u << cb); it_t++) {
+        const uint64_t tile = t0 | uint64_t(it_t ^ (it_t >> 1));
         const uint64_t r = tile << T;  // out-of-tile real bits of this tile
         E *base = state + r;
 
@@ -131,22 +160,15 @@ __global__ void __launch_bounds__(kThreads) diag_kernel(const uint8_t *__restric
             if (it < NI && e0 < tile_elems) data[it] = __ldcs(reinterpret_cast<const VT *>(base + e0));
         }
 
-        // 2. tile coefficients: lane k < T owns tile bit k; every lane takes a share
-        //    of the out-of-tile constant
-        int64_t da = 0;
-        if (lane < int(T))
-            for (uint32_t q = kidx[lane]; q < kidx[lane + 1]; q++) {
-                const QuadTerm t = cr[q];
-                if ((r >> t.j) & 1) da += t.coef;
-            }
-        int64_t kp = 0;
-        for (uint32_t q = uint32_t(lane); q < d.n_out_lin; q += 32)
-            if ((r >> ol[q].bit) & 1) kp += ol[q].coef;
-        for (uint32_t q = uint32_t(lane); q < d.n_out_quad; q += 32) {
-            const QuadTerm t = oq[q];
-            if (((r >> t.i) & 1) && ((r >> t.j) & 1)) kp += t.coef;
+        // 2. one out-of-tile bit o flipped since the previous tile of the chunk
+        if (it_t > 0) {
+            const int o = __ffs(it_t) - 1;
+            const bool up = (tile >> o) & 1;
+            const int64_t go = __shfl_sync(0xffffffffu, g, o);
+            kp += up ? go : -go;
+            if (lane < int(nout)) g += up ? s_quad[o][lane] : -s_quad[o][lane];
+            if (lane < int(T)) da += up ? s_cross[lane][o] : -s_cross[lane][o];
         }
-        kp = warp_sum_i64(kp) + d.c0;
         if (ngen) {
             for (uint32_t q = uint32_t(lane); q < ngen; q += 32) {
                 const GenTerm t = gt[q];
@@ -173,7 +195,45 @@ __global__ void __launch_bounds__(kThreads) diag_kernel(const uint8_t *__restric
             for (int v = 0; v < V; v++) w[l][v] = (l < IB) ? (d.lin_in[F + l] + dk + rho[l][v]) : 0;
         }
 
-        // 3. rows in Gray-code order: one int64 add per amplitude walks the row bits
+        // 3. rows in Gray-code order: one add per amplitude walks the row bits.
+        //    complex64 carries the per-amplitude phase in 32-bit turns (2 pi / 2^32
+        //    resolution, a few ulp of rounding per amplitude).
+        if constexpr (V == 2) {
+            uint32_t a32[V], w32[ROWB][V];
+#pragma unroll
+            for (int v = 0; v < V; v++) {
+                a32[v] = turns32(acc[v]);
+#pragma unroll
+                for (int l = 0; l < ROWB; l++) w32[l][v] = turns32(w[l][v]);
+            }
+#pragma unroll
+            for (int it = 0; it < ROWS; it++) {
+                const uint32_t gi = uint32_t(it ^ (it >> 1));
+                if (it > 0) {
+                    const int fb = ctz_const(it);
+                    const bool up = (gi >> fb) & 1;
+#pragma unroll
+                    for (int v = 0; v < V; v++) a32[v] += up ? w32[fb][v] : 0u - w32[fb][v];
+                }
+                const uint32_t e0 = (uint32_t(lane) << LV) | (gi << F);
+                if (it >= NI || e0 >= tile_elems) continue;
+                const uint32_t qrow = turns32(s_qi[gi]);
+                VT x = data[it];
+#pragma unroll
+                for (int v = 0; v < V; v++) {
+                    uint32_t th = a32[v] + qrow;
+                    const uint32_t e = e0 | uint32_t(v);
+                    for (uint32_t q = 0; q < ngen; q++) {
+                        const uint32_t bb = s_gb[warp][q];
+                        const int s1 = par64(gt[q].a1_t & e) ^ int(bb & 1);
+                        const int s2 = par64(gt[q].a2_t & e) ^ int(bb >> 1);
+                        if (s1 & s2) th += turns32(gt[q].coef);
+                    }
+                    vset(x, v, cmul(vget(x, v), phase_factor32(reinterpret_cast<const float2 *>(s_exp), th)));
+                }
+                __stcs(reinterpret_cast<VT *>(base + e0), x);
+            }
+        } else {
 #pragma unroll
         for (int it = 0; it < ROWS; it++) {
             const uint32_t gi = uint32_t(it ^ (it >> 1));
@@ -201,35 +261,63 @@ __global__ void __launch_bounds__(kThreads) diag_kernel(const uint8_t *__restric
             }
             __stcs(reinterpret_cast<VT *>(base + e0), x);
         }
+        }
         if (ngen) __syncwarp();
+    }
     }
 }
 
 }  // namespace
 
-cudaError_t run_diag(const uint8_t *dblob, uint64_t doff, uint64_t toff, int m, int elem_bytes, void *state, int sms,
-                     cudaStream_t st)
+namespace {
+
+template <typename E, int ROWB>
+cudaError_t launch_diag(const uint8_t *dblob, uint64_t doff, uint64_t toff, int m, int chunk_bits, E *state, int sms,
+                        cudaStream_t st)
 {
-    const int Tfull = elem_bytes == 8 ? (6 + DiagCfg<float2>::ROWB) : (5 + DiagCfg<double2>::ROWB);
+    const int Tfull = (ET<E>::V == 2 ? 6 : 5) + ROWB;
     const int T = std::min(m, Tfull);
-    const uint64_t ntiles = 1ULL << (m - T);
-    const uint64_t ctas_needed = (ntiles + kThreads / 32 - 1) / (kThreads / 32);
+    const int nout = m - T;
+    if (nout > kDiagOut) return cudaErrorInvalidValue;
     int per_sm = 1;
-    if (elem_bytes == 8) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, diag_kernel<float2>, kThreads, 0);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, diag_kernel<double2>, kThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, diag_kernel<E, ROWB>, kThreads, 0);
     if (per_sm < 1) per_sm = 1;
+    // chunks of 2^cb tiles: at least 16 chunks per warp of a full grid (tail balance),
+    // at most 256 tiles per chunk
+    const uint64_t warps_full = uint64_t(sms) * uint64_t(per_sm) * (kThreads / 32);
+    int lw = 0;
+    while ((1ULL << lw) < 16 * warps_full) lw++;
+    const int cb = chunk_bits >= 0 ? std::min(chunk_bits, nout) : std::max(0, std::min(8, nout - lw));
+    const uint64_t nchunks = 1ULL << (nout - cb);
+    const uint64_t ctas_needed = (nchunks + kThreads / 32 - 1) / (kThreads / 32);
     const unsigned grid = unsigned(std::max<uint64_t>(1, std::min<uint64_t>(ctas_needed, uint64_t(sms) * uint64_t(per_sm))));
-    if (elem_bytes == 8)
-        diag_kernel<float2><<<grid, kThreads, 0, st>>>(dblob, doff, toff, uint32_t(T), ntiles, static_cast<float2 *>(state));
-    else
-        diag_kernel<double2><<<grid, kThreads, 0, st>>>(dblob, doff, toff, uint32_t(T), ntiles,
-                                                        static_cast<double2 *>(state));
+    diag_kernel<E, ROWB><<<grid, kThreads, 0, st>>>(dblob, doff, toff, uint32_t(T), uint32_t(nout), uint32_t(cb), state);
     return cudaGetLastError();
 }
 
-int diag_tile_bits(int elem_bytes)
+}  // namespace
+
+cudaError_t run_diag(const uint8_t *dblob, uint64_t doff, uint64_t toff, int m, int elem_bytes, int row_bits,
+                     int chunk_bits, void *state, int sms, cudaStream_t st)
 {
-    return elem_bytes == 8 ? (6 + DiagCfg<float2>::ROWB) : (5 + DiagCfg<double2>::ROWB);
+    if (elem_bytes == 8) {
+        auto *s = static_cast<float2 *>(state);
+        switch (row_bits) {
+        case 2: return launch_diag<float2, 2>(dblob, doff, toff, m, chunk_bits, s, sms, st);
+        case 3: return launch_diag<float2, 3>(dblob, doff, toff, m, chunk_bits, s, sms, st);
+        case 4: return launch_diag<float2, 4>(dblob, doff, toff, m, chunk_bits, s, sms, st);
+        default: return cudaErrorInvalidValue;
+        }
+    }
+    auto *s = static_cast<double2 *>(state);
+    switch (row_bits) {
+    case 2: return launch_diag<double2, 2>(dblob, doff, toff, m, chunk_bits, s, sms, st);
+    case 3: return launch_diag<double2, 3>(dblob, doff, toff, m, chunk_bits, s, sms, st);
+    case 4: return launch_diag<double2, 4>(dblob, doff, toff, m, chunk_bits, s, sms, st);
+    default: return cudaErrorInvalidValue;
+    }
 }
+
+int diag_tile_bits(int elem_bytes, int row_bits) { return (elem_bytes == 8 ? 6 : 5) + row_bits; }
 
 }  // namespace zxh

@@ -732,11 +732,14 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
     };
     auto standalone_diag = [&](int mm, const std::vector<DiagTerm> &w) {
         ensure_exp();
-        const int T = std::min(mm, diag_tile_bits(elem_bytes));
+        const int rb = elem_bytes == 8 ? pp.diag_row_bits_c64 : pp.diag_row_bits_c128;
+        const int T = std::min(mm, diag_tile_bits(elem_bytes, rb));
         TileDev g = make_geom(mm, T, std::vector<int>());
         Pass ps;
         ps.kind = Pass::DIAG;
         ps.m = mm;
+        ps.chunk_bits = pp.diag_chunk_bits;
+        ps.row_bits = rb;
         ps.geom = g;
         ps.off = compile_diag(out.blob, w, g);
         ps.off2 = exp_off;

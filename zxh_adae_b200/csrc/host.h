@@ -38,7 +38,10 @@ struct PlanParams {
     int row_wide_c64 = 0;       // strided high-qubit pass shape, complex64: 0 = 16-byte lanes x 16 rows, 1 = 8-byte x 32
     int row_wide_c128 = 1;      // complex128: 0 = 8 rows, 1 = 16 rows
     int max_steps = 16;
-    int diag_tile_bits = 12;    // tile size of a standalone diagonal pass
+    int diag_row_bits_c64 = 3;  // log2 rows of a warp tile in a diagonal pass (tile = 64 amplitudes x rows)
+    int diag_row_bits_c128 = 2; // same for complex128 (tile = 32 amplitudes x rows)
+    int diag_chunk_bits = -1;   // log2 tiles a warp walks in Gray-code order in a diagonal pass (-1: chosen
+                                // per launch so every warp of a full grid gets at least 16 chunks)
     int product_table_bits = 12;
 };
 
@@ -52,6 +55,8 @@ struct Pass {
     FastDev fast;                        // FAST
     RowPassDev row;                      // ROW
     int wide = 0;                        // ROW: kernel shape
+    int chunk_bits = -1;                 // DIAG: tiles per Gray-code chunk (log2, -1 = automatic)
+    int row_bits = 0;                    // DIAG: log2 rows of a warp tile
     std::vector<FastGateDev> fgates;     // FAST
 };
 
@@ -63,7 +68,7 @@ struct Plan {
 
 // Tile bits of the standalone diagonal pass (diag.cu) and of the fast U3 pass
 // (u3pass.cu), and the register bits of one fast-pass round.
-int diag_tile_bits(int elem_bytes);
+int diag_tile_bits(int elem_bytes, int row_bits);
 int fast_tile_bits(int elem_bytes);
 int fast_reg_bits(int elem_bytes);
 int row_reg_bits(int elem_bytes, int wide);

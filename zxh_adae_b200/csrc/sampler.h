@@ -38,9 +38,9 @@ cudaError_t run_sampler_real(const void *state, int elem_bytes, int m, uint64_t 
 struct Pass;
 cudaError_t run_passes(const std::vector<Pass> &passes, const uint8_t *dblob, void *state, int elem_bytes,
                        DevStatus *status, int sms, cudaStream_t st, uint64_t &kernels);
-cudaError_t run_diag(const uint8_t *dblob, uint64_t doff, uint64_t toff, int m, int elem_bytes, void *state, int sms,
+cudaError_t run_diag(const uint8_t *dblob, uint64_t doff, uint64_t toff, int m, int elem_bytes, int row_bits, int chunk_bits, void *state, int sms,
                      cudaStream_t st);
-int diag_tile_bits(int elem_bytes);
+int diag_tile_bits(int elem_bytes, int row_bits);
 cudaError_t run_fast_tile(const uint8_t *dblob, uint64_t foff, uint64_t toff, uint64_t ntiles, int elem_bytes,
                           void *state, DevStatus *status, int sms, cudaStream_t st);
 cudaError_t run_row_pass(const uint8_t *dblob, uint64_t poff, uint64_t toff, uint64_t nitems, int elem_bytes,
