@@ -1,23 +1,25 @@
 """Benchmark of the B200-native ZXH path (one JSON line on stdout, rank 0).
 
-Workload (configuration 2, the diagonal-batch microbenchmark): a 30-qubit
-complex64 state (8 GiB) prepared with H on every qubit; one step applies one
-batch of B = 4096 seeded random p/cp gates (50/50, angles uniform [0, 2 pi)) as
-one read-modify-write pass of the state. The state (8 GiB) is larger than L2
+Default workload (configuration 2, the diagonal-batch microbenchmark): a
+30-qubit complex64 state (8 GiB) prepared with H on every qubit; one step applies
+one batch of B = 4096 seeded random p/cp gates (50/50, angles uniform [0, 2 pi))
+as one read-modify-write pass of the state. The state (8 GiB) is larger than L2
 (126 MB), so no flush is needed between steps.
 
 * value        whole-job GB/s from the device time of the pass kernels
-               (algorithmic bytes 2 * 2^30 * 8 per step), inputs resident.
+               (algorithmic bytes 2 * 2^30 * 8 per pass), inputs resident.
 * e2e          the same metric through the C ABI (zxh_apply with host gate
                records: host planning, program upload, launch, status read-back),
                timed on the host around K calls.
-* roofline     the dominant kernel (the diagonal pass) against the measured HBM
-               copy bandwidth in MEASURED_PEAKS.json.
+* roofline     the dominant kernel against the measured HBM copy bandwidth in
+               MEASURED_PEAKS.json; traffic = its DRAM bytes per launch from the
+               committed ncu summary under profiles/.
 * cpu_baseline the reference ZXH-Sim OpenMP backend (compiled from its own sources
                into oracle/_ref) on a bounded sample: the same B = 4096 batch
-               distribution on a 20-qubit complex128 state, timed with the
+               distribution on an 18-qubit complex128 state, timed with the
                reference's header-subtraction method, GB/s at 16 B/amplitude.
-
+* u3_layer     the U3-batch half of the 30-qubit target: one layer of U3 on every
+               qubit of the same complex64 state, its passes and GB/s per pass.
 * adjoint      the second half of the metric, on the 24-qubit, 432-parameter
                hardware-efficient ansatz (8 x [RY, RZ on every qubit; CX chain] +
                final RY/RZ, parameters uniform [-pi, pi)) with the TFIM observable
@@ -28,9 +30,11 @@ one read-modify-write pass of the state. The state (8 GiB) is larger than L2
                API, and the max |error| of both against FP64 central differences
                (step 1e-6) on the complex128 forward path. Rank 0 at N = 1 only.
 
-``--impl reference`` runs that reference CPU backend alone and prints its line.
-Multi-GPU (``torchrun``): the path does not shard, each rank runs an independent
-replica; value is the sum over ranks, times are the max over ranks.
+``--workload u3`` / ``--workload adjoint`` time those legs alone (the commands the
+ncu summaries under profiles/ were taken with). ``--impl reference`` runs the
+reference CPU backend alone and prints its line. Multi-GPU (``torchrun``): the
+path does not shard, each rank runs an independent replica; value is the sum over
+ranks, times are the max over ranks.
 """
 from __future__ import annotations
 
@@ -64,7 +68,9 @@ def parse():
     ap.add_argument("--qubits", type=int, default=N_QUBITS)
     ap.add_argument("--batch", type=int, default=BATCH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--workload", default="diag", choices=["diag", "u3", "adjoint"])
+    ap.add_argument("--no-extras", action="store_true", help="skip the U3-layer and adjoint legs of the diag line")
+    ap.add_argument("--no-adjoint-checks", action="store_true", help="adjoint workload: skip parameter shift and FD")
     return ap.parse_args()
 
 
@@ -253,7 +259,8 @@ def run_reference(args):
 # --------------------------------------------------------------------------- ours
 
 
-def adjoint_leg(local: int, n: int = 24, reps: int = 8, checkpoint_every: int = 48) -> dict:
+def adjoint_leg(local: int, n: int = 24, reps: int = 8, checkpoint_every: int = 48, steps: int = 5,
+                warmup: int = 1, checks: bool = True) -> dict:
     """Adjoint gradients/s vs parameter-shift gradients/s on the same GPU."""
     import zxh_adae_b200 as zx
     from zxh_adae_b200 import adjoint as ad
@@ -262,41 +269,87 @@ def adjoint_leg(local: int, n: int = 24, reps: int = 8, checkpoint_every: int = 
     terms = ad.tfim_terms(n)
     p = np.random.default_rng(2024).uniform(-np.pi, np.pi, circ.nparams)
     s64 = zx.ZXH(n, dtype="complex64", device=local)
-    ad.adjoint(s64, circ, p, terms, checkpoint_every)  # warm-up
-    reps_t = 5
+    for _ in range(max(warmup, 1)):
+        ad.adjoint(s64, circ, p, terms, checkpoint_every)
+    dev = []
     t0 = time.perf_counter()
-    for _ in range(reps_t):
+    for _ in range(steps):
         e, g = ad.adjoint(s64, circ, p, terms, checkpoint_every)
-    t_adj = (time.perf_counter() - t0) / reps_t
-    kernels, passes, dev_ms = s64.last_stats()
-    ad.energy(s64, circ, p, terms)  # warm-up of the forward path
-    t0 = time.perf_counter()
-    g_ps = ad.parameter_shift(s64, circ, p, terms)
-    t_ps = time.perf_counter() - t0
-    s64.close()
-    s128 = zx.ZXH(n, dtype="complex128", device=local)
-    e128 = ad.energy(s128, circ, p, terms)
-    fd = ad.finite_difference(s128, circ, p, terms, 1e-6)
-    s128.close()
-    return {
+        dev.append(s64.last_stats()[2])
+    t_adj = (time.perf_counter() - t0) / steps
+    kernels = s64.last_stats()[0]
+    d = {
         "workload": f"{n}q complex64 hardware-efficient ansatz L={reps} (RY, RZ all + CX chain, final RY/RZ), "
                     f"{circ.nparams} params, TFIM sum ZZ + 1.0 sum X (open)",
         "params": circ.nparams,
         "adjoint_ms": 1e3 * t_adj,
-        "adjoint_device_ms": dev_ms,
+        "adjoint_device_ms": statistics.mean(dev),
         "adjoint_kernels": kernels,
         "adjoint_grads_per_s": circ.nparams / t_adj,
-        "param_shift_s": t_ps,
-        "param_shift_grads_per_s": circ.nparams / t_ps,
-        "speedup": t_ps / t_adj,
         "energy": e,
-        "energy_err_vs_c128": abs(e - e128),
-        "max_abs_err_vs_fp64_fd": float(np.max(np.abs(g - fd))),
-        "param_shift_max_abs_err_vs_fp64_fd": float(np.max(np.abs(g_ps - fd))),
         "checkpoint_every": checkpoint_every,
-        "fd": "central differences, step 1e-6, complex128 forward path",
     }
+    if checks:
+        ad.energy(s64, circ, p, terms)  # warm-up of the forward path
+        t0 = time.perf_counter()
+        g_ps = ad.parameter_shift(s64, circ, p, terms)
+        t_ps = time.perf_counter() - t0
+        s128 = zx.ZXH(n, dtype="complex128", device=local)
+        e128 = ad.energy(s128, circ, p, terms)
+        fd = ad.finite_difference(s128, circ, p, terms, 1e-6)
+        s128.close()
+        d.update({
+            "param_shift_s": t_ps,
+            "param_shift_grads_per_s": circ.nparams / t_ps,
+            "speedup": t_ps / t_adj,
+            "energy_err_vs_c128": abs(e - e128),
+            "max_abs_err_vs_fp64_fd": float(np.max(np.abs(g - fd))),
+            "param_shift_max_abs_err_vs_fp64_fd": float(np.max(np.abs(g_ps - fd))),
+            "fd": "central differences, step 1e-6, complex128 forward path",
+        })
+    s64.close()
+    return d
 
+
+def timed_applies(sim, batches, warmup, steps, pg, local):
+    """W untimed applies, then K timed ones: per-step device ms (CUDA events on the
+    library's stream around the pass kernels), launches, passes, host wall time."""
+    for k in range(warmup):
+        sim.apply(batches[k])
+    barrier(pg)
+    dev_ms, launches, passes = [], 0, 0
+    with Clocks(local) as clk:
+        t0 = time.perf_counter()
+        for k in range(steps):
+            sim.apply(batches[warmup + k])
+            kk, pp, ms = sim.last_stats()
+            dev_ms.append(ms)
+            launches += kk
+            passes += pp
+        wall = time.perf_counter() - t0
+    barrier(pg)
+    return dev_ms, launches, passes, wall, clk.summary()
+
+
+def u3_leg(local: int, n: int = N_QUBITS, steps: int = 5, warmup: int = 3) -> dict:
+    """One U3 layer (U3 on every qubit) per step on the n-qubit complex64 state."""
+    import zxh_adae_b200 as zx
+    from zxh_adae_b200 import workloads as wl
+
+    sim = zx.ZXH(n, dtype="complex64", device=local)
+    sim.push_gates(wl.h_all(n))
+    sim.execute()
+    layers = [wl.u3_layer(n, seed=500 + k) for k in range(warmup + steps)]
+    dev_ms, launches, passes, wall, _ = timed_applies(sim, layers, warmup, steps, None, local)
+    sim.close()
+    state = (1 << n) * 8
+    ms = sum(dev_ms) / steps
+    gbps = (passes / steps) * 2 * state / (ms / 1e3) / 1e9
+    peak, kind = peaks()
+    return {"workload": f"U3 on all {n} qubits of a complex64 state, random angles, one layer per step",
+            "ms_per_layer": ms, "passes_per_layer": passes / steps, "kernels_per_layer": launches / steps,
+            "pass_GBps": gbps, "frac_of_peak": gbps / peak, "peak": peak, "peak_kind": kind,
+            "bytes": "2 x state per pass (one read and one write)"}
 
 
 def run_ours(args):
@@ -307,46 +360,45 @@ def run_ours(args):
     n, B = args.qubits, args.batch
     dtype = "complex64"
     eb = 8
-    bytes_step = 2 * (1 << n) * eb
+    state = (1 << n) * eb
+    peak, peak_kind = peaks()
+    if args.workload == "adjoint":
+        if rank == 0:
+            d = adjoint_leg(local, n=n, reps=8, checkpoint_every=48, steps=args.steps, warmup=args.warmup,
+                            checks=not args.no_adjoint_checks)
+            print(json.dumps({"metric": METRIC, "workload": "adjoint", **d}))
+        return
     sim = zx.ZXH(n, dtype=dtype, device=local)
     sim.push_gates(wl.h_all(n))
     sim.execute()
-    batches = [wl.diag_batch(n, B, seed=rank * 100000 + k) for k in range(args.warmup + args.steps)]
-    for k in range(args.warmup):
-        sim.apply(batches[k])
-
-    # device-timed: kernel time of each step
-    barrier(pg)
-    dev_ms = []
-    launches = 0
-    with Clocks(local) as clk:
-        t0 = time.perf_counter()
-        for k in range(args.steps):
-            sim.apply(batches[args.warmup + k])
-            kk, _, ms = sim.last_stats()
-            dev_ms.append(ms)
-            launches += kk
-        wall = time.perf_counter() - t0
-    barrier(pg)
+    if args.workload == "u3":
+        batches = [wl.u3_layer(n, seed=rank * 100000 + k) for k in range(args.warmup + args.steps)]
+        desc = f"U3 layer on all {n} qubits, complex64, H-prepared, random angles per step"
+        dominant, traffic_file = "row_pass_kernel", f"row_pass_{n}q_c64.md"
+    else:
+        batches = [wl.diag_batch(n, B, seed=rank * 100000 + k) for k in range(args.warmup + args.steps)]
+        desc = f"diag-batch {n}q complex64, H-prepared, B={B} random p/cp (50/50) per step"
+        dominant, traffic_file = "diag_kernel", f"diag_pass_{n}q_c64.md"
+    dev_ms, launches, passes, wall, clocks = timed_applies(sim, batches, args.warmup, args.steps, pg, local)
+    sim.close()
+    bytes_step = (passes / args.steps) * 2 * state
     dev_total_ms = max_over_ranks(pg, sum(dev_ms), local)
     wall = max_over_ranks(pg, wall, local)
     value = world * args.steps * bytes_step / (dev_total_ms / 1e3) / 1e9
     e2e_value = world * args.steps * bytes_step / wall / 1e9
-    peak, peak_kind = peaks()
     achieved = bytes_step / (statistics.mean(dev_ms) / 1e3) / 1e9
-    traffic = profile_traffic(f"diag_pass_{n}q_c64.md")
+    traffic = profile_traffic(traffic_file)
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = ref_cpu_sample(3, 1, B)
-        if cpu is not None:
-            cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
-
-    clocks = clk.summary()
-    sim.close()
-    adj = None
-    if rank == 0 and world == 1 and not args.no_adjoint:
-        adj = adjoint_leg(local)
+    extras = {}
+    if rank == 0 and world == 1:
+        if not args.no_cpu_baseline and args.workload == "diag":
+            cpu = ref_cpu_sample(3, 1, B)
+            if cpu is not None:
+                cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        if not args.no_extras and args.workload == "diag":
+            extras["u3_layer"] = u3_leg(local, n)
+            extras["adjoint"] = adjoint_leg(local)
     if rank != 0:
         return
     line = {
@@ -363,15 +415,18 @@ def run_ours(args):
         "dtype": "c64",
         "data": "synthetic",
         "config": {
-            "workload": f"diag-batch {n}q complex64, H-prepared, B={B} random p/cp (50/50) per step",
+            "workload": desc,
             "qubits": n,
-            "batch": B,
-            "state_bytes": (1 << n) * eb,
-            "l2": "state larger than L2, no flush",
+            "batch": B if args.workload == "diag" else n,
+            "passes_per_step": passes / args.steps,
+            "state_bytes": state,
+            "l2": "state larger than L2, no flush" if state > 126 * 2**20 else "state fits in L2",
             "parallelism": f"replicas x{world}",
         },
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(B * 40), "d2h_bytes_per_step": 16},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(len(batches[0]) * 40),
+                "d2h_bytes_per_step": 16},
         "roofline": {
+            "kernel": dominant,
             "bound": "hbm",
             "achieved": achieved,
             "peak": peak,
@@ -383,7 +438,7 @@ def run_ours(args):
         "cpu_baseline": cpu,
         "gpu_launches": launches,
         "clocks": clocks,
-        "adjoint": adj,
+        **extras,
     }
     print(json.dumps(line))
 

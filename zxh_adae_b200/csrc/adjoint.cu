@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
 
 namespace zxh {
 
@@ -127,48 +128,51 @@ __global__ void __launch_bounds__(kThreads) adj_pair_kernel(E *__restrict__ psi,
     }
 }
 
-template <typename E>
+template <int NG>
+struct AdjDiagParams {
+    AdjDiagGate g[NG];
+    uint32_t slot[NG];
+    uint32_t ng;
+};
+
+// The group's gates travel as a kernel parameter, so every gate field is a
+// constant-bank operand of the instructions that use it rather than a register.
+template <typename E, int NG>
 __global__ void __launch_bounds__(kThreads) adj_diag_kernel(E *__restrict__ psi, E *__restrict__ lam, uint64_t n,
-                                                            const AdjDiagGate *__restrict__ gates, uint32_t ng,
-                                                            double *grads, const uint32_t *__restrict__ slots)
+                                                            const __grid_constant__ AdjDiagParams<NG> P,
+                                                            double *grads, const E *__restrict__ exp_tab)
 {
-    using R = typename ET<E>::R;
-    __shared__ AdjDiagGate sg[kAdjDiagMax];
+    __shared__ E s_exp[1 << kExpTableBits];
     __shared__ double sh[kThreads / 32];
-    if (threadIdx.x < ng) sg[threadIdx.x] = gates[threadIdx.x];
+    for (int i = threadIdx.x; i < (1 << kExpTableBits); i += kThreads) s_exp[i] = exp_tab[i];
     __syncthreads();
-    double acc[kAdjDiagMax];
+    double acc[NG];
 #pragma unroll
-    for (int j = 0; j < kAdjDiagMax; j++) acc[j] = 0.0;
+    for (int j = 0; j < NG; j++) acc[j] = 0.0;
     for (uint64_t r = uint64_t(blockIdx.x) * kThreads + threadIdx.x; r < n; r += uint64_t(gridDim.x) * kThreads) {
         const E p = psi[r], l = lam[r];
         const double w = dre(l) * dim(p) - dim(l) * dre(p);  // Im(conj(lambda) psi)
-        double th = 0.0;
+        int64_t th = 0;
 #pragma unroll
-        for (int j = 0; j < kAdjDiagMax; j++) {
-            if (j >= int(ng)) break;
-            const AdjDiagGate &G = sg[j];
+        for (int j = 0; j < NG; j++) {
+            if (j >= int(P.ng)) break;
+            const AdjDiagGate &G = P.g[j];
             const int s0 = par64(r & G.a0) ^ int(G.b0);
             const int s = G.two ? (s0 & (par64(r & G.a1) ^ int(G.b1))) : s0;
-            if (G.kind == 1) acc[j] += s0 ? -w : w;              // RZ: Im<lambda|Z|psi>
-            else if (G.kind == 2) acc[j] += s ? -2.0 * w : 0.0;  // P, CP: -2 Im<lambda|Pi1|psi>
-            if (s) th += G.theta;
+            acc[j] = fma(w, s ? G.m1 : G.m0, acc[j]);
+            th += s ? G.tq : 0;
         }
-        double sn, cs;
-        sincos(-th, &sn, &cs);
-        E a, b;
-        a.x = R(double(p.x) * cs - double(p.y) * sn);
-        a.y = R(double(p.x) * sn + double(p.y) * cs);
-        b.x = R(double(l.x) * cs - double(l.y) * sn);
-        b.y = R(double(l.x) * sn + double(l.y) * cs);
-        psi[r] = a;
-        lam[r] = b;
+        E ph;
+        if constexpr (ET<E>::V == 2) ph = phase_factor32(s_exp, turns32(-th));
+        else ph = phase_factor(s_exp, -th);
+        psi[r] = cmul(p, ph);
+        lam[r] = cmul(l, ph);
     }
 #pragma unroll
-    for (int j = 0; j < kAdjDiagMax; j++) {
-        if (j >= int(ng)) break;
+    for (int j = 0; j < NG; j++) {
+        if (j >= int(P.ng)) break;
         const double t = block_sum(acc[j], sh);
-        if (threadIdx.x == 0 && sg[j].kind) atomicAdd(&grads[slots[j]], t);
+        if (threadIdx.x == 0 && P.g[j].kind) atomicAdd(&grads[P.slot[j]], t);
     }
 }
 
@@ -211,19 +215,45 @@ cudaError_t run_adj_pair(void *psi, void *lam, int elem_bytes, const AdjPairDev 
     return cudaGetLastError();
 }
 
-cudaError_t run_adj_diag(void *psi, void *lam, int m, int elem_bytes, const AdjDiagGate *dgates, uint32_t ng,
-                         double *grads, const uint32_t *dslots, int sms, cudaStream_t st)
+namespace {
+
+template <typename E, int NG>
+cudaError_t launch_adj_diag(E *psi, E *lam, uint64_t n, const AdjDiagGate *gates, uint32_t ng, double *grads,
+                            const uint32_t *slots, const void *exp_tab, int sms, cudaStream_t st)
+{
+    AdjDiagParams<NG> P;
+    std::memset(&P, 0, sizeof(P));
+    for (uint32_t j = 0; j < ng; j++) {
+        P.g[j] = gates[j];
+        P.slot[j] = slots[j];
+    }
+    P.ng = ng;
+    adj_diag_kernel<E, NG><<<grid_for(n, sms), kThreads, 0, st>>>(psi, lam, n, P, grads, static_cast<const E *>(exp_tab));
+    return cudaGetLastError();
+}
+
+template <typename E>
+cudaError_t adj_diag_typed(E *psi, E *lam, uint64_t n, const AdjDiagGate *gates, uint32_t ng, double *grads,
+                           const uint32_t *slots, const void *exp_tab, int sms, cudaStream_t st)
+{
+    if (ng <= 8) return launch_adj_diag<E, 8>(psi, lam, n, gates, ng, grads, slots, exp_tab, sms, st);
+    if (ng <= 16) return launch_adj_diag<E, 16>(psi, lam, n, gates, ng, grads, slots, exp_tab, sms, st);
+    if (ng <= uint32_t(kAdjDiagMax))
+        return launch_adj_diag<E, kAdjDiagMax>(psi, lam, n, gates, ng, grads, slots, exp_tab, sms, st);
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace
+
+cudaError_t run_adj_diag(void *psi, void *lam, int m, int elem_bytes, const AdjDiagGate *gates, uint32_t ng,
+                         double *grads, const uint32_t *slots, const void *exp_tab, int sms, cudaStream_t st)
 {
     const uint64_t n = 1ULL << m;
     if (elem_bytes == 8)
-        adj_diag_kernel<float2><<<grid_for(n, sms), kThreads, 0, st>>>(static_cast<float2 *>(psi),
-                                                                      static_cast<float2 *>(lam), n, dgates, ng, grads,
-                                                                      dslots);
-    else
-        adj_diag_kernel<double2><<<grid_for(n, sms), kThreads, 0, st>>>(static_cast<double2 *>(psi),
-                                                                       static_cast<double2 *>(lam), n, dgates, ng,
-                                                                       grads, dslots);
-    return cudaGetLastError();
+        return adj_diag_typed(static_cast<float2 *>(psi), static_cast<float2 *>(lam), n, gates, ng, grads, slots,
+                              exp_tab, sms, st);
+    return adj_diag_typed(static_cast<double2 *>(psi), static_cast<double2 *>(lam), n, gates, ng, grads, slots,
+                          exp_tab, sms, st);
 }
 
 }  // namespace zxh

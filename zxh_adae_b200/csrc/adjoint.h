@@ -31,13 +31,16 @@ struct AdjPairDev {
 
 constexpr int kAdjDiagMax = 32;
 
-// One diagonal gate of a commuting group: phase theta where the selector (or
-// both selectors, two = 1) is 1. kind 0: no gradient (Z), 1: RZ, 2: P or CP.
+// One diagonal gate of a commuting group: phase tq (64-bit turns) where the
+// selector s (s0, or s0 and s1 when two = 1) is 1. Its gradient is
+// sum_r Im(conj(lambda_r) psi_r) * (s(r) ? m1 : m0): RZ m0 = 1, m1 = -1 (Im<lambda|Z|psi>);
+// P and CP m0 = 0, m1 = -2 (-2 Im<lambda|Pi_1|psi>); Z 0, 0.
 struct AdjDiagGate {
     uint64_t a0, a1;
     uint32_t b0, b1;
-    uint32_t kind, two;
-    double theta;
+    uint32_t kind, two;  // kind 0: no gradient
+    int64_t tq;
+    double m0, m1;
 };
 
 // lambda = H psi over 2^m amplitudes (lam may be null: energy only); adds
@@ -49,7 +52,10 @@ cudaError_t run_adj_pair(void *psi, void *lam, int elem_bytes, const AdjPairDev 
                          cudaStream_t st);
 // For each gate j of the group adds its gradient to grads[slots[j]], then
 // multiplies psi and lam by the inverse of the group's phase.
-cudaError_t run_adj_diag(void *psi, void *lam, int m, int elem_bytes, const AdjDiagGate *dgates, uint32_t ng,
-                         double *grads, const uint32_t *dslots, int sms, cudaStream_t st);
+// gates and slots are HOST arrays of ng <= kAdjDiagMax entries, passed to the
+// kernel by value (its constant bank); exp_tab: exp(2 pi i j / 1024) in the
+// state's element type (device memory).
+cudaError_t run_adj_diag(void *psi, void *lam, int m, int elem_bytes, const AdjDiagGate *gates, uint32_t ng,
+                         double *grads, const uint32_t *slots, const void *exp_tab, int sms, cudaStream_t st);
 
 }  // namespace zxh

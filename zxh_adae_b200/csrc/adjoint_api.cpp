@@ -118,18 +118,17 @@ struct RevStep {
     size_t ckpt = 0;   // RESTORE: checkpoint index
 };
 
-// Region layout of d_adj: grads | energy | terms | diag gates | diag slots.
+// Region layout of d_adj: grads | energy | terms | exp table.
 struct AdjLayout {
-    size_t grads, energy, terms, gates, slots, total;
-    AdjLayout(size_t ngrads, size_t nterms, size_t ndiag)
+    size_t grads, energy, terms, exp, total;
+    AdjLayout(size_t ngrads, size_t nterms)
     {
         auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
         grads = 0;
         energy = up(ngrads * sizeof(double));
         terms = energy + 256;
-        gates = up(terms + nterms * sizeof(TermDev));
-        slots = up(gates + ndiag * sizeof(AdjDiagGate));
-        total = up(slots + ndiag * sizeof(uint32_t)) + 256;
+        exp = up(terms + nterms * sizeof(TermDev));
+        total = exp + (size_t(16) << zxh::kExpTableBits);
     }
 };
 
@@ -225,7 +224,9 @@ int reverse_program(zxh_sim *s, const std::vector<size_t> &ends, AffineMap A, st
                 d.two = 1;
             }
             d.kind = g.type == zxh::G_Z ? 0 : g.type == zxh::G_RZ ? 1 : 2;
-            d.theta = g.type == zxh::G_Z ? kPi : g.theta;
+            d.tq = zxh::phase_turns(g.type == zxh::G_Z ? kPi : g.theta);
+            d.m0 = d.kind == 1 ? 1.0 : 0.0;
+            d.m1 = d.kind == 1 ? -1.0 : d.kind == 2 ? -2.0 : 0.0;
             dgates.push_back(d);
             dslots.push_back(uint32_t(gi));
             steps[size_t(open)].ng++;
@@ -283,7 +284,7 @@ int zxh_expectation(zxh_sim *s, const zxh_term *terms, size_t nterms, double *va
     if (int rc = use_device(s)) return rc;
     std::vector<TermDev> dt;
     if (int rc = compile_terms(s, terms, nterms, s->ws.map, s->ws.m, true, dt)) return rc;
-    const AdjLayout L(0, dt.size(), 0);
+    const AdjLayout L(0, dt.size());
     if (int rc = ensure_dev(s, reinterpret_cast<void **>(&s->d_adj), s->adj_cap, L.total, "cudaMalloc(adjoint)"))
         return rc;
     double *d_energy = reinterpret_cast<double *>(s->d_adj + L.energy);
@@ -346,25 +347,21 @@ int zxh_adjoint_gradient(zxh_sim *s, const zxh_term *terms, size_t nterms, size_
     const size_t bytes = size_t(s->elem_bytes) << N;
     if (int rc = ensure_dev(s, &s->d_psi, s->psi_cap, bytes, "cudaMalloc(adjoint psi)")) return rc;
     if (int rc = ensure_dev(s, &s->d_lam, s->lam_cap, bytes, "cudaMalloc(adjoint lambda)")) return rc;
-    const AdjLayout L(count, dt.size(), dgates.size());
+    const AdjLayout L(count, dt.size());
     if (int rc = ensure_dev(s, reinterpret_cast<void **>(&s->d_adj), s->adj_cap, L.total, "cudaMalloc(adjoint)"))
         return rc;
     double *d_grads = reinterpret_cast<double *>(s->d_adj + L.grads);
     double *d_energy = reinterpret_cast<double *>(s->d_adj + L.energy);
     auto *d_terms = reinterpret_cast<TermDev *>(s->d_adj + L.terms);
-    auto *d_gates = reinterpret_cast<AdjDiagGate *>(s->d_adj + L.gates);
-    auto *d_slots = reinterpret_cast<uint32_t *>(s->d_adj + L.slots);
     CK(s, cudaMemsetAsync(s->d_adj, 0, L.terms, s->stream), "reset gradients");
     if (!dt.empty())
         CK(s, cudaMemcpyAsync(d_terms, dt.data(), dt.size() * sizeof(TermDev), cudaMemcpyHostToDevice, s->stream),
            "upload terms");
+    std::vector<uint8_t> etab;
     if (!dgates.empty()) {
-        CK(s, cudaMemcpyAsync(d_gates, dgates.data(), dgates.size() * sizeof(AdjDiagGate), cudaMemcpyHostToDevice,
-                              s->stream),
-           "upload diagonal groups");
-        CK(s, cudaMemcpyAsync(d_slots, dslots.data(), dslots.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
-                              s->stream),
-           "upload diagonal slots");
+        zxh::exp_table(s->elem_bytes, etab);
+        CK(s, cudaMemcpyAsync(s->d_adj + L.exp, etab.data(), etab.size(), cudaMemcpyHostToDevice, s->stream),
+           "upload phase table");
     }
 
     // reverse sweep
@@ -387,8 +384,8 @@ int zxh_adjoint_gradient(zxh_sim *s, const zxh_term *terms, size_t nterms, size_
             kernels++;
             break;
         case RevStep::DIAG:
-            CK(s, zxh::run_adj_diag(s->d_psi, s->d_lam, N, s->elem_bytes, d_gates + r.first, r.ng, d_grads,
-                                    d_slots + r.first, s->sms, s->stream),
+            CK(s, zxh::run_adj_diag(s->d_psi, s->d_lam, N, s->elem_bytes, dgates.data() + r.first, r.ng, d_grads,
+                                    dslots.data() + r.first, s->d_adj + L.exp, s->sms, s->stream),
                "adjoint diagonal launch");
             kernels++;
             break;

@@ -550,6 +550,26 @@ TileDev make_geom(int m, int c, const std::vector<int> &dirs)
 
 }  // namespace
 
+int64_t phase_turns(double theta) { return turns(theta); }
+
+void exp_table(int elem_bytes, std::vector<uint8_t> &bytes)
+{
+    // exp(2 pi i j / 1024) rounded from long double, as the planner's passes use it
+    const int nt = 1 << kExpTableBits;
+    std::vector<double> t(2 * nt);
+    for (int j = 0; j < nt; j++) {
+        const long double a = 2.0L * 3.141592653589793238462643383279502884L * j / nt;
+        t[2 * j] = double(cosl(a));
+        t[2 * j + 1] = double(sinl(a));
+    }
+    if (elem_bytes == 8) {
+        std::vector<float> f(t.begin(), t.end());
+        bytes.assign(reinterpret_cast<const uint8_t *>(f.data()), reinterpret_cast<const uint8_t *>(f.data() + f.size()));
+    } else {
+        bytes.assign(reinterpret_cast<const uint8_t *>(t.data()), reinterpret_cast<const uint8_t *>(t.data() + t.size()));
+    }
+}
+
 void Plan::clear()
 {
     blob.clear();

@@ -23,6 +23,11 @@ int walk(const Gate *gates, size_t count, bool disable_x, int M, WalkState &ws, 
 // u00, u01, u10, u11.
 void u3_matrix(double theta, double lambda, double phi, cd u[4]);
 
+// theta / (2 pi) as a 64-bit fixed-point fraction of a turn (wraps modulo 2^64).
+int64_t phase_turns(double theta);
+// exp(2 pi i j / 2^kExpTableBits), j = 0..1023, as complex64 or complex128 bytes.
+void exp_table(int elem_bytes, std::vector<uint8_t> &bytes);
+
 // calc_mem (zxh.cpp:648-681): real address bits the gate list needs.
 int calc_mem(const Gate *gates, size_t count, int n, bool disable_x);
 

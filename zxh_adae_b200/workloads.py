@@ -70,6 +70,14 @@ def cp_cascade(n: int) -> np.ndarray:
     return as_records(recs)
 
 
+def u3_layer(n: int, seed: int) -> np.ndarray:
+    """U3 on every qubit, angles (theta, phi, lambda) uniform [0, 2 pi) drawn qubit
+    by qubit: one U3 batch of configuration 3, without its cz matching."""
+    rng = np.random.default_rng(seed)
+    ang = rng.uniform(0.0, TWO_PI, size=(n, 3))
+    return as_records([(U3, 0, q, ang[q][0], ang[q][2], ang[q][1]) for q in range(n)])
+
+
 def u3_matching_layers(n: int, layers: int, seed: int) -> np.ndarray:
     """`layers` x [U3 on every qubit (angles uniform [0, 2 pi)); cz on a random
     perfect matching] after H on every qubit (configuration 3, first part).
