@@ -217,10 +217,10 @@ int zxh_gate_count(const zxh_sim *sim, size_t *out);
 
 /* Host-only dry run of execute(): lowers the records, runs calc_mem, the
  * reference's execute() schedule and the pass planner, and launches nothing
- * (no CUDA call is made). out[10]: [0] M, [1] final real bits, [2..8] passes
+ * (no CUDA call is made). out[11]: [0] M, [1] final real bits, [2..9] passes
  * per kind (product, expand, tile, pair, diagonal, fast low-qubit, strided
- * high-qubit), [9] state passes (all but product). No counterpart in the
- * reference. */
+ * high-qubit, general strided), [10] state passes (all but product). No
+ * counterpart in the reference. */
 int zxh_plan_stats(size_t n, int disable_x, int eager_expand_all, int dtype, const zxh_gate *gates, size_t count,
                    uint64_t *out);
 
@@ -229,7 +229,9 @@ int zxh_plan_stats(size_t n, int disable_x, int eager_expand_all, int dtype, con
  * pass), fast_fuse_quad, fast_contig_c64, fast_contig_c128, row_wide_c64,
  * row_wide_c128 (shape of the strided high-qubit pass), diag_chunk_bits (log2
  * tiles a warp of the diagonal pass walks in Gray-code order; -1 = automatic),
- * diag_row_bits_c64, diag_row_bits_c128 (log2 rows of its warp tile).
+ * diag_row_bits_c64, diag_row_bits_c128 (log2 rows of its warp tile), grow (1:
+ * U3 batches whose pair deltas span several bits use the general strided pass,
+ * 0: the TMA tile / global pair passes).
  * Takes effect at the
  * next zxh_execute / zxh_apply. No counterpart in the reference. */
 int zxh_set_param(zxh_sim *sim, const char *name, int value);

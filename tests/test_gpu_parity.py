@@ -10,6 +10,7 @@ import pytest
 import zxh_adae_b200 as zx
 from oracle.bridge import Oracle
 from zxh_adae_b200 import workloads as wl
+from zxh_adae_b200._core import plan_stats
 
 pytestmark = pytest.mark.gpu
 TOL = {"complex128": 1e-12, "complex64": 1e-6}
@@ -90,6 +91,48 @@ def test_diag_pass_gray_code_chunks(dtype, chunk_bits):
     s.push_gates(gates)
     s.execute()
     assert max_err(s, o) <= TOL[dtype]
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+@pytest.mark.parametrize("n,seed", [(6, 1), (9, 2), (12, 3), (16, 4)])
+def test_general_strided_pass_after_cx_transport(dtype, n, seed):
+    # CX gates make the pair deltas span several real bits; those U3 batches run as
+    # general strided passes with their diagonal windows fused
+    gates = wl.random_circuit(n, 400, 300 + seed)
+    assert plan_stats(n, gates, dtype=dtype)["grow"] > 0
+    o, s = run_pair(n, gates, dtype)
+    assert max_err(s, o) <= TOL[dtype]
+    s2 = zx.ZXH(n, dtype=dtype)
+    s2.set_param("grow", 0)
+    s2.push_gates(gates)
+    s2.execute()
+    assert max_err(s2, o) <= TOL[dtype]
+
+
+@pytest.mark.parametrize("seed", range(24))
+def test_general_strided_pass_random(seed):
+    n = 6 + seed % 9
+    gates = wl.random_circuit(n, 250, 4000 + seed)
+    for dtype in DTYPES:
+        o, s = run_pair(n, gates, dtype)
+        assert max_err(s, o) <= TOL[dtype], (n, dtype, plan_stats(n, gates, dtype=dtype))
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_general_strided_pass_ansatz_and_hidden_string(dtype):
+    from zxh_adae_b200 import adjoint as ad
+
+    circ = ad.hardware_efficient_ansatz(12, 4)
+    rec = circ.records(np.random.default_rng(5).uniform(-3.1, 3.1, circ.nparams))
+    for eager in (False, True):
+        o, s = run_pair(12, rec, dtype, eager=eager)
+        assert max_err(s, o) <= TOL[dtype]
+    recs, secret = wl.hidden_string(13, seed=8)
+    o, s = run_pair(14, recs, dtype)
+    assert max_err(s, o) <= TOL[dtype]
+    s.set_seed(4)
+    s.measure(2000)
+    assert set((s.results_words() & ((1 << 13) - 1)).tolist()) == {secret}
 
 
 @pytest.mark.parametrize("dtype", DTYPES)

@@ -141,19 +141,19 @@ def as_terms(terms) -> np.ndarray:
     return out
 
 
-PASS_KINDS = ("product", "expand", "tile", "pair", "diagonal", "fast", "row")
+PASS_KINDS = ("product", "expand", "tile", "pair", "diagonal", "fast", "row", "grow")
 
 
 def plan_stats(n: int, gates, dtype: str = "complex64", disable_x: bool = False,
                eager_expand_all: bool = False) -> dict:
     """Host-only dry run of execute() (no GPU needed): state bits and pass counts."""
     rec = as_records(gates)
-    out = np.zeros(10, np.uint64)
+    out = np.zeros(11, np.uint64)
     rc = _lib.zxh_plan_stats(int(n), int(bool(disable_x)), int(bool(eager_expand_all)),
                              C64 if dtype == "complex64" else C128, rec.ctypes.data, len(rec), out.ctypes.data)
     if rc != 0:
         _raise(rc, None)
-    d = {"M": int(out[0]), "m": int(out[1]), "passes": int(out[9])}
+    d = {"M": int(out[0]), "m": int(out[1]), "passes": int(out[10])}
     d.update({k: int(out[2 + i]) for i, k in enumerate(PASS_KINDS)})
     return d
 

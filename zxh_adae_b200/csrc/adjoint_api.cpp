@@ -110,27 +110,92 @@ int compile_terms(zxh_sim *s, const zxh_term *terms, size_t nterms, AffineMap &A
 }
 
 struct RevStep {
-    enum Kind { PAIR, DIAG, RESTORE } kind;
+    enum Kind { PAIR, DIAG, RESTORE, GROW } kind;
     AdjPairDev pair;
     size_t slot = 0;   // PAIR: gradient slot
     size_t first = 0;  // DIAG: first gate in the uploaded group array
     uint32_t ng = 0;   // DIAG: gates in the group
     size_t ckpt = 0;   // RESTORE: checkpoint index
+    zxh::GrowBuild gb; // GROW: commuting 2x2 gates on distinct qubits, adjoint form
+    uint64_t off = 0;  // GROW: descriptor offset in the uploaded blob
 };
 
-// Region layout of d_adj: grads | energy | terms | exp table.
+// A run of 2x2 gates on distinct qubits with no CX between them, collected in
+// reverse order; closed into one general strided adjoint pass (or single pair
+// passes when the state is too small for one).
+struct PairGroup {
+    struct G {
+        zxh::U3Op op;
+        uint32_t gen;
+        uint32_t slot;
+        int q;
+    };
+    std::vector<G> gates;
+    std::vector<uint64_t> basis;  // reduced high parts of the register deltas
+    int nreg = 0;
+    // Whether g can join (distinct qubit, room, independent high part).
+    bool fits(const G &g, int F, int R, int m, int maxg) const
+    {
+        if (int(gates.size()) >= maxg) return false;
+        for (const G &h : gates)
+            if (h.q == g.q) return false;
+        uint64_t hp = g.op.delta >> F;
+        if (!hp) return true;
+        if (nreg >= R || m < F + nreg + 1) return false;
+        for (uint64_t b : basis)
+            if ((hp >> (63 - __builtin_clzll(b))) & 1) hp ^= b;
+        return hp != 0;
+    }
+    void add(const G &g, int F)
+    {
+        uint64_t hp = g.op.delta >> F;
+        if (hp) {
+            for (uint64_t b : basis)
+                if ((hp >> (63 - __builtin_clzll(b))) & 1) hp ^= b;
+            basis.push_back(hp);
+            std::sort(basis.begin(), basis.end(), [](uint64_t a, uint64_t b) { return a > b; });
+            nreg++;
+        }
+        gates.push_back(g);
+    }
+};
+
+// Region layout of d_adj: grads | energy | terms | exp table | grow-pass blob.
 struct AdjLayout {
-    size_t grads, energy, terms, exp, total;
-    AdjLayout(size_t ngrads, size_t nterms)
+    size_t grads, energy, terms, exp, grow, total;
+    AdjLayout(size_t ngrads, size_t nterms, size_t grow_bytes = 0)
     {
         auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
         grads = 0;
         energy = up(ngrads * sizeof(double));
         terms = energy + 256;
         exp = up(terms + nterms * sizeof(TermDev));
-        total = exp + (size_t(16) << zxh::kExpTableBits);
+        grow = up(exp + (size_t(16) << zxh::kExpTableBits));
+        total = grow + up(grow_bytes);
     }
 };
+
+// Descriptors of the general strided adjoint passes, packed into one blob.
+std::vector<uint8_t> pack_grow(std::vector<RevStep> &steps)
+{
+    std::vector<uint8_t> blob;
+    auto put = [&](const void *p, size_t n) -> uint64_t {
+        const uint64_t off = (blob.size() + 15) & ~uint64_t(15);
+        blob.resize(off + n + 16, 0);
+        if (n) std::memcpy(blob.data() + off, p, n);
+        return off;
+    };
+    for (RevStep &r : steps) {
+        if (r.kind != RevStep::GROW) continue;
+        zxh::GrowBuild &gb = r.gb;
+        gb.dev.nsel = uint32_t(gb.sels.size());
+        gb.dev.off_gates = put(gb.gates.data(), gb.gates.size() * sizeof(zxh::GrowGateDev));
+        gb.dev.off_sel = put(gb.sels.data(), gb.sels.size() * sizeof(zxh::GrowSelDev));
+        gb.dev.off_terms[0] = gb.dev.off_terms[1] = put(nullptr, 0);
+        r.off = put(&gb.dev, sizeof(zxh::GrowDev));
+    }
+    return blob;
+}
 
 // Forward pass in segments [0, ends[0]), [ends[0], ends[1]), ... with every qubit
 // expanded; the state after segment k < ends.size() - 1 is saved as checkpoint k.
@@ -185,8 +250,44 @@ int reverse_program(zxh_sim *s, const std::vector<size_t> &ends, AffineMap A, st
     const size_t count = s->gates.size();
     long open = -1;                    // diagonal group being filled
     size_t next_ck = ends.size() - 1;  // checkpoints are restored from the last one down
+    const int F = zxh::grow_fixed_bits(s->elem_bytes), R = zxh::grow_reg_bits(s->elem_bytes, true);
+    const int maxg = zxh::grow_adjoint_gates();
+    PairGroup pg;
+    auto close_pairs = [&]() {
+        if (pg.gates.empty()) return;
+        std::vector<uint64_t> regs;
+        for (const PairGroup::G &g : pg.gates)
+            if (g.op.delta >> F) regs.push_back(g.op.delta);
+        RevStep r;
+        r.kind = RevStep::GROW;
+        bool ok = N >= F && r.gb.init(s->elem_bytes, N, regs);
+        for (const PairGroup::G &g : pg.gates) ok = ok && r.gb.add_gate(g.op, g.gen, g.slot, true);
+        if (ok) {
+            steps.push_back(r);
+        } else {  // one global pair pass per gate
+            for (const PairGroup::G &g : pg.gates) {
+                RevStep p;
+                p.kind = RevStep::PAIR;
+                std::memset(&p.pair, 0, sizeof(p.pair));
+                p.pair.m = uint32_t(N);
+                p.pair.pivot = uint32_t(__builtin_ctzll(g.op.delta));
+                p.pair.delta = g.op.delta;
+                p.pair.alpha = g.op.sel.alpha;
+                p.pair.beta = uint32_t(g.op.sel.beta);
+                p.pair.gen = g.gen;
+                for (int k = 0; k < 4; k++) {
+                    p.pair.u[2 * k] = g.op.u[k].real();
+                    p.pair.u[2 * k + 1] = g.op.u[k].imag();
+                }
+                p.slot = g.slot;
+                steps.push_back(p);
+            }
+        }
+        pg = PairGroup();
+    };
     for (size_t gi = count; gi-- > 0;) {
         if (next_ck > 0 && ends[next_ck - 1] == gi + 1) {
+            close_pairs();
             next_ck--;
             RevStep r;
             r.kind = RevStep::RESTORE;
@@ -198,6 +299,7 @@ int reverse_program(zxh_sim *s, const std::vector<size_t> &ends, AffineMap A, st
         switch (g.type) {
         case zxh::G_X: A.flip_b(int(g.q)); break;
         case zxh::G_CX:
+            close_pairs();
             A.row_xor(int(g.q), int(g.cq));
             A.b_xor(int(g.q), int(g.cq));
             break;
@@ -205,6 +307,7 @@ int reverse_program(zxh_sim *s, const std::vector<size_t> &ends, AffineMap A, st
         case zxh::G_RZ:
         case zxh::G_P:
         case zxh::G_CP: {
+            close_pairs();
             if (open < 0 || steps[size_t(open)].ng == uint32_t(zxh::kAdjDiagMax)) {
                 RevStep r;
                 r.kind = RevStep::DIAG;
@@ -235,33 +338,24 @@ int reverse_program(zxh_sim *s, const std::vector<size_t> &ends, AffineMap A, st
         case zxh::G_H:
         case zxh::G_U3: {
             open = -1;
-            RevStep r;
-            r.kind = RevStep::PAIR;
-            std::memset(&r.pair, 0, sizeof(r.pair));
+            PairGroup::G pgt;
             uint64_t delta = 0;
             if (!A.solve(int(g.q), delta)) return fail(s, ZXH_ERR_STATE, "adjoint sweep: qubit outside the map");
-            delta &= zxh::low_mask(N);
-            const zxh::Sel sl = A.selector(int(g.q));
-            r.pair.m = uint32_t(N);
-            r.pair.pivot = uint32_t(__builtin_ctzll(delta));
-            r.pair.delta = delta;
-            r.pair.alpha = sl.alpha;
-            r.pair.beta = uint32_t(sl.beta);
-            r.pair.gen = pair_generator(g);
-            zxh::cd u[4];
-            if (g.type == zxh::G_H) zxh::u3_matrix(kPi / 2.0, kPi, 0.0, u);
-            else zxh::u3_matrix(g.theta, g.lambda, g.phi, u);
-            for (int k = 0; k < 4; k++) {
-                r.pair.u[2 * k] = u[k].real();
-                r.pair.u[2 * k + 1] = u[k].imag();
-            }
-            r.slot = gi;
-            steps.push_back(r);
+            pgt.op.delta = delta & zxh::low_mask(N);
+            pgt.op.sel = A.selector(int(g.q));
+            if (g.type == zxh::G_H) zxh::u3_matrix(kPi / 2.0, kPi, 0.0, pgt.op.u);
+            else zxh::u3_matrix(g.theta, g.lambda, g.phi, pgt.op.u);
+            pgt.gen = pair_generator(g);
+            pgt.slot = uint32_t(gi);
+            pgt.q = int(g.q);
+            if (!pg.fits(pgt, F, R, N, maxg)) close_pairs();
+            pg.add(pgt, F);
             break;
         }
         default: break;
         }
     }
+    close_pairs();
     return ZXH_OK;
 }
 
@@ -347,9 +441,13 @@ int zxh_adjoint_gradient(zxh_sim *s, const zxh_term *terms, size_t nterms, size_
     const size_t bytes = size_t(s->elem_bytes) << N;
     if (int rc = ensure_dev(s, &s->d_psi, s->psi_cap, bytes, "cudaMalloc(adjoint psi)")) return rc;
     if (int rc = ensure_dev(s, &s->d_lam, s->lam_cap, bytes, "cudaMalloc(adjoint lambda)")) return rc;
-    const AdjLayout L(count, dt.size());
+    const std::vector<uint8_t> gblob = pack_grow(steps);
+    const AdjLayout L(count, dt.size(), gblob.size());
     if (int rc = ensure_dev(s, reinterpret_cast<void **>(&s->d_adj), s->adj_cap, L.total, "cudaMalloc(adjoint)"))
         return rc;
+    if (!gblob.empty())
+        CK(s, cudaMemcpyAsync(s->d_adj + L.grow, gblob.data(), gblob.size(), cudaMemcpyHostToDevice, s->stream),
+           "upload pass descriptors");
     double *d_grads = reinterpret_cast<double *>(s->d_adj + L.grads);
     double *d_energy = reinterpret_cast<double *>(s->d_adj + L.energy);
     auto *d_terms = reinterpret_cast<TermDev *>(s->d_adj + L.terms);
@@ -381,6 +479,12 @@ int zxh_adjoint_gradient(zxh_sim *s, const zxh_term *terms, size_t nterms, size_
         case RevStep::PAIR:
             CK(s, zxh::run_adj_pair(s->d_psi, s->d_lam, s->elem_bytes, r.pair, d_grads + r.slot, s->sms, s->stream),
                "adjoint pair launch");
+            kernels++;
+            break;
+        case RevStep::GROW:
+            CK(s, zxh::run_grow(s->d_adj + L.grow, r.off, 0, int(r.gb.regs.size()), r.gb.dev.nitems, s->elem_bytes,
+                                s->d_psi, s->d_lam, d_grads, s->sms, s->stream),
+               "adjoint strided launch");
             kernels++;
             break;
         case RevStep::DIAG:

@@ -565,12 +565,12 @@ int zxh_plan_stats(size_t n, int disable_x, int eager_expand_all, int dtype, con
     if (int rc = zxh::walk(gl.data(), gl.size(), disable_x != 0, M, ws, ops, err)) return fail(nullptr, rc, err);
     zxh::Plan pl;
     if (int rc = zxh::plan(ops, eb, tmp.pp, start, pl, err)) return fail(nullptr, rc, err);
-    for (int k = 0; k < 10; k++) out[k] = 0;
+    for (int k = 0; k < 11; k++) out[k] = 0;
     out[0] = uint64_t(M);
     out[1] = uint64_t(ws.m);
     for (const zxh::Pass &p : pl.passes) {
         out[2 + int(p.kind)]++;
-        if (p.kind != zxh::Pass::PRODUCT) out[9]++;
+        if (p.kind != zxh::Pass::PRODUCT) out[10]++;
     }
     return ZXH_OK;
 }
@@ -591,6 +591,7 @@ int zxh_set_param(zxh_sim *s, const char *name, int value)
         {"row_wide_c64", &s->pp.row_wide_c64, 0, 1},
         {"row_wide_c128", &s->pp.row_wide_c128, 0, 1},
         {"diag_chunk_bits", &s->pp.diag_chunk_bits, -1, 8},
+        {"grow", &s->pp.grow, 0, 1},
         {"diag_row_bits_c64", &s->pp.diag_row_bits_c64, 2, 4},
         {"diag_row_bits_c128", &s->pp.diag_row_bits_c128, 2, 4},
     };

@@ -237,6 +237,57 @@ struct RowPassDev {
     uint64_t off_pre, off_post;
 };
 
+// General strided pass (grow.cu): like RowPassDev, but the R register
+// coordinates are arbitrary pair deltas (several bits each, as after CX
+// transport). A thread's row k holds the amplitudes at r0 ^ D[k] ^ (lane, vector)
+// with D[k] = xor of delta_i over the set bits i of k; items r0 enumerate the
+// addresses with zeros at bits [0, F) and at the pivot bits of the deltas'
+// high parts. Gates whose delta lies inside [0, F) are lane gates (partner by
+// shfl.xor / vector slot). Selectors are evaluated as parity(alpha & r0) (one
+// per lane, ballot) xor a per-thread lane part; a gate's own selector depends on
+// the row only through its own register coordinate.
+constexpr int kGrowMaxSel = 64;
+constexpr int kGrowMaxGates = 16;
+constexpr int kGrowMaxTerms = 128;
+
+struct GrowGateDev {
+    uint32_t kind;    // 0: register coordinate `reg`; 1: lane gate
+    uint32_t reg;
+    uint32_t lane_x;  // lane gate: partner lane xor
+    uint32_t vec_x;   // lane gate: partner vector-slot xor (complex64)
+    uint32_t sel;     // index of the gate's selector
+    uint32_t gen;     // adjoint passes: gradient generator (0 none, 1 Y, 2 X)
+    uint32_t slot;    // adjoint passes: gradient slot
+    uint32_t pad;
+    double u[8];      // u00, u01, u10, u11 (re, im); adjoint passes hold U^dagger
+};
+
+struct GrowSelDev {
+    uint64_t alpha;
+    uint32_t beta;
+    int32_t kbit;     // register coordinate the selector flips with, -1 if none
+};
+
+// One window term: phase coef (64-bit turns) where selector s0 (and s1 unless
+// s1 == 0xffff) is 1.
+struct GrowTermDev {
+    uint16_t s0, s1;
+    uint32_t pad;
+    int64_t coef;
+};
+
+struct GrowDev {
+    uint32_t m, F, R, ngates;
+    uint64_t D[16];
+    uint8_t piv[4];          // pivot bits, ascending
+    uint32_t nsel;
+    uint32_t ncls[2][3];     // pre / post window: end of class 0 (one selector, no row dependence),
+                             // end of class 1 (two selectors, no row dependence), total terms
+    uint64_t nitems;
+    uint64_t off_gates, off_sel;
+    uint64_t off_terms[2];
+};
+
 // Status word shared with the device (bounded waits report here).
 struct DevStatus { uint32_t code; uint32_t where; uint64_t info; };
 

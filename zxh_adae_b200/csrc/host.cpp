@@ -552,6 +552,151 @@ TileDev make_geom(int m, int c, const std::vector<int> &dirs)
 
 int64_t phase_turns(double theta) { return turns(theta); }
 
+// ---------------------------------------------------------------------------
+// General strided pass records (grow.cu)
+
+bool GrowBuild::init(int eb, int mm, const std::vector<uint64_t> &rg)
+{
+    elem_bytes = eb;
+    m = mm;
+    regs = rg;
+    gates.clear();
+    sels.clear();
+    terms[0].clear();
+    terms[1].clear();
+    std::memset(&dev, 0, sizeof(dev));
+    const int F = grow_fixed_bits(eb);
+    const int R = int(regs.size());
+    if (R > 4 || m < F + R) return false;
+    // reduced high parts with distinct leading bits: the items enumerate the
+    // addresses with zeros at [0, F) and at those leading bits (coset representatives)
+    std::vector<uint64_t> basis;  // sorted by leading bit, descending
+    std::vector<int> piv;
+    for (uint64_t d : regs) {
+        uint64_t h = d >> F;
+        for (uint64_t b : basis)
+            if ((h >> (63 - __builtin_clzll(b))) & 1) h ^= b;
+        if (!h) return false;  // dependent
+        basis.push_back(h);
+        std::sort(basis.begin(), basis.end(), [](uint64_t a, uint64_t b) { return a > b; });
+        piv.push_back(63 - __builtin_clzll(h) + F);
+    }
+    std::sort(piv.begin(), piv.end());
+    dev.m = uint32_t(m);
+    dev.F = uint32_t(F);
+    dev.R = uint32_t(R);
+    for (int i = 0; i < R; i++) dev.piv[i] = uint8_t(piv[size_t(i)]);
+    for (int k = 0; k < (1 << R); k++) {
+        uint64_t D = 0;
+        for (int i = 0; i < R; i++)
+            if ((k >> i) & 1) D ^= regs[size_t(i)];
+        dev.D[k] = D;
+    }
+    dev.nitems = 1ULL << (m - F - R);
+    return true;
+}
+
+int GrowBuild::selector(const Sel &s)
+{
+    const uint64_t a = s.alpha & low_mask(m);
+    for (size_t i = 0; i < sels.size(); i++)
+        if (sels[i].alpha == a && sels[i].beta == uint32_t(s.beta)) return int(i);
+    if (sels.size() >= size_t(kGrowMaxSel)) return -1;
+    int kb = -1;
+    for (size_t i = 0; i < regs.size(); i++)
+        if (parity64(a & regs[i])) {
+            if (kb >= 0) return -1;  // flips with two register coordinates
+            kb = int(i);
+        }
+    GrowSelDev d;
+    d.alpha = a;
+    d.beta = uint32_t(s.beta);
+    d.kbit = kb;
+    sels.push_back(d);
+    return int(sels.size()) - 1;
+}
+
+bool GrowBuild::add_gate(const U3Op &u, uint32_t gen, uint32_t slot, bool adjoint_matrix)
+{
+    if (gates.size() >= size_t(kGrowMaxGates) || u.has_ctrl || !u.delta) return false;
+    const int F = int(dev.F);
+    GrowGateDev g;
+    std::memset(&g, 0, sizeof(g));
+    const int sel = selector(u.sel);
+    if (sel < 0) return false;
+    int reg = -1;
+    for (size_t i = 0; i < regs.size(); i++)
+        if (regs[i] == u.delta) reg = int(i);
+    if (reg >= 0) {
+        if (sels[size_t(sel)].kbit != reg) return false;
+        g.kind = 0;
+        g.reg = uint32_t(reg);
+    } else {
+        if ((u.delta >> F) != 0 || sels[size_t(sel)].kbit != -1) return false;
+        const int LV = elem_bytes == 8 ? 1 : 0;
+        g.kind = 1;
+        g.lane_x = uint32_t((u.delta >> LV) & 31);
+        g.vec_x = LV ? uint32_t(u.delta & 1) : 0;
+    }
+    g.sel = uint32_t(sel);
+    g.gen = gen;
+    g.slot = slot;
+    cd w[4] = {u.u[0], u.u[1], u.u[2], u.u[3]};
+    if (adjoint_matrix) {  // U^dagger
+        w[0] = std::conj(u.u[0]);
+        w[1] = std::conj(u.u[2]);
+        w[2] = std::conj(u.u[1]);
+        w[3] = std::conj(u.u[3]);
+    }
+    for (int q = 0; q < 4; q++) {
+        g.u[2 * q] = w[q].real();
+        g.u[2 * q + 1] = w[q].imag();
+    }
+    gates.push_back(g);
+    dev.ngates = uint32_t(gates.size());
+    return true;
+}
+
+bool GrowBuild::add_window(int which, const std::vector<DiagTerm> &w)
+{
+    const size_t mark = sels.size();
+    std::vector<GrowTermDev> cls[3];
+    for (const DiagTerm &t : w) {
+        GrowTermDev d;
+        std::memset(&d, 0, sizeof(d));
+        const int s0 = selector(t.s0);
+        const int s1 = t.two ? selector(t.s1) : 0xffff;
+        if (s0 < 0 || s1 < 0) {
+            sels.resize(mark);
+            return false;
+        }
+        d.s0 = uint16_t(s0);
+        d.s1 = uint16_t(s1);
+        d.coef = turns(t.theta);
+        const bool k0 = sels[size_t(s0)].kbit >= 0;
+        const bool k1 = t.two && sels[size_t(s1)].kbit >= 0;
+        if (t.two && s0 == s1) {  // S and S = S
+            d.s1 = 0xffff;
+            cls[k0 ? 2 : 0].push_back(d);
+        } else if (!t.two) {
+            cls[k0 ? 2 : 0].push_back(d);
+        } else {
+            cls[(k0 || k1) ? 2 : 1].push_back(d);
+        }
+    }
+    const size_t n = cls[0].size() + cls[1].size() + cls[2].size();
+    if (n > size_t(kGrowMaxTerms)) {
+        sels.resize(mark);
+        return false;
+    }
+    terms[which].clear();
+    for (int c = 0; c < 3; c++) terms[which].insert(terms[which].end(), cls[c].begin(), cls[c].end());
+    dev.ncls[which][0] = uint32_t(cls[0].size());
+    dev.ncls[which][1] = uint32_t(cls[0].size() + cls[1].size());
+    dev.ncls[which][2] = uint32_t(n);
+    return true;
+}
+
 void exp_table(int elem_bytes, std::vector<uint8_t> &bytes)
 {
     // exp(2 pi i j / 1024) rounded from long double, as the planner's passes use it
@@ -854,6 +999,62 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
         return int(out.passes.size()) - 1;
     };
 
+    const int fgrow = grow_fixed_bits(elem_bytes), rgrow = grow_reg_bits(elem_bytes, false);
+    auto grow_ok = [&](const Op &op) {
+        if (op.m < fgrow) return false;
+        for (const U3Op &u : op.u3)
+            if (u.has_ctrl || !u.delta) return false;
+        return true;
+    };
+    // General strided passes for one batch: lane gates (delta inside the low
+    // fgrow bits) ride in the first pass; the rest go in groups of up to rgrow
+    // whose high parts are linearly independent.
+    auto emit_grow = [&](const Op &op) -> bool {
+        const int mm = op.m;
+        std::vector<const U3Op *> lane, rest;
+        for (const U3Op &u : op.u3) ((u.delta >> fgrow) == 0 ? lane : rest).push_back(&u);
+        std::vector<std::vector<const U3Op *>> groups;
+        std::vector<const U3Op *> remaining = rest;
+        while (!remaining.empty()) {
+            std::vector<const U3Op *> grp, defer;
+            std::vector<uint64_t> basis;
+            for (const U3Op *u : remaining) {
+                if (int(grp.size()) == rgrow || mm < fgrow + int(grp.size()) + 1) {
+                    defer.push_back(u);
+                    continue;
+                }
+                uint64_t h = u->delta >> fgrow;
+                for (uint64_t b : basis)
+                    if ((h >> (63 - __builtin_clzll(b))) & 1) h ^= b;
+                if (!h) {
+                    defer.push_back(u);
+                    continue;
+                }
+                basis.push_back(h);
+                std::sort(basis.begin(), basis.end(), [](uint64_t a, uint64_t b) { return a > b; });
+                grp.push_back(u);
+            }
+            if (grp.empty()) return false;
+            groups.push_back(grp);
+            remaining.swap(defer);
+        }
+        if (groups.empty()) groups.emplace_back();
+        for (size_t gi = 0; gi < groups.size(); gi++) {
+            std::vector<uint64_t> regs;
+            for (const U3Op *u : groups[gi]) regs.push_back(u->delta);
+            Pass ps;
+            ps.kind = Pass::GROW;
+            ps.m = mm;
+            bool ok = ps.gb.init(elem_bytes, mm, regs);
+            for (const U3Op *u : groups[gi]) ok = ok && ps.gb.add_gate(*u, 0, 0, false);
+            if (gi == 0)
+                for (const U3Op *u : lane) ok = ok && ps.gb.add_gate(*u, 0, 0, false);
+            if (!ok) return false;
+            out.passes.push_back(ps);
+        }
+        return true;
+    };
+
     for (; i < ops.size(); i++) {
         const Op &op = ops[i];
         if (op.kind == Op::U3BATCH && fast_ok(op)) {
@@ -936,6 +1137,12 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
                 (out.passes[last_tile_pass].kind == Pass::FAST || out.passes[last_tile_pass].kind == Pass::ROW) &&
                 out.passes[last_tile_pass].m == op.m && fuse_fast(out.passes[last_tile_pass], op.diag, false)) {
                 last_tile_pass = -1;
+            } else if (last_tile_pass >= 0 && out.passes[last_tile_pass].kind == Pass::GROW &&
+                       out.passes[last_tile_pass].m == op.m && out.passes[last_tile_pass].gb.dev.ncls[1][2] == 0 &&
+                       out.passes[last_tile_pass].gb.add_window(1, op.diag)) {
+                ensure_exp();
+                out.passes[last_tile_pass].off2 = exp_off;
+                last_tile_pass = -1;
             } else if (last_tile_pass >= 0 && out.passes[last_tile_pass].kind == Pass::TILE &&
                        out.passes[last_tile_pass].m == op.m &&
                        out.passes[last_tile_pass].steps.size() < size_t(pp.max_steps)) {
@@ -972,6 +1179,30 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
             m = op.m;
             last_tile_pass = -1;
             continue;
+        }
+        // U3BATCH with multi-bit deltas: general strided passes (grow.cu)
+        if (pp.grow && grow_ok(op)) {
+            const int mm = op.m;
+            const size_t first = out.passes.size();
+            if (emit_grow(op)) {
+                if (held) {
+                    GrowBuild &gb = out.passes[first].gb;
+                    if (gb.add_window(0, *held)) {
+                        ensure_exp();
+                        out.passes[first].off2 = exp_off;
+                    } else {
+                        std::vector<Pass> batch(out.passes.begin() + long(first), out.passes.end());
+                        out.passes.resize(first);
+                        standalone_diag(mm, *held);
+                        for (Pass &p2 : batch) out.passes.push_back(p2);
+                    }
+                    held = nullptr;
+                }
+                last_tile_pass = int(out.passes.size()) - 1;
+                m = mm;
+                continue;
+            }
+            out.passes.resize(first);
         }
         // U3BATCH: group pair ops into tiles.
         const int mm = op.m;
@@ -1054,6 +1285,16 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
 
     // finalize step arrays
     for (Pass &ps : out.passes) {
+        if (ps.kind == Pass::GROW) {
+            GrowBuild &gb = ps.gb;
+            gb.dev.nsel = uint32_t(gb.sels.size());
+            gb.dev.off_gates = put_vec(out.blob, gb.gates);
+            gb.dev.off_sel = put_vec(out.blob, gb.sels);
+            gb.dev.off_terms[0] = put_vec(out.blob, gb.terms[0]);
+            gb.dev.off_terms[1] = put_vec(out.blob, gb.terms[1]);
+            ps.off = put(out.blob, gb.dev);
+            continue;
+        }
         if (ps.kind == Pass::ROW) {
             ps.row.off_gates = put_vec(out.blob, ps.fgates);
             ps.off = put(out.blob, ps.row);

@@ -45,13 +45,35 @@ struct PlanParams {
     int max_steps = 16;
     int diag_row_bits_c64 = 3;  // log2 rows of a warp tile in a diagonal pass (tile = 64 amplitudes x rows)
     int diag_row_bits_c128 = 2; // same for complex128 (tile = 32 amplitudes x rows)
+    int grow = 1;               // 1: U3 batches with multi-bit deltas use the general strided pass (grow.cu)
     int diag_chunk_bits = -1;   // log2 tiles a warp walks in Gray-code order in a diagonal pass (-1: chosen
                                 // per launch so every warp of a full grid gets at least 16 chunks)
     int product_table_bits = 12;
 };
 
+// General strided pass shape (grow.cu): fixed low bits and register coordinates.
+int grow_reg_bits(int elem_bytes, bool adjoint);
+int grow_fixed_bits(int elem_bytes);
+
+// Builds the selector table and gate / window records of one general strided pass
+// over register deltas `regs` (full real-address deltas) on a 2^m state. Returns
+// false if a window's selector flips with more than one register coordinate or
+// the tables overflow (the caller then runs the window on its own).
+struct GrowBuild {
+    int elem_bytes = 8, m = 0;
+    std::vector<uint64_t> regs;
+    GrowDev dev;
+    std::vector<GrowGateDev> gates;
+    std::vector<GrowSelDev> sels;
+    std::vector<GrowTermDev> terms[2];
+    bool init(int elem_bytes, int m, const std::vector<uint64_t> &regs);
+    int selector(const Sel &s);  // -1 on overflow or a multi-coordinate flip
+    bool add_gate(const U3Op &u, uint32_t gen, uint32_t slot, bool adjoint_matrix);
+    bool add_window(int which, const std::vector<DiagTerm> &w);
+};
+
 struct Pass {
-    enum Kind { PRODUCT, EXPAND, TILE, PAIR, DIAG, FAST, ROW } kind;
+    enum Kind { PRODUCT, EXPAND, TILE, PAIR, DIAG, FAST, ROW, GROW } kind;
     int m = 0;
     uint64_t off = 0;    // blob offset of the pass descriptor
     uint64_t off2 = 0;   // PRODUCT: lookup table; DIAG: exp table
@@ -63,6 +85,7 @@ struct Pass {
     int chunk_bits = -1;                 // DIAG: tiles per Gray-code chunk (log2, -1 = automatic)
     int row_bits = 0;                    // DIAG: log2 rows of a warp tile
     std::vector<FastGateDev> fgates;     // FAST
+    GrowBuild gb;                        // GROW
 };
 
 struct Plan {

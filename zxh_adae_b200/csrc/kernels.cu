@@ -526,6 +526,9 @@ cudaError_t run_passes(const std::vector<Pass> &passes, const uint8_t *dblob, vo
             e = run_row_pass(dblob, ps.off, ps.off2, ps.row.nitems, elem_bytes, ps.wide, state, sms, st);
         } else if (ps.kind == Pass::FAST) {
             e = run_fast_tile(dblob, ps.off, ps.off2, ps.geom.ntiles, elem_bytes, state, status, sms, st);
+        } else if (ps.kind == Pass::GROW) {
+            e = run_grow(dblob, ps.off, ps.off2, int(ps.gb.regs.size()), ps.gb.dev.nitems, elem_bytes, state, nullptr,
+                         nullptr, sms, st);
         } else if (ps.kind == Pass::DIAG) {
             e = run_diag(dblob, ps.off, ps.off2, ps.m, elem_bytes, ps.row_bits, ps.chunk_bits, state, sms, st);
         } else if (ps.kind == Pass::PAIR) {

@@ -45,6 +45,13 @@ cudaError_t run_fast_tile(const uint8_t *dblob, uint64_t foff, uint64_t toff, ui
                           void *state, DevStatus *status, int sms, cudaStream_t st);
 cudaError_t run_row_pass(const uint8_t *dblob, uint64_t poff, uint64_t toff, uint64_t nitems, int elem_bytes,
                          int wide, void *state, int sms, cudaStream_t st);
+// General strided pass (grow.cu): lam == nullptr applies the pass to psi; otherwise
+// the adjoint form on psi and lam with gradients added to grads[slot].
+cudaError_t run_grow(const uint8_t *dblob, uint64_t poff, uint64_t toff, int R, uint64_t nitems, int elem_bytes,
+                     void *psi, void *lam, double *grads, int sms, cudaStream_t st);
+int grow_reg_bits(int elem_bytes, bool adjoint);
+int grow_fixed_bits(int elem_bytes);
+int grow_adjoint_gates();
 cudaError_t run_scatter(const void *state, uint64_t n_real, const uint64_t *dcoltab, uint64_t b, int N, int order,
                         double gre, double gim, void *out, int elem_bytes, int sms, cudaStream_t st);
 
