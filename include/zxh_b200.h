@@ -215,6 +215,43 @@ int zxh_adjoint_gradient(zxh_sim *sim, const zxh_term *terms, size_t nterms, siz
 /* Number of recorded gates (after CRz / Rx lowering). */
 int zxh_gate_count(const zxh_sim *sim, size_t *out);
 
+/* ---- Batched circuits (no counterpart in the reference, which runs one circuit
+ * per ZXH object) ---------------------------------------------------------------- */
+
+/* Many independent circuits, each with its own qubit count (6..34), gate records
+ * and observable: circuit c has records gates[gate_offsets[c] .. gate_offsets[c+1])
+ * and terms terms[term_offsets[c] .. term_offsets[c+1]]. Every circuit is compiled
+ * once at creation (every qubit expanded, X/CX transported) into a chain of
+ * passes: |0...0>, general strided passes with fused diagonal windows, lambda =
+ * H psi with <H>, and the adjoint reverse passes. All states live in one device
+ * arena. Errors of creation are reported by zxh_batch_last_error(NULL). */
+typedef struct zxh_batch zxh_batch;
+enum { ZXH_BATCH_SEQUENTIAL = 0, ZXH_BATCH_PERSISTENT = 1, ZXH_BATCH_GRAPH = 2 };
+int zxh_batch_create(zxh_batch **out, size_t count, const uint32_t *nqubits, const size_t *gate_offsets,
+                     const zxh_gate *gates, const size_t *term_offsets, const zxh_term *terms, int dtype, int device);
+int zxh_batch_destroy(zxh_batch *batch);
+const char *zxh_batch_last_error(const zxh_batch *batch);
+/* offsets[count + 1]: circuit c's gradients are grads[offsets[c] .. offsets[c+1]),
+ * one per recorded gate after lowering (CRz records count as two). */
+int zxh_batch_gradient_offsets(const zxh_batch *batch, size_t *offsets);
+/* Energies (count) and gradients of every circuit. mode ZXH_BATCH_SEQUENTIAL runs
+ * every pass as its own launch, circuit after circuit; ZXH_BATCH_PERSISTENT runs
+ * all of them in one persistent kernel that takes tasks from a queue (a task
+ * waits, bounded, for the previous pass of its circuit); ZXH_BATCH_GRAPH replays
+ * that launch from a CUDA graph captured on first use. */
+int zxh_batch_run(zxh_batch *batch, int mode, double *energies, double *grads, size_t ngrads);
+/* Knobs: grow_regs (1..4, gates with high deltas per general strided pass),
+ * task_items (pass items per task), task_elems (amplitudes per task of the
+ * element-wise passes). Setting one recompiles the batch. */
+int zxh_batch_set(zxh_batch *batch, const char *name, int value);
+int zxh_batch_get(const zxh_batch *batch, const char *name, int *value);
+/* Times the persistent launch over grow_regs in {2, 3, 4} x task_items in {32,
+ * 128, 512} (task_elems = 1024 x task_items; reps timed runs each after one
+ * warm-up) and keeps the fastest. */
+int zxh_batch_tune(zxh_batch *batch, int reps);
+/* ops and tasks of the compiled batch; device ms of the last run. */
+int zxh_batch_stats(const zxh_batch *batch, uint64_t *ops, uint64_t *tasks, double *device_ms);
+
 /* Host-only dry run of execute(): lowers the records, runs calc_mem, the
  * reference's execute() schedule and the pass planner, and launches nothing
  * (no CUDA call is made). out[11]: [0] M, [1] final real bits, [2..9] passes
@@ -231,7 +268,10 @@ int zxh_plan_stats(size_t n, int disable_x, int eager_expand_all, int dtype, con
  * tiles a warp of the diagonal pass walks in Gray-code order; -1 = automatic),
  * diag_row_bits_c64, diag_row_bits_c128 (log2 rows of its warp tile), grow (1:
  * U3 batches whose pair deltas span several bits use the general strided pass,
- * 0: the TMA tile / global pair passes).
+ * 0: the TMA tile / global pair passes), grow_regs (1..4: gates with high deltas per
+ * general strided pass), grow_only (1: plan every batch and window as general
+ * strided passes after a |0...0> init, the pass set of the batched launch; needs
+ * eager_expand_all).
  * Takes effect at the
  * next zxh_execute / zxh_apply. No counterpart in the reference. */
 int zxh_set_param(zxh_sim *sim, const char *name, int value);

@@ -1,0 +1,109 @@
+"""GPU tests of the batched launch (zxh_batch_*): every mode against the
+per-circuit adjoint sweep (itself checked against the oracle in
+test_gpu_adjoint.py), energies against the oracle, complex64 against complex128,
+the CUDA-graph replay, the autotuner, and the planner's batch pass set on a
+single simulator."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import observables as ob
+from oracle.bridge import Oracle
+from tests.test_adjoint_host import mixed_circuit, random_terms
+from zxh_adae_b200 import _core
+from zxh_adae_b200 import workloads as wl
+from zxh_adae_b200.batch import Batch
+
+pytestmark = pytest.mark.gpu
+
+
+def per_circuit(circuits, dtype="complex128"):
+    es, gs = [], []
+    for n, rec, terms, *_ in circuits:
+        s = _core.ZXH(n, dtype=dtype)
+        s.push_gates(rec)
+        e, g = s.adjoint_gradient(terms)
+        es.append(e)
+        gs.append(g)
+    return np.array(es), gs
+
+
+def small_batch(seed=3):
+    circ = wl.batch_tfim(14, seed, nmin=6, nmax=11, layers=3)
+    # plus circuits with CX / H / X (dense maps) and every gate kind
+    for k, n in enumerate((6, 8, 10)):
+        c = mixed_circuit(n, 50 + k)
+        p = np.random.default_rng(k).uniform(-math.pi, math.pi, c.nparams)
+        circ.append((n, c.records(p), random_terms(n, 60 + k)))
+    return circ
+
+
+@pytest.mark.parametrize("mode", ["sequential", "persistent", "graph"])
+def test_batch_matches_per_circuit_adjoint(mode):
+    circ = small_batch()
+    e_ref, g_ref = per_circuit(circ)
+    b = Batch([(c[0], c[1], c[2]) for c in circ], dtype="complex128")
+    for _ in range(2):  # the graph is captured on the first run and replayed on the second
+        e, g = b.run(mode)
+        assert np.max(np.abs(e - e_ref)) < 1e-11
+        for gi, gr in zip(b.gradients(g), g_ref):
+            assert np.max(np.abs(gi - gr)) < 1e-10
+
+
+def test_batch_energies_match_oracle():
+    circ = small_batch(seed=4)[:6]
+    b = Batch([(c[0], c[1], c[2]) for c in circ], dtype="complex128")
+    e, _ = b.run("persistent")
+    for k, (n, rec, terms, *_) in enumerate(circ):
+        assert abs(e[k] - ob.oracle_energy(n, rec, terms)) < 1e-11
+
+
+def test_batch_complex64_against_complex128():
+    circ = small_batch(seed=5)
+    e_ref, g_ref = per_circuit(circ)
+    b = Batch([(c[0], c[1], c[2]) for c in circ], dtype="complex64")
+    e, g = b.run("graph")
+    assert np.max(np.abs(e - e_ref)) < 1e-5
+    for gi, gr in zip(b.gradients(g), g_ref):
+        assert np.max(np.abs(gi - gr)) < 1e-5
+
+
+def test_batch_tune_and_knobs():
+    circ = wl.batch_tfim(24, 6, nmin=6, nmax=13, layers=2)
+    b = Batch([(c[0], c[1], c[2]) for c in circ], dtype="complex64")
+    e0, g0 = b.run("persistent")
+    best = b.tune(reps=1)
+    assert best["grow_regs"] in (2, 3, 4) and best["task_items"] in (32, 128, 512)
+    e1, g1 = b.run("graph")
+    assert np.max(np.abs(e1 - e0)) < 1e-5 and np.max(np.abs(g1 - g0)) < 1e-5
+    b.set("grow_regs", 1)
+    b.set("task_items", 3)
+    e2, g2 = b.run("persistent")
+    assert np.max(np.abs(e2 - e0)) < 1e-5 and np.max(np.abs(g2 - g0)) < 1e-5
+    ops, tasks, ms = b.stats()
+    assert ops > 0 and tasks >= ops and ms > 0
+
+
+def test_batch_errors():
+    with pytest.raises(ValueError):
+        Batch([(4, wl.h_all(4), [(1, 0, 0, 1.0)])])
+    with pytest.raises(ValueError):
+        Batch([(6, wl.h_all(6), [(9, 0, 0, 1.0)])])
+
+
+@pytest.mark.parametrize("dtype", ["complex128", "complex64"])
+def test_batch_pass_set_on_one_simulator(dtype):
+    # grow_only: |0...0> then general strided passes only, every qubit expanded
+    for seed in range(4):
+        n = 7 + seed
+        gates = wl.random_circuit(n, 200, 7000 + seed)
+        o = Oracle(n, False, True)
+        o.push(gates)
+        o.execute()
+        s = _core.ZXH(n, False, True, dtype=dtype)
+        s.set_param("grow_only", 1)
+        s.push_gates(gates)
+        s.execute()
+        err = np.max(np.abs(s.get_state().astype(np.complex128) - o.get_state()))
+        assert err <= (1e-12 if dtype == "complex128" else 1e-6)

@@ -95,6 +95,15 @@ _sig("zxh_last_stats", [_P, ctypes.POINTER(_U64), ctypes.POINTER(_U64), ctypes.P
 _sig("zxh_expectation", [_P, _P, _SZ, ctypes.POINTER(_D)])
 _sig("zxh_adjoint_gradient", [_P, _P, _SZ, _SZ, ctypes.POINTER(_D), _P, _SZ])
 _sig("zxh_gate_count", [_P, ctypes.POINTER(_SZ)])
+_sig("zxh_batch_create", [ctypes.POINTER(_P), _SZ, _P, _P, _P, _P, _P, ctypes.c_int, ctypes.c_int])
+_sig("zxh_batch_destroy", [_P])
+_sig("zxh_batch_last_error", [_P], ctypes.c_char_p)
+_sig("zxh_batch_gradient_offsets", [_P, _P])
+_sig("zxh_batch_run", [_P, ctypes.c_int, _P, _P, _SZ])
+_sig("zxh_batch_set", [_P, ctypes.c_char_p, ctypes.c_int])
+_sig("zxh_batch_get", [_P, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)])
+_sig("zxh_batch_tune", [_P, ctypes.c_int])
+_sig("zxh_batch_stats", [_P, ctypes.POINTER(_U64), ctypes.POINTER(_U64), ctypes.POINTER(_D)])
 
 _ERRORS = {1: ValueError, 2: RuntimeError, 3: RuntimeError, 4: MemoryError, 5: ValueError, 6: RuntimeError}
 

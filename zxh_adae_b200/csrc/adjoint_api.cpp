@@ -23,6 +23,7 @@
 // Im<lambda|G|psi> does not see it, and a checkpoint's factor differs from the
 // reverse state's only by rounding of the accumulated phase.
 #include "adjoint.h"
+#include "adjoint_host.h"
 #include "sim.h"
 
 #include <cuda_runtime.h>
@@ -34,12 +35,8 @@
 
 using namespace zxh::api;
 
-namespace {
-
-using zxh::AdjDiagGate;
-using zxh::AdjPairDev;
-using zxh::AffineMap;
-using zxh::TermDev;
+namespace zxh {
+namespace adj {
 
 // gradient generator of a lowered 2x2 record: RY = U3(theta, 0, 0), RX =
 // U3(theta, pi/2, -pi/2) (the lowering of zxh_rx and ZXH_GATE_RX)
@@ -108,57 +105,6 @@ int compile_terms(zxh_sim *s, const zxh_term *terms, size_t nterms, AffineMap &A
     }
     return ZXH_OK;
 }
-
-struct RevStep {
-    enum Kind { PAIR, DIAG, RESTORE, GROW } kind;
-    AdjPairDev pair;
-    size_t slot = 0;   // PAIR: gradient slot
-    size_t first = 0;  // DIAG: first gate in the uploaded group array
-    uint32_t ng = 0;   // DIAG: gates in the group
-    size_t ckpt = 0;   // RESTORE: checkpoint index
-    zxh::GrowBuild gb; // GROW: commuting 2x2 gates on distinct qubits, adjoint form
-    uint64_t off = 0;  // GROW: descriptor offset in the uploaded blob
-};
-
-// A run of 2x2 gates on distinct qubits with no CX between them, collected in
-// reverse order; closed into one general strided adjoint pass (or single pair
-// passes when the state is too small for one).
-struct PairGroup {
-    struct G {
-        zxh::U3Op op;
-        uint32_t gen;
-        uint32_t slot;
-        int q;
-    };
-    std::vector<G> gates;
-    std::vector<uint64_t> basis;  // reduced high parts of the register deltas
-    int nreg = 0;
-    // Whether g can join (distinct qubit, room, independent high part).
-    bool fits(const G &g, int F, int R, int m, int maxg) const
-    {
-        if (int(gates.size()) >= maxg) return false;
-        for (const G &h : gates)
-            if (h.q == g.q) return false;
-        uint64_t hp = g.op.delta >> F;
-        if (!hp) return true;
-        if (nreg >= R || m < F + nreg + 1) return false;
-        for (uint64_t b : basis)
-            if ((hp >> (63 - __builtin_clzll(b))) & 1) hp ^= b;
-        return hp != 0;
-    }
-    void add(const G &g, int F)
-    {
-        uint64_t hp = g.op.delta >> F;
-        if (hp) {
-            for (uint64_t b : basis)
-                if ((hp >> (63 - __builtin_clzll(b))) & 1) hp ^= b;
-            basis.push_back(hp);
-            std::sort(basis.begin(), basis.end(), [](uint64_t a, uint64_t b) { return a > b; });
-            nreg++;
-        }
-        gates.push_back(g);
-    }
-};
 
 // Region layout of d_adj: grads | energy | terms | exp table | grow-pass blob.
 struct AdjLayout {
@@ -244,7 +190,7 @@ int forward_segments(zxh_sim *s, const std::vector<size_t> &ends, double &ms, ui
 
 // The reverse program: gates walked backwards from the forward output's map.
 int reverse_program(zxh_sim *s, const std::vector<size_t> &ends, AffineMap A, std::vector<RevStep> &steps,
-                    std::vector<AdjDiagGate> &dgates, std::vector<uint32_t> &dslots)
+                    std::vector<AdjDiagGate> &dgates, std::vector<uint32_t> &dslots, int diag_max)
 {
     const int N = int(s->n);
     const size_t count = s->gates.size();
@@ -308,7 +254,7 @@ int reverse_program(zxh_sim *s, const std::vector<size_t> &ends, AffineMap A, st
         case zxh::G_P:
         case zxh::G_CP: {
             close_pairs();
-            if (open < 0 || steps[size_t(open)].ng == uint32_t(zxh::kAdjDiagMax)) {
+            if (open < 0 || steps[size_t(open)].ng == uint32_t(diag_max)) {
                 RevStep r;
                 r.kind = RevStep::DIAG;
                 r.first = dgates.size();
@@ -359,7 +305,13 @@ int reverse_program(zxh_sim *s, const std::vector<size_t> &ends, AffineMap A, st
     return ZXH_OK;
 }
 
-}  // namespace
+}  // namespace adj
+}  // namespace zxh
+
+using namespace zxh::adj;
+using zxh::AdjDiagGate;
+using zxh::AffineMap;
+using zxh::TermDev;
 
 extern "C" {
 

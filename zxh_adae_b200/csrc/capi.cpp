@@ -569,6 +569,7 @@ int zxh_plan_stats(size_t n, int disable_x, int eager_expand_all, int dtype, con
     out[0] = uint64_t(M);
     out[1] = uint64_t(ws.m);
     for (const zxh::Pass &p : pl.passes) {
+        if (p.kind > zxh::Pass::GROW) continue;
         out[2 + int(p.kind)]++;
         if (p.kind != zxh::Pass::PRODUCT) out[10]++;
     }
@@ -592,6 +593,8 @@ int zxh_set_param(zxh_sim *s, const char *name, int value)
         {"row_wide_c128", &s->pp.row_wide_c128, 0, 1},
         {"diag_chunk_bits", &s->pp.diag_chunk_bits, -1, 8},
         {"grow", &s->pp.grow, 0, 1},
+        {"grow_regs", &s->pp.grow_regs, 1, 4},
+        {"grow_only", &s->pp.grow_only, 0, 1},
         {"diag_row_bits_c64", &s->pp.diag_row_bits_c64, 2, 4},
         {"diag_row_bits_c128", &s->pp.diag_row_bits_c128, 2, 4},
     };

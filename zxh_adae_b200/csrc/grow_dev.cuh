@@ -1,0 +1,501 @@
+// grow_dev.cuh -- device side of the general strided pass: shared by its own
+// kernel (grow.cu) and the persistent batch kernel (batch.cu).
+#pragma once
+
+#include "core.h"
+#include "dev.cuh"
+
+#include <cuda_runtime.h>
+
+namespace zxh {
+namespace gdev {
+
+
+template <typename E>
+struct GrowCfg;
+template <>
+struct GrowCfg<float2> {
+    using VT = float4;
+    static constexpr int V = 2;
+};
+template <>
+struct GrowCfg<double2> {
+    using VT = double2;
+    static constexpr int V = 1;
+};
+
+constexpr int kGrowAdjGates = 8;  // gates of one adjoint pass (per-thread FP64 accumulators)
+
+template <typename E>
+__device__ __forceinline__ E shfl_xor_c(E v, int m);
+template <>
+__device__ __forceinline__ float2 shfl_xor_c(float2 v, int m)
+{
+    return make_float2(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
+}
+template <>
+__device__ __forceinline__ double2 shfl_xor_c(double2 v, int m)
+{
+    return make_double2(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
+}
+
+template <typename E, typename RT>
+__device__ __forceinline__ E mad2(const RT *m, E a, E b)  // m[0..3] = (x re, x im, y re, y im): x a + y b
+{
+    E o;
+    o.x = m[0] * a.x - m[1] * a.y + m[2] * b.x - m[3] * b.y;
+    o.y = m[0] * a.y + m[1] * a.x + m[2] * b.y + m[3] * b.x;
+    return o;
+}
+
+template <typename E>
+__device__ __forceinline__ double re_cj(E a, E b) { return double(a.x) * double(b.x) + double(a.y) * double(b.y); }
+template <typename E>
+__device__ __forceinline__ double im_cj(E a, E b) { return double(a.x) * double(b.y) - double(a.y) * double(b.x); }
+
+// One row vector of the state at amplitude address a (zeros in the lane bits);
+// complex64 vectors hold two amplitudes whose order follows bit 0 of a. Loads and
+// stores go through L2 only (.cg): in the persistent batch kernel another SM may
+// have written the previous pass of the same state.
+template <typename E>
+__device__ __forceinline__ typename GrowCfg<E>::VT grow_load(const E *s, uint64_t a, int lane)
+{
+    using VT = typename GrowCfg<E>::VT;
+    if constexpr (GrowCfg<E>::V == 2) {
+        VT t = __ldcg(reinterpret_cast<const VT *>(s) + ((a >> 1) ^ uint64_t(lane)));
+        if (a & 1) t = make_float4(t.z, t.w, t.x, t.y);
+        return t;
+    } else {
+        return __ldcg(reinterpret_cast<const VT *>(s) + (a ^ uint64_t(lane)));
+    }
+}
+
+template <typename E>
+__device__ __forceinline__ void grow_store(E *s, uint64_t a, int lane, typename GrowCfg<E>::VT t)
+{
+    using VT = typename GrowCfg<E>::VT;
+    if constexpr (GrowCfg<E>::V == 2) {
+        if (a & 1) t = make_float4(t.z, t.w, t.x, t.y);
+        __stcg(reinterpret_cast<VT *>(s) + ((a >> 1) ^ uint64_t(lane)), t);
+    } else {
+        __stcg(reinterpret_cast<VT *>(s) + (a ^ uint64_t(lane)), t);
+    }
+}
+
+// Register gate on coordinate RR: rows j (bit RR clear) and j | 2^RR.
+template <int RR, int NR, int V, bool ADJ, typename VT, typename RT>
+__device__ __forceinline__ void grow_reg_gate(VT (&x)[NR], VT (&y)[NR], const RT (&m)[V][8], uint32_t orient,
+                                              uint32_t gen, double &acc)
+{
+    using E = decltype(vget(x[0], 0));
+#pragma unroll
+    for (int j = 0; j < NR; j++) {
+        if ((j >> RR) & 1) continue;
+        constexpr int B = 1 << RR;
+#pragma unroll
+        for (int v = 0; v < V; v++) {
+            const E lo = vget(x[j], v), hi = vget(x[j | B], v);
+            if constexpr (ADJ) {
+                const E llo = vget(y[j], v), lhi = vget(y[j | B], v);
+                if (gen == 1) {  // Im<l|Y|p> = Re(conj(l1) p0) - Re(conj(l0) p1), |0> member = lo unless flipped
+                    const double t = re_cj(lhi, lo) - re_cj(llo, hi);
+                    acc += ((orient >> v) & 1) ? -t : t;
+                } else if (gen == 2) {  // Im<l|X|p> = Im(conj(l0) p1 + conj(l1) p0)
+                    acc += im_cj(llo, hi) + im_cj(lhi, lo);
+                }
+                vset(y[j], v, mad2(&m[v][0], llo, lhi));
+                vset(y[j | B], v, mad2(&m[v][4], llo, lhi));
+            }
+            vset(x[j], v, mad2(&m[v][0], lo, hi));
+            vset(x[j | B], v, mad2(&m[v][4], lo, hi));
+        }
+    }
+}
+
+template <int R, int NR, int V, bool ADJ, typename VT, typename RT>
+__device__ __forceinline__ void grow_reg_dispatch(int rr, VT (&x)[NR], VT (&y)[NR], const RT (&m)[V][8],
+                                                  uint32_t orient, uint32_t gen, double &acc)
+{
+    switch (rr) {
+    case 0: if constexpr (R > 0) grow_reg_gate<0, NR, V, ADJ>(x, y, m, orient, gen, acc); break;
+    case 1: if constexpr (R > 1) grow_reg_gate<(R > 1 ? 1 : 0), NR, V, ADJ>(x, y, m, orient, gen, acc); break;
+    case 2: if constexpr (R > 2) grow_reg_gate<(R > 2 ? 2 : 0), NR, V, ADJ>(x, y, m, orient, gen, acc); break;
+    case 3: if constexpr (R > 3) grow_reg_gate<(R > 3 ? 3 : 0), NR, V, ADJ>(x, y, m, orient, gen, acc); break;
+    default: break;
+    }
+}
+
+// Window polynomial over the register row bits for one vector slot: K + sum_i
+// k_i w_i + sum_{i<j} k_i k_j q_ij. Term classes (sorted on the host): [0, n1)
+// single selector without row dependence, [n1, n2) two selectors without row
+// dependence, [n2, n) the rest.
+template <int R>
+struct WinPoly {
+    int64_t K;
+    int64_t w[R];
+    int64_t q[R][R];
+};
+
+template <int R>
+__device__ __forceinline__ void add_w(WinPoly<R> &P, int kb, int64_t val)
+{
+#pragma unroll
+    for (int i = 0; i < R; i++)
+        if (i == kb) P.w[i] += val;
+}
+
+template <int R>
+__device__ __forceinline__ void add_q(WinPoly<R> &P, int a, int b, int64_t val)
+{
+    const int i = min(a, b), j = max(a, b);
+#pragma unroll
+    for (int ii = 0; ii < R; ii++)
+#pragma unroll
+        for (int jj = ii + 1; jj < R; jj++)
+            if (ii == i && jj == j) P.q[ii][jj] += val;
+}
+
+template <int R>
+__device__ __forceinline__ void window_poly(WinPoly<R> &P, const GrowTermDev *t, uint32_t n1, uint32_t n2, uint32_t n,
+                                            const int8_t *kb, uint64_t c)
+{
+    P.K = 0;
+#pragma unroll
+    for (int i = 0; i < R; i++) {
+        P.w[i] = 0;
+#pragma unroll
+        for (int j = 0; j < R; j++) P.q[i][j] = 0;
+    }
+    for (uint32_t q = 0; q < n1; q++)
+        if ((c >> t[q].s0) & 1) P.K += t[q].coef;
+    for (uint32_t q = n1; q < n2; q++)
+        if ((c >> t[q].s0) & (c >> t[q].s1) & 1) P.K += t[q].coef;
+    for (uint32_t q = n2; q < n; q++) {
+        const GrowTermDev tt = t[q];
+        const int c0 = int((c >> tt.s0) & 1), k0 = kb[tt.s0];
+        if (tt.s1 == 0xffff) {  // (c0 ^ k) = c0 + k (1 - 2 c0)
+            if (c0) P.K += tt.coef;
+            add_w(P, k0, c0 ? -tt.coef : tt.coef);
+            continue;
+        }
+        const int c1 = int((c >> tt.s1) & 1), k1 = kb[tt.s1];
+        if (k0 >= 0 && k1 >= 0) {
+            if (c0 & c1) P.K += tt.coef;
+            add_w(P, k0, int64_t(1 - 2 * c0) * int64_t(c1) * tt.coef);
+            add_w(P, k1, int64_t(c0) * int64_t(1 - 2 * c1) * tt.coef);
+            const int64_t qv = int64_t((1 - 2 * c0) * (1 - 2 * c1)) * tt.coef;
+            if (k0 == k1) add_w(P, k0, qv);  // k * k = k: both selectors flip with the same row bit
+            else add_q(P, k0, k1, qv);
+        } else {
+            const int cf = k0 >= 0 ? c1 : c0, cv = k0 >= 0 ? c0 : c1, kk = k0 >= 0 ? k0 : k1;
+            if (cf) {
+                if (cv) P.K += tt.coef;
+                add_w(P, kk, cv ? -tt.coef : tt.coef);
+            }
+        }
+    }
+}
+
+template <int R>
+struct WinPoly32 {
+    uint32_t K;
+    uint32_t w[R];
+    uint32_t q[R][R];
+};
+
+template <int R>
+__device__ __forceinline__ WinPoly32<R> to32(const WinPoly<R> &P)
+{
+    WinPoly32<R> o;
+    o.K = turns32(P.K);
+#pragma unroll
+    for (int i = 0; i < R; i++) {
+        o.w[i] = turns32(P.w[i]);
+#pragma unroll
+        for (int j = 0; j < R; j++) o.q[i][j] = j > i ? turns32(P.q[i][j]) : 0u;
+    }
+    return o;
+}
+
+// complex64: the window's phase in 32-bit turns per amplitude
+template <int R, typename VT>
+__device__ __forceinline__ void apply_poly32(VT (&x)[1 << R], const WinPoly32<R> (&P)[2], const float2 *s_exp)
+{
+    constexpr int NR = 1 << R;
+    constexpr int V = 2;
+    uint32_t acc[V];
+#pragma unroll
+    for (int v = 0; v < V; v++) acc[v] = P[v].K;
+#pragma unroll
+    for (int jj = 0; jj < NR; jj++) {
+        const int g = jj ^ (jj >> 1);
+        if (jj > 0) {
+            const int fb = ctz_const(jj);
+            const bool up = (g >> fb) & 1;
+#pragma unroll
+            for (int v = 0; v < V; v++) {
+                uint32_t d = P[v].w[fb];
+#pragma unroll
+                for (int o = 0; o < R; o++)
+                    if (o != fb && ((g >> o) & 1)) d += (o < fb) ? P[v].q[o][fb] : P[v].q[fb][o];
+                acc[v] += up ? d : 0u - d;
+            }
+        }
+#pragma unroll
+        for (int v = 0; v < V; v++) vset(x[g], v, cmul(vget(x[g], v), phase_factor32(s_exp, acc[v])));
+    }
+}
+
+template <typename E, int R, int V, typename VT>
+__device__ __forceinline__ void apply_poly(VT (&x)[1 << R], const WinPoly<R> (&P)[V], const E *s_exp)
+{
+    constexpr int NR = 1 << R;
+    {
+        int64_t acc[V];
+#pragma unroll
+        for (int v = 0; v < V; v++) acc[v] = P[v].K;
+#pragma unroll
+        for (int jj = 0; jj < NR; jj++) {
+            const int g = jj ^ (jj >> 1);
+            if (jj > 0) {
+                const int fb = ctz_const(jj);
+                const bool up = (g >> fb) & 1;
+#pragma unroll
+                for (int v = 0; v < V; v++) {
+                    int64_t d = P[v].w[fb];
+#pragma unroll
+                    for (int o = 0; o < R; o++)
+                        if (o != fb && ((g >> o) & 1)) d += (o < fb) ? P[v].q[o][fb] : P[v].q[fb][o];
+                    acc[v] += up ? d : -d;
+                }
+            }
+#pragma unroll
+            for (int v = 0; v < V; v++) vset(x[g], v, cmul(vget(x[g], v), phase_factor(s_exp, acc[v])));
+        }
+    }
+}
+
+template <typename E>
+struct GrowShared {
+    using RT = typename ET<E>::R;
+    E s_exp[1 << kExpTableBits];
+    RT s_u[kGrowMaxGates][2][8];
+    uint32_t s_g[kGrowMaxGates][4];  // kind | reg << 8, lane_x, vec_x, sel | gen << 8
+    uint64_t s_D[16];
+    uint64_t s_alpha[kGrowMaxSel];
+    int8_t s_kb[kGrowMaxSel];
+    GrowTermDev s_t[2][kGrowMaxTerms];
+    double s_red[kThreads / 32];
+};
+
+// One general strided pass (or the part of it made of items first + warp,
+// first + warp + step, ... below end) on the calling CTA. Every thread of the CTA
+// calls it; it synchronises the CTA on entry and exit.
+template <typename E, int R, bool ADJ>
+__device__ __forceinline__ void grow_body(const uint8_t *__restrict__ blob, uint64_t poff, uint64_t toff,
+                                          E *__restrict__ psi, E *__restrict__ lam, double *grads, uint64_t first,
+                                          uint64_t step, uint64_t end, GrowShared<E> &sm)
+{
+    using VT = typename GrowCfg<E>::VT;
+    using RT = typename ET<E>::R;
+    constexpr int V = GrowCfg<E>::V;
+    constexpr int LV = (V == 2) ? 1 : 0;
+    constexpr int F = 5 + LV;
+    constexpr int NR = 1 << R;
+    constexpr int WARPS = kThreads / 32;
+
+    const GrowDev &p = *reinterpret_cast<const GrowDev *>(blob + poff);
+    const GrowGateDev *gates = reinterpret_cast<const GrowGateDev *>(blob + p.off_gates);
+    const GrowSelDev *sels = reinterpret_cast<const GrowSelDev *>(blob + p.off_sel);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t ngates = p.ngates, nsel = p.nsel;
+    const bool win0 = p.ncls[0][2] != 0, win1 = p.ncls[1][2] != 0;
+
+    auto &s_exp = sm.s_exp;
+    auto &s_u = sm.s_u;
+    auto &s_g = sm.s_g;
+    auto &s_D = sm.s_D;
+    auto &s_alpha = sm.s_alpha;
+    auto &s_kb = sm.s_kb;
+    auto &s_t = sm.s_t;
+    auto &s_red = sm.s_red;
+    __syncthreads();  // the shared tables may still be read by a previous call
+
+    if (win0 || win1) {
+        const E *tab = reinterpret_cast<const E *>(blob + toff);
+        for (int i = tid; i < (1 << kExpTableBits); i += kThreads) s_exp[i] = tab[i];
+    }
+    for (int w = 0; w < 2; w++) {
+        const GrowTermDev *tt = reinterpret_cast<const GrowTermDev *>(blob + p.off_terms[w]);
+        for (uint32_t i = uint32_t(tid); i < p.ncls[w][2]; i += kThreads) s_t[w][i] = tt[i];
+    }
+    if (tid < int(ngates)) {
+        const GrowGateDev &gg = gates[tid];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            s_u[tid][0][i] = RT(gg.u[i]);
+            s_u[tid][1][i] = RT(gg.u[i ^ 6]);  // |1> member first: [[u11, u10], [u01, u00]]
+        }
+        s_g[tid][0] = gg.kind | (gg.reg << 8);
+        s_g[tid][1] = gg.lane_x;
+        s_g[tid][2] = gg.vec_x;
+        s_g[tid][3] = gg.sel | (gg.gen << 8);
+    }
+    if (tid < NR) s_D[tid] = p.D[tid];
+    if (tid < int(nsel)) {
+        s_alpha[tid] = sels[tid].alpha;
+        s_kb[tid] = int8_t(sels[tid].kbit);
+    }
+    // lane part of every selector (with beta), per vector slot
+    uint64_t lb[V];
+#pragma unroll
+    for (int v = 0; v < V; v++) {
+        lb[v] = 0;
+        const uint64_t e = (uint64_t(lane) << LV) | uint64_t(v);
+        for (uint32_t s = 0; s < nsel; s++)
+            lb[v] |= uint64_t(par64(sels[s].alpha & e) ^ int(sels[s].beta & 1)) << s;
+    }
+    __syncthreads();
+
+    double acc[ADJ ? kGrowAdjGates : 1];
+#pragma unroll
+    for (int g = 0; g < (ADJ ? kGrowAdjGates : 1); g++) acc[g] = 0.0;
+
+    for (uint64_t item = first + uint64_t(warp); item < end; item += step) {
+        uint64_t r0 = item << F;
+#pragma unroll
+        for (int i = 0; i < R; i++) {
+            const uint32_t b = p.piv[i];
+            r0 = ((r0 >> b) << (b + 1)) | (r0 & ((1ULL << b) - 1ULL));
+        }
+        VT x[NR], y[NR];
+#pragma unroll
+        for (int k = 0; k < NR; k++) {
+            x[k] = grow_load(psi, r0 ^ s_D[k], lane);
+            if constexpr (ADJ) y[k] = grow_load(lam, r0 ^ s_D[k], lane);
+        }
+        // selector bits of this item: lane s takes selectors s and s + 32
+        const bool p0 = lane < int(nsel) && par64(s_alpha[lane] & r0);
+        const bool p1 = lane + 32 < int(nsel) && par64(s_alpha[lane + 32] & r0);
+        const uint64_t P = uint64_t(__ballot_sync(0xffffffffu, p0)) | (uint64_t(__ballot_sync(0xffffffffu, p1)) << 32);
+        uint64_t c[V];
+#pragma unroll
+        for (int v = 0; v < V; v++) c[v] = P ^ lb[v];
+
+        if constexpr (!ADJ) {
+            if (win0) {
+                if constexpr (V == 2) {
+                    WinPoly32<R> W[2];
+#pragma unroll
+                    for (int v = 0; v < 2; v++) {
+                        WinPoly<R> t;
+                        window_poly(t, s_t[0], p.ncls[0][0], p.ncls[0][1], p.ncls[0][2], s_kb, c[v]);
+                        W[v] = to32(t);
+                    }
+                    apply_poly32<R>(x, W, reinterpret_cast<const float2 *>(s_exp));
+                } else {
+                    WinPoly<R> W[V];
+#pragma unroll
+                    for (int v = 0; v < V; v++)
+                        window_poly(W[v], s_t[0], p.ncls[0][0], p.ncls[0][1], p.ncls[0][2], s_kb, c[v]);
+                    apply_poly<E, R, V>(x, W, s_exp);
+                }
+            }
+        }
+        for (uint32_t g = 0; g < ngates; g++) {
+            const uint32_t kr = s_g[g][0], sg = s_g[g][3];
+            const uint32_t sel = sg & 0xff, gen = sg >> 8;
+            uint32_t orient = 0;
+#pragma unroll
+            for (int v = 0; v < V; v++) orient |= uint32_t((c[v] >> sel) & 1) << v;
+            RT m[V][8];
+#pragma unroll
+            for (int v = 0; v < V; v++)
+#pragma unroll
+                for (int i = 0; i < 8; i++) m[v][i] = s_u[g][(orient >> v) & 1][i];
+            double ga = 0.0;
+            if ((kr & 0xff) == 0) {
+                grow_reg_dispatch<R, NR, V, ADJ>(int(kr >> 8), x, y, m, orient, gen, ga);
+            } else {
+                using EE = decltype(vget(x[0], 0));
+                const int lx = int(s_g[g][1]), vx = int(s_g[g][2]);
+#pragma unroll
+                for (int j = 0; j < NR; j++) {
+                    EE nx[V], ny[V];
+#pragma unroll
+                    for (int v = 0; v < V; v++) {
+                        const EE own = vget(x[j], v);
+                        const EE src = vget(x[j], v ^ (V == 2 ? vx : 0));
+                        const EE pt = lx ? shfl_xor_c(src, lx) : src;
+                        nx[v] = mad2(&m[v][0], own, pt);
+                        if constexpr (ADJ) {
+                            const EE lown = vget(y[j], v);
+                            const EE lsrc = vget(y[j], v ^ (V == 2 ? vx : 0));
+                            const EE lpt = lx ? shfl_xor_c(lsrc, lx) : lsrc;
+                            if (gen == 1) {  // own |0>: -Re(conj(l) p'), own |1>: +Re(conj(l) p')
+                                const double t = re_cj(lown, pt);
+                                ga += ((orient >> v) & 1) ? t : -t;
+                            } else if (gen == 2) {
+                                ga += im_cj(lown, pt);
+                            }
+                            ny[v] = mad2(&m[v][0], lown, lpt);
+                        }
+                    }
+#pragma unroll
+                    for (int v = 0; v < V; v++) {
+                        vset(x[j], v, nx[v]);
+                        if constexpr (ADJ) vset(y[j], v, ny[v]);
+                    }
+                }
+            }
+            if constexpr (ADJ) {
+#pragma unroll
+                for (int i = 0; i < kGrowAdjGates; i++)
+                    if (uint32_t(i) == g) acc[i] += ga;
+            }
+        }
+        if constexpr (!ADJ) {
+            if (win1) {
+                if constexpr (V == 2) {
+                    WinPoly32<R> W[2];
+#pragma unroll
+                    for (int v = 0; v < 2; v++) {
+                        WinPoly<R> t;
+                        window_poly(t, s_t[1], p.ncls[1][0], p.ncls[1][1], p.ncls[1][2], s_kb, c[v]);
+                        W[v] = to32(t);
+                    }
+                    apply_poly32<R>(x, W, reinterpret_cast<const float2 *>(s_exp));
+                } else {
+                    WinPoly<R> W[V];
+#pragma unroll
+                    for (int v = 0; v < V; v++)
+                        window_poly(W[v], s_t[1], p.ncls[1][0], p.ncls[1][1], p.ncls[1][2], s_kb, c[v]);
+                    apply_poly<E, R, V>(x, W, s_exp);
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < NR; k++) {
+            grow_store(psi, r0 ^ s_D[k], lane, x[k]);
+            if constexpr (ADJ) grow_store(lam, r0 ^ s_D[k], lane, y[k]);
+        }
+    }
+    if constexpr (ADJ) {
+        for (uint32_t g = 0; g < ngates && g < uint32_t(kGrowAdjGates); g++) {
+            if ((s_g[g][3] >> 8) == 0) continue;  // uniform: no gradient for this gate
+            double v = warp_sum_f64(acc[g]);
+            if (lane == 0) s_red[warp] = v;
+            __syncthreads();
+            if (tid == 0) {
+                double t = 0.0;
+                for (int w = 0; w < WARPS; w++) t += s_red[w];
+                atomicAdd(&grads[gates[g].slot], t);
+            }
+            __syncthreads();
+        }
+    }
+}
+
+
+}  // namespace gdev
+}  // namespace zxh

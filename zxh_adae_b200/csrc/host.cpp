@@ -762,7 +762,12 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
     // 1. Product-state prefix: expansions whose selector is constant on the old
     //    bits, starting from |0...0>, and diagonal windows made only of P phases on
     //    existing bits / constant selectors. The prefix is written in one pass.
-    if (start.fresh) {
+    if (start.fresh && pp.grow_only) {
+        Pass ps;
+        ps.kind = Pass::INIT;
+        ps.m = start.m;
+        out.passes.push_back(ps);
+    } else if (start.fresh) {
         ProductDev pd;
         std::memset(&pd, 0, sizeof(pd));
         cd a0(1.0, 0.0);
@@ -897,6 +902,16 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
     };
     auto standalone_diag = [&](int mm, const std::vector<DiagTerm> &w) {
         ensure_exp();
+        if (pp.grow_only && mm >= grow_fixed_bits(elem_bytes)) {  // a general strided pass with no gates
+            Pass ps;
+            ps.kind = Pass::GROW;
+            ps.m = mm;
+            if (ps.gb.init(elem_bytes, mm, std::vector<uint64_t>()) && ps.gb.add_window(0, w)) {
+                ps.off2 = exp_off;
+                out.passes.push_back(ps);
+                return;
+            }
+        }
         const int rb = elem_bytes == 8 ? pp.diag_row_bits_c64 : pp.diag_row_bits_c128;
         const int T = std::min(mm, diag_tile_bits(elem_bytes, rb));
         TileDev g = make_geom(mm, T, std::vector<int>());
@@ -935,7 +950,7 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
     const int clo_fast = std::max(elem_bytes == 8 ? 1 : 0,
                                   std::min(tfast - 1, elem_bytes == 8 ? pp.fast_contig_c64 : pp.fast_contig_c128));
     auto fast_ok = [&](const Op &op) {
-        if (op.m < tfast) return false;
+        if (pp.grow_only || op.m < tfast) return false;
         for (const U3Op &u : op.u3)
             if (u.has_ctrl || !u.delta || (u.delta & (u.delta - 1)) || u.sel.alpha != u.delta) return false;
         return true;
@@ -999,7 +1014,8 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
         return int(out.passes.size()) - 1;
     };
 
-    const int fgrow = grow_fixed_bits(elem_bytes), rgrow = grow_reg_bits(elem_bytes, false);
+    const int fgrow = grow_fixed_bits(elem_bytes);
+    const int rgrow = std::max(1, std::min(pp.grow_regs, grow_reg_bits(elem_bytes, false)));
     auto grow_ok = [&](const Op &op) {
         if (op.m < fgrow) return false;
         for (const U3Op &u : op.u3)
@@ -1181,7 +1197,7 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
             continue;
         }
         // U3BATCH with multi-bit deltas: general strided passes (grow.cu)
-        if (pp.grow && grow_ok(op)) {
+        if ((pp.grow || pp.grow_only) && grow_ok(op)) {
             const int mm = op.m;
             const size_t first = out.passes.size();
             if (emit_grow(op)) {

@@ -46,6 +46,8 @@ struct PlanParams {
     int diag_row_bits_c64 = 3;  // log2 rows of a warp tile in a diagonal pass (tile = 64 amplitudes x rows)
     int diag_row_bits_c128 = 2; // same for complex128 (tile = 32 amplitudes x rows)
     int grow = 1;               // 1: U3 batches with multi-bit deltas use the general strided pass (grow.cu)
+    int grow_regs = 4;          // register coordinates (gates with high deltas) per general strided pass
+    int grow_only = 0;          // 1: only INIT and general strided passes (the persistent batch kernel's set)
     int diag_chunk_bits = -1;   // log2 tiles a warp walks in Gray-code order in a diagonal pass (-1: chosen
                                 // per launch so every warp of a full grid gets at least 16 chunks)
     int product_table_bits = 12;
@@ -73,7 +75,7 @@ struct GrowBuild {
 };
 
 struct Pass {
-    enum Kind { PRODUCT, EXPAND, TILE, PAIR, DIAG, FAST, ROW, GROW } kind;
+    enum Kind { PRODUCT, EXPAND, TILE, PAIR, DIAG, FAST, ROW, GROW, INIT } kind;  // INIT: |0...0> (grow_only)
     int m = 0;
     uint64_t off = 0;    // blob offset of the pass descriptor
     uint64_t off2 = 0;   // PRODUCT: lookup table; DIAG: exp table

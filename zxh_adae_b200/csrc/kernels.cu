@@ -499,6 +499,22 @@ static cudaError_t launch_tile(const uint8_t *blob, uint64_t off, uint32_t T, ui
     return cudaGetLastError();
 }
 
+namespace {
+template <typename E>
+__global__ void set_one_kernel(E *state)
+{
+    state[0].x = 1;
+    state[0].y = 0;
+}
+}  // namespace
+
+cudaError_t run_set_one(void *state, int elem_bytes, cudaStream_t st)
+{
+    if (elem_bytes == 8) set_one_kernel<float2><<<1, 1, 0, st>>>(static_cast<float2 *>(state));
+    else set_one_kernel<double2><<<1, 1, 0, st>>>(static_cast<double2 *>(state));
+    return cudaGetLastError();
+}
+
 cudaError_t run_passes(const std::vector<Pass> &passes, const uint8_t *dblob, void *state, int elem_bytes,
                        DevStatus *status, int sms, cudaStream_t st, uint64_t &kernels)
 {
@@ -526,6 +542,10 @@ cudaError_t run_passes(const std::vector<Pass> &passes, const uint8_t *dblob, vo
             e = run_row_pass(dblob, ps.off, ps.off2, ps.row.nitems, elem_bytes, ps.wide, state, sms, st);
         } else if (ps.kind == Pass::FAST) {
             e = run_fast_tile(dblob, ps.off, ps.off2, ps.geom.ntiles, elem_bytes, state, status, sms, st);
+        } else if (ps.kind == Pass::INIT) {
+            const size_t bytes = size_t(elem_bytes) << ps.m;
+            e = cudaMemsetAsync(state, 0, bytes, st);
+            if (e == cudaSuccess) e = run_set_one(state, elem_bytes, st);
         } else if (ps.kind == Pass::GROW) {
             e = run_grow(dblob, ps.off, ps.off2, int(ps.gb.regs.size()), ps.gb.dev.nitems, elem_bytes, state, nullptr,
                          nullptr, sms, st);

@@ -45,6 +45,8 @@ cudaError_t run_fast_tile(const uint8_t *dblob, uint64_t foff, uint64_t toff, ui
                           void *state, DevStatus *status, int sms, cudaStream_t st);
 cudaError_t run_row_pass(const uint8_t *dblob, uint64_t poff, uint64_t toff, uint64_t nitems, int elem_bytes,
                          int wide, void *state, int sms, cudaStream_t st);
+// amplitude 0 := 1 (the rest of an INIT pass is a memset)
+cudaError_t run_set_one(void *state, int elem_bytes, cudaStream_t st);
 // General strided pass (grow.cu): lam == nullptr applies the pass to psi; otherwise
 // the adjoint form on psi and lam with gradients added to grads[slot].
 cudaError_t run_grow(const uint8_t *dblob, uint64_t poff, uint64_t toff, int R, uint64_t nitems, int elem_bytes,

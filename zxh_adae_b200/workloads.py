@@ -133,3 +133,36 @@ def random_circuit(n: int, count: int, seed: int, kinds=None) -> np.ndarray:
         a = rng.uniform(0.0, TWO_PI, size=3)
         recs.append((t, cq, q, a[0], a[1], a[2]))
     return as_records(recs)
+
+
+def batch_tfim(count: int, seed: int, nmin: int = 10, nmax: int = 22, layers: int = 20):
+    """Configuration 5: `count` circuits, n uniform in {nmin..nmax}; each has
+    `layers` x [U3(theta, phi, lambda) on every qubit; cp(alpha) on (i, i+1)] with
+    angles uniform [0, 2 pi), and its own TFIM observable sum Z_i Z_{i+1} + h sum X_i,
+    h uniform [0.5, 1.5]. U3 is recorded as P(lambda), RY(theta) = U3(theta, 0, 0),
+    P(phi) (the same matrix, U = P(phi) RY(theta) P(lambda)) so that every angle is
+    a parameter of the adjoint gradient; within a layer the P(lambda) of all qubits
+    come first, then the RY, then the P(phi) (gates on different qubits commute).
+    Returns a list of (n, records, terms, h).
+    Draw order: n and h per circuit, then per layer (theta, phi, lambda) per qubit
+    and the n - 1 alphas."""
+    from ._core import TERM_X, TERM_ZZ, as_terms
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(rng.integers(nmin, nmax + 1))
+        h = float(rng.uniform(0.5, 1.5))
+        recs = []
+        for _ in range(layers):
+            ang = rng.uniform(0.0, TWO_PI, size=(n, 3))
+            alpha = rng.uniform(0.0, TWO_PI, size=n - 1)
+            recs += [(P, 0, q, ang[q][2]) for q in range(n)]
+            recs += [(U3, 0, q, ang[q][0], 0.0, 0.0) for q in range(n)]
+            recs += [(P, 0, q, ang[q][1]) for q in range(n)]
+            for i in range(n - 1):
+                recs.append((CP, i, i + 1, alpha[i]))
+        terms = as_terms([(TERM_ZZ, i, i + 1, 1.0) for i in range(n - 1)] + [(TERM_X, i, 0, h) for i in range(n)])
+        out.append((n, as_records(recs), terms, h))
+    return out
+
