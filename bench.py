@@ -20,6 +20,9 @@ as one read-modify-write pass of the state. The state (8 GiB) is larger than L2
                reference's header-subtraction method, GB/s at 16 B/amplitude.
 * u3_layer     the U3-batch half of the 30-qubit target: one layer of U3 on every
                qubit of the same complex64 state, its passes and GB/s per pass.
+* batch        configuration 5: energies and adjoint gradients of 512 uneven
+               circuits, every pass as its own launch vs one persistent launch vs
+               its CUDA-graph replay (autotuned), and the plain per-circuit API.
 * adjoint      the second half of the metric, on the 24-qubit, 432-parameter
                hardware-efficient ansatz (8 x [RY, RZ on every qubit; CX chain] +
                final RY/RZ, parameters uniform [-pi, pi)) with the TFIM observable
@@ -30,7 +33,7 @@ as one read-modify-write pass of the state. The state (8 GiB) is larger than L2
                API, and the max |error| of both against FP64 central differences
                (step 1e-6) on the complex128 forward path. Rank 0 at N = 1 only.
 
-``--workload u3`` / ``--workload adjoint`` time those legs alone (the commands the
+``--workload u3|adjoint|batch`` time those legs alone (the commands the
 ncu summaries under profiles/ were taken with). ``--impl reference`` runs the
 reference CPU backend alone and prints its line. Multi-GPU (``torchrun``): the
 path does not shard, each rank runs an independent replica; value is the sum over
@@ -68,7 +71,8 @@ def parse():
     ap.add_argument("--qubits", type=int, default=N_QUBITS)
     ap.add_argument("--batch", type=int, default=BATCH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="diag", choices=["diag", "u3", "adjoint"])
+    ap.add_argument("--workload", default="diag", choices=["diag", "u3", "adjoint", "batch"])
+    ap.add_argument("--no-tune", action="store_true", help="batch workload: skip the autotuner")
     ap.add_argument("--no-extras", action="store_true", help="skip the U3-layer and adjoint legs of the diag line")
     ap.add_argument("--no-adjoint-checks", action="store_true", help="adjoint workload: skip parameter shift and FD")
     return ap.parse_args()
@@ -311,6 +315,52 @@ def adjoint_leg(local: int, n: int = 24, reps: int = 8, checkpoint_every: int = 
     return d
 
 
+def batch_leg(local: int, count: int = 512, seed: int = 2025, tune: bool = True, api: bool = True) -> dict:
+    """Configuration 5: 512 circuits (n uniform in {10..22}, 20 layers of U3 on every
+    qubit + cp chain, own TFIM each) -> energies and adjoint gradients of all of
+    them, complex64: every pass as its own launch vs one persistent launch vs its
+    CUDA-graph replay (after the autotuner), device time (CUDA events)."""
+    import zxh_adae_b200 as zx
+    from zxh_adae_b200 import workloads as wl
+    from zxh_adae_b200.batch import Batch
+
+    circ = wl.batch_tfim(count, seed)
+    t0 = time.perf_counter()
+    b = Batch([(c[0], c[1], c[2]) for c in circ], dtype="complex64", device=local)
+    create_s = time.perf_counter() - t0
+    tuned = b.tune(1) if tune else None
+    ops, tasks, _ = b.stats()
+    d = {"workload": f"{count} circuits, n uniform in 10..22, 20 x [U3 all; cp chain], TFIM h in [0.5, 1.5], "
+                     "energy + adjoint gradient of every circuit, complex64",
+         "circuits": count, "amplitudes": int(sum(1 << c[0] for c in circ)),
+         "gradients": int(b.grad_offsets[-1]), "ops": ops, "tasks": tasks, "create_s": create_s, "tuned": tuned}
+    res = {}
+    for mode in ("sequential", "persistent", "graph"):
+        b.run(mode)
+        best = 1e300
+        for _ in range(2):
+            e, g = b.run(mode)
+            best = min(best, b.stats()[2])
+        res[mode] = (best, e, g)
+        d[f"{mode}_ms"] = best
+    d["speedup_persistent_vs_sequential"] = d["sequential_ms"] / d["persistent_ms"]
+    d["speedup_graph_vs_sequential"] = d["sequential_ms"] / d["graph_ms"]
+    d["max_grad_diff_modes"] = float(max(np.max(np.abs(res[m][2] - res["sequential"][2])) for m in res))
+    if api:  # the plain per-circuit API, one circuit after another (host planning included)
+        sims = {}
+        t0 = time.perf_counter()
+        for n, rec, terms, _h in circ:
+            s = sims.get(n) or sims.setdefault(n, zx.ZXH(n, dtype="complex64", device=local))
+            s.clear_gates()
+            s.push_gates(rec)
+            s.adjoint_gradient(terms)
+        d["api_per_circuit_ms"] = 1e3 * (time.perf_counter() - t0)
+        for s in sims.values():
+            s.close()
+    b.close()
+    return d
+
+
 def timed_applies(sim, batches, warmup, steps, pg, local):
     """W untimed applies, then K timed ones: per-step device ms (CUDA events on the
     library's stream around the pass kernels), launches, passes, host wall time."""
@@ -362,6 +412,10 @@ def run_ours(args):
     eb = 8
     state = (1 << n) * eb
     peak, peak_kind = peaks()
+    if args.workload == "batch":
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "workload": "batch", **batch_leg(local, tune=not args.no_tune)}))
+        return
     if args.workload == "adjoint":
         if rank == 0:
             d = adjoint_leg(local, n=n, reps=8, checkpoint_every=48, steps=args.steps, warmup=args.warmup,
@@ -399,6 +453,7 @@ def run_ours(args):
         if not args.no_extras and args.workload == "diag":
             extras["u3_layer"] = u3_leg(local, n)
             extras["adjoint"] = adjoint_leg(local)
+            extras["batch"] = batch_leg(local)
     if rank != 0:
         return
     line = {

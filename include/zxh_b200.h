@@ -271,7 +271,8 @@ int zxh_plan_stats(size_t n, int disable_x, int eager_expand_all, int dtype, con
  * 0: the TMA tile / global pair passes), grow_regs (1..4: gates with high deltas per
  * general strided pass), grow_only (1: plan every batch and window as general
  * strided passes after a |0...0> init, the pass set of the batched launch; needs
- * eager_expand_all).
+ * eager_expand_all), adj_windows (1: the adjoint sweep undoes diagonal gates
+ * inside its general strided passes, 0: in separate diagonal-group passes).
  * Takes effect at the
  * next zxh_execute / zxh_apply. No counterpart in the reference. */
 int zxh_set_param(zxh_sim *sim, const char *name, int value);

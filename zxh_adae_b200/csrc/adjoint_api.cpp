@@ -131,13 +131,23 @@ std::vector<uint8_t> pack_grow(std::vector<RevStep> &steps)
         if (n) std::memcpy(blob.data() + off, p, n);
         return off;
     };
+    uint64_t toff = 0;
+    bool have_tab = false;
     for (RevStep &r : steps) {
         if (r.kind != RevStep::GROW) continue;
         zxh::GrowBuild &gb = r.gb;
+        if (gb.dev.ncls[1][2] && !have_tab) {  // the phase table of the windows
+            std::vector<uint8_t> t;
+            zxh::exp_table(gb.elem_bytes, t);
+            toff = put(t.data(), t.size());
+            have_tab = true;
+        }
+        r.toff = toff;
         gb.dev.nsel = uint32_t(gb.sels.size());
         gb.dev.off_gates = put(gb.gates.data(), gb.gates.size() * sizeof(zxh::GrowGateDev));
         gb.dev.off_sel = put(gb.sels.data(), gb.sels.size() * sizeof(zxh::GrowSelDev));
-        gb.dev.off_terms[0] = gb.dev.off_terms[1] = put(nullptr, 0);
+        gb.dev.off_terms[0] = put(gb.terms[0].data(), gb.terms[0].size() * sizeof(zxh::GrowTermDev));
+        gb.dev.off_terms[1] = put(gb.terms[1].data(), gb.terms[1].size() * sizeof(zxh::GrowTermDev));
         r.off = put(&gb.dev, sizeof(zxh::GrowDev));
     }
     return blob;
@@ -194,46 +204,80 @@ int reverse_program(zxh_sim *s, const std::vector<size_t> &ends, AffineMap A, st
 {
     const int N = int(s->n);
     const size_t count = s->gates.size();
-    long open = -1;                    // diagonal group being filled
+    long open = -1;                    // diagonal group being filled (states too small for strided passes)
     size_t next_ck = ends.size() - 1;  // checkpoints are restored from the last one down
     const int F = zxh::grow_fixed_bits(s->elem_bytes), R = zxh::grow_reg_bits(s->elem_bytes, true);
     const int maxg = zxh::grow_adjoint_gates();
+    const bool fuse = N >= F && s->pp.adj_windows;  // diagonal gates ride in the general strided passes
     PairGroup pg;
-    auto close_pairs = [&]() {
-        if (pg.gates.empty()) return;
+    // Diagonal gates met since the last pair group: in forward order they follow the
+    // gates of the group collected next, so that group's pass undoes them first.
+    std::vector<zxh::DiagTerm> pw;
+    std::vector<uint32_t> pwk, pws;
+    auto pair_steps = [&]() {  // one global pair pass per gate
+        for (const PairGroup::G &g : pg.gates) {
+            RevStep p;
+            p.kind = RevStep::PAIR;
+            std::memset(&p.pair, 0, sizeof(p.pair));
+            p.pair.m = uint32_t(N);
+            p.pair.pivot = uint32_t(__builtin_ctzll(g.op.delta));
+            p.pair.delta = g.op.delta;
+            p.pair.alpha = g.op.sel.alpha;
+            p.pair.beta = uint32_t(g.op.sel.beta);
+            p.pair.gen = g.gen;
+            for (int k = 0; k < 4; k++) {
+                p.pair.u[2 * k] = g.op.u[k].real();
+                p.pair.u[2 * k + 1] = g.op.u[k].imag();
+            }
+            p.slot = g.slot;
+            steps.push_back(p);
+        }
+    };
+    auto window_steps = [&]() -> bool {  // the pending window alone, in chunks that fit
+        for (size_t a = 0; a < pw.size(); a += 32) {
+            const size_t e = std::min(pw.size(), a + 32);
+            const std::vector<zxh::DiagTerm> w(pw.begin() + long(a), pw.begin() + long(e));
+            const std::vector<uint32_t> k(pwk.begin() + long(a), pwk.begin() + long(e));
+            const std::vector<uint32_t> sl(pws.begin() + long(a), pws.begin() + long(e));
+            RevStep r;
+            r.kind = RevStep::GROW;
+            if (!r.gb.init(s->elem_bytes, N, std::vector<uint64_t>()) || !r.gb.add_window(1, w, &k, &sl, true))
+                return false;
+            steps.push_back(r);
+        }
+        return true;
+    };
+    auto close_group = [&]() -> int {
+        if (pg.gates.empty() && pw.empty()) return ZXH_OK;
         std::vector<uint64_t> regs;
         for (const PairGroup::G &g : pg.gates)
             if (g.op.delta >> F) regs.push_back(g.op.delta);
         RevStep r;
         r.kind = RevStep::GROW;
-        bool ok = N >= F && r.gb.init(s->elem_bytes, N, regs);
+        bool ok = fuse && r.gb.init(s->elem_bytes, N, regs);
         for (const PairGroup::G &g : pg.gates) ok = ok && r.gb.add_gate(g.op, g.gen, g.slot, true);
-        if (ok) {
+        if (ok && (pw.empty() || r.gb.add_window(1, pw, &pwk, &pws, true))) {
             steps.push_back(r);
-        } else {  // one global pair pass per gate
-            for (const PairGroup::G &g : pg.gates) {
-                RevStep p;
-                p.kind = RevStep::PAIR;
-                std::memset(&p.pair, 0, sizeof(p.pair));
-                p.pair.m = uint32_t(N);
-                p.pair.pivot = uint32_t(__builtin_ctzll(g.op.delta));
-                p.pair.delta = g.op.delta;
-                p.pair.alpha = g.op.sel.alpha;
-                p.pair.beta = uint32_t(g.op.sel.beta);
-                p.pair.gen = g.gen;
-                for (int k = 0; k < 4; k++) {
-                    p.pair.u[2 * k] = g.op.u[k].real();
-                    p.pair.u[2 * k + 1] = g.op.u[k].imag();
-                }
-                p.slot = g.slot;
-                steps.push_back(p);
+        } else {
+            if (!pw.empty() && !window_steps()) return fail(s, ZXH_ERR_STATE, "adjoint sweep: window not placeable");
+            if (!pg.gates.empty()) {
+                RevStep r2;
+                r2.kind = RevStep::GROW;
+                bool ok2 = fuse && r2.gb.init(s->elem_bytes, N, regs);
+                for (const PairGroup::G &g : pg.gates) ok2 = ok2 && r2.gb.add_gate(g.op, g.gen, g.slot, true);
+                if (ok2) steps.push_back(r2);
+                else pair_steps();
             }
         }
         pg = PairGroup();
+        pw.clear();
+        pwk.clear();
+        pws.clear();
+        return ZXH_OK;
     };
     for (size_t gi = count; gi-- > 0;) {
         if (next_ck > 0 && ends[next_ck - 1] == gi + 1) {
-            close_pairs();
+            if (int rc = close_group()) return rc;
             next_ck--;
             RevStep r;
             r.kind = RevStep::RESTORE;
@@ -245,7 +289,7 @@ int reverse_program(zxh_sim *s, const std::vector<size_t> &ends, AffineMap A, st
         switch (g.type) {
         case zxh::G_X: A.flip_b(int(g.q)); break;
         case zxh::G_CX:
-            close_pairs();
+            if (int rc = close_group()) return rc;
             A.row_xor(int(g.q), int(g.cq));
             A.b_xor(int(g.q), int(g.cq));
             break;
@@ -253,7 +297,23 @@ int reverse_program(zxh_sim *s, const std::vector<size_t> &ends, AffineMap A, st
         case zxh::G_RZ:
         case zxh::G_P:
         case zxh::G_CP: {
-            close_pairs();
+            const uint32_t kind = g.type == zxh::G_Z ? 0 : g.type == zxh::G_RZ ? 1 : 2;
+            const double th = g.type == zxh::G_Z ? kPi : g.theta;
+            const zxh::Sel s0 = A.selector(int(g.type == zxh::G_CP ? g.cq : g.q));
+            const zxh::Sel s1 = A.selector(int(g.q));
+            if (fuse) {
+                if (!pg.gates.empty() || pw.size() >= size_t(zxh::kGrowMaxTerms))
+                    if (int rc = close_group()) return rc;
+                zxh::DiagTerm t;
+                t.s0 = s0;
+                t.s1 = s1;
+                t.two = g.type == zxh::G_CP;
+                t.theta = th;
+                pw.push_back(t);
+                pwk.push_back(kind);
+                pws.push_back(uint32_t(gi));
+                break;
+            }
             if (open < 0 || steps[size_t(open)].ng == uint32_t(diag_max)) {
                 RevStep r;
                 r.kind = RevStep::DIAG;
@@ -263,19 +323,17 @@ int reverse_program(zxh_sim *s, const std::vector<size_t> &ends, AffineMap A, st
             }
             AdjDiagGate d;
             std::memset(&d, 0, sizeof(d));
-            const zxh::Sel s0 = A.selector(int(g.type == zxh::G_CP ? g.cq : g.q));
             d.a0 = s0.alpha;
             d.b0 = uint32_t(s0.beta);
             if (g.type == zxh::G_CP) {
-                const zxh::Sel s1 = A.selector(int(g.q));
                 d.a1 = s1.alpha;
                 d.b1 = uint32_t(s1.beta);
                 d.two = 1;
             }
-            d.kind = g.type == zxh::G_Z ? 0 : g.type == zxh::G_RZ ? 1 : 2;
-            d.tq = zxh::phase_turns(g.type == zxh::G_Z ? kPi : g.theta);
-            d.m0 = d.kind == 1 ? 1.0 : 0.0;
-            d.m1 = d.kind == 1 ? -1.0 : d.kind == 2 ? -2.0 : 0.0;
+            d.kind = kind;
+            d.tq = zxh::phase_turns(th);
+            d.m0 = kind == 1 ? 1.0 : 0.0;
+            d.m1 = kind == 1 ? -1.0 : kind == 2 ? -2.0 : 0.0;
             dgates.push_back(d);
             dslots.push_back(uint32_t(gi));
             steps[size_t(open)].ng++;
@@ -294,15 +352,15 @@ int reverse_program(zxh_sim *s, const std::vector<size_t> &ends, AffineMap A, st
             pgt.gen = pair_generator(g);
             pgt.slot = uint32_t(gi);
             pgt.q = int(g.q);
-            if (!pg.fits(pgt, F, R, N, maxg)) close_pairs();
+            if (!pg.fits(pgt, F, R, N, maxg))
+                if (int rc = close_group()) return rc;
             pg.add(pgt, F);
             break;
         }
         default: break;
         }
     }
-    close_pairs();
-    return ZXH_OK;
+    return close_group();
 }
 
 }  // namespace adj
@@ -434,7 +492,7 @@ int zxh_adjoint_gradient(zxh_sim *s, const zxh_term *terms, size_t nterms, size_
             kernels++;
             break;
         case RevStep::GROW:
-            CK(s, zxh::run_grow(s->d_adj + L.grow, r.off, 0, int(r.gb.regs.size()), r.gb.dev.nitems, s->elem_bytes,
+            CK(s, zxh::run_grow(s->d_adj + L.grow, r.off, r.toff, int(r.gb.regs.size()), r.gb.dev.nitems, s->elem_bytes,
                                 s->d_psi, s->d_lam, d_grads, s->sms, s->stream),
                "adjoint strided launch");
             kernels++;

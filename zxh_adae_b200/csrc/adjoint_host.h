@@ -33,6 +33,7 @@ struct RevStep {
     size_t ckpt = 0;   // RESTORE: checkpoint index
     zxh::GrowBuild gb; // GROW: commuting 2x2 gates on distinct qubits, adjoint form
     uint64_t off = 0;  // GROW: descriptor offset in the uploaded blob
+    uint64_t toff = 0; // GROW: phase-table offset in the uploaded blob
 };
 
 // A run of 2x2 gates on distinct qubits with no CX between them, collected in

@@ -216,6 +216,7 @@ int compile(zxh_batch *b)
                 op.units = r.gb.dev.nitems;
                 op.base = gbase;
                 op.off0 = r.off;
+                op.off1 = r.toff;
             } else if (r.kind == zxh::adj::RevStep::DIAG) {
                 op.kind = zxh::BOP_DIAG_ADJ;
                 op.units = uint64_t(1) << N;
@@ -333,7 +334,7 @@ int launch_op(zxh_batch *b, const BatchOp &op)
                             op.aux, b->d_energy + op.energy, b->sms, b->stream);
         break;
     case zxh::BOP_GROW_ADJ:
-        e = zxh::run_grow(b->d_blob + op.base, op.off0, 0, int(op.R), op.units, b->eb, psi, lam, gr, b->sms,
+        e = zxh::run_grow(b->d_blob + op.base, op.off0, op.off1, int(op.R), op.units, b->eb, psi, lam, gr, b->sms,
                           b->stream);
         break;
     case zxh::BOP_DIAG_ADJ:

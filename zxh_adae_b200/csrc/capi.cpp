@@ -595,6 +595,7 @@ int zxh_set_param(zxh_sim *s, const char *name, int value)
         {"grow", &s->pp.grow, 0, 1},
         {"grow_regs", &s->pp.grow_regs, 1, 4},
         {"grow_only", &s->pp.grow_only, 0, 1},
+        {"adj_windows", &s->pp.adj_windows, 0, 1},
         {"diag_row_bits_c64", &s->pp.diag_row_bits_c64, 2, 4},
         {"diag_row_bits_c128", &s->pp.diag_row_bits_c128, 2, 4},
     };

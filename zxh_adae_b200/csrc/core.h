@@ -269,10 +269,13 @@ struct GrowSelDev {
 };
 
 // One window term: phase coef (64-bit turns) where selector s0 (and s1 unless
-// s1 == 0xffff) is 1.
+// s1 == 0xff) is 1. In adjoint passes coef is the inverse phase and the term's
+// gradient sum_r Im(conj(lambda_r) psi_r) * (S(r) ? m1 : m0) goes to grads[slot]
+// (gk 1: RZ, m0 = 1, m1 = -1; gk 2: P or CP, m0 = 0, m1 = -2; gk 0: none).
 struct GrowTermDev {
-    uint16_t s0, s1;
-    uint32_t pad;
+    uint8_t s0, s1;
+    uint8_t gk, pad;
+    uint32_t slot;
     int64_t coef;
 };
 

@@ -173,7 +173,7 @@ __device__ __forceinline__ void window_poly(WinPoly<R> &P, const GrowTermDev *t,
     for (uint32_t q = n2; q < n; q++) {
         const GrowTermDev tt = t[q];
         const int c0 = int((c >> tt.s0) & 1), k0 = kb[tt.s0];
-        if (tt.s1 == 0xffff) {  // (c0 ^ k) = c0 + k (1 - 2 c0)
+        if (tt.s1 == 0xff) {  // (c0 ^ k) = c0 + k (1 - 2 c0)
             if (c0) P.K += tt.coef;
             add_w(P, k0, c0 ? -tt.coef : tt.coef);
             continue;
@@ -286,7 +286,146 @@ struct GrowShared {
     int8_t s_kb[kGrowMaxSel];
     GrowTermDev s_t[2][kGrowMaxTerms];
     double s_red[kThreads / 32];
+    uint8_t s_mu[kGrowMaxSel];                     // selector bits inside the lane / vector bits
+    uint64_t s_bmask;                              // selector betas
+    double s_tacc[kThreads / 32][kGrowMaxTerms];   // adjoint windows: per-warp term gradients
 };
+
+// Adjoint window gradients of one item, before the inverse phases are applied.
+// Term q's gradient sum_a w_a (S_q(a) ? m1 : m0), w = Im(conj(lambda) psi), is
+// split into terms whose selectors do not flip with the register rows (their
+// sum over the warp comes from one Walsh-Hadamard transform of the per-lane row
+// sums over the lane / vector bits: sum_x [P ^ mu.x] W(x) = (Wt +- What(mu)) / 2;
+// lane q mod 32 owns term q) and the rest (per-thread sums over the rows, then a
+// warp sum). Results are added to tacc[q] (one warp's row of the shared array).
+template <int R, int V, typename VT>
+__device__ __forceinline__ void adj_window_grad(const VT (&x)[1 << R], const VT (&y)[1 << R], const uint64_t (&c)[V],
+                                                uint64_t pb, int lane, const GrowTermDev *t, const uint8_t *mu,
+                                                const int8_t *kb, uint32_t n2, uint32_t n, double *tacc)
+{
+    constexpr int NR = 1 << R;
+    constexpr int LV = (V == 2) ? 1 : 0;
+    constexpr int RR = R > 0 ? R : 1;
+    double W[V], Wi[RR][V], Wij[RR][RR][V];
+#pragma unroll
+    for (int v = 0; v < V; v++) {
+        W[v] = 0.0;
+#pragma unroll
+        for (int i = 0; i < RR; i++) {
+            Wi[i][v] = 0.0;
+#pragma unroll
+            for (int j = 0; j < RR; j++) Wij[i][j][v] = 0.0;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < NR; k++)
+#pragma unroll
+        for (int v = 0; v < V; v++) {
+            const auto a = vget(x[k], v);
+            const auto l = vget(y[k], v);
+            const double w = double(l.x) * double(a.y) - double(l.y) * double(a.x);
+            W[v] += w;
+#pragma unroll
+            for (int i = 0; i < R; i++) {
+                if (!((k >> i) & 1)) continue;
+                Wi[i][v] += w;
+#pragma unroll
+                for (int j = i + 1; j < R; j++)
+                    if ((k >> j) & 1) Wij[i][j][v] += w;
+            }
+        }
+    // row-independent terms: Walsh-Hadamard transform over the 2^F low positions
+    double h[V];
+#pragma unroll
+    for (int v = 0; v < V; v++) h[v] = W[v];
+    if constexpr (V == 2) {
+        const double a = h[0], b = h[1];
+        h[0] = a + b;
+        h[1] = a - b;
+    }
+#pragma unroll
+    for (int m = 1; m < 32; m <<= 1)
+#pragma unroll
+        for (int v = 0; v < V; v++) {
+            const double o = __shfl_xor_sync(0xffffffffu, h[v], m);
+            h[v] = (lane & m) ? (o - h[v]) : (h[v] + o);
+        }
+    const double Wt = __shfl_sync(0xffffffffu, h[0], 0);
+    auto fetch = [&](uint32_t m) -> double {
+        const int src = int(m >> LV) & 31;
+        const double a = __shfl_sync(0xffffffffu, h[0], src);
+        if constexpr (V == 2) {
+            const double b = __shfl_sync(0xffffffffu, h[1], src);
+            return (m & 1) ? b : a;
+        }
+        return a;
+    };
+    auto S = [&](int p, double wh) { return 0.5 * (Wt + (p ? wh : -wh)); };
+    for (uint32_t r0 = 0; r0 < n2; r0 += 32) {
+        const uint32_t q = r0 + uint32_t(lane);
+        const bool live = q < n2;
+        const GrowTermDev tt = t[live ? q : r0];
+        const bool two = tt.s1 != 0xff;
+        const uint32_t m0 = mu[tt.s0], m1 = two ? mu[tt.s1] : 0u;
+        const int p0 = int((pb >> tt.s0) & 1), p1 = two ? int((pb >> tt.s1) & 1) : 0;
+        const double f0 = fetch(m0), f1 = fetch(m1), f01 = fetch(m0 ^ m1);  // every lane shuffles
+        const double sv = two ? 0.5 * (S(p0, f0) + S(p1, f1) - S(p0 ^ p1, f01)) : S(p0, f0);
+        if (live && tt.gk) {
+            const double g0 = tt.gk == 1 ? 1.0 : 0.0, g1 = tt.gk == 1 ? -1.0 : -2.0;
+            tacc[q] += g0 * Wt + (g1 - g0) * sv;
+        }
+    }
+    // row-dependent terms: per-thread sums over the rows, then a warp sum
+    auto wsel = [&](int k, int v) {
+        double r = 0.0;
+#pragma unroll
+        for (int i = 0; i < R; i++)
+            if (i == k) r = Wi[i][v];
+        return r;
+    };
+    auto wpair = [&](int a, int b, int v) {
+        const int i = min(a, b), j = max(a, b);
+        double r = 0.0;
+#pragma unroll
+        for (int ii = 0; ii < R; ii++)
+#pragma unroll
+            for (int jj = ii + 1; jj < R; jj++)
+                if (ii == i && jj == j) r = Wij[ii][jj][v];
+        return r;
+    };
+    for (uint32_t q = n2; q < n; q++) {
+        const GrowTermDev tt = t[q];
+        double g = 0.0;
+        const double g0 = tt.gk == 1 ? 1.0 : 0.0, g1 = tt.gk == 1 ? -1.0 : -2.0;
+#pragma unroll
+        for (int v = 0; v < V; v++) {
+            const int c0 = int((c[v] >> tt.s0) & 1), k0 = kb[tt.s0];
+            double sv;
+            if (tt.s1 == 0xff) {
+                const double Wa = wsel(k0, v);
+                sv = c0 ? W[v] - Wa : Wa;
+            } else {
+                const int c1 = int((c[v] >> tt.s1) & 1), k1 = kb[tt.s1];
+                if (k0 >= 0 && k1 >= 0 && k0 != k1) {
+                    const double Wa = wsel(k0, v), Wb = wsel(k1, v), Wab = wpair(k0, k1, v);
+                    const double W11 = Wab, W10 = Wa - Wab, W01 = Wb - Wab, W00 = W[v] - Wa - Wb + Wab;
+                    sv = ((c0 & c1) ? W00 : 0.0) + (((1 - c0) & c1) ? W10 : 0.0) + ((c0 & (1 - c1)) ? W01 : 0.0) +
+                         (((1 - c0) & (1 - c1)) ? W11 : 0.0);
+                } else if (k0 >= 0 && k1 >= 0) {  // both flip with the same row bit
+                    const double Wa = wsel(k0, v);
+                    sv = c0 == c1 ? (c0 ? W[v] - Wa : Wa) : 0.0;
+                } else {
+                    const int cd = k0 >= 0 ? c0 : c1, cf = k0 >= 0 ? c1 : c0, kd = k0 >= 0 ? k0 : k1;
+                    const double Wa = wsel(kd, v);
+                    sv = cf ? (cd ? W[v] - Wa : Wa) : 0.0;
+                }
+            }
+            g += g0 * W[v] + (g1 - g0) * sv;
+        }
+        g = warp_sum_f64(g);
+        if (lane == 0 && tt.gk) tacc[q] += g;
+    }
+}
 
 // One general strided pass (or the part of it made of items first + warp,
 // first + warp + step, ... below end) on the calling CTA. Every thread of the CTA
@@ -345,6 +484,15 @@ __device__ __forceinline__ void grow_body(const uint8_t *__restrict__ blob, uint
     if (tid < int(nsel)) {
         s_alpha[tid] = sels[tid].alpha;
         s_kb[tid] = int8_t(sels[tid].kbit);
+        sm.s_mu[tid] = uint8_t(sels[tid].alpha & ((1u << F) - 1u));
+    }
+    if (tid == 0) {
+        uint64_t bm = 0;
+        for (uint32_t s = 0; s < nsel; s++) bm |= uint64_t(sels[s].beta & 1) << s;
+        sm.s_bmask = bm;
+    }
+    if constexpr (ADJ) {
+        for (uint32_t i = uint32_t(tid); i < uint32_t(WARPS) * kGrowMaxTerms; i += kThreads) (&sm.s_tacc[0][0])[i] = 0.0;
     }
     // lane part of every selector (with beta), per vector slot
     uint64_t lb[V];
@@ -399,6 +547,30 @@ __device__ __forceinline__ void grow_body(const uint8_t *__restrict__ blob, uint
                     for (int v = 0; v < V; v++)
                         window_poly(W[v], s_t[0], p.ncls[0][0], p.ncls[0][1], p.ncls[0][2], s_kb, c[v]);
                     apply_poly<E, R, V>(x, W, s_exp);
+                }
+            }
+        }
+        if constexpr (ADJ) {
+            if (win1) {  // the window after the gates, undone first: gradients, then inverse phases
+                adj_window_grad<R, V>(x, y, c, P ^ sm.s_bmask, lane, s_t[1], sm.s_mu, s_kb, p.ncls[1][1],
+                                      p.ncls[1][2], sm.s_tacc[warp]);
+                if constexpr (V == 2) {
+                    WinPoly32<R> W[2];
+#pragma unroll
+                    for (int v = 0; v < 2; v++) {
+                        WinPoly<R> t;
+                        window_poly(t, s_t[1], p.ncls[1][0], p.ncls[1][1], p.ncls[1][2], s_kb, c[v]);
+                        W[v] = to32(t);
+                    }
+                    apply_poly32<R>(x, W, reinterpret_cast<const float2 *>(s_exp));
+                    apply_poly32<R>(y, W, reinterpret_cast<const float2 *>(s_exp));
+                } else {
+                    WinPoly<R> W[V];
+#pragma unroll
+                    for (int v = 0; v < V; v++)
+                        window_poly(W[v], s_t[1], p.ncls[1][0], p.ncls[1][1], p.ncls[1][2], s_kb, c[v]);
+                    apply_poly<E, R, V>(x, W, s_exp);
+                    apply_poly<E, R, V>(y, W, s_exp);
                 }
             }
         }
@@ -481,6 +653,15 @@ __device__ __forceinline__ void grow_body(const uint8_t *__restrict__ blob, uint
         }
     }
     if constexpr (ADJ) {
+        if (win1) {
+            __syncthreads();
+            for (uint32_t q = uint32_t(tid); q < p.ncls[1][2]; q += kThreads) {
+                if (!s_t[1][q].gk) continue;
+                double t = 0.0;
+                for (int w = 0; w < WARPS; w++) t += sm.s_tacc[w][q];
+                atomicAdd(&grads[s_t[1][q].slot], t);
+            }
+        }
         for (uint32_t g = 0; g < ngates && g < uint32_t(kGrowAdjGates); g++) {
             if ((s_g[g][3] >> 8) == 0) continue;  // uniform: no gradient for this gate
             double v = warp_sum_f64(acc[g]);

@@ -657,26 +657,30 @@ bool GrowBuild::add_gate(const U3Op &u, uint32_t gen, uint32_t slot, bool adjoin
     return true;
 }
 
-bool GrowBuild::add_window(int which, const std::vector<DiagTerm> &w)
+bool GrowBuild::add_window(int which, const std::vector<DiagTerm> &w, const std::vector<uint32_t> *gk,
+                           const std::vector<uint32_t> *slot, bool inverse)
 {
     const size_t mark = sels.size();
     std::vector<GrowTermDev> cls[3];
-    for (const DiagTerm &t : w) {
+    for (size_t ti = 0; ti < w.size(); ti++) {
+        const DiagTerm &t = w[ti];
         GrowTermDev d;
         std::memset(&d, 0, sizeof(d));
         const int s0 = selector(t.s0);
-        const int s1 = t.two ? selector(t.s1) : 0xffff;
+        const int s1 = t.two ? selector(t.s1) : 0xff;
         if (s0 < 0 || s1 < 0) {
             sels.resize(mark);
             return false;
         }
-        d.s0 = uint16_t(s0);
-        d.s1 = uint16_t(s1);
-        d.coef = turns(t.theta);
+        d.s0 = uint8_t(s0);
+        d.s1 = uint8_t(s1);
+        d.coef = turns(inverse ? -t.theta : t.theta);
+        if (gk) d.gk = uint8_t((*gk)[ti]);
+        if (slot) d.slot = (*slot)[ti];
         const bool k0 = sels[size_t(s0)].kbit >= 0;
         const bool k1 = t.two && sels[size_t(s1)].kbit >= 0;
         if (t.two && s0 == s1) {  // S and S = S
-            d.s1 = 0xffff;
+            d.s1 = 0xff;
             cls[k0 ? 2 : 0].push_back(d);
         } else if (!t.two) {
             cls[k0 ? 2 : 0].push_back(d);

@@ -48,6 +48,7 @@ struct PlanParams {
     int grow = 1;               // 1: U3 batches with multi-bit deltas use the general strided pass (grow.cu)
     int grow_regs = 4;          // register coordinates (gates with high deltas) per general strided pass
     int grow_only = 0;          // 1: only INIT and general strided passes (the persistent batch kernel's set)
+    int adj_windows = 1;        // adjoint sweep: diagonal gates ride in the general strided passes as windows
     int diag_chunk_bits = -1;   // log2 tiles a warp walks in Gray-code order in a diagonal pass (-1: chosen
                                 // per launch so every warp of a full grid gets at least 16 chunks)
     int product_table_bits = 12;
@@ -71,7 +72,10 @@ struct GrowBuild {
     bool init(int elem_bytes, int m, const std::vector<uint64_t> &regs);
     int selector(const Sel &s);  // -1 on overflow or a multi-coordinate flip
     bool add_gate(const U3Op &u, uint32_t gen, uint32_t slot, bool adjoint_matrix);
-    bool add_window(int which, const std::vector<DiagTerm> &w);
+    // which: 0 before the gates, 1 after. Adjoint passes give per-term gradient
+    // kinds and slots and inverse = true (the inverse phase is applied).
+    bool add_window(int which, const std::vector<DiagTerm> &w, const std::vector<uint32_t> *gk = nullptr,
+                    const std::vector<uint32_t> *slot = nullptr, bool inverse = false);
 };
 
 struct Pass {
