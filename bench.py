@@ -73,6 +73,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="diag", choices=["diag", "u3", "adjoint", "batch"])
     ap.add_argument("--no-tune", action="store_true", help="batch workload: skip the autotuner")
+    ap.add_argument("--batch-count", type=int, default=512, help="batch workload: circuits")
     ap.add_argument("--no-extras", action="store_true", help="skip the U3-layer and adjoint legs of the diag line")
     ap.add_argument("--no-adjoint-checks", action="store_true", help="adjoint workload: skip parameter shift and FD")
     return ap.parse_args()
@@ -343,6 +344,11 @@ def batch_leg(local: int, count: int = 512, seed: int = 2025, tune: bool = True,
             best = min(best, b.stats()[2])
         res[mode] = (best, e, g)
         d[f"{mode}_ms"] = best
+    d["state_bytes_per_run"] = b.state_bytes()
+    peak, kind = peaks()
+    for mode in ("sequential", "persistent", "graph"):
+        d[f"{mode}_GBps"] = d["state_bytes_per_run"] / (d[f"{mode}_ms"] / 1e3) / 1e9
+    d["graph_frac_of_peak"] = d["graph_GBps"] / peak
     d["speedup_persistent_vs_sequential"] = d["sequential_ms"] / d["persistent_ms"]
     d["speedup_graph_vs_sequential"] = d["sequential_ms"] / d["graph_ms"]
     d["max_grad_diff_modes"] = float(max(np.max(np.abs(res[m][2] - res["sequential"][2])) for m in res))
@@ -414,7 +420,8 @@ def run_ours(args):
     peak, peak_kind = peaks()
     if args.workload == "batch":
         if rank == 0:
-            print(json.dumps({"metric": METRIC, "workload": "batch", **batch_leg(local, tune=not args.no_tune)}))
+            print(json.dumps({"metric": METRIC, "workload": "batch",
+                              **batch_leg(local, count=args.batch_count, tune=not args.no_tune)}))
         return
     if args.workload == "adjoint":
         if rank == 0:

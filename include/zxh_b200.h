@@ -249,8 +249,10 @@ int zxh_batch_get(const zxh_batch *batch, const char *name, int *value);
  * 128, 512} (task_elems = 1024 x task_items; reps timed runs each after one
  * warm-up) and keeps the fastest. */
 int zxh_batch_tune(zxh_batch *batch, int reps);
-/* ops and tasks of the compiled batch; device ms of the last run. */
-int zxh_batch_stats(const zxh_batch *batch, uint64_t *ops, uint64_t *tasks, double *device_ms);
+/* ops and tasks of the compiled batch, device ms of the last run, and the
+ * algorithmic state bytes of one run (each pass reads and writes its states once:
+ * init 1x, forward and lambda passes 2x, adjoint passes 4x the state). */
+int zxh_batch_stats(const zxh_batch *batch, uint64_t *ops, uint64_t *tasks, double *device_ms, uint64_t *bytes);
 
 /* Host-only dry run of execute(): lowers the records, runs calc_mem, the
  * reference's execute() schedule and the pass planner, and launches nothing

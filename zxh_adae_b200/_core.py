@@ -103,7 +103,7 @@ _sig("zxh_batch_run", [_P, ctypes.c_int, _P, _P, _SZ])
 _sig("zxh_batch_set", [_P, ctypes.c_char_p, ctypes.c_int])
 _sig("zxh_batch_get", [_P, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)])
 _sig("zxh_batch_tune", [_P, ctypes.c_int])
-_sig("zxh_batch_stats", [_P, ctypes.POINTER(_U64), ctypes.POINTER(_U64), ctypes.POINTER(_D)])
+_sig("zxh_batch_stats", [_P, ctypes.POINTER(_U64), ctypes.POINTER(_U64), ctypes.POINTER(_D), ctypes.POINTER(_U64)])
 
 _ERRORS = {1: ValueError, 2: RuntimeError, 3: RuntimeError, 4: MemoryError, 5: ValueError, 6: RuntimeError}
 

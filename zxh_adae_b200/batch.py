@@ -95,6 +95,12 @@ class Batch:
 
     def stats(self) -> tuple:
         """(ops, tasks, device ms of the last run)."""
-        o, t, ms = _U64(0), _U64(0), _D(0.0)
-        self._ck(_lib.zxh_batch_stats(self._h, ctypes.byref(o), ctypes.byref(t), ctypes.byref(ms)))
+        o, t, ms, by = _U64(0), _U64(0), _D(0.0), _U64(0)
+        self._ck(_lib.zxh_batch_stats(self._h, ctypes.byref(o), ctypes.byref(t), ctypes.byref(ms), ctypes.byref(by)))
         return int(o.value), int(t.value), float(ms.value)
+
+    def state_bytes(self) -> int:
+        """Algorithmic state bytes of one run (the roofline numerator)."""
+        by = _U64(0)
+        self._ck(_lib.zxh_batch_stats(self._h, None, None, None, ctypes.byref(by)))
+        return int(by.value)

@@ -61,6 +61,7 @@ struct zxh_batch {
     cudaGraphExec_t gexec = nullptr;
 
     int grow_regs = 4, task_items = 128, task_elems = 1 << 17;
+    uint64_t bytes = 0;  // algorithmic state bytes of one run
     float last_ms = 0.0f;
 };
 
@@ -122,6 +123,7 @@ int compile(zxh_batch *b)
     b->rem_init.clear();
     b->blob.clear();
     b->chain.assign(b->n.size(), std::vector<uint32_t>());
+    b->bytes = 0;
     b->hgates.clear();
     b->arena_elems = 0;
     zxh::PlanParams pp;
@@ -163,6 +165,8 @@ int compile(zxh_batch *b)
             op.grad_base = uint32_t(b->grad_off[c]);
             op.energy = uint32_t(c);
             op.dep = b->chain[c].empty() ? zxh::kNoDep : b->chain[c].back();
+            const uint64_t sb = uint64_t(b->eb) << N;  // one state
+            b->bytes += op.kind == zxh::BOP_INIT ? sb : (op.kind == zxh::BOP_GROW || op.kind == zxh::BOP_LAMBDA) ? 2 * sb : 4 * sb;
             b->chain[c].push_back(uint32_t(b->ops.size()));
             b->ops.push_back(op);
         };
@@ -523,9 +527,10 @@ int zxh_batch_get(const zxh_batch *b, const char *name, int *value)
     return ZXH_OK;
 }
 
-int zxh_batch_stats(const zxh_batch *b, uint64_t *ops, uint64_t *tasks, double *device_ms)
+int zxh_batch_stats(const zxh_batch *b, uint64_t *ops, uint64_t *tasks, double *device_ms, uint64_t *bytes)
 {
     if (!b) return ZXH_ERR_ARG;
+    if (bytes) *bytes = b->bytes;
     if (ops) *ops = b->ops.size();
     if (tasks) *tasks = b->tasks.size();
     if (device_ms) *device_ms = double(b->last_ms);
