@@ -71,7 +71,7 @@ def parse():
     ap.add_argument("--qubits", type=int, default=N_QUBITS)
     ap.add_argument("--batch", type=int, default=BATCH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="diag", choices=["diag", "u3", "adjoint", "batch"])
+    ap.add_argument("--workload", default="diag", choices=["diag", "u3", "adjoint", "batch", "sample"])
     ap.add_argument("--no-tune", action="store_true", help="batch workload: skip the autotuner")
     ap.add_argument("--batch-count", type=int, default=512, help="batch workload: circuits")
     ap.add_argument("--no-extras", action="store_true", help="skip the U3-layer and adjoint legs of the diag line")
@@ -367,6 +367,32 @@ def batch_leg(local: int, count: int = 512, seed: int = 2025, tune: bool = True,
     return d
 
 
+def sampler_leg(local: int, n: int = N_QUBITS, shots: int = 1_000_000, steps: int = 5) -> dict:
+    """10^6 multinomial shots from an n-qubit complex64 state (H on all + one U3
+    layer); roofline = one read of the state (2^n x 8 B)."""
+    import zxh_adae_b200 as zx
+    from zxh_adae_b200 import workloads as wl
+
+    sim = zx.ZXH(n, dtype="complex64", device=local)
+    sim.push_gates(np.concatenate([wl.h_all(n), wl.u3_layer(n, seed=5)]))
+    sim.execute()
+    sim.set_seed(11)
+    sim.measure(shots)
+    ms = []
+    for k in range(steps):
+        sim.set_seed(100 + k)
+        sim.measure(shots)
+        ms.append(sim.last_stats()[2])
+    kernels = sim.last_stats()[0]
+    sim.close()
+    t = statistics.median(ms)
+    peak, kind = peaks()
+    gbps = (1 << n) * 8 / (t / 1e3) / 1e9
+    return {"workload": f"{shots} shots from a {n}-qubit complex64 state (H all + one U3 layer)", "ms": t,
+            "shots_per_s": shots / (t / 1e3), "state_read_GBps": gbps, "frac_of_peak": gbps / peak,
+            "kernels": kernels, "bytes": "one read of the state"}
+
+
 def timed_applies(sim, batches, warmup, steps, pg, local):
     """W untimed applies, then K timed ones: per-step device ms (CUDA events on the
     library's stream around the pass kernels), launches, passes, host wall time."""
@@ -418,6 +444,11 @@ def run_ours(args):
     eb = 8
     state = (1 << n) * eb
     peak, peak_kind = peaks()
+    if args.workload == "sample":
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "workload": "sample",
+                              **sampler_leg(local, n, steps=args.steps)}))
+        return
     if args.workload == "batch":
         if rank == 0:
             print(json.dumps({"metric": METRIC, "workload": "batch",
@@ -459,6 +490,7 @@ def run_ours(args):
                 cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
         if not args.no_extras and args.workload == "diag":
             extras["u3_layer"] = u3_leg(local, n)
+            extras["sampler"] = sampler_leg(local, n)
             extras["adjoint"] = adjoint_leg(local)
             extras["batch"] = batch_leg(local)
     if rank != 0:

@@ -15,8 +15,8 @@
 //                        once, lane-scans it and places each shot with a warp-
 //                        cooperative search (ballot over lane prefixes, then over
 //                        4-amplitude sub-ranges).
-//   resolve_cta_kernel   heavier segments: the CTA builds the segment CDF in shared
-//                        memory and binary-searches it, split over CTAs by shot chunk.
+//   resolve_cta_kernel   heavier segments, one per CTA (round robin): the CTA builds
+//                        the segment CDF in shared memory and binary-searches it.
 //   map_kernel           real index -> packed virtual bits (measure_cuda.cu:315-338).
 // Every spin on a predecessor flag is bounded and reports ZXH_ERR_TIMEOUT.
 #include "core.h"
@@ -32,7 +32,7 @@ namespace {
 
 constexpr uint64_t kSeedShot = 0x510e527fade682d1ULL;    // measure_cuda.cu:427
 constexpr uint64_t kSeedOffset = 0x9b05688c2b3e6c1fULL;  // measure_cuda.cu:499
-constexpr int kSegsPerChunk = 8;
+constexpr int kSegsPerChunk = 32;
 constexpr int kWarpMax = 32;
 constexpr uint32_t kCtaShots = 16384;
 constexpr int kScanBlock = 4096;
@@ -67,6 +67,69 @@ __device__ __forceinline__ uint32_t ld_flag(const uint32_t *p)
 
 __device__ __forceinline__ double ld_val(const double *p) { return *reinterpret_cast<const volatile double *>(p); }
 
+// A lane's share of a segment's |amp|^2 mass: 16-byte loads, four independent
+// accumulators (more loads in flight per warp).
+__device__ __forceinline__ double seg_partial(const float2 *seg, uint32_t seglen, int lane)
+{
+    const float4 *v = reinterpret_cast<const float4 *>(seg);
+    const uint32_t nv = seglen / 2;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    uint32_t k = uint32_t(lane);
+    for (; k + 96 < nv; k += 128) {
+        const float4 x0 = __ldg(v + k), x1 = __ldg(v + k + 32), x2 = __ldg(v + k + 64), x3 = __ldg(v + k + 96);
+        a0 += double(x0.x) * x0.x + double(x0.y) * x0.y + double(x0.z) * x0.z + double(x0.w) * x0.w;
+        a1 += double(x1.x) * x1.x + double(x1.y) * x1.y + double(x1.z) * x1.z + double(x1.w) * x1.w;
+        a2 += double(x2.x) * x2.x + double(x2.y) * x2.y + double(x2.z) * x2.z + double(x2.w) * x2.w;
+        a3 += double(x3.x) * x3.x + double(x3.y) * x3.y + double(x3.z) * x3.z + double(x3.w) * x3.w;
+    }
+    for (; k < nv; k += 32) {
+        const float4 x = __ldg(v + k);
+        a0 += double(x.x) * x.x + double(x.y) * x.y + double(x.z) * x.z + double(x.w) * x.w;
+    }
+    if ((seglen & 1) && lane == 0) a1 += prob(seg[seglen - 1]);
+    return (a0 + a1) + (a2 + a3);
+}
+
+__device__ __forceinline__ double seg_partial(const double2 *seg, uint32_t seglen, int lane)
+{
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    uint32_t k = uint32_t(lane);
+    for (; k + 96 < seglen; k += 128) {
+        const double2 x0 = __ldg(seg + k), x1 = __ldg(seg + k + 32), x2 = __ldg(seg + k + 64), x3 = __ldg(seg + k + 96);
+        a0 += x0.x * x0.x + x0.y * x0.y;
+        a1 += x1.x * x1.x + x1.y * x1.y;
+        a2 += x2.x * x2.x + x2.y * x2.y;
+        a3 += x3.x * x3.x + x3.y * x3.y;
+    }
+    for (; k < seglen; k += 32) a0 += prob(seg[k]);
+    return (a0 + a1) + (a2 + a3);
+}
+
+// |amp|^2 mass of seg[lo, hi), in order; complex64 ranges with even bounds use
+// 16-byte loads.
+__device__ __forceinline__ double range_mass(const float2 *seg, uint32_t lo, uint32_t hi)
+{
+    double part = 0.0;
+    if (!((lo | hi) & 1)) {
+        const float4 *v = reinterpret_cast<const float4 *>(seg);
+        for (uint32_t k = lo / 2; k < hi / 2; k++) {
+            const float4 x = __ldg(v + k);
+            part += double(x.x) * x.x + double(x.y) * x.y;
+            part += double(x.z) * x.z + double(x.w) * x.w;
+        }
+        return part;
+    }
+    for (uint32_t k = lo; k < hi; k++) part += prob(seg[k]);
+    return part;
+}
+
+__device__ __forceinline__ double range_mass(const double2 *seg, uint32_t lo, uint32_t hi)
+{
+    double part = 0.0;
+    for (uint32_t k = lo; k < hi; k++) part += prob(__ldg(seg + k));
+    return part;
+}
+
 // ---------------------------------------------------------------------------
 
 template <typename E>
@@ -92,9 +155,7 @@ __global__ void __launch_bounds__(kThreads) seg_scan_kernel(const E *__restrict_
         const int nloc = int((nseg - base < uint64_t(kSegsPerChunk) ? nseg - base : uint64_t(kSegsPerChunk)));
         for (int sl = warp; sl < nloc; sl += kThreads / 32) {
             const E *seg = state + (base + uint64_t(sl)) * seglen;
-            double acc = 0.0;
-            for (uint32_t k = uint32_t(lane); k < seglen; k += 32) acc += prob(seg[k]);
-            acc = warp_sum_f64(acc);
+            const double acc = warp_sum_f64(seg_partial(seg, seglen, lane));
             if (lane == 0) s_mass[sl] = acc;
         }
         __syncthreads();
@@ -265,8 +326,7 @@ __global__ void __launch_bounds__(kThreads) resolve_warp_kernel(const E *__restr
             // lane range [lane*per_lane, (lane+1)*per_lane)
             const uint32_t lo = uint32_t(lane) * per_lane;
             const uint32_t hi = min(seglen, lo + per_lane);
-            double part = 0.0;
-            for (uint32_t k = lo; k < hi; k++) part += prob(seg[k]);
+            const double part = range_mass(seg, lo, hi);
             double incl = part;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -337,24 +397,21 @@ __global__ void __launch_bounds__(kThreads) resolve_cta_kernel(const E *__restri
     extern __shared__ double cdf[];
     __shared__ double s_tot[kThreads];
     const uint32_t nh = *heavy_count;
-    uint64_t item = 0;
-    for (uint32_t h = 0; h < nh; h++) {
+    // heavy segment h goes to CTA h mod grid, which places all of its shots
+    for (uint32_t h = blockIdx.x; h < nh; h += gridDim.x) {
         const uint64_t g = heavy_list[h];
         const unsigned long long cnt = counts[g], off = offsets[g];
         const uint64_t nchunks = (cnt + kCtaShots - 1) / kCtaShots;
-        const uint64_t first = item;
-        item += nchunks;
-        // this CTA's chunks of segment g
-        uint64_t c0 = first % gridDim.x == 0 ? 0 : gridDim.x - first % gridDim.x;
-        c0 = (c0 + blockIdx.x) % gridDim.x;
-        if (c0 >= nchunks) continue;
-        // build the segment CDF once for all of this CTA's chunks
+        const uint64_t c0 = 0;
+        // build the segment CDF once for all of its shots
         const E *seg = state + g * seglen;
         const uint32_t per = (seglen + kThreads - 1) / kThreads;
         const uint32_t lo = threadIdx.x * per, hi = min(seglen, lo + per);
+        for (uint32_t k = threadIdx.x; k < seglen; k += kThreads) cdf[k] = prob(__ldg(seg + k));  // coalesced
+        __syncthreads();
         double run = 0.0;
         for (uint32_t k = lo; k < hi; k++) {
-            run += prob(seg[k]);
+            run += cdf[k];
             cdf[k] = run;
         }
         s_tot[threadIdx.x] = run;
@@ -372,7 +429,7 @@ __global__ void __launch_bounds__(kThreads) resolve_cta_kernel(const E *__restri
         for (uint32_t k = lo; k < hi; k++) cdf[k] += add;
         __syncthreads();
         const double total = cdf[seglen - 1];
-        for (uint64_t c = c0; c < nchunks; c += gridDim.x) {
+        for (uint64_t c = c0; c < nchunks; c++) {
             const uint64_t j0 = c * kCtaShots, j1 = (cnt < j0 + kCtaShots ? cnt : j0 + kCtaShots);
             for (uint64_t j = j0 + threadIdx.x; j < j1; j += kThreads) {
                 const double tau = uniform_open01(stream2 ^ (kSeedOffset + off + j)) * total;
