@@ -88,6 +88,7 @@ __device__ __forceinline__ void grow_reg_gate(VT (&x)[NR], VT (&y)[NR], const RT
                                               uint32_t gen, double &acc)
 {
     using E = decltype(vget(x[0], 0));
+    RT part = 0;  // this item's share of the gradient, in the state's precision; added to acc in FP64
 #pragma unroll
     for (int j = 0; j < NR; j++) {
         if ((j >> RR) & 1) continue;
@@ -98,10 +99,10 @@ __device__ __forceinline__ void grow_reg_gate(VT (&x)[NR], VT (&y)[NR], const RT
             if constexpr (ADJ) {
                 const E llo = vget(y[j], v), lhi = vget(y[j | B], v);
                 if (gen == 1) {  // Im<l|Y|p> = Re(conj(l1) p0) - Re(conj(l0) p1), |0> member = lo unless flipped
-                    const double t = re_cj(lhi, lo) - re_cj(llo, hi);
-                    acc += ((orient >> v) & 1) ? -t : t;
+                    const RT t = (lhi.x * lo.x + lhi.y * lo.y) - (llo.x * hi.x + llo.y * hi.y);
+                    part += ((orient >> v) & 1) ? -t : t;
                 } else if (gen == 2) {  // Im<l|X|p> = Im(conj(l0) p1 + conj(l1) p0)
-                    acc += im_cj(llo, hi) + im_cj(lhi, lo);
+                    part += (llo.x * hi.y - llo.y * hi.x) + (lhi.x * lo.y - lhi.y * lo.x);
                 }
                 vset(y[j], v, mad2(&m[v][0], llo, lhi));
                 vset(y[j | B], v, mad2(&m[v][4], llo, lhi));
@@ -110,6 +111,7 @@ __device__ __forceinline__ void grow_reg_gate(VT (&x)[NR], VT (&y)[NR], const RT
             vset(x[j | B], v, mad2(&m[v][4], lo, hi));
         }
     }
+    if constexpr (ADJ) acc += double(part);
 }
 
 template <int R, int NR, int V, bool ADJ, typename VT, typename RT>
@@ -323,7 +325,7 @@ __device__ __forceinline__ void adj_window_grad(const VT (&x)[1 << R], const VT 
         for (int v = 0; v < V; v++) {
             const auto a = vget(x[k], v);
             const auto l = vget(y[k], v);
-            const double w = double(l.x) * double(a.y) - double(l.y) * double(a.x);
+            const double w = double(l.x * a.y - l.y * a.x);  // Im(conj(lambda) psi), one conversion
             W[v] += w;
 #pragma unroll
             for (int i = 0; i < R; i++) {
@@ -591,6 +593,7 @@ __device__ __forceinline__ void grow_body(const uint8_t *__restrict__ blob, uint
             } else {
                 using EE = decltype(vget(x[0], 0));
                 const int lx = int(s_g[g][1]), vx = int(s_g[g][2]);
+                RT gpart = 0;
 #pragma unroll
                 for (int j = 0; j < NR; j++) {
                     EE nx[V], ny[V];
@@ -605,10 +608,10 @@ __device__ __forceinline__ void grow_body(const uint8_t *__restrict__ blob, uint
                             const EE lsrc = vget(y[j], v ^ (V == 2 ? vx : 0));
                             const EE lpt = lx ? shfl_xor_c(lsrc, lx) : lsrc;
                             if (gen == 1) {  // own |0>: -Re(conj(l) p'), own |1>: +Re(conj(l) p')
-                                const double t = re_cj(lown, pt);
-                                ga += ((orient >> v) & 1) ? t : -t;
+                                const RT t = lown.x * pt.x + lown.y * pt.y;
+                                gpart += ((orient >> v) & 1) ? t : -t;
                             } else if (gen == 2) {
-                                ga += im_cj(lown, pt);
+                                gpart += lown.x * pt.y - lown.y * pt.x;
                             }
                             ny[v] = mad2(&m[v][0], lown, lpt);
                         }
@@ -619,6 +622,7 @@ __device__ __forceinline__ void grow_body(const uint8_t *__restrict__ blob, uint
                         if constexpr (ADJ) vset(y[j], v, ny[v]);
                     }
                 }
+                if constexpr (ADJ) ga += double(gpart);
             }
             if constexpr (ADJ) {
 #pragma unroll
