@@ -219,9 +219,11 @@ __device__ __forceinline__ WinPoly32<R> to32(const WinPoly<R> &P)
     return o;
 }
 
-// complex64: the window's phase in 32-bit turns per amplitude
+// complex64: the window's phase in 32-bit turns per amplitude; applied to x and,
+// when given, to y (adjoint passes: psi and lambda get the same phase)
 template <int R, typename VT>
-__device__ __forceinline__ void apply_poly32(VT (&x)[1 << R], const WinPoly32<R> (&P)[2], const float2 *s_exp)
+__device__ __forceinline__ void apply_poly32(VT (&x)[1 << R], const WinPoly32<R> (&P)[2], const float2 *s_exp,
+                                             VT *y = nullptr)
 {
     constexpr int NR = 1 << R;
     constexpr int V = 2;
@@ -244,12 +246,17 @@ __device__ __forceinline__ void apply_poly32(VT (&x)[1 << R], const WinPoly32<R>
             }
         }
 #pragma unroll
-        for (int v = 0; v < V; v++) vset(x[g], v, cmul(vget(x[g], v), phase_factor32(s_exp, acc[v])));
+        for (int v = 0; v < V; v++) {
+            const float2 ph = phase_factor32(s_exp, acc[v]);
+            vset(x[g], v, cmul(vget(x[g], v), ph));
+            if (y) vset(y[g], v, cmul(vget(y[g], v), ph));
+        }
     }
 }
 
 template <typename E, int R, int V, typename VT>
-__device__ __forceinline__ void apply_poly(VT (&x)[1 << R], const WinPoly<R> (&P)[V], const E *s_exp)
+__device__ __forceinline__ void apply_poly(VT (&x)[1 << R], const WinPoly<R> (&P)[V], const E *s_exp,
+                                           VT *y = nullptr)
 {
     constexpr int NR = 1 << R;
     {
@@ -272,7 +279,11 @@ __device__ __forceinline__ void apply_poly(VT (&x)[1 << R], const WinPoly<R> (&P
                 }
             }
 #pragma unroll
-            for (int v = 0; v < V; v++) vset(x[g], v, cmul(vget(x[g], v), phase_factor(s_exp, acc[v])));
+            for (int v = 0; v < V; v++) {
+                const E ph = phase_factor(s_exp, acc[v]);
+                vset(x[g], v, cmul(vget(x[g], v), ph));
+                if (y) vset(y[g], v, cmul(vget(y[g], v), ph));
+            }
         }
     }
 }
@@ -564,15 +575,13 @@ __device__ __forceinline__ void grow_body(const uint8_t *__restrict__ blob, uint
                         window_poly(t, s_t[1], p.ncls[1][0], p.ncls[1][1], p.ncls[1][2], s_kb, c[v]);
                         W[v] = to32(t);
                     }
-                    apply_poly32<R>(x, W, reinterpret_cast<const float2 *>(s_exp));
-                    apply_poly32<R>(y, W, reinterpret_cast<const float2 *>(s_exp));
+                    apply_poly32<R>(x, W, reinterpret_cast<const float2 *>(s_exp), y);
                 } else {
                     WinPoly<R> W[V];
 #pragma unroll
                     for (int v = 0; v < V; v++)
                         window_poly(W[v], s_t[1], p.ncls[1][0], p.ncls[1][1], p.ncls[1][2], s_kb, c[v]);
-                    apply_poly<E, R, V>(x, W, s_exp);
-                    apply_poly<E, R, V>(y, W, s_exp);
+                    apply_poly<E, R, V>(x, W, s_exp, y);
                 }
             }
         }
