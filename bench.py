@@ -71,7 +71,7 @@ def parse():
     ap.add_argument("--qubits", type=int, default=N_QUBITS)
     ap.add_argument("--batch", type=int, default=BATCH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="diag", choices=["diag", "u3", "adjoint", "batch", "sample"])
+    ap.add_argument("--workload", default="diag", choices=["diag", "u3", "adjoint", "batch", "sample", "config3"])
     ap.add_argument("--no-tune", action="store_true", help="batch workload: skip the autotuner")
     ap.add_argument("--batch-count", type=int, default=512, help="batch workload: circuits")
     ap.add_argument("--no-extras", action="store_true", help="skip the U3-layer and adjoint legs of the diag line")
@@ -367,6 +367,105 @@ def batch_leg(local: int, count: int = 512, seed: int = 2025, tune: bool = True,
     return d
 
 
+def fidelity_err(sim_a, sim_b) -> float:
+    """1 - |<a|b>|^2 / (<a|a><b|b>) of two simulators' states (same map and size),
+    computed on the device in FP64, chunked."""
+    import torch
+
+    class _CAI:
+        def __init__(self, ptr, n, ts):
+            self.__cuda_array_interface__ = {"shape": (n,), "typestr": ts, "data": (ptr, False), "version": 3}
+
+    def view(s):
+        ptr, m, eb, g = s.state_view()
+        return torch.as_tensor(_CAI(ptr, 1 << m, "<c8" if eb == 8 else "<c16"), device="cuda"), g
+
+    a, ga = view(sim_a)
+    b, gb = view(sim_b)
+    if a.numel() != b.numel():
+        return float("nan")
+    acc = torch.zeros((), dtype=torch.complex128, device="cuda")
+    na = torch.zeros((), dtype=torch.float64, device="cuda")
+    nb = torch.zeros((), dtype=torch.float64, device="cuda")
+    step = 1 << 26
+    for i in range(0, a.numel(), step):
+        x = a[i:i + step].to(torch.complex128)
+        y = b[i:i + step].to(torch.complex128)
+        acc += torch.vdot(y, x)
+        na += (x.abs() ** 2).sum()
+        nb += (y.abs() ** 2).sum()
+    return float(1.0 - abs(complex(acc)) ** 2 / (float(na) * float(nb)))
+
+
+def config1_leg(local: int, seed: int = 2024) -> dict:
+    """Configuration 1: 20 qubits, complex128, H on all + 10 x [U3 all; cp chain], 1024
+    shots; device ms of execute and measure, and the complex64 run's fidelity error."""
+    import zxh_adae_b200 as zx
+    from zxh_adae_b200 import workloads as wl
+
+    g = wl.plain_layers(20, 10, seed)
+    out = {"workload": "20q complex128, H all + 10 x [U3 all; cp (i, i+1)], 1024 shots"}
+    sims = {}
+    for dtype in ("complex128", "complex64"):
+        s = zx.ZXH(20, dtype=dtype, device=local)
+        s.push_gates(g)
+        s.execute()
+        s.execute()
+        k, p, ms = s.last_stats()
+        s.set_seed(seed)
+        s.measure(1024)
+        out[dtype] = {"execute_ms": ms, "passes": p, "kernels": k, "measure_1024_ms": s.last_stats()[2]}
+        sims[dtype] = s
+    out["complex64_fidelity_err_vs_complex128"] = fidelity_err(sims["complex64"], sims["complex128"])
+    w64, w128 = sims["complex64"].results_words(), sims["complex128"].results_words()
+    out["complex64_sample_mismatch_vs_complex128"] = float(np.mean(w64 != w128))
+    for s in sims.values():
+        s.close()
+    return out
+
+
+def config3_leg(local: int, seed: int = 33) -> dict:
+    """Configuration 3: 32 qubits complex64, 40 x [U3 all; cz matching] (4 layers also in
+    complex128 for the fidelity error), then the 31+1-qubit hidden-string circuit and
+    10^6 shots (every shot must read the secret)."""
+    import zxh_adae_b200 as zx
+    from zxh_adae_b200 import workloads as wl
+
+    n = 32
+    out = {"workload": "32q complex64: 40 x [U3 all; cz on a random perfect matching]; hidden string 31+1, 10^6 shots"}
+    g4 = wl.u3_matching_layers(n, 4, seed)
+    s64 = zx.ZXH(n, dtype="complex64", device=local)
+    s64.push_gates(g4)
+    s64.execute()
+    s128 = zx.ZXH(n, dtype="complex128", device=local)
+    s128.push_gates(g4)
+    s128.execute()
+    out["layers4_fidelity_err_vs_complex128"] = fidelity_err(s64, s128)
+    s128.close()
+    g40 = wl.u3_matching_layers(n, 40, seed)
+    s64.clear_gates()
+    s64.push_gates(g40)
+    s64.execute()
+    k, p, ms = s64.last_stats()
+    out["layers40_ms"] = ms
+    out["layers40_passes"] = p
+    out["layers40_pass_GBps"] = p * 2 * (1 << n) * 8 / (ms / 1e3) / 1e9
+    recs, secret = wl.hidden_string(31, seed + 1)
+    s64.clear_gates()
+    s64.push_gates(recs)
+    s64.execute()
+    out["hidden_execute_ms"] = s64.last_stats()[2]
+    out["hidden_passes"] = s64.last_stats()[1]
+    s64.set_seed(99)
+    s64.measure(1_000_000)
+    out["hidden_measure_1e6_ms"] = s64.last_stats()[2]
+    w = s64.results_words()
+    data = np.unique(w & np.uint64((1 << 31) - 1))
+    out["hidden_all_shots_read_secret"] = bool(len(data) == 1 and int(data[0]) == secret)
+    s64.close()
+    return out
+
+
 def sampler_leg(local: int, n: int = N_QUBITS, shots: int = 1_000_000, steps: int = 5) -> dict:
     """10^6 multinomial shots from an n-qubit complex64 state (H on all + one U3
     layer); roofline = one read of the state (2^n x 8 B)."""
@@ -444,6 +543,10 @@ def run_ours(args):
     eb = 8
     state = (1 << n) * eb
     peak, peak_kind = peaks()
+    if args.workload == "config3":
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "workload": "config3", **config3_leg(local)}))
+        return
     if args.workload == "sample":
         if rank == 0:
             print(json.dumps({"metric": METRIC, "workload": "sample",
@@ -472,6 +575,14 @@ def run_ours(args):
         desc = f"diag-batch {n}q complex64, H-prepared, B={B} random p/cp (50/50) per step"
         dominant, traffic_file = "diag_kernel", f"diag_pass_{n}q_c64.md"
     dev_ms, launches, passes, wall, clocks = timed_applies(sim, batches, args.warmup, args.steps, pg, local)
+    fid = None
+    if rank == 0 and world == 1 and not args.no_extras:
+        # the same gates in complex128, executed as one list: fidelity error of the timed complex64 state
+        ref = zx.ZXH(n, dtype="complex128", device=local)
+        ref.push_gates(np.concatenate([wl.h_all(n)] + batches))
+        ref.execute()
+        fid = fidelity_err(sim, ref)
+        ref.close()
     sim.close()
     bytes_step = (passes / args.steps) * 2 * state
     dev_total_ms = max_over_ranks(pg, sum(dev_ms), local)
@@ -491,6 +602,7 @@ def run_ours(args):
         if not args.no_extras and args.workload == "diag":
             extras["u3_layer"] = u3_leg(local, n)
             extras["sampler"] = sampler_leg(local, n)
+            extras["config1"] = config1_leg(local)
             extras["adjoint"] = adjoint_leg(local)
             extras["batch"] = batch_leg(local)
     if rank != 0:
@@ -515,6 +627,7 @@ def run_ours(args):
             "passes_per_step": passes / args.steps,
             "state_bytes": state,
             "l2": "state larger than L2, no flush" if state > 126 * 2**20 else "state fits in L2",
+            "fidelity_err_vs_complex128": fid,
             "parallelism": f"replicas x{world}",
         },
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(len(batches[0]) * 40),
