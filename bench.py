@@ -352,6 +352,14 @@ def batch_leg(local: int, count: int = 512, seed: int = 2025, tune: bool = True,
     d["speedup_persistent_vs_sequential"] = d["sequential_ms"] / d["persistent_ms"]
     d["speedup_graph_vs_sequential"] = d["sequential_ms"] / d["graph_ms"]
     d["max_grad_diff_modes"] = float(max(np.max(np.abs(res[m][2] - res["sequential"][2])) for m in res))
+    # every result against complex128: the same batch in complex128
+    e64, g64 = res["graph"][1], res["graph"][2]
+    b.close()
+    b128 = Batch([(c[0], c[1], c[2]) for c in circ], dtype="complex128", device=local)
+    e128, g128 = b128.run("persistent")
+    b128.close()
+    d["energy_max_err_vs_complex128"] = float(np.max(np.abs(e64 - e128)))
+    d["grad_max_err_vs_complex128"] = float(np.max(np.abs(g64 - g128)))
     if api:  # the plain per-circuit API, one circuit after another (host planning included)
         sims = {}
         t0 = time.perf_counter()
@@ -363,7 +371,6 @@ def batch_leg(local: int, count: int = 512, seed: int = 2025, tune: bool = True,
         d["api_per_circuit_ms"] = 1e3 * (time.perf_counter() - t0)
         for s in sims.values():
             s.close()
-    b.close()
     return d
 
 
@@ -522,6 +529,11 @@ def u3_leg(local: int, n: int = N_QUBITS, steps: int = 5, warmup: int = 3) -> di
     sim.execute()
     layers = [wl.u3_layer(n, seed=500 + k) for k in range(warmup + steps)]
     dev_ms, launches, passes, wall, _ = timed_applies(sim, layers, warmup, steps, None, local)
+    ref = zx.ZXH(n, dtype="complex128", device=local)
+    ref.push_gates(np.concatenate([wl.h_all(n)] + layers))
+    ref.execute()
+    fid = fidelity_err(sim, ref)
+    ref.close()
     sim.close()
     state = (1 << n) * 8
     ms = sum(dev_ms) / steps
@@ -529,8 +541,9 @@ def u3_leg(local: int, n: int = N_QUBITS, steps: int = 5, warmup: int = 3) -> di
     peak, kind = peaks()
     return {"workload": f"U3 on all {n} qubits of a complex64 state, random angles, one layer per step",
             "ms_per_layer": ms, "passes_per_layer": passes / steps, "kernels_per_layer": launches / steps,
+            "gates_per_s": n / (ms / 1e3), "passes_per_s": (passes / steps) / (ms / 1e3),
             "pass_GBps": gbps, "frac_of_peak": gbps / peak, "peak": peak, "peak_kind": kind,
-            "bytes": "2 x state per pass (one read and one write)"}
+            "fidelity_err_vs_complex128": fid, "bytes": "2 x state per pass (one read and one write)"}
 
 
 def run_ours(args):
@@ -625,6 +638,8 @@ def run_ours(args):
             "qubits": n,
             "batch": B if args.workload == "diag" else n,
             "passes_per_step": passes / args.steps,
+            "gates_per_s": (len(batches[0]) if args.workload == "diag" else n) / (dev_total_ms / args.steps / 1e3),
+            "passes_per_s": (passes / args.steps) / (dev_total_ms / args.steps / 1e3),
             "state_bytes": state,
             "l2": "state larger than L2, no flush" if state > 126 * 2**20 else "state fits in L2",
             "fidelity_err_vs_complex128": fid,
