@@ -51,32 +51,46 @@ __global__ void __launch_bounds__(kThreads) lambda_kernel(const E *__restrict__ 
     using R = typename ET<E>::R;
     __shared__ TermDev st[kMaxTerms];
     __shared__ double sh[kThreads / 32];
+    __shared__ uint32_t s_nx;
     for (uint32_t i = threadIdx.x; i < nterms; i += kThreads) st[i] = terms[i];
+    if (threadIdx.x == 0) {  // X terms come first (the host sorts them)
+        uint32_t k = 0;
+        while (k < nterms && terms[k].kind == 3) k++;
+        s_nx = k;
+    }
     __syncthreads();
+    const uint32_t nx = s_nx;
+    // lambda is accumulated in the state's precision (it is stored in it); the
+    // energy <psi|lambda> is reduced in FP64
     double en = 0.0;
     for (uint64_t r = uint64_t(blockIdx.x) * kThreads + threadIdx.x; r < n; r += uint64_t(gridDim.x) * kThreads) {
         const E p = psi[r];
-        double dg = 0.0, xr = 0.0, xi = 0.0;
-        for (uint32_t t = 0; t < nterms; t++) {
+        R dg = 0, xr = 0, xi = 0;
+        uint32_t t = 0;
+        for (; t + 4 <= nx; t += 4) {  // four gathers in flight
+            const E q0 = psi[r ^ st[t].delta], q1 = psi[r ^ st[t + 1].delta];
+            const E q2 = psi[r ^ st[t + 2].delta], q3 = psi[r ^ st[t + 3].delta];
+            xr += R(st[t].coef) * q0.x + R(st[t + 1].coef) * q1.x + R(st[t + 2].coef) * q2.x + R(st[t + 3].coef) * q3.x;
+            xi += R(st[t].coef) * q0.y + R(st[t + 1].coef) * q1.y + R(st[t + 2].coef) * q2.y + R(st[t + 3].coef) * q3.y;
+        }
+        for (; t < nterms; t++) {
             const TermDev &tm = st[t];
+            const R cf = R(tm.coef);
             if (tm.kind == 3) {
                 const E q = psi[r ^ tm.delta];
-                xr += tm.coef * double(q.x);
-                xi += tm.coef * double(q.y);
+                xr += cf * q.x;
+                xi += cf * q.y;
             } else {
                 int s = par64(r & tm.a0) ^ int(tm.b0);
                 if (tm.kind == 2) s ^= par64(r & tm.a1) ^ int(tm.b1);
-                dg += s ? -tm.coef : tm.coef;
+                dg += s ? -cf : cf;
             }
         }
-        const double lr = dg * double(p.x) + xr, li = dg * double(p.y) + xi;
-        if (WRITE) {
-            E l;
-            l.x = R(lr);
-            l.y = R(li);
-            lam[r] = l;
-        }
-        en += double(p.x) * lr + double(p.y) * li;  // Re(conj(psi) lambda)
+        E l;
+        l.x = dg * p.x + xr;
+        l.y = dg * p.y + xi;
+        if (WRITE) lam[r] = l;
+        en += double(p.x) * double(l.x) + double(p.y) * double(l.y);  // Re(conj(psi) lambda)
     }
     en = block_sum(en, sh);
     if (threadIdx.x == 0) atomicAdd(energy, en);

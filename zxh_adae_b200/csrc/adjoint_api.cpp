@@ -103,6 +103,8 @@ int compile_terms(zxh_sim *s, const zxh_term *terms, size_t nterms, AffineMap &A
         }
         out.push_back(d);
     }
+    // X terms first: the lambda kernels issue their gathers back to back
+    std::stable_partition(out.begin(), out.end(), [](const TermDev &t) { return t.kind == ZXH_TERM_X; });
     return ZXH_OK;
 }
 

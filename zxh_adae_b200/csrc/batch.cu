@@ -87,25 +87,25 @@ __device__ __forceinline__ void lambda_body(const E *psi, E *lam, uint64_t b, ui
     double en = 0.0;
     for (uint64_t r = b + threadIdx.x; r < e; r += kThreads) {
         const E p = __ldcg(psi + r);
-        double dg = 0.0, xr = 0.0, xi = 0.0;
+        R dg = 0, xr = 0, xi = 0;  // lambda in the state's precision, the energy in FP64
         for (uint32_t t = 0; t < nterms; t++) {
             const TermDev &tm = sm.t[t];
+            const R cf = R(tm.coef);
             if (tm.kind == 3) {
                 const E q = __ldcg(psi + (r ^ tm.delta));
-                xr += tm.coef * double(q.x);
-                xi += tm.coef * double(q.y);
+                xr += cf * q.x;
+                xi += cf * q.y;
             } else {
                 int s = par64(r & tm.a0) ^ int(tm.b0);
                 if (tm.kind == 2) s ^= par64(r & tm.a1) ^ int(tm.b1);
-                dg += s ? -tm.coef : tm.coef;
+                dg += s ? -cf : cf;
             }
         }
-        const double lr = dg * double(p.x) + xr, li = dg * double(p.y) + xi;
         E l;
-        l.x = R(lr);
-        l.y = R(li);
+        l.x = dg * p.x + xr;
+        l.y = dg * p.y + xi;
         __stcg(lam + r, l);
-        en += double(p.x) * lr + double(p.y) * li;
+        en += double(p.x) * double(l.x) + double(p.y) * double(l.y);
     }
     en = cta_sum(en, sm.red);
     if (threadIdx.x == 0) atomicAdd(energy, en);
