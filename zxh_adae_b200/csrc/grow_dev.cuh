@@ -675,17 +675,19 @@ __device__ __forceinline__ void grow_body(const uint8_t *__restrict__ blob, uint
                 atomicAdd(&grads[s_t[1][q].slot], t);
             }
         }
-        for (uint32_t g = 0; g < ngates && g < uint32_t(kGrowAdjGates); g++) {
-            if ((s_g[g][3] >> 8) == 0) continue;  // uniform: no gradient for this gate
-            double v = warp_sum_f64(acc[g]);
-            if (lane == 0) s_red[warp] = v;
-            __syncthreads();
-            if (tid == 0) {
-                double t = 0.0;
-                for (int w = 0; w < WARPS; w++) t += s_red[w];
-                atomicAdd(&grads[gates[g].slot], t);
-            }
-            __syncthreads();
+        // every gate's warp sums in one shared table, one barrier, one atomic per gate
+        __syncthreads();  // s_tacc may still be read by the window reduction above
+#pragma unroll
+        for (int g = 0; g < kGrowAdjGates; g++) {
+            if (uint32_t(g) >= ngates) break;
+            const double v = warp_sum_f64(acc[g]);
+            if (lane == 0) sm.s_tacc[warp][g] = v;
+        }
+        __syncthreads();
+        if (tid < int(ngates) && tid < kGrowAdjGates && (s_g[tid][3] >> 8) != 0) {
+            double t = 0.0;
+            for (int w = 0; w < WARPS; w++) t += sm.s_tacc[w][tid];
+            atomicAdd(&grads[gates[tid].slot], t);
         }
     }
 }
