@@ -251,3 +251,50 @@ def test_fast_u3_pass_edges(dtype, n):
     gates = _layers_with_x(n, 4, seed=n)
     o, s = run_pair(n, gates, dtype)
     assert max_err(s, o) <= TOL[dtype]
+
+
+def _run_knobs(n, gates, dtype, knobs):
+    o = Oracle(n)
+    o.push(gates)
+    o.execute()
+    s = zx.ZXH(n, dtype=dtype)
+    for k, v in knobs.items():
+        s.set_param(k, v)
+    s.push_gates(gates)
+    s.execute()
+    return o, s
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+@pytest.mark.parametrize("knobs", [{"low_pass": 0}, {"low_regs_c64": 0, "low_regs_c128": 0},
+                                   {"low_regs_c64": 2, "low_regs_c128": 3}, {"real_split": 0}, {}])
+@pytest.mark.parametrize("n", [10, 12, 13, 18])
+def test_low_pass_forms(dtype, knobs, n):
+    # TMA fast pass + strided passes, and the strided low pass (lane bits swapped
+    # into registers through shared memory) with 0..4 register gates, with the
+    # gates as complex matrices or as real rotations whose phases ride in the
+    # windows: the same state, with X-flipped selectors and fused windows
+    gates = _layers_with_x(n, 4, seed=40 + n)
+    o, s = _run_knobs(n, gates, dtype, knobs)
+    assert max_err(s, o) <= TOL[dtype]
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+@pytest.mark.parametrize("seed", range(8))
+def test_low_pass_gate_subsets(dtype, seed):
+    # U3 layers on random qubit subsets: low passes with and without gates on the
+    # swapped lane bits, on the unswapped lane bit, on the vector bit, with padded
+    # register bits; windows between the layers fuse before and after
+    n = 11 + seed % 4
+    rng = np.random.default_rng(900 + seed)
+    recs = [(zx._core.H, 0, q) for q in range(n)]
+    for layer in range(4):
+        qs = [q for q in range(n) if rng.random() < 0.5] or [0]
+        for q in qs:
+            recs.append((zx._core.U3, 0, q, *rng.uniform(0, 2 * np.pi, 3)))
+        for i in range(n - 1):
+            if rng.random() < 0.5:
+                recs.append((zx._core.CP, i, i + 1, rng.uniform(0, 2 * np.pi)))
+        recs.append((zx._core.P, 0, int(rng.integers(n)), rng.uniform(0, 2 * np.pi)))
+    o, s = _run_knobs(n, zx.as_records(recs), dtype, {})
+    assert max_err(s, o) <= TOL[dtype]

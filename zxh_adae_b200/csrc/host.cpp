@@ -7,6 +7,7 @@
 #include "host.h"
 
 #include <algorithm>
+#include <deque>
 #include <cmath>
 #include <map>
 #include <stdexcept>
@@ -440,6 +441,29 @@ uint64_t pext_pos(uint64_t x, const uint8_t *pos, int T)
     return r;
 }
 
+// Splits a 2x2 unitary into e^{i a} P(b) [[c, -s], [s, c]] P(d), P(t) = diag(1,
+// e^{i t}): a = arg u00, b = arg u10 - a, and d from the larger of u11 (c >= s) and
+// -u01, so every entry is reproduced from the phases of the entries that carry
+// its weight (a tiny c or s makes the other phase ill-defined, not the product).
+struct RealSplit {
+    double c, s, a, b, d;
+};
+
+RealSplit real_split(const cd u[4])
+{
+    double c = std::abs(u[0]), s = std::abs(u[2]);
+    const double r = std::hypot(c, s);
+    c /= r;
+    s /= r;
+    RealSplit o;
+    o.c = c;
+    o.s = s;
+    o.a = std::arg(u[0]);
+    o.b = std::arg(u[2]) - o.a;
+    o.d = c >= s ? std::arg(u[3]) - o.a - o.b : std::arg(-u[1]) - o.a;
+    return o;
+}
+
 // Compiles one window for a tile geometry; returns its blob offset.
 uint64_t compile_diag(std::vector<uint8_t> &blob, const std::vector<DiagTerm> &terms, const TileDev &g)
 {
@@ -868,6 +892,8 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
     const int tmax = elem_bytes == 8 ? pp.tile_bits_c64 : pp.tile_bits_c128;
     int last_tile_pass = -1;          // index of a tile pass that can take an epilogue
     const std::vector<DiagTerm> *held = nullptr;  // window waiting for the next tile pass
+    std::deque<std::vector<DiagTerm>> owned;       // windows the planner builds (stable addresses)
+    std::vector<DiagTerm> carry;                   // phases split off the last U3 batch, due after it
 
     auto emit_tile = [&](int mm, int c, const std::vector<int> &dirs, const std::vector<const U3Op *> &u3s,
                          const std::vector<DiagTerm> *pro) {
@@ -947,6 +973,20 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
         slot = off;
         ps.off2 = exp_off;
         return true;
+    };
+
+    // The carried phases as the last pass's epilogue, else on their own.
+    auto flush_carry = [&]() {
+        if (carry.empty()) return;
+        const std::vector<DiagTerm> w = carry;
+        carry.clear();
+        if (last_tile_pass >= 0 && out.passes[last_tile_pass].kind == Pass::ROW && out.passes[last_tile_pass].m == m &&
+            fuse_fast(out.passes[last_tile_pass], w, false)) {
+            last_tile_pass = -1;
+            return;
+        }
+        standalone_diag(m, w);
+        last_tile_pass = -1;
     };
 
     const int tfast = fast_tile_bits(elem_bytes);
@@ -1077,36 +1117,65 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
 
     for (; i < ops.size(); i++) {
         const Op &op = ops[i];
+        const std::vector<DiagTerm> *wd = op.kind == Op::DIAG ? &op.diag : nullptr;  // this op's window
+        if (!carry.empty()) {
+            if (op.kind == Op::DIAG) {  // diagonal windows commute: one window
+                owned.push_back(carry);
+                owned.back().insert(owned.back().end(), op.diag.begin(), op.diag.end());
+                wd = &owned.back();
+                carry.clear();
+            } else if (op.kind == Op::U3BATCH && fast_ok(op) && !held && op.m == m) {
+                owned.push_back(carry);  // the next batch's prologue
+                held = &owned.back();
+                carry.clear();
+            } else {
+                flush_carry();
+            }
+        }
         if (op.kind == Op::U3BATCH && fast_ok(op)) {
             const int mm = op.m;
-            std::vector<const U3Op *> gs;
-            for (const U3Op &u : op.u3) gs.push_back(&u);
-            std::sort(gs.begin(), gs.end(), [](const U3Op *a, const U3Op *b) { return a->delta < b->delta; });
-            const int G = std::max(pp.fast_gates, row_fixed_bits(elem_bytes, (elem_bytes == 8 ? pp.row_wide_c64 : pp.row_wide_c128)));
-            std::vector<std::pair<std::vector<int>, std::vector<const U3Op *>>> groups;
-            size_t k = 0;
-            {
-                std::vector<const U3Op *> first;
-                while (k < gs.size() && int(first.size()) < G && (gs[k]->delta >> tfast) == 0) first.push_back(gs[k++]);
-                if (!first.empty()) groups.push_back({std::vector<int>(), first});
+            // strided register passes: fixed gates (bits below frow: vector and lane
+            // coordinates) plus up to rrow gates on register bits
+            const int rwide = elem_bytes == 8 ? pp.row_wide_c64 : pp.row_wide_c128;
+            const int frow = row_fixed_bits(elem_bytes, rwide), rrow = row_reg_bits(elem_bytes, rwide);
+            const bool low_path = pp.low_pass && row_low_ok(elem_bytes, rwide) && mm >= frow + rrow;
+            // real split: gate = e^{i a} P(b) rotation P(d); the P(d) of every gate
+            // joins the prologue, P(b) and e^{i a} are carried to after the batch
+            const bool split = low_path && pp.real_split;
+            std::vector<U3Op> rot;
+            std::vector<DiagTerm> pre_ph;
+            if (split) {
+                rot = op.u3;
+                for (U3Op &u : rot) {
+                    const RealSplit r = real_split(u.u);
+                    u.u[0] = cd(r.c, 0.0);
+                    u.u[1] = cd(-r.s, 0.0);
+                    u.u[2] = cd(r.s, 0.0);
+                    u.u[3] = cd(r.c, 0.0);
+                    DiagTerm t;
+                    t.s0 = u.sel;
+                    t.theta = r.d;
+                    pre_ph.push_back(t);
+                    t.theta = r.b;
+                    carry.push_back(t);
+                    t.s0 = Sel{0, 1};  // constant selector: global phase
+                    t.theta = r.a;
+                    carry.push_back(t);
+                }
+                owned.push_back(held ? *held : std::vector<DiagTerm>());
+                owned.back().insert(owned.back().end(), pre_ph.begin(), pre_ph.end());
+                held = &owned.back();
             }
-            const int first_pass = int(out.passes.size());
-            for (size_t gidx = 0; gidx < groups.size(); gidx++)
-                last_tile_pass = emit_fast(mm, tfast, groups[gidx].first, groups[gidx].second);
-            // the rest: strided register passes over the high bits
-            const int frow = row_fixed_bits(elem_bytes, (elem_bytes == 8 ? pp.row_wide_c64 : pp.row_wide_c128)), rrow = row_reg_bits(elem_bytes, (elem_bytes == 8 ? pp.row_wide_c64 : pp.row_wide_c128));
-            while (k < gs.size()) {
-                std::vector<const U3Op *> grp;
-                while (k < gs.size() && int(grp.size()) < rrow) grp.push_back(gs[k++]);
+            std::vector<const U3Op *> gs;
+            for (const U3Op &u : (split ? rot : op.u3)) gs.push_back(&u);
+            std::sort(gs.begin(), gs.end(), [](const U3Op *a, const U3Op *b) { return a->delta < b->delta; });
+            auto emit_row = [&](const std::vector<const U3Op *> &fixed, const std::vector<const U3Op *> &grp, int low) {
                 std::vector<int> rb;
                 for (const U3Op *u : grp) rb.push_back(__builtin_ctzll(u->delta));
                 // pad with the lowest free bits so every thread keeps 2^R rows in flight
                 for (int b = frow; int(rb.size()) < rrow && b < mm; b++)
                     if (std::find(rb.begin(), rb.end(), b) == rb.end()) rb.push_back(b);
                 std::sort(rb.begin(), rb.end());
-                std::vector<int> coord_of(grp.size());
-                for (size_t r = 0; r < grp.size(); r++)
-                    coord_of[r] = frow + int(std::find(rb.begin(), rb.end(), __builtin_ctzll(grp[r]->delta)) - rb.begin());
                 Pass ps;
                 ps.kind = Pass::ROW;
                 ps.m = mm;
@@ -1115,26 +1184,56 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
                 ps.row.m = uint32_t(mm);
                 ps.row.F = uint32_t(frow);
                 ps.row.R = uint32_t(rb.size());
-                ps.row.ngates = uint32_t(grp.size());
+                ps.row.ngates = uint32_t(fixed.size() + grp.size());
                 for (size_t r = 0; r < rb.size(); r++) ps.row.rb[r] = uint8_t(rb[r]);
                 ps.row.tile_mask = ps.geom.tile_mask;
                 ps.row.nitems = 1ULL << (mm - frow - int(rb.size()));
-                ps.wide = (elem_bytes == 8 ? pp.row_wide_c64 : pp.row_wide_c128);
-                for (size_t r = 0; r < grp.size(); r++) {
+                ps.wide = rwide;
+                ps.low = low;
+                ps.real = split ? 1 : 0;
+                auto add = [&](const U3Op *u, int coord) {
                     FastGateDev fg;
                     std::memset(&fg, 0, sizeof(fg));
-                    fg.coord = uint32_t(coord_of[r]);
-                    fg.alpha_out = grp[r]->sel.alpha & ~ps.geom.tile_mask;
-                    fg.beta = uint32_t(grp[r]->sel.beta);
+                    fg.coord = uint32_t(coord);
+                    fg.alpha_out = u->sel.alpha & ~ps.geom.tile_mask;
+                    fg.beta = uint32_t(u->sel.beta);
                     for (int q = 0; q < 4; q++) {
-                        fg.u[2 * q] = grp[r]->u[q].real();
-                        fg.u[2 * q + 1] = grp[r]->u[q].imag();
+                        fg.u[2 * q] = u->u[q].real();
+                        fg.u[2 * q + 1] = u->u[q].imag();
                     }
                     ps.fgates.push_back(fg);
-                }
+                };
+                for (const U3Op *u : fixed) add(u, __builtin_ctzll(u->delta));
+                for (const U3Op *u : grp)
+                    add(u, frow + int(std::find(rb.begin(), rb.end(), __builtin_ctzll(u->delta)) - rb.begin()));
                 out.passes.push_back(ps);
                 last_tile_pass = int(out.passes.size()) - 1;
+            };
+            size_t k = 0;
+            const int first_pass = int(out.passes.size());
+            std::vector<const U3Op *> lows, lgrp;  // the low pass: gates on the fixed bits + low_regs more
+            if (low_path) {
+                const int nreg = std::min(rrow, elem_bytes == 8 ? pp.low_regs_c64 : pp.low_regs_c128);
+                while (k < gs.size() && (gs[k]->delta >> frow) == 0) lows.push_back(gs[k++]);
+                if (!lows.empty())
+                    while (k < gs.size() && int(lgrp.size()) < nreg) lgrp.push_back(gs[k++]);
+                // with split gates the low pass runs last (gates on different bits
+                // commute): the phase windows then ride in the strided passes,
+                // which have issue slots to spare, and the low pass has none
+                if (!lows.empty() && !split) emit_row(lows, lgrp, 1);
+            } else {
+                const int G = std::max(pp.fast_gates, frow);
+                std::vector<const U3Op *> first;
+                while (k < gs.size() && int(first.size()) < G && (gs[k]->delta >> tfast) == 0) first.push_back(gs[k++]);
+                if (!first.empty()) last_tile_pass = emit_fast(mm, tfast, std::vector<int>(), first);
             }
+            // the rest: strided register passes over the high bits
+            while (k < gs.size()) {
+                std::vector<const U3Op *> grp;
+                while (k < gs.size() && int(grp.size()) < rrow) grp.push_back(gs[k++]);
+                emit_row(std::vector<const U3Op *>(), grp, 0);
+            }
+            if (!lows.empty() && split) emit_row(lows, lgrp, 1);
             if (held) {
                 if (!fuse_fast(out.passes[first_pass], *held, true)) {
                     // not fusable: run it on its own, before the batch
@@ -1153,25 +1252,28 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
         }
         if (op.kind == Op::DIAG) {
             if (held) standalone_diag(m, *held), held = nullptr;
-            if (last_tile_pass >= 0 &&
+            // a window after a low pass waits for the next batch's first pass if there is one
+            const bool next_u3 = i + 1 < ops.size() && ops[i + 1].kind == Op::U3BATCH && ops[i + 1].m == op.m;
+            const bool spare_low = last_tile_pass >= 0 && out.passes[last_tile_pass].low && next_u3;
+            if (!spare_low && last_tile_pass >= 0 &&
                 (out.passes[last_tile_pass].kind == Pass::FAST || out.passes[last_tile_pass].kind == Pass::ROW) &&
-                out.passes[last_tile_pass].m == op.m && fuse_fast(out.passes[last_tile_pass], op.diag, false)) {
+                out.passes[last_tile_pass].m == op.m && fuse_fast(out.passes[last_tile_pass], *wd, false)) {
                 last_tile_pass = -1;
             } else if (last_tile_pass >= 0 && out.passes[last_tile_pass].kind == Pass::GROW &&
                        out.passes[last_tile_pass].m == op.m && out.passes[last_tile_pass].gb.dev.ncls[1][2] == 0 &&
-                       out.passes[last_tile_pass].gb.add_window(1, op.diag)) {
+                       out.passes[last_tile_pass].gb.add_window(1, *wd)) {
                 ensure_exp();
                 out.passes[last_tile_pass].off2 = exp_off;
                 last_tile_pass = -1;
             } else if (last_tile_pass >= 0 && out.passes[last_tile_pass].kind == Pass::TILE &&
                        out.passes[last_tile_pass].m == op.m &&
                        out.passes[last_tile_pass].steps.size() < size_t(pp.max_steps)) {
-                attach_epilogue(last_tile_pass, op.diag);
+                attach_epilogue(last_tile_pass, *wd);
                 last_tile_pass = -1;  // keep one epilogue window per pass
-            } else if (i + 1 < ops.size() && ops[i + 1].kind == Op::U3BATCH && ops[i + 1].m == op.m) {
-                held = &op.diag;
+            } else if (next_u3) {
+                held = wd;
             } else {
-                standalone_diag(op.m, op.diag);
+                standalone_diag(op.m, *wd);
                 last_tile_pass = -1;
             }
             continue;
@@ -1301,6 +1403,7 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
         held = nullptr;
         m = mm;
     }
+    flush_carry();
     if (held) standalone_diag(m, *held);
 
     // finalize step arrays

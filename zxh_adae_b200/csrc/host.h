@@ -42,6 +42,12 @@ struct PlanParams {
     int fast_contig_c128 = 3;   // same for complex128
     int row_wide_c64 = 0;       // strided high-qubit pass shape, complex64: 0 = 16-byte lanes x 16 rows, 1 = 8-byte x 32
     int row_wide_c128 = 1;      // complex128: 0 = 8 rows, 1 = 16 rows
+    int low_pass = 1;           // 1: gates on the lane / vector bits ride in a strided low pass (lane bits
+                                // swapped into registers) instead of the TMA fast pass
+    int low_regs_c64 = 4;       // gates on register bits that join the low pass, complex64 (0..4)
+    int low_regs_c128 = 4;      // same for complex128
+    int real_split = 1;         // 1: in all-strided U3 batches each gate runs as a real rotation; its phases
+                                // ride in the windows before / after the batch (half the multiply-adds)
     int max_steps = 16;
     int diag_row_bits_c64 = 3;  // log2 rows of a warp tile in a diagonal pass (tile = 64 amplitudes x rows)
     int diag_row_bits_c128 = 2; // same for complex128 (tile = 32 amplitudes x rows)
@@ -88,6 +94,8 @@ struct Pass {
     FastDev fast;                        // FAST
     RowPassDev row;                      // ROW
     int wide = 0;                        // ROW: kernel shape
+    int low = 0;                         // ROW: the low pass (lane bits 0..3 swapped into registers)
+    int real = 0;                        // ROW: every gate matrix is real
     int chunk_bits = -1;                 // DIAG: tiles per Gray-code chunk (log2, -1 = automatic)
     int row_bits = 0;                    // DIAG: log2 rows of a warp tile
     std::vector<FastGateDev> fgates;     // FAST
@@ -107,6 +115,7 @@ int fast_tile_bits(int elem_bytes);
 int fast_reg_bits(int elem_bytes);
 int row_reg_bits(int elem_bytes, int wide);
 int row_fixed_bits(int elem_bytes, int wide);
+bool row_low_ok(int elem_bytes, int wide);  // the shape has the 16 rows of 16 bytes the low pass swaps
 
 int plan(const std::vector<Op> &ops, int elem_bytes, const PlanParams &pp, const WalkState &start, Plan &out,
          std::string &err);

@@ -539,7 +539,8 @@ cudaError_t run_passes(const std::vector<Pass> &passes, const uint8_t *dblob, vo
                 expand_kernel<double2><<<grid, kThreads, 0, st>>>(dblob, ps.off, static_cast<double2 *>(state));
             e = cudaGetLastError();
         } else if (ps.kind == Pass::ROW) {
-            e = run_row_pass(dblob, ps.off, ps.off2, ps.row.nitems, elem_bytes, ps.wide, state, sms, st);
+            e = run_row_pass(dblob, ps.off, ps.off2, ps.row.nitems, elem_bytes, ps.wide, ps.low != 0, ps.real != 0,
+                             ps.row.off_pre != 0 || ps.row.off_post != 0, state, sms, st);
         } else if (ps.kind == Pass::FAST) {
             e = run_fast_tile(dblob, ps.off, ps.off2, ps.geom.ntiles, elem_bytes, state, status, sms, st);
         } else if (ps.kind == Pass::INIT) {

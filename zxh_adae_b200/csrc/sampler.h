@@ -43,8 +43,10 @@ cudaError_t run_diag(const uint8_t *dblob, uint64_t doff, uint64_t toff, int m, 
 int diag_tile_bits(int elem_bytes, int row_bits);
 cudaError_t run_fast_tile(const uint8_t *dblob, uint64_t foff, uint64_t toff, uint64_t ntiles, int elem_bytes,
                           void *state, DevStatus *status, int sms, cudaStream_t st);
+// low: the low pass (lane bits swapped into registers); real: every gate of the
+// pass has a real matrix (both need row_low_ok); win: the pass has a window.
 cudaError_t run_row_pass(const uint8_t *dblob, uint64_t poff, uint64_t toff, uint64_t nitems, int elem_bytes,
-                         int wide, void *state, int sms, cudaStream_t st);
+                         int wide, bool low, bool real, bool win, void *state, int sms, cudaStream_t st);
 // amplitude 0 := 1 (the rest of an INIT pass is a memset)
 cudaError_t run_set_one(void *state, int elem_bytes, cudaStream_t st);
 // General strided pass (grow.cu): lam == nullptr applies the pass to psi; otherwise

@@ -156,9 +156,21 @@ __device__ __forceinline__ E cmad2(RT ar, RT ai, E x, RT br, RT bi, E y)
     return o;
 }
 
+// a * x + b * y for real a, b: complex64 amplitudes as (re, im) pairs take paired
+// FP32 FMAs (two lanes of work per instruction).
+__device__ __forceinline__ float2 rmad2(float a, float2 x, float b, float2 y)
+{
+    return __ffma2_rn(make_float2(b, b), y, __fmul2_rn(make_float2(a, a), x));
+}
+__device__ __forceinline__ double2 rmad2(double a, double2 x, double b, double2 y)
+{
+    return make_double2(fma(b, y.x, a * x.x), fma(b, y.y, a * x.y));
+}
+
 // 2x2 gate on register bit RR of every row pair: compile-time positions keep the
-// amplitudes in registers.
-template <int RR, int NR, int V, typename VT, typename RT>
+// amplitudes in registers. REAL: the matrix has no imaginary parts (a rotation
+// split off a U3 by the planner), half the multiply-adds.
+template <int RR, int NR, int V, bool REAL, typename VT, typename RT>
 __device__ __forceinline__ void reg_gate(VT (&x)[NR], const RT *u)
 {
     using E = decltype(vget(x[0], 0));
@@ -170,15 +182,20 @@ __device__ __forceinline__ void reg_gate(VT (&x)[NR], const RT *u)
 #pragma unroll
         for (int v = 0; v < V; v++) {
             const E lo = vget(x[j], v), hi = vget(x[j | (1 << RR)], v);
-            vset(x[j], v, cmad2(m00r, m00i, lo, m01r, m01i, hi));
-            vset(x[j | (1 << RR)], v, cmad2(m10r, m10i, lo, m11r, m11i, hi));
+            if constexpr (REAL) {
+                vset(x[j], v, rmad2(m00r, lo, m01r, hi));
+                vset(x[j | (1 << RR)], v, rmad2(m10r, lo, m11r, hi));
+            } else {
+                vset(x[j], v, cmad2(m00r, m00i, lo, m01r, m01i, hi));
+                vset(x[j | (1 << RR)], v, cmad2(m10r, m10i, lo, m11r, m11i, hi));
+            }
         }
     }
 }
 
 // One gate on tile coordinate c of a row-pass thread's amplitudes: c < LV is the
 // vector bit, c < F a lane bit (partner by shfl.xor), otherwise register bit c - F.
-template <int R, int V, int LV, int F, typename VT, typename RT>
+template <int R, int V, int LV, int F, bool REAL = false, typename VT, typename RT>
 __device__ __forceinline__ void row_gate(VT (&x)[1 << R], uint32_t c, const RT *u, int lane)
 {
     using E = decltype(vget(x[0], 0));
@@ -189,8 +206,13 @@ __device__ __forceinline__ void row_gate(VT (&x)[1 << R], uint32_t c, const RT *
 #pragma unroll
         for (int j = 0; j < NR; j++) {
             const E lo = vget(x[j], 0), hi = vget(x[j], V - 1);
-            vset(x[j], 0, cmad2(m00r, m00i, lo, m01r, m01i, hi));
-            vset(x[j], V - 1, cmad2(m10r, m10i, lo, m11r, m11i, hi));
+            if constexpr (REAL) {
+                vset(x[j], 0, rmad2(m00r, lo, m01r, hi));
+                vset(x[j], V - 1, rmad2(m10r, lo, m11r, hi));
+            } else {
+                vset(x[j], 0, cmad2(m00r, m00i, lo, m01r, m01i, hi));
+                vset(x[j], V - 1, cmad2(m10r, m10i, lo, m11r, m11i, hi));
+            }
         }
     } else if (int(c) < F) {
         const int lb = int(c) - LV;
@@ -203,15 +225,16 @@ __device__ __forceinline__ void row_gate(VT (&x)[1 << R], uint32_t c, const RT *
             for (int v = 0; v < V; v++) {
                 const E mine = vget(x[j], v);
                 const E pt = shfl_xor_e(mine, 1 << lb);
-                vset(x[j], v, cmad2(ar, ai, mine, br, bi, pt));
+                if constexpr (REAL) vset(x[j], v, rmad2(ar, mine, br, pt));
+                else vset(x[j], v, cmad2(ar, ai, mine, br, bi, pt));
             }
     } else {
         switch (int(c) - F) {
-        case 0: reg_gate<0, NR, V>(x, u); break;
-        case 1: if constexpr (R > 1) reg_gate<(R > 1 ? 1 : 0), NR, V>(x, u); break;
-        case 2: if constexpr (R > 2) reg_gate<(R > 2 ? 2 : 0), NR, V>(x, u); break;
-        case 3: if constexpr (R > 3) reg_gate<(R > 3 ? 3 : 0), NR, V>(x, u); break;
-        case 4: if constexpr (R > 4) reg_gate<(R > 4 ? 4 : 0), NR, V>(x, u); break;
+        case 0: reg_gate<0, NR, V, REAL>(x, u); break;
+        case 1: if constexpr (R > 1) reg_gate<(R > 1 ? 1 : 0), NR, V, REAL>(x, u); break;
+        case 2: if constexpr (R > 2) reg_gate<(R > 2 ? 2 : 0), NR, V, REAL>(x, u); break;
+        case 3: if constexpr (R > 3) reg_gate<(R > 3 ? 3 : 0), NR, V, REAL>(x, u); break;
+        case 4: if constexpr (R > 4) reg_gate<(R > 4 ? 4 : 0), NR, V, REAL>(x, u); break;
         default: break;
         }
     }
@@ -473,7 +496,159 @@ struct RowCfg<double2, 1> {
 };
 
 
-template <typename E, int W>
+// Phases of a window fused into a strided pass, at one thread's amplitudes. Tile
+// coordinates are [0, F) = vector and lane bits, then F + r = register bit r;
+// base holds the item's out-of-tile bits. apply(row, v, turns) is called for every
+// row (in Gray-code order) and vector slot v.
+// A window with linear terms only: the phase is K(item) + A(lane, vector slot) +
+// B(row), so each amplitude takes one product of two factors: e^{i (K + A)} per
+// thread and item, e^{i B} per row from rowf (per CTA, shared). apply(row, v,
+// factor) is called for every amplitude.
+template <int F, int LV, int R, int V, typename E, typename Apply>
+__device__ __forceinline__ void row_window_linear(const uint8_t *blob, const DiagDev &dd, const E *rowf,
+                                                  const E *s_exp, uint64_t base, int lane, Apply &&apply)
+{
+    constexpr int NR = 1 << R;
+    const LinTerm *ol = reinterpret_cast<const LinTerm *>(blob + dd.off_out_lin);
+    int64_t K = 0;
+    for (uint32_t q = uint32_t(lane); q < dd.n_out_lin; q += 32)
+        if ((base >> ol[q].bit) & 1) K += ol[q].coef;
+    K = warp_sum_i64(K) + dd.c0;
+    E fa[V];
+#pragma unroll
+    for (int v = 0; v < V; v++) {
+        const uint32_t e = uint32_t(v) | (uint32_t(lane) << LV);
+        int64_t a = K;
+#pragma unroll
+        for (int k = 0; k < F; k++)
+            if ((e >> k) & 1) a += dd.lin_in[k];
+        fa[v] = phase_factor(s_exp, a);
+    }
+#pragma unroll
+    for (int j = 0; j < NR; j++) {
+        const E fb = rowf[j];
+#pragma unroll
+        for (int v = 0; v < V; v++) apply(j, v, cmul(fa[v], fb));
+    }
+}
+
+template <int F, int LV, int R, int V, typename Apply>
+__device__ __forceinline__ void row_window(const uint8_t *blob, const DiagDev &dd, const int64_t *qreg, uint64_t base,
+                                           int lane, Apply &&apply)
+{
+    constexpr int T = F + R;
+    constexpr int NR = 1 << R;
+    int64_t da = 0, K = 0;
+    const QuadTerm *cr = reinterpret_cast<const QuadTerm *>(blob + dd.off_cross);
+    const LinTerm *ol = reinterpret_cast<const LinTerm *>(blob + dd.off_out_lin);
+    const QuadTerm *oq = reinterpret_cast<const QuadTerm *>(blob + dd.off_out_quad);
+    const uint32_t *kidx = reinterpret_cast<const uint32_t *>(blob + dd.off_kidx);
+    if (lane < T) {
+        da = dd.lin_in[lane];
+        for (uint32_t q = kidx[lane]; q < kidx[lane + 1]; q++) {
+            const QuadTerm t = cr[q];
+            if ((base >> t.j) & 1) da += t.coef;
+        }
+    }
+    for (uint32_t q = uint32_t(lane); q < dd.n_out_lin; q += 32)
+        if ((base >> ol[q].bit) & 1) K += ol[q].coef;
+    for (uint32_t q = uint32_t(lane); q < dd.n_out_quad; q += 32) {
+        const QuadTerm t = oq[q];
+        if (((base >> t.i) & 1) && ((base >> t.j) & 1)) K += t.coef;
+    }
+    K = warp_sum_i64(K) + dd.c0;
+    int64_t acc[V], w[R][V];
+#pragma unroll
+    for (int v = 0; v < V; v++) {
+        acc[v] = K;
+#pragma unroll
+        for (int r = 0; r < R; r++) w[r][v] = 0;
+    }
+    // in-tile quadratic terms touching this thread's fixed (vector / lane) bits
+    const QuadTerm *iq = reinterpret_cast<const QuadTerm *>(blob + dd.off_in_quad);
+    for (uint32_t q = 0; q < dd.n_in_quad; q++) {
+        const QuadTerm t = iq[q];  // t.i < t.j
+        if (int(t.i) >= F) continue;
+#pragma unroll
+        for (int v = 0; v < V; v++) {
+            const uint32_t e = uint32_t(v) | (uint32_t(lane) << LV);
+            if (!((e >> t.i) & 1)) continue;
+            if (int(t.j) < F) {
+                if ((e >> t.j) & 1) acc[v] += t.coef;
+            } else {
+#pragma unroll
+                for (int r = 0; r < R; r++)
+                    if (int(t.j) - F == r) w[r][v] += t.coef;
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < F; k++) {
+        const int64_t dk = __shfl_sync(0xffffffffu, da, k);
+#pragma unroll
+        for (int v = 0; v < V; v++)
+            if (((uint32_t(v) | (uint32_t(lane) << LV)) >> k) & 1) acc[v] += dk;
+    }
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+        const int64_t dk = __shfl_sync(0xffffffffu, da, F + r);
+#pragma unroll
+        for (int v = 0; v < V; v++) w[r][v] += dk;
+    }
+#pragma unroll
+    for (int jj = 0; jj < NR; jj++) {
+        const int gj = jj ^ (jj >> 1);
+        if (jj > 0) {
+            const int fb = ctz_const(jj);
+#pragma unroll
+            for (int v = 0; v < V; v++) acc[v] += ((gj >> fb) & 1) ? w[fb][v] : -w[fb][v];
+        }
+        const int64_t qr = qreg[gj];
+#pragma unroll
+        for (int v = 0; v < V; v++) apply(gj, v, acc[v] + qr);
+    }
+}
+
+__device__ __forceinline__ float4 as_f4(const float4 &v) { return v; }
+__device__ __forceinline__ float4 as_f4(const double2 &v)
+{
+    return make_float4(__int_as_float(__double2loint(v.x)), __int_as_float(__double2hiint(v.x)),
+                       __int_as_float(__double2loint(v.y)), __int_as_float(__double2hiint(v.y)));
+}
+__device__ __forceinline__ void from_f4(float4 &v, const float4 &t) { v = t; }
+__device__ __forceinline__ void from_f4(double2 &v, const float4 &t)
+{
+    v.x = __hiloint2double(__float_as_int(t.y), __float_as_int(t.x));
+    v.y = __hiloint2double(__float_as_int(t.w), __float_as_int(t.z));
+}
+
+// Swaps lane bits 0..3 with register bits 0..3 of a strided-pass thread (16-byte
+// rows, 16 of them) through the warp's 16 x 32 shared-memory slots: slot of (lane
+// l, row j) = j * 32 + (l ^ (j & 7)), conflict-free both ways. Afterwards thread
+// L's row j holds what lane (L & 16) | j had in row L & 15. back = true undoes it.
+template <typename VT>
+__device__ __forceinline__ void lane_row_transpose(VT (&x)[16], float4 *tb, int lane, bool back)
+{
+    const int jr = lane & 15, hi = lane & 16;
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+        const int slot = back ? jr * 32 + (hi | (j ^ (jr & 7))) : j * 32 + (lane ^ (j & 7));
+        tb[slot] = as_f4(x[j]);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+        const int slot = back ? j * 32 + (lane ^ (j & 7)) : jr * 32 + (hi | (j ^ (jr & 7)));
+        from_f4(x[j], tb[slot]);
+    }
+}
+
+// XP (the low pass): the pass also owns the lowest bits. Gates on lane bits 0..3
+// run as register updates after lane_row_transpose (a second transpose restores
+// the layout before the store); the top lane bit keeps its shfl.xor gate. One pass
+// then applies gates on the F lowest bits and on 4 more with one read and one
+// write of every amplitude.
+template <typename E, int W, bool XP, bool REAL, bool WIN>
 __global__ void __launch_bounds__(kThreads, 2) row_pass_kernel(const uint8_t *__restrict__ blob, uint64_t poff,
                                                             uint64_t toff, E *__restrict__ state)
 {
@@ -485,6 +660,8 @@ __global__ void __launch_bounds__(kThreads, 2) row_pass_kernel(const uint8_t *__
     constexpr int R = RowCfg<E, W>::R;
     constexpr int NR = 1 << R;
     constexpr int WARPS = kThreads / 32;
+    static_assert(!XP || (R == 4 && sizeof(VT) == 16), "the low pass swaps 4 lane bits with 16 rows of 16 bytes");
+    extern __shared__ __align__(16) float4 s_xp[];  // XP: 16 x 32 slots per warp
 
     const RowPassDev &p = *reinterpret_cast<const RowPassDev *>(blob + poff);
     const FastGateDev *gates = reinterpret_cast<const FastGateDev *>(blob + p.off_gates);
@@ -501,8 +678,10 @@ __global__ void __launch_bounds__(kThreads, 2) row_pass_kernel(const uint8_t *__
     __shared__ uint32_t s_gc[kFastMaxGates];
     __shared__ int64_t s_qreg[2][NR];
     __shared__ uint64_t s_off[NR];
+    __shared__ E s_rowf[2][NR];  // linear windows: e^{i B(row)}
+    __shared__ int s_linear[2];
 
-    if (offw0 || offw1) {
+    if (WIN && (offw0 || offw1)) {
         const E *tab = reinterpret_cast<const E *>(blob + toff);
         for (int i = tid; i < (1 << kExpTableBits); i += kThreads) s_exp[i] = tab[i];
     }
@@ -539,6 +718,23 @@ __global__ void __launch_bounds__(kThreads, 2) row_pass_kernel(const uint8_t *__
         s_qreg[d][tid] = acc;
     }
     __syncthreads();
+    if (WIN) {
+#pragma unroll
+        for (int d = 0; d < 2; d++) {
+            const uint64_t ow = d ? offw1 : offw0;
+            if (!ow) continue;
+            const DiagDev &dd = *reinterpret_cast<const DiagDev *>(blob + ow);
+            const bool lin = dd.n_in_quad == 0 && dd.n_cross == 0 && dd.n_out_quad == 0 && dd.n_gen == 0;
+            if (tid == 0) s_linear[d] = lin ? 1 : 0;
+            if (lin && tid < NR) {
+                int64_t b = 0;
+                for (int r = 0; r < R; r++)
+                    if ((tid >> r) & 1) b += dd.lin_in[F + r];
+                s_rowf[d][tid] = phase_factor(s_exp, b);
+            }
+        }
+        __syncthreads();
+    }
 
     const uint64_t stride = uint64_t(gridDim.x) * WARPS;
     for (uint64_t item = uint64_t(blockIdx.x) * WARPS + uint64_t(warp); item < nitems; item += stride) {
@@ -562,82 +758,47 @@ __global__ void __launch_bounds__(kThreads, 2) row_pass_kernel(const uint8_t *__
         }
         const uint32_t omask = __ballot_sync(0xffffffffu, ob);
 
-        auto window = [&](const DiagDev &dd, const int64_t *qreg) {
-            constexpr int T = F + R;
-            int64_t da = 0, K = 0;
-            const QuadTerm *cr = reinterpret_cast<const QuadTerm *>(blob + dd.off_cross);
-            const LinTerm *ol = reinterpret_cast<const LinTerm *>(blob + dd.off_out_lin);
-            const QuadTerm *oq = reinterpret_cast<const QuadTerm *>(blob + dd.off_out_quad);
-            const uint32_t *kidx = reinterpret_cast<const uint32_t *>(blob + dd.off_kidx);
-            if (lane < T) {
-                da = dd.lin_in[lane];
-                for (uint32_t q = kidx[lane]; q < kidx[lane + 1]; q++) {
-                    const QuadTerm t = cr[q];
-                    if ((base >> t.j) & 1) da += t.coef;
-                }
-            }
-            for (uint32_t q = uint32_t(lane); q < dd.n_out_lin; q += 32)
-                if ((base >> ol[q].bit) & 1) K += ol[q].coef;
-            for (uint32_t q = uint32_t(lane); q < dd.n_out_quad; q += 32) {
-                const QuadTerm t = oq[q];
-                if (((base >> t.i) & 1) && ((base >> t.j) & 1)) K += t.coef;
-            }
-            K = warp_sum_i64(K) + dd.c0;
-            int64_t acc[V], w[R][V];
-#pragma unroll
-            for (int v = 0; v < V; v++) {
-                acc[v] = K;
-#pragma unroll
-                for (int r = 0; r < R; r++) w[r][v] = 0;
-            }
-            // in-tile quadratic terms touching this thread's fixed (vector / lane) bits
-            const QuadTerm *iq = reinterpret_cast<const QuadTerm *>(blob + dd.off_in_quad);
-            for (uint32_t q = 0; q < dd.n_in_quad; q++) {
-                const QuadTerm t = iq[q];  // t.i < t.j
-                if (int(t.i) >= F) continue;
-#pragma unroll
-                for (int v = 0; v < V; v++) {
-                    const uint32_t e = uint32_t(v) | (uint32_t(lane) << LV);
-                    if (!((e >> t.i) & 1)) continue;
-                    if (int(t.j) < F) {
-                        if ((e >> t.j) & 1) acc[v] += t.coef;
-                    } else {
-#pragma unroll
-                        for (int r = 0; r < R; r++)
-                            if (int(t.j) - F == r) w[r][v] += t.coef;
-                    }
-                }
-            }
-#pragma unroll
-            for (int k = 0; k < F; k++) {
-                const int64_t dk = __shfl_sync(0xffffffffu, da, k);
-#pragma unroll
-                for (int v = 0; v < V; v++)
-                    if (((uint32_t(v) | (uint32_t(lane) << LV)) >> k) & 1) acc[v] += dk;
-            }
-#pragma unroll
-            for (int r = 0; r < R; r++) {
-                const int64_t dk = __shfl_sync(0xffffffffu, da, F + r);
-#pragma unroll
-                for (int v = 0; v < V; v++) w[r][v] += dk;
-            }
-#pragma unroll
-            for (int jj = 0; jj < NR; jj++) {
-                const int gj = jj ^ (jj >> 1);
-                if (jj > 0) {
-                    const int fb = ctz_const(jj);
-#pragma unroll
-                    for (int v = 0; v < V; v++) acc[v] += ((gj >> fb) & 1) ? w[fb][v] : -w[fb][v];
-                }
-                const int64_t qr = qreg[gj];
-#pragma unroll
-                for (int v = 0; v < V; v++) vset(x[gj], v, cmul(vget(x[gj], v), phase_factor(s_exp, acc[v] + qr)));
-            }
+        auto window = [&](int d, uint64_t ow) {
+            const DiagDev &dd = *reinterpret_cast<const DiagDev *>(blob + ow);
+            if (s_linear[d])
+                row_window_linear<F, LV, R, V>(blob, dd, s_rowf[d], s_exp, base, lane, [&](int j, int v, E f) {
+                    vset(x[j], v, cmul(vget(x[j], v), f));
+                });
+            else
+                row_window<F, LV, R, V>(blob, dd, s_qreg[d], base, lane, [&](int j, int v, int64_t th) {
+                    vset(x[j], v, cmul(vget(x[j], v), phase_factor(s_exp, th)));
+                });
         };
-        if (offw0) window(*reinterpret_cast<const DiagDev *>(blob + offw0), s_qreg[0]);
-        for (uint32_t gi = 0; gi < ngates; gi++)
-            row_gate<R, V, LV, F>(x, s_gc[gi], &s_u[gi][(omask >> gi) & 1][0], lane);
-        if (offw1) window(*reinterpret_cast<const DiagDev *>(blob + offw1), s_qreg[1]);
+        if constexpr (WIN) {
+            if (offw0) window(0, offw0);
+        }
+        // XP: phase 0 runs the gates on the vector, top lane and register bits,
+        // phase 1 (after the transpose) those on lane bits 0..3 as register gates
+        bool swapped = false;
+        float4 *tb = s_xp + warp * (NR * 32);
+#pragma unroll 1
+        for (int ph = 0; ph < (XP ? 2 : 1); ph++) {
+            if constexpr (XP) {
+                if (ph == 1) {
+                    if (!swapped) break;
+                    lane_row_transpose(x, tb, lane, false);
+                }
+            }
+            for (uint32_t gi = 0; gi < ngates; gi++) {
+                uint32_t c = s_gc[gi];
+                const bool sw = XP && c - uint32_t(LV) < uint32_t(R);  // lane bits 0..R-1
+                swapped |= sw;
+                if (sw != (ph == 1)) continue;
+                if (sw) c = uint32_t(F) + c - uint32_t(LV);
+                row_gate<R, V, LV, F, REAL>(x, c, &s_u[gi][(omask >> gi) & 1][0], lane);
+            }
+        }
+        if constexpr (XP) {
+            if (swapped) lane_row_transpose(x, tb, lane, true);
+        }
+        if constexpr (WIN) {
+            if (offw1) window(1, offw1);
+        }
 #pragma unroll
         for (int j = 0; j < NR; j++)
             __stcs(reinterpret_cast<VT *>(rowp + s_off[j]), x[j]);
@@ -659,27 +820,56 @@ int row_fixed_bits(int elem_bytes, int wide)
     return 5 + (v == 2 ? 1 : 0);
 }
 
-template <typename E, int W>
+bool row_low_ok(int elem_bytes, int wide) { return row_reg_bits(elem_bytes, wide) == 4; }
+
+template <typename E, int W, bool XP, bool REAL, bool WIN>
 static cudaError_t launch_row(const uint8_t *dblob, uint64_t poff, uint64_t toff, uint64_t nitems, void *state,
                               int sms, cudaStream_t st)
 {
+    auto kern = row_pass_kernel<E, W, XP, REAL, WIN>;
+    const size_t smem = XP ? size_t(kThreads / 32) * 16 * 32 * sizeof(float4) : 0;
+    if (XP) {
+        const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        if (e != cudaSuccess) return e;
+    }
     int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, row_pass_kernel<E, W>, kThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem);
     if (per_sm < 1) per_sm = 1;
     const uint64_t ctas = (nitems + kThreads / 32 - 1) / (kThreads / 32);
     const unsigned grid = unsigned(std::max<uint64_t>(1, std::min<uint64_t>(ctas, uint64_t(sms) * uint64_t(per_sm))));
-    row_pass_kernel<E, W><<<grid, kThreads, 0, st>>>(dblob, poff, toff, static_cast<E *>(state));
+    kern<<<grid, kThreads, smem, st>>>(dblob, poff, toff, static_cast<E *>(state));
     return cudaGetLastError();
 }
 
-cudaError_t run_row_pass(const uint8_t *dblob, uint64_t poff, uint64_t toff, uint64_t nitems, int elem_bytes,
-                         int wide, void *state, int sms, cudaStream_t st)
+template <typename E, int W, bool XP, bool REAL>
+static cudaError_t launch_row_win(const uint8_t *dblob, uint64_t poff, uint64_t toff, uint64_t nitems, bool win,
+                                  void *state, int sms, cudaStream_t st)
 {
-    if (elem_bytes == 8)
-        return wide ? launch_row<float2, 1>(dblob, poff, toff, nitems, state, sms, st)
-                    : launch_row<float2, 0>(dblob, poff, toff, nitems, state, sms, st);
-    return wide ? launch_row<double2, 1>(dblob, poff, toff, nitems, state, sms, st)
-                : launch_row<double2, 0>(dblob, poff, toff, nitems, state, sms, st);
+    return win ? launch_row<E, W, XP, REAL, true>(dblob, poff, toff, nitems, state, sms, st)
+               : launch_row<E, W, XP, REAL, false>(dblob, poff, toff, nitems, state, sms, st);
+}
+
+// The low-pass shapes (16 rows of 16 bytes) also run with real gates.
+template <typename E, int W>
+static cudaError_t launch_row_low(const uint8_t *dblob, uint64_t poff, uint64_t toff, uint64_t nitems, bool low,
+                                  bool real, bool win, void *state, int sms, cudaStream_t st)
+{
+    if (low) return real ? launch_row_win<E, W, true, true>(dblob, poff, toff, nitems, win, state, sms, st)
+                         : launch_row_win<E, W, true, false>(dblob, poff, toff, nitems, win, state, sms, st);
+    return real ? launch_row_win<E, W, false, true>(dblob, poff, toff, nitems, win, state, sms, st)
+                : launch_row_win<E, W, false, false>(dblob, poff, toff, nitems, win, state, sms, st);
+}
+
+cudaError_t run_row_pass(const uint8_t *dblob, uint64_t poff, uint64_t toff, uint64_t nitems, int elem_bytes,
+                         int wide, bool low, bool real, bool win, void *state, int sms, cudaStream_t st)
+{
+    if (row_low_ok(elem_bytes, wide)) {
+        if (elem_bytes == 8) return launch_row_low<float2, 0>(dblob, poff, toff, nitems, low, real, win, state, sms, st);
+        return launch_row_low<double2, 1>(dblob, poff, toff, nitems, low, real, win, state, sms, st);
+    }
+    if (low || real) return cudaErrorInvalidValue;
+    if (elem_bytes == 8) return launch_row_win<float2, 1, false, false>(dblob, poff, toff, nitems, win, state, sms, st);
+    return launch_row_win<double2, 0, false, false>(dblob, poff, toff, nitems, win, state, sms, st);
 }
 
 }  // namespace zxh
