@@ -1206,6 +1206,22 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
                 for (const U3Op *u : fixed) add(u, __builtin_ctzll(u->delta));
                 for (const U3Op *u : grp)
                     add(u, frow + int(std::find(rb.begin(), rb.end(), __builtin_ctzll(u->delta)) - rb.begin()));
+                if (split) {
+                    // real passes take a dense table: one slot per coordinate (all of
+                    // them in the low pass, the register ones otherwise), identity
+                    // where the pass has no gate
+                    const int c0 = low ? 0 : frow, ns = low ? frow + int(rb.size()) : int(rb.size());
+                    std::vector<FastGateDev> dense(static_cast<size_t>(ns));
+                    for (int k2 = 0; k2 < ns; k2++) {
+                        std::memset(&dense[size_t(k2)], 0, sizeof(FastGateDev));
+                        dense[size_t(k2)].coord = uint32_t(c0 + k2);
+                        dense[size_t(k2)].u[0] = 1.0;
+                        dense[size_t(k2)].u[6] = 1.0;
+                    }
+                    for (const FastGateDev &fg : ps.fgates) dense[size_t(int(fg.coord) - c0)] = fg;
+                    ps.fgates = dense;
+                    ps.row.ngates = uint32_t(ns);
+                }
                 out.passes.push_back(ps);
                 last_tile_pass = int(out.passes.size()) - 1;
             };

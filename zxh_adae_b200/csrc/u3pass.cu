@@ -772,29 +772,48 @@ __global__ void __launch_bounds__(kThreads, 2) row_pass_kernel(const uint8_t *__
         if constexpr (WIN) {
             if (offw0) window(0, offw0);
         }
-        // XP: phase 0 runs the gates on the vector, top lane and register bits,
-        // phase 1 (after the transpose) those on lane bits 0..3 as register gates
-        bool swapped = false;
         float4 *tb = s_xp + warp * (NR * 32);
-#pragma unroll 1
-        for (int ph = 0; ph < (XP ? 2 : 1); ph++) {
+        if constexpr (REAL) {
+            // dense table (real passes): slot i holds the gate of coordinate C0 + i
+            // (identity where the pass has none), so the loop unrolls with
+            // compile-time coordinates and no per-gate dispatch
+            constexpr int C0 = XP ? 0 : F, NS = XP ? F + R : R;
+#pragma unroll
+            for (int i = 0; i < NS; i++) {
+                if (XP && i >= LV && i < LV + R) continue;  // lane bits 0..R-1: after the transpose
+                row_gate<R, V, LV, F, true>(x, uint32_t(C0 + i), &s_u[i][(omask >> i) & 1][0], lane);
+            }
             if constexpr (XP) {
-                if (ph == 1) {
-                    if (!swapped) break;
-                    lane_row_transpose(x, tb, lane, false);
+                lane_row_transpose(x, tb, lane, false);
+#pragma unroll
+                for (int b = 0; b < R; b++)
+                    row_gate<R, V, LV, F, true>(x, uint32_t(F + b), &s_u[LV + b][(omask >> (LV + b)) & 1][0], lane);
+                lane_row_transpose(x, tb, lane, true);
+            }
+        } else {
+            // XP: phase 0 runs the gates on the vector, top lane and register bits,
+            // phase 1 (after the transpose) those on lane bits 0..3 as register gates
+            bool swapped = false;
+#pragma unroll 1
+            for (int ph = 0; ph < (XP ? 2 : 1); ph++) {
+                if constexpr (XP) {
+                    if (ph == 1) {
+                        if (!swapped) break;
+                        lane_row_transpose(x, tb, lane, false);
+                    }
+                }
+                for (uint32_t gi = 0; gi < ngates; gi++) {
+                    uint32_t c = s_gc[gi];
+                    const bool sw = XP && c - uint32_t(LV) < uint32_t(R);  // lane bits 0..R-1
+                    swapped |= sw;
+                    if (sw != (ph == 1)) continue;
+                    if (sw) c = uint32_t(F) + c - uint32_t(LV);
+                    row_gate<R, V, LV, F, false>(x, c, &s_u[gi][(omask >> gi) & 1][0], lane);
                 }
             }
-            for (uint32_t gi = 0; gi < ngates; gi++) {
-                uint32_t c = s_gc[gi];
-                const bool sw = XP && c - uint32_t(LV) < uint32_t(R);  // lane bits 0..R-1
-                swapped |= sw;
-                if (sw != (ph == 1)) continue;
-                if (sw) c = uint32_t(F) + c - uint32_t(LV);
-                row_gate<R, V, LV, F, REAL>(x, c, &s_u[gi][(omask >> gi) & 1][0], lane);
+            if constexpr (XP) {
+                if (swapped) lane_row_transpose(x, tb, lane, true);
             }
-        }
-        if constexpr (XP) {
-            if (swapped) lane_row_transpose(x, tb, lane, true);
         }
         if constexpr (WIN) {
             if (offw1) window(1, offw1);
