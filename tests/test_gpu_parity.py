@@ -78,9 +78,11 @@ def test_diag_batch_and_cascade_16q(dtype):
 
 @pytest.mark.parametrize("dtype", DTYPES)
 @pytest.mark.parametrize("chunk_bits", [0, 1, 3, 6])
-def test_diag_pass_gray_code_chunks(dtype, chunk_bits):
+@pytest.mark.parametrize("prefetch", [0, 1])
+def test_diag_pass_gray_code_chunks(dtype, chunk_bits, prefetch):
     # the diagonal pass walks chunks of 2^chunk_bits tiles in Gray-code order,
-    # updating the out-of-tile coefficients one flipped bit at a time
+    # updating the out-of-tile coefficients one flipped bit at a time; with
+    # prefetch each warp stages its next tile by a TMA bulk copy
     n = 17
     gates = np.concatenate([wl.h_all(n), wl.diag_batch(n, 900, 8), wl.cp_cascade(n)])
     o = Oracle(n)
@@ -88,6 +90,7 @@ def test_diag_pass_gray_code_chunks(dtype, chunk_bits):
     o.execute()
     s = zx.ZXH(n, dtype=dtype)
     s.set_param("diag_chunk_bits", chunk_bits)
+    s.set_param("diag_prefetch_c64" if dtype == "complex64" else "diag_prefetch_c128", prefetch)
     s.push_gates(gates)
     s.execute()
     assert max_err(s, o) <= TOL[dtype]

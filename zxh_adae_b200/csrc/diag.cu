@@ -38,9 +38,10 @@ constexpr int kDiagGen = 32;  // general terms handled per window (more are spli
 constexpr int kDiagOut = 32;  // out-of-tile bits of the incremental walk (2^(32 + T) amplitudes at most)
 constexpr int kDiagTileMax = 10;
 
-template <typename E, int ROWB>
+template <typename E, int ROWB, bool PF>
 __global__ void __launch_bounds__(kThreads) diag_kernel(const uint8_t *__restrict__ blob, uint64_t doff, uint64_t toff,
-                                                        uint32_t T, uint32_t nout, uint32_t cb, E *__restrict__ state)
+                                                        uint32_t T, uint32_t nout, uint32_t cb, E *__restrict__ state,
+                                                        DevStatus *status)
 {
     using VT = typename ET<E>::VT;
     constexpr int V = ET<E>::V;
@@ -62,6 +63,9 @@ __global__ void __launch_bounds__(kThreads) diag_kernel(const uint8_t *__restric
     __shared__ int64_t s_cross[kDiagTileMax][kDiagOut];  // [tile bit][out bit]
     __shared__ int64_t s_quad[kDiagOut][kDiagOut];       // symmetric, zero diagonal
     __shared__ int64_t s_lin[kDiagOut];
+    // PF: two tile buffers per warp, filled by TMA bulk copies one tile ahead
+    extern __shared__ __align__(128) unsigned char s_tiles[];
+    __shared__ __align__(8) uint64_t s_bar[WARPS][2];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const E *tab = reinterpret_cast<const E *>(blob + toff);
@@ -69,6 +73,10 @@ __global__ void __launch_bounds__(kThreads) diag_kernel(const uint8_t *__restric
     for (int i = tid; i < kDiagOut * kDiagOut; i += kThreads) (&s_quad[0][0])[i] = 0;
     for (int i = tid; i < kDiagTileMax * kDiagOut; i += kThreads) (&s_cross[0][0])[i] = 0;
     if (tid < kDiagOut) s_lin[tid] = 0;
+    if (PF && tid < WARPS * 2) {
+        mbar_init(&s_bar[tid >> 1][tid & 1], 1);
+        fence_mbar_init();
+    }
     __syncthreads();
     // every (tile bit, out bit), (out bit, out bit) and out bit occurs at most once
     for (uint32_t q = uint32_t(tid); q < d.n_cross; q += kThreads) s_cross[cr[q].i][cr[q].j - T] = cr[q].coef;
@@ -96,18 +104,14 @@ __global__ void __launch_bounds__(kThreads) diag_kernel(const uint8_t *__restric
     }
     for (uint32_t q = 0; q < d.n_in_quad; q++) {
         const QuadTerm t = iq[q];  // t.i < t.j
+        // branch-free, so qf and rho stay in registers
 #pragma unroll
         for (int v = 0; v < V; v++) {
             const uint32_t e = uint32_t(v) | (uint32_t(lane) << LV);
-            const bool bi = int(t.i) < F && ((e >> t.i) & 1);
-            if (!bi) continue;
-            if (int(t.j) < F) {
-                if ((e >> t.j) & 1) qf[v] += t.coef;
-            } else {
+            const int64_t c = (int(t.i) < F && ((e >> t.i) & 1)) ? t.coef : 0;
+            qf[v] += (int(t.j) < F && ((e >> t.j) & 1)) ? c : 0;
 #pragma unroll
-                for (int l = 0; l < ROWB; l++)
-                    if (int(t.j) - F == l) rho[l][v] += t.coef;
-            }
+            for (int l = 0; l < ROWB; l++) rho[l][v] += int(t.j) == F + l ? c : 0;
         }
     }
 #pragma unroll
@@ -128,6 +132,14 @@ __global__ void __launch_bounds__(kThreads) diag_kernel(const uint8_t *__restric
 
     const uint64_t nchunks = 1ULL << (nout - cb);
     const uint64_t stride = uint64_t(gridDim.x) * WARPS;
+    const uint32_t tile_bytes = uint32_t(sizeof(E)) << T;
+    E *tbuf = reinterpret_cast<E *>(s_tiles) + size_t(warp) * 2 * tile_elems;
+    uint32_t k = 0;  // tiles this warp has taken
+    if (PF && lane == 0 && uint64_t(blockIdx.x) * WARPS + uint64_t(warp) < nchunks) {
+        const uint64_t t = (uint64_t(blockIdx.x) * WARPS + uint64_t(warp)) << cb;
+        mbar_arrive_expect_tx(&s_bar[warp][0], tile_bytes);
+        bulk_g2s(tbuf, state + (t << T), tile_bytes, &s_bar[warp][0]);
+    }
     for (uint64_t chunk = uint64_t(blockIdx.x) * WARPS + uint64_t(warp); chunk < nchunks; chunk += stride) {
         const uint64_t t0 = chunk << cb;
         // coefficients of the chunk's first tile, from the dense tables
@@ -146,18 +158,42 @@ __global__ void __launch_bounds__(kThreads) diag_kernel(const uint8_t *__restric
         }
         int64_t kp = warp_sum_i64(h) + d.c0;
 
-    for (uint32_t it_t = 0; it_t < (1u << cb); it_t++) {
+    for (uint32_t it_t = 0; it_t < (1u << cb); it_t++, k++) {
         const uint64_t tile = t0 | uint64_t(it_t ^ (it_t >> 1));
         const uint64_t r = tile << T;  // out-of-tile real bits of this tile
         E *base = state + r;
 
-        // 1. all rows in flight
+        // 1. all rows in flight. PF: the tile is in shared memory (or on its way);
+        //    first start the copy of the next one into the other buffer, last read
+        //    by the previous tile (whose values every lane has consumed)
+        const E *src = base;
+        if constexpr (PF) {
+            __syncwarp();
+            uint64_t nt = 0;
+            bool has = true;
+            if (it_t + 1 < (1u << cb)) nt = t0 | uint64_t((it_t + 1) ^ ((it_t + 1) >> 1));
+            else if (chunk + stride < nchunks) nt = (chunk + stride) << cb;
+            else has = false;
+            if (has && lane == 0) {
+                uint64_t *nb = &s_bar[warp][(k + 1) & 1];
+                mbar_arrive_expect_tx(nb, tile_bytes);
+                bulk_g2s(tbuf + size_t((k + 1) & 1) * tile_elems, state + (nt << T), tile_bytes, nb);
+            }
+            if (!mbar_wait_bounded(&s_bar[warp][k & 1], (k >> 1) & 1)) {
+                if (lane == 0) report(status, kErrTimeout, 7, tile);
+                return;
+            }
+            src = tbuf + size_t(k & 1) * tile_elems;
+        }
         VT data[ROWS];
 #pragma unroll
         for (int it = 0; it < ROWS; it++) {
             const uint32_t gi = uint32_t(it ^ (it >> 1));
             const uint32_t e0 = (uint32_t(lane) << LV) | (gi << F);
-            if (it < NI && e0 < tile_elems) data[it] = __ldcs(reinterpret_cast<const VT *>(base + e0));
+            if (it < NI && e0 < tile_elems) {
+                if constexpr (PF) data[it] = *reinterpret_cast<const VT *>(src + e0);
+                else data[it] = __ldcs(reinterpret_cast<const VT *>(src + e0));
+            }
         }
 
         // 2. one out-of-tile bit o flipped since the previous tile of the chunk
@@ -271,16 +307,22 @@ __global__ void __launch_bounds__(kThreads) diag_kernel(const uint8_t *__restric
 
 namespace {
 
-template <typename E, int ROWB>
-cudaError_t launch_diag(const uint8_t *dblob, uint64_t doff, uint64_t toff, int m, int chunk_bits, E *state, int sms,
-                        cudaStream_t st)
+template <typename E, int ROWB, bool PF>
+cudaError_t launch_diag(const uint8_t *dblob, uint64_t doff, uint64_t toff, int m, int chunk_bits, E *state,
+                        DevStatus *status, int sms, cudaStream_t st)
 {
     const int Tfull = (ET<E>::V == 2 ? 6 : 5) + ROWB;
     const int T = std::min(m, Tfull);
     const int nout = m - T;
     if (nout > kDiagOut) return cudaErrorInvalidValue;
+    auto kern = diag_kernel<E, ROWB, PF>;
+    const size_t smem = PF ? size_t(kThreads / 32) * 2 * (sizeof(E) << T) : 0;
+    if (PF) {
+        const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        if (e != cudaSuccess) return e;
+    }
     int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, diag_kernel<E, ROWB>, kThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem);
     if (per_sm < 1) per_sm = 1;
     // chunks of 2^cb tiles: at least 16 chunks per warp of a full grid (tail balance),
     // at most 256 tiles per chunk
@@ -291,29 +333,37 @@ cudaError_t launch_diag(const uint8_t *dblob, uint64_t doff, uint64_t toff, int 
     const uint64_t nchunks = 1ULL << (nout - cb);
     const uint64_t ctas_needed = (nchunks + kThreads / 32 - 1) / (kThreads / 32);
     const unsigned grid = unsigned(std::max<uint64_t>(1, std::min<uint64_t>(ctas_needed, uint64_t(sms) * uint64_t(per_sm))));
-    diag_kernel<E, ROWB><<<grid, kThreads, 0, st>>>(dblob, doff, toff, uint32_t(T), uint32_t(nout), uint32_t(cb), state);
+    kern<<<grid, kThreads, smem, st>>>(dblob, doff, toff, uint32_t(T), uint32_t(nout), uint32_t(cb), state, status);
     return cudaGetLastError();
+}
+
+template <typename E, int ROWB>
+cudaError_t launch_diag_pf(const uint8_t *dblob, uint64_t doff, uint64_t toff, int m, int chunk_bits, bool pf,
+                           E *state, DevStatus *status, int sms, cudaStream_t st)
+{
+    return pf ? launch_diag<E, ROWB, true>(dblob, doff, toff, m, chunk_bits, state, status, sms, st)
+              : launch_diag<E, ROWB, false>(dblob, doff, toff, m, chunk_bits, state, status, sms, st);
 }
 
 }  // namespace
 
 cudaError_t run_diag(const uint8_t *dblob, uint64_t doff, uint64_t toff, int m, int elem_bytes, int row_bits,
-                     int chunk_bits, void *state, int sms, cudaStream_t st)
+                     int chunk_bits, bool prefetch, void *state, DevStatus *status, int sms, cudaStream_t st)
 {
     if (elem_bytes == 8) {
         auto *s = static_cast<float2 *>(state);
         switch (row_bits) {
-        case 2: return launch_diag<float2, 2>(dblob, doff, toff, m, chunk_bits, s, sms, st);
-        case 3: return launch_diag<float2, 3>(dblob, doff, toff, m, chunk_bits, s, sms, st);
-        case 4: return launch_diag<float2, 4>(dblob, doff, toff, m, chunk_bits, s, sms, st);
+        case 2: return launch_diag_pf<float2, 2>(dblob, doff, toff, m, chunk_bits, prefetch, s, status, sms, st);
+        case 3: return launch_diag_pf<float2, 3>(dblob, doff, toff, m, chunk_bits, prefetch, s, status, sms, st);
+        case 4: return launch_diag_pf<float2, 4>(dblob, doff, toff, m, chunk_bits, prefetch, s, status, sms, st);
         default: return cudaErrorInvalidValue;
         }
     }
     auto *s = static_cast<double2 *>(state);
     switch (row_bits) {
-    case 2: return launch_diag<double2, 2>(dblob, doff, toff, m, chunk_bits, s, sms, st);
-    case 3: return launch_diag<double2, 3>(dblob, doff, toff, m, chunk_bits, s, sms, st);
-    case 4: return launch_diag<double2, 4>(dblob, doff, toff, m, chunk_bits, s, sms, st);
+    case 2: return launch_diag_pf<double2, 2>(dblob, doff, toff, m, chunk_bits, prefetch, s, status, sms, st);
+    case 3: return launch_diag_pf<double2, 3>(dblob, doff, toff, m, chunk_bits, prefetch, s, status, sms, st);
+    case 4: return launch_diag_pf<double2, 4>(dblob, doff, toff, m, chunk_bits, prefetch, s, status, sms, st);
     default: return cudaErrorInvalidValue;
     }
 }

@@ -950,6 +950,7 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
         ps.m = mm;
         ps.chunk_bits = pp.diag_chunk_bits;
         ps.row_bits = rb;
+        ps.prefetch = elem_bytes == 8 ? pp.diag_prefetch_c64 : pp.diag_prefetch_c128;
         ps.geom = g;
         ps.off = compile_diag(out.blob, w, g);
         ps.off2 = exp_off;

@@ -55,6 +55,8 @@ struct PlanParams {
     int grow_regs = 4;          // register coordinates (gates with high deltas) per general strided pass
     int grow_only = 0;          // 1: only INIT and general strided passes (the persistent batch kernel's set)
     int adj_windows = 1;        // adjoint sweep: diagonal gates ride in the general strided passes as windows
+    int diag_prefetch_c64 = 1;  // diagonal pass: each warp stages its next tile with a TMA bulk copy
+    int diag_prefetch_c128 = 0; // same for complex128 (no gain measured there)
     int diag_chunk_bits = -1;   // log2 tiles a warp walks in Gray-code order in a diagonal pass (-1: chosen
                                 // per launch so every warp of a full grid gets at least 16 chunks)
     int product_table_bits = 12;
@@ -98,6 +100,7 @@ struct Pass {
     int real = 0;                        // ROW: every gate matrix is real
     int chunk_bits = -1;                 // DIAG: tiles per Gray-code chunk (log2, -1 = automatic)
     int row_bits = 0;                    // DIAG: log2 rows of a warp tile
+    int prefetch = 0;                    // DIAG: tiles staged one ahead by TMA bulk copies
     std::vector<FastGateDev> fgates;     // FAST
     GrowBuild gb;                        // GROW
 };

@@ -38,8 +38,10 @@ cudaError_t run_sampler_real(const void *state, int elem_bytes, int m, uint64_t 
 struct Pass;
 cudaError_t run_passes(const std::vector<Pass> &passes, const uint8_t *dblob, void *state, int elem_bytes,
                        DevStatus *status, int sms, cudaStream_t st, uint64_t &kernels);
-cudaError_t run_diag(const uint8_t *dblob, uint64_t doff, uint64_t toff, int m, int elem_bytes, int row_bits, int chunk_bits, void *state, int sms,
-                     cudaStream_t st);
+// prefetch: each warp stages the next tile in shared memory with a TMA bulk copy
+// while it works on the current one (waits bounded; a timeout sets status).
+cudaError_t run_diag(const uint8_t *dblob, uint64_t doff, uint64_t toff, int m, int elem_bytes, int row_bits,
+                     int chunk_bits, bool prefetch, void *state, DevStatus *status, int sms, cudaStream_t st);
 int diag_tile_bits(int elem_bytes, int row_bits);
 cudaError_t run_fast_tile(const uint8_t *dblob, uint64_t foff, uint64_t toff, uint64_t ntiles, int elem_bytes,
                           void *state, DevStatus *status, int sms, cudaStream_t st);
