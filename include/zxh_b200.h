@@ -274,9 +274,14 @@ int zxh_plan_stats(size_t n, int disable_x, int eager_expand_all, int dtype, con
  * general strided pass), grow_only (1: plan every batch and window as general
  * strided passes after a |0...0> init, the pass set of the batched launch; needs
  * eager_expand_all), adj_windows (1: the adjoint sweep undoes diagonal gates
- * inside its general strided passes, 0: in separate diagonal-group passes).
- * Takes effect at the
- * next zxh_execute / zxh_apply. No counterpart in the reference. */
+ * inside its general strided passes, 0: in separate diagonal-group passes),
+ * low_pass (1: gates on the lane / vector bits ride in a strided low pass with
+ * lane bits swapped into registers, 0: the TMA fast tile pass), low_regs_c64,
+ * low_regs_c128 (0..4: register-bit gates that join the low pass), real_split
+ * (1: single-bit U3 gates run as real rotations with their phases in the
+ * windows), diag_prefetch_c64, diag_prefetch_c128 (1: the diagonal pass stages
+ * each warp's next tile with a TMA bulk copy). Takes effect at the next
+ * zxh_execute / zxh_apply. No counterpart in the reference. */
 int zxh_set_param(zxh_sim *sim, const char *name, int value);
 
 #ifdef __cplusplus
