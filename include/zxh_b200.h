@@ -263,6 +263,18 @@ int zxh_batch_stats(const zxh_batch *batch, uint64_t *ops, uint64_t *tasks, doub
 int zxh_plan_stats(size_t n, int disable_x, int eager_expand_all, int dtype, const zxh_gate *gates, size_t count,
                    uint64_t *out);
 
+/* Host circuit compiler: the reference's boundary scheduler
+ * (src/zxh/zxhsim/circ_optimizer.py:218-420, optimize_circuit) over gate records.
+ * Single-qubit gates merge per qubit until a two-qubit gate or a barrier needs
+ * the qubit and are re-emitted as RZ (+ X), H or U3; a CX between two pending
+ * exact H gates is emitted reversed with the H's kept pending. level 0 emits every
+ * gate at once (identities dropped), level >= 1 schedules. The result equals the
+ * input up to a global phase. out may be NULL (a size query: *out_count gives
+ * the size); with capacity < *out_count the call returns ZXH_ERR_LIMIT. Accepts the record
+ * types zxh_push_gates accepts. No GPU work. */
+int zxh_optimize_gates(size_t n, int level, const zxh_gate *gates, size_t count, zxh_gate *out, size_t capacity,
+                       size_t *out_count);
+
 /* Pass-planner tuning (used by the autotuner): tile_bits_c64, tile_bits_c128,
  * contig_bits, max_gates (generic tile pass), fast_gates (gates per fast U3
  * pass), fast_fuse_quad, fast_contig_c64, fast_contig_c128, row_wide_c64,

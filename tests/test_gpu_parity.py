@@ -301,3 +301,28 @@ def test_low_pass_gate_subsets(dtype, seed):
         recs.append((zx._core.P, 0, int(rng.integers(n)), rng.uniform(0, 2 * np.pi)))
     o, s = _run_knobs(n, zx.as_records(recs), dtype, {})
     assert max_err(s, o) <= TOL[dtype]
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+@pytest.mark.parametrize("seed", range(3))
+def test_load_circuit_through_the_host_compiler(dtype, seed):
+    # frontend gates (swap, ccx, rzz, ...) lowered and scheduled by the host
+    # circuit compiler at level 2, run on the GPU; the state equals the oracle's
+    # run of the level-0 compile up to a global phase
+    from tests.test_optimize import _Circuit, _random_frontend
+
+    n = 9 + seed
+    circ = _Circuit(_random_frontend(n, 120, 7700 + seed))
+    (base, _), = zx.compile_circuit(circ, n, 0)
+    o = Oracle(n)
+    o.push(base)
+    o.execute()
+    ref = o.get_state()
+    s = zx.ZXH(n, dtype=dtype)
+    zx.load_circuit(s, circ, optimize_level=2)
+    s.execute()
+    got = s.get_state().astype(np.complex128)
+    k = int(np.argmax(np.abs(ref)))
+    ph = got[k] / ref[k]
+    ph /= abs(ph)
+    assert float(np.max(np.abs(got - ph * ref))) <= TOL[dtype] * 10

@@ -2,7 +2,8 @@
 
 Drop-in for the reference's ``zxhsim`` package entry points on the single-GPU
 path (src/zxh/zxhsim/__init__.py of ZXH-Sim): ``ZXH``, ``init``, ``finalize``,
-``active``, ``rank``, ``nprocs``, ``PrintRes`` and ``load_circuit_transpiled``.
+``active``, ``rank``, ``nprocs``, ``PrintRes``, ``load_circuit`` (with the host
+circuit compiler, ``optimize_records``) and ``load_circuit_transpiled``.
 """
 from __future__ import annotations
 
@@ -16,10 +17,11 @@ from ._core import (
     init,
     library_path,
     nprocs,
+    optimize_records,
     rank,
     version,
 )
-from .loader import load_circuit_transpiled
+from .loader import compile_circuit, load_circuit, load_circuit_transpiled
 
 __version__ = _core.__version__
 
@@ -35,4 +37,7 @@ __all__ = [
     "library_path",
     "version",
     "load_circuit_transpiled",
+    "load_circuit",
+    "compile_circuit",
+    "optimize_records",
 ]

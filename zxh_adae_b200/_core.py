@@ -91,6 +91,7 @@ _sig("zxh_state_view", [_P, ctypes.POINTER(_P), ctypes.POINTER(_SZ), ctypes.POIN
 _sig("zxh_stream", [_P, ctypes.POINTER(_P)])
 _sig("zxh_set_param", [_P, ctypes.c_char_p, ctypes.c_int])
 _sig("zxh_plan_stats", [_SZ, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _SZ, _P])
+_sig("zxh_optimize_gates", [_SZ, ctypes.c_int, _P, _SZ, _P, _SZ, ctypes.POINTER(_SZ)])
 _sig("zxh_last_stats", [_P, ctypes.POINTER(_U64), ctypes.POINTER(_U64), ctypes.POINTER(_D)])
 _sig("zxh_expectation", [_P, _P, _SZ, ctypes.POINTER(_D)])
 _sig("zxh_adjoint_gradient", [_P, _P, _SZ, _SZ, ctypes.POINTER(_D), _P, _SZ])
@@ -165,6 +166,24 @@ def plan_stats(n: int, gates, dtype: str = "complex64", disable_x: bool = False,
     d = {"M": int(out[0]), "m": int(out[1]), "passes": int(out[10])}
     d.update({k: int(out[2 + i]) for i, k in enumerate(PASS_KINDS)})
     return d
+
+
+def optimize_records(n: int, gates, level: int = 2) -> np.ndarray:
+    """The host circuit compiler (zxh_optimize_gates): the reference's boundary
+    scheduler (circ_optimizer.py:218-420) over gate records. Returns records equal
+    to the input up to a global phase."""
+    rec = as_records(gates)
+    cnt = _SZ(0)
+    rc = _lib.zxh_optimize_gates(int(n), int(level), rec.ctypes.data if len(rec) else None, len(rec), None, 0,
+                                 ctypes.byref(cnt))
+    if rc != 0:
+        _raise(rc, None)
+    out = np.zeros(cnt.value, GATE_DTYPE)
+    rc = _lib.zxh_optimize_gates(int(n), int(level), rec.ctypes.data if len(rec) else None, len(rec),
+                                 out.ctypes.data if len(out) else None, len(out), ctypes.byref(cnt))
+    if rc != 0:
+        _raise(rc, None)
+    return out
 
 
 # Module-level runtime calls of the reference (bindings.cpp:86-90). One process

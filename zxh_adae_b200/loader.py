@@ -12,6 +12,8 @@ pushed in one ``push_gates`` call.
 """
 from __future__ import annotations
 
+import math
+
 import numpy as np
 
 from . import _core
@@ -79,6 +81,106 @@ def load_circuit_transpiled(sim, circuit) -> None:
         elif name == "crz":
             recs.append((_core.CRZ, qs[0], qs[1], _to_float(op.params[0])))
     flush()
+
+
+# Gates the circuit compiler accepts (the reference's frontend set,
+# src/zxh/zxhsim/gate_sets.py ZXH_FRONTEND_GATES); those outside NATIVE_GATES are
+# lowered to native records first.
+FRONTEND_GATES = NATIVE_GATES | frozenset(
+    ("swap", "cz", "ry", "u1", "u2", "s", "sdg", "t", "tdg", "rzz", "ccz", "ccx")
+)
+
+
+def _ccz(c0: int, c1: int, t: int) -> list:
+    """CCZ as 6 CX and 7 RZ(+-pi/4), equal to CCZ up to a global phase: the
+    textbook Toffoli phase network the reference's compiler also emits
+    (circ_optimizer.py:153-168)."""
+    a = math.pi / 4.0
+    seq = [("cx", c1, t), ("rz", t, -a), ("cx", c0, t), ("rz", t, a), ("cx", c1, t), ("rz", t, -a),
+           ("cx", c0, t), ("rz", c1, a), ("rz", t, a), ("cx", c0, c1), ("rz", c0, a), ("rz", c1, -a),
+           ("cx", c0, c1)]
+    return [(_core.CX, x, y) if k == "cx" else (_core.RZ, 0, x, y) for k, x, y in seq]
+
+
+def frontend_records(name: str, qs, params) -> list:
+    """One frontend instruction as native gate records: the reference's lowering of
+    swap / cz / rzz / ccz / ccx (circ_optimizer.py:171-209) and the standard
+    definitions of ry, u1, u2, s, sdg, t, tdg. measure / reset / id give []."""
+    C = _core
+    p = [_to_float(v) for v in params]
+    if name in ("measure", "reset", "id"):
+        return []
+    one = {
+        "x": lambda: [(C.X, 0, qs[0])],
+        "h": lambda: [(C.H, 0, qs[0])],
+        "z": lambda: [(C.Z, 0, qs[0])],
+        "rz": lambda: [(C.RZ, 0, qs[0], p[0])],
+        "rx": lambda: [(C.RX, 0, qs[0], p[0])],
+        "ry": lambda: [(C.U3, 0, qs[0], p[0], 0.0, 0.0)],
+        "p": lambda: [(C.P, 0, qs[0], p[0])],
+        "u1": lambda: [(C.P, 0, qs[0], p[0])],
+        "u2": lambda: [(C.U3, 0, qs[0], math.pi / 2.0, p[1], p[0])],  # u2(phi, lambda)
+        "s": lambda: [(C.P, 0, qs[0], math.pi / 2.0)],
+        "sdg": lambda: [(C.P, 0, qs[0], -math.pi / 2.0)],
+        "t": lambda: [(C.P, 0, qs[0], math.pi / 4.0)],
+        "tdg": lambda: [(C.P, 0, qs[0], -math.pi / 4.0)],
+        "u": lambda: [(C.U3, 0, qs[0], p[0], p[2], p[1])],  # (theta, phi, lambda) -> (theta, lambda, phi)
+        "u3": lambda: [(C.U3, 0, qs[0], p[0], p[2], p[1])],
+        "barrier": lambda: [(C.BARRIER, 0, 0)],
+        "cx": lambda: [(C.CX, qs[0], qs[1])],
+        "cp": lambda: [(C.CP, qs[0], qs[1], p[0])],
+        "crz": lambda: [(C.CRZ, qs[0], qs[1], p[0])],
+        "cz": lambda: [(C.CP, qs[0], qs[1], math.pi)],
+        "swap": lambda: [(C.CX, qs[0], qs[1]), (C.CX, qs[1], qs[0]), (C.CX, qs[0], qs[1])],
+        "rzz": lambda: [(C.CX, qs[0], qs[1]), (C.RZ, 0, qs[1], p[0]), (C.CX, qs[0], qs[1])],
+        "ccz": lambda: _ccz(qs[0], qs[1], qs[2]),
+        "ccx": lambda: [(C.H, 0, qs[2])] + _ccz(qs[0], qs[1], qs[2]) + [(C.H, 0, qs[2])],
+    }
+    if name not in one:
+        raise NotImplementedError(
+            f"Circuit contains gates outside the allowed set: {[name]}. allowed_gates={sorted(FRONTEND_GATES)}"
+        )
+    return one[name]()
+
+
+def compile_circuit(circuit, n: int, optimize_level: int = 2):
+    """The circuit as segments of compiled records: ``(records, reset_before)``.
+
+    Frontend gates are lowered (frontend_records) and each stretch between
+    measure / reset instructions (where the reference's scheduler flushes every
+    qubit) goes through the host circuit compiler (``zxh_optimize_gates``, the
+    reference's boundary scheduler at ``optimize_level``)."""
+    segments, cur, reset = [], [], False
+
+    def close():
+        nonlocal cur, reset
+        if cur or reset:
+            recs = _core.optimize_records(n, cur, optimize_level) if cur else np.zeros(0, _core.GATE_DTYPE)
+            segments.append((recs, reset))
+        cur, reset = [], False
+
+    for inst in circuit.data:
+        name = inst.operation.name.lower()
+        qs = [_qubit_index(circuit, q) for q in inst.qubits]
+        if name in ("measure", "reset"):
+            close()
+            reset = name == "reset"
+            continue
+        cur.extend(frontend_records(name, qs, inst.operation.params))
+    close()
+    return segments
+
+
+def load_circuit(sim, circuit, optimize_level: int | None = None) -> None:
+    """The reference's ``load_circuit`` (qasm.py:54-62): compile the circuit with
+    the boundary scheduler at ``optimize_level`` (default 0: gates re-emitted one
+    by one, identities dropped), then record it on ``sim``."""
+    level = 0 if optimize_level is None else int(optimize_level)
+    for recs, reset in compile_circuit(circuit, sim.num_qubits(), level):
+        if reset:
+            sim.clear_gates()
+        if len(recs):
+            sim.push_gates(recs)
 
 
 def bitrow_to_str(row) -> str:
