@@ -17,7 +17,6 @@ from __future__ import annotations
 
 import ctypes
 import os
-from collections import Counter
 from pathlib import Path
 
 import numpy as np
@@ -346,8 +345,8 @@ class ZXH:
         self.measure(shots)
         words = self.results_words(shots)
         n = self._n
-        cnt = Counter(words.tolist())
-        return {format(int(k), f"0{n}b"): int(v) for k, v in sorted(cnt.items())}
+        keys, cnt = np.unique(words, return_counts=True)  # sorted, as the reference's std::map
+        return {format(k, f"0{n}b"): c for k, c in zip(keys.tolist(), cnt.tolist())}
 
     def get_state(self, order: int = ORDER_REFERENCE) -> np.ndarray:
         """2^n amplitudes in the reference's get_state order (zxh.cpp:579-636)."""
