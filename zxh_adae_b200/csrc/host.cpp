@@ -10,6 +10,7 @@
 #include <deque>
 #include <cmath>
 #include <map>
+#include <memory>
 #include <stdexcept>
 
 namespace zxh {
@@ -370,26 +371,44 @@ bool single_bit_or_zero(uint64_t a) { return (a & (a - 1)) == 0; }
 
 int bit_index(uint64_t a) { return __builtin_ctzll(a); }
 
+// Dense over the 64 address bits; an entry is live where its mask bit is set
+// (so nothing is cleared up front). Visiting rows and columns in bit order gives
+// the terms sorted by (i, j).
 struct Poly {
     int64_t c0 = 0;
-    std::map<int, int64_t> lin;
-    std::map<std::pair<int, int>, int64_t> quad;
+    int64_t lin[64];
+    uint64_t lin_mask = 0;
+    int64_t quad[64][64];  // [i][j], i < j
+    uint64_t quad_mask[64];
+    uint64_t quad_rows = 0;
     std::vector<DiagTerm> general;
 
-    void add_lin(int i, int64_t c) { lin[i] += c; }
+    Poly() { std::memset(quad_mask, 0, sizeof(quad_mask)); }
+    void add_lin(int i, int64_t c)
+    {
+        if (!((lin_mask >> i) & 1)) {
+            lin[i] = 0;
+            lin_mask |= 1ULL << i;
+        }
+        lin[i] += c;
+    }
     void add_quad(int i, int j, int64_t c)
     {
-        if (i == j) { lin[i] += c; return; }
+        if (i == j) { add_lin(i, c); return; }
         if (i > j) std::swap(i, j);
-        quad[{i, j}] += c;
+        if (!((quad_mask[i] >> j) & 1)) {
+            quad[i][j] = 0;
+            quad_mask[i] |= 1ULL << j;
+            quad_rows |= 1ULL << i;
+        }
+        quad[i][j] += c;
     }
 };
 
 // Expands a window into a polynomial over real address bits where every selector
 // is a single bit (or constant), and keeps the rest as general terms.
-Poly to_poly(const std::vector<DiagTerm> &terms)
+void to_poly(const std::vector<DiagTerm> &terms, Poly &p)
 {
-    Poly p;
     for (const DiagTerm &t : terms) {
         const bool simple = single_bit_or_zero(t.s0.alpha) && (!t.two || single_bit_or_zero(t.s1.alpha));
         if (!simple) {
@@ -412,7 +431,6 @@ Poly to_poly(const std::vector<DiagTerm> &terms)
         if (s0) p.add_lin(i0, th * c1 * s0);
         if (s0 && s1) p.add_quad(i0, i1, th * s0 * s1);
     }
-    return p;
 }
 
 template <typename T>
@@ -467,7 +485,9 @@ RealSplit real_split(const cd u[4])
 // Compiles one window for a tile geometry; returns its blob offset.
 uint64_t compile_diag(std::vector<uint8_t> &blob, const std::vector<DiagTerm> &terms, const TileDev &g)
 {
-    const Poly p = to_poly(terms);
+    const std::unique_ptr<Poly> pp(new Poly());
+    to_poly(terms, *pp);
+    const Poly &p = *pp;
     int coord_of_bit[64];
     for (int i = 0; i < 64; i++) coord_of_bit[i] = -1;
     for (uint32_t k = 0; k < g.T; k++) coord_of_bit[g.pos[k]] = int(k);
@@ -477,20 +497,26 @@ uint64_t compile_diag(std::vector<uint8_t> &blob, const std::vector<DiagTerm> &t
     d.c0 = p.c0;
     std::vector<LinTerm> out_lin;
     std::vector<QuadTerm> out_quad, in_quad, cross;
-    for (const auto &kv : p.lin) {
-        if (kv.second == 0) continue;
-        const int k = coord_of_bit[kv.first];
-        if (k >= 0) d.lin_in[k] += kv.second;
-        else out_lin.push_back(LinTerm{uint32_t(kv.first), 0, kv.second});
+    for (uint64_t lm = p.lin_mask; lm; lm &= lm - 1) {
+        const int b = __builtin_ctzll(lm);
+        const int64_t c = p.lin[b];
+        if (c == 0) continue;
+        const int k = coord_of_bit[b];
+        if (k >= 0) d.lin_in[k] += c;
+        else out_lin.push_back(LinTerm{uint32_t(b), 0, c});
     }
-    for (const auto &kv : p.quad) {
-        if (kv.second == 0) continue;
-        const int i = kv.first.first, j = kv.first.second;
-        const int ki = coord_of_bit[i], kj = coord_of_bit[j];
-        if (ki >= 0 && kj >= 0) in_quad.push_back(QuadTerm{uint32_t(std::min(ki, kj)), uint32_t(std::max(ki, kj)), kv.second});
-        else if (ki >= 0) cross.push_back(QuadTerm{uint32_t(ki), uint32_t(j), kv.second});
-        else if (kj >= 0) cross.push_back(QuadTerm{uint32_t(kj), uint32_t(i), kv.second});
-        else out_quad.push_back(QuadTerm{uint32_t(i), uint32_t(j), kv.second});
+    for (uint64_t rows = p.quad_rows; rows; rows &= rows - 1) {
+        const int i = __builtin_ctzll(rows);
+        for (uint64_t cm = p.quad_mask[i]; cm; cm &= cm - 1) {
+            const int j = __builtin_ctzll(cm);
+            const int64_t c = p.quad[i][j];
+            if (c == 0) continue;
+            const int ki = coord_of_bit[i], kj = coord_of_bit[j];
+            if (ki >= 0 && kj >= 0) in_quad.push_back(QuadTerm{uint32_t(std::min(ki, kj)), uint32_t(std::max(ki, kj)), c});
+            else if (ki >= 0) cross.push_back(QuadTerm{uint32_t(ki), uint32_t(j), c});
+            else if (kj >= 0) cross.push_back(QuadTerm{uint32_t(kj), uint32_t(i), c});
+            else out_quad.push_back(QuadTerm{uint32_t(i), uint32_t(j), c});
+        }
     }
     std::vector<GenTerm> gen;
     for (const DiagTerm &t : p.general) {
@@ -725,16 +751,32 @@ bool GrowBuild::add_window(int which, const std::vector<DiagTerm> &w, const std:
     return true;
 }
 
+// exp(2 pi i j / 1024), j = 0..1023, rounded from long double; computed once
+const std::vector<double> &exp_table_f64()
+{
+    static const std::vector<double> tab = [] {
+        const int nt = 1 << kExpTableBits;
+        std::vector<double> t(2 * nt);
+        for (int j = 0; j < nt; j++) {
+            const long double a = 2.0L * 3.141592653589793238462643383279502884L * j / nt;
+            t[2 * j] = double(cosl(a));
+            t[2 * j + 1] = double(sinl(a));
+        }
+        return t;
+    }();
+    return tab;
+}
+
+const std::vector<float> &exp_table_f32()
+{
+    static const std::vector<float> tab(exp_table_f64().begin(), exp_table_f64().end());
+    return tab;
+}
+
 void exp_table(int elem_bytes, std::vector<uint8_t> &bytes)
 {
-    // exp(2 pi i j / 1024) rounded from long double, as the planner's passes use it
-    const int nt = 1 << kExpTableBits;
-    std::vector<double> t(2 * nt);
-    for (int j = 0; j < nt; j++) {
-        const long double a = 2.0L * 3.141592653589793238462643383279502884L * j / nt;
-        t[2 * j] = double(cosl(a));
-        t[2 * j + 1] = double(sinl(a));
-    }
+    // the table the planner's passes use
+    const std::vector<double> &t = exp_table_f64();
     if (elem_bytes == 8) {
         std::vector<float> f(t.begin(), t.end());
         bytes.assign(reinterpret_cast<const uint8_t *>(f.data()), reinterpret_cast<const uint8_t *>(f.data() + f.size()));
@@ -783,7 +825,18 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
          std::string &err)
 {
     out.clear();
-    const std::vector<Op> ops = split_windows(ops_in, 32);
+    // windows with more than 32 general terms are split; otherwise the ops are used as given
+    bool need_split = false;
+    for (const Op &op : ops_in) {
+        if (op.kind != Op::DIAG) continue;
+        size_t ngen = 0;
+        for (const DiagTerm &t : op.diag)
+            ngen += !(single_bit_or_zero(t.s0.alpha) && (!t.two || single_bit_or_zero(t.s1.alpha)));
+        need_split = need_split || ngen > 32;
+    }
+    std::vector<Op> split_ops;
+    if (need_split) split_ops = split_windows(ops_in, 32);
+    const std::vector<Op> &ops = need_split ? split_ops : ops_in;
     size_t i = 0;
     int m = start.m;
 
@@ -917,18 +970,7 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
 
     uint64_t exp_off = 0;
     auto ensure_exp = [&]() {
-        if (!exp_off) {
-            // exp(2 pi i j / 1024) rounded from long double
-            const int nt = 1 << kExpTableBits;
-            std::vector<double> t(2 * nt);
-            for (int j = 0; j < nt; j++) {
-                const long double a = 2.0L * 3.141592653589793238462643383279502884L * j / nt;
-                t[2 * j] = double(cosl(a));
-                t[2 * j + 1] = double(sinl(a));
-            }
-            if (elem_bytes == 8) exp_off = put_vec(out.blob, std::vector<float>(t.begin(), t.end()));
-            else exp_off = put_vec(out.blob, t);
-        }
+        if (!exp_off) exp_off = elem_bytes == 8 ? put_vec(out.blob, exp_table_f32()) : put_vec(out.blob, exp_table_f64());
     };
     auto standalone_diag = [&](int mm, const std::vector<DiagTerm> &w) {
         ensure_exp();
