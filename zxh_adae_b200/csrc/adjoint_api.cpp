@@ -495,7 +495,7 @@ int zxh_adjoint_gradient(zxh_sim *s, const zxh_term *terms, size_t nterms, size_
             break;
         case RevStep::GROW:
             CK(s, zxh::run_grow(s->d_adj + L.grow, r.off, r.toff, int(r.gb.regs.size()), r.gb.dev.nitems, s->elem_bytes,
-                                s->d_psi, s->d_lam, d_grads, s->sms, s->stream),
+                                s->d_psi, s->d_lam, d_grads, r.gb.all_real(), s->sms, s->stream),
                "adjoint strided launch");
             kernels++;
             break;

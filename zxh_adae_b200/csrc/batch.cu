@@ -153,7 +153,7 @@ __device__ __forceinline__ void diag_adj_body(E *psi, E *lam, uint64_t b, uint64
     }
 }
 
-template <typename E>
+template <typename E, bool REAL>
 __device__ __forceinline__ void run_op_slice(const BatchOp &op, const uint8_t *blob, E *arena, double *grads,
                                              double *energies, uint64_t b, uint64_t e, uint64_t first, uint64_t step,
                                              BatchShared<E> &sm)
@@ -166,20 +166,20 @@ __device__ __forceinline__ void run_op_slice(const BatchOp &op, const uint8_t *b
     case BOP_INIT: init_body(psi, b, e); break;
     case BOP_GROW:
         switch (op.R) {
-        case 0: grow_body<E, 0, false>(ob, op.off0, op.off1, psi, nullptr, nullptr, first, step, e, sm.g); break;
-        case 1: grow_body<E, 1, false>(ob, op.off0, op.off1, psi, nullptr, nullptr, first, step, e, sm.g); break;
-        case 2: grow_body<E, 2, false>(ob, op.off0, op.off1, psi, nullptr, nullptr, first, step, e, sm.g); break;
-        case 3: grow_body<E, 3, false>(ob, op.off0, op.off1, psi, nullptr, nullptr, first, step, e, sm.g); break;
-        case 4: grow_body<E, 4, false>(ob, op.off0, op.off1, psi, nullptr, nullptr, first, step, e, sm.g); break;
+        case 0: grow_body<E, 0, false, REAL>(ob, op.off0, op.off1, psi, nullptr, nullptr, first, step, e, sm.g); break;
+        case 1: grow_body<E, 1, false, REAL>(ob, op.off0, op.off1, psi, nullptr, nullptr, first, step, e, sm.g); break;
+        case 2: grow_body<E, 2, false, REAL>(ob, op.off0, op.off1, psi, nullptr, nullptr, first, step, e, sm.g); break;
+        case 3: grow_body<E, 3, false, REAL>(ob, op.off0, op.off1, psi, nullptr, nullptr, first, step, e, sm.g); break;
+        case 4: grow_body<E, 4, false, REAL>(ob, op.off0, op.off1, psi, nullptr, nullptr, first, step, e, sm.g); break;
         default: break;
         }
         break;
     case BOP_GROW_ADJ:
         switch (op.R) {
-        case 0: grow_body<E, 0, true>(ob, op.off0, op.off1, psi, lam, gr, first, step, e, sm.g); break;
-        case 1: grow_body<E, 1, true>(ob, op.off0, op.off1, psi, lam, gr, first, step, e, sm.g); break;
-        case 2: grow_body<E, 2, true>(ob, op.off0, op.off1, psi, lam, gr, first, step, e, sm.g); break;
-        case 3: grow_body<E, 3, true>(ob, op.off0, op.off1, psi, lam, gr, first, step, e, sm.g); break;
+        case 0: grow_body<E, 0, true, REAL>(ob, op.off0, op.off1, psi, lam, gr, first, step, e, sm.g); break;
+        case 1: grow_body<E, 1, true, REAL>(ob, op.off0, op.off1, psi, lam, gr, first, step, e, sm.g); break;
+        case 2: grow_body<E, 2, true, REAL>(ob, op.off0, op.off1, psi, lam, gr, first, step, e, sm.g); break;
+        case 3: grow_body<E, 3, true, REAL>(ob, op.off0, op.off1, psi, lam, gr, first, step, e, sm.g); break;
         default: break;
         }
         break;
@@ -195,7 +195,7 @@ __device__ __forceinline__ void run_op_slice(const BatchOp &op, const uint8_t *b
     }
 }
 
-template <typename E>
+template <typename E, bool REAL>
 __global__ void __launch_bounds__(kThreads, 2) batch_kernel(const uint8_t *__restrict__ blob,
                                                              const BatchOp *__restrict__ ops,
                                                              const BatchTask *__restrict__ tasks, uint32_t ntasks,
@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(kThreads, 2) batch_kernel(const uint8_t *__res
         __syncthreads();
         if (s_abort) break;
         const bool grow = op.kind == BOP_GROW || op.kind == BOP_GROW_ADJ;
-        run_op_slice<E>(op, blob, arena, grads, energies, task.begin, task.end, grow ? task.begin : 0,
+        run_op_slice<E, REAL>(op, blob, arena, grads, energies, task.begin, task.end, grow ? task.begin : 0,
                         grow ? uint64_t(kWarps) : 0, sm);
         __threadfence();
         __syncthreads();
@@ -238,30 +238,41 @@ __global__ void __launch_bounds__(kThreads, 2) batch_kernel(const uint8_t *__res
     }
 }
 
-template <typename E>
+template <typename E, bool REAL>
 cudaError_t persistent_typed(const uint8_t *blob, const BatchOp *ops, const BatchTask *tasks, uint32_t ntasks,
                              uint32_t *next, uint32_t *remaining, E *arena, double *grads, double *energies,
                              DevStatus *status, int sms, cudaStream_t st)
 {
     int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<E>, kThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<E, REAL>, kThreads, 0);
     if (per_sm < 1) per_sm = 1;
-    batch_kernel<E><<<unsigned(sms * per_sm), kThreads, 0, st>>>(blob, ops, tasks, ntasks, next, remaining, arena,
-                                                                 grads, energies, status);
+    batch_kernel<E, REAL><<<unsigned(sms * per_sm), kThreads, 0, st>>>(blob, ops, tasks, ntasks, next, remaining,
+                                                                       arena, grads, energies, status);
     return cudaGetLastError();
+}
+
+template <typename E>
+cudaError_t persistent_real(bool real, const uint8_t *blob, const BatchOp *ops, const BatchTask *tasks,
+                            uint32_t ntasks, uint32_t *next, uint32_t *remaining, E *arena, double *grads,
+                            double *energies, DevStatus *status, int sms, cudaStream_t st)
+{
+    return real ? persistent_typed<E, true>(blob, ops, tasks, ntasks, next, remaining, arena, grads, energies, status,
+                                            sms, st)
+                : persistent_typed<E, false>(blob, ops, tasks, ntasks, next, remaining, arena, grads, energies,
+                                             status, sms, st);
 }
 
 }  // namespace
 
 cudaError_t run_batch_persistent(const uint8_t *blob, const BatchOp *ops, const BatchTask *tasks, uint32_t ntasks,
                                  uint32_t *next, uint32_t *remaining, void *arena, double *grads, double *energies,
-                                 DevStatus *status, int elem_bytes, int sms, cudaStream_t st)
+                                 DevStatus *status, int elem_bytes, bool real, int sms, cudaStream_t st)
 {
     if (elem_bytes == 8)
-        return persistent_typed(blob, ops, tasks, ntasks, next, remaining, static_cast<float2 *>(arena), grads,
-                                energies, status, sms, st);
-    return persistent_typed(blob, ops, tasks, ntasks, next, remaining, static_cast<double2 *>(arena), grads, energies,
-                            status, sms, st);
+        return persistent_real(real, blob, ops, tasks, ntasks, next, remaining, static_cast<float2 *>(arena), grads,
+                               energies, status, sms, st);
+    return persistent_real(real, blob, ops, tasks, ntasks, next, remaining, static_cast<double2 *>(arena), grads,
+                           energies, status, sms, st);
 }
 
 }  // namespace zxh

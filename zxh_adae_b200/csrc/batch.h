@@ -30,7 +30,7 @@ struct BatchOp {
     uint64_t base;                   // this op's descriptors start at blob + base
     uint64_t off0, off1, off2;       // GROW*: pass descriptor, phase table; LAMBDA: terms;
                                      // DIAG_ADJ: gates, slots, phase table (all from base)
-    uint32_t aux, m;                 // LAMBDA: terms; DIAG_ADJ: gates; m: state bits
+    uint32_t aux, m;                 // LAMBDA: terms; DIAG_ADJ: gates; GROW*: 1 if every gate is real; m: state bits
     uint64_t psi, lam;               // element offsets of the circuit's states in the arena
     uint32_t grad_base, energy;      // the circuit's first gradient slot and its energy slot
 };
@@ -41,9 +41,10 @@ struct BatchTask {
 };
 
 // Runs every task of the queue; counters: `next` (queue head, zeroed) and
-// `remaining[op]` (tasks of each op, preset). grid = resident CTAs.
+// `remaining[op]` (tasks of each op, preset). grid = resident CTAs. real: every
+// strided op of the queue has real gates (the kernel's real-gate form).
 cudaError_t run_batch_persistent(const uint8_t *blob, const BatchOp *ops, const BatchTask *tasks, uint32_t ntasks,
                                  uint32_t *next, uint32_t *remaining, void *arena, double *grads, double *energies,
-                                 DevStatus *status, int elem_bytes, int sms, cudaStream_t st);
+                                 DevStatus *status, int elem_bytes, bool real, int sms, cudaStream_t st);
 
 }  // namespace zxh

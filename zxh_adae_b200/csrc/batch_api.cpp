@@ -62,6 +62,7 @@ struct zxh_batch {
 
     int grow_regs = 4, task_items = 128, task_elems = 1 << 17;
     uint64_t bytes = 0;  // algorithmic state bytes of one run
+    bool real = false;   // every strided op has real gates: the persistent kernel's real-gate form
     float last_ms = 0.0f;
 };
 
@@ -183,6 +184,7 @@ int compile(zxh_batch *b)
                 op.base = base;
                 op.off0 = ps.off;
                 op.off1 = ps.off2;
+                op.aux = ps.gb.all_real() ? 1u : 0u;
             } else {
                 return bfail(b, ZXH_ERR_ARG, "circuit " + std::to_string(c) +
                                                  " needs a pass the batched launch does not run (n >= 6 required)");
@@ -221,6 +223,7 @@ int compile(zxh_batch *b)
                 op.base = gbase;
                 op.off0 = r.off;
                 op.off1 = r.toff;
+                op.aux = r.gb.all_real() ? 1u : 0u;
             } else if (r.kind == zxh::adj::RevStep::DIAG) {
                 op.kind = zxh::BOP_DIAG_ADJ;
                 op.units = uint64_t(1) << N;
@@ -310,7 +313,8 @@ int enqueue_persistent(zxh_batch *b)
                            b->stream),
         "reset counters");
     BCK(b, zxh::run_batch_persistent(b->d_blob, b->d_ops, b->d_tasks, uint32_t(b->tasks.size()), b->d_next, b->d_rem,
-                                     b->d_arena, b->d_grads, b->d_energy, b->d_status, b->eb, b->sms, b->stream),
+                                     b->d_arena, b->d_grads, b->d_energy, b->d_status, b->eb, b->real, b->sms,
+                                     b->stream),
         "batch launch");
     return ZXH_OK;
 }
@@ -331,15 +335,15 @@ int launch_op(zxh_batch *b, const BatchOp &op)
         break;
     case zxh::BOP_GROW:
         e = zxh::run_grow(b->d_blob + op.base, op.off0, op.off1, int(op.R), op.units, b->eb, psi, nullptr, nullptr,
-                          b->sms, b->stream);
+                          op.aux != 0, b->sms, b->stream);
         break;
     case zxh::BOP_LAMBDA:
         e = zxh::run_lambda(psi, lam, int(op.m), b->eb, reinterpret_cast<const zxh::TermDev *>(b->d_blob + op.off0),
                             op.aux, b->d_energy + op.energy, b->sms, b->stream);
         break;
     case zxh::BOP_GROW_ADJ:
-        e = zxh::run_grow(b->d_blob + op.base, op.off0, op.off1, int(op.R), op.units, b->eb, psi, lam, gr, b->sms,
-                          b->stream);
+        e = zxh::run_grow(b->d_blob + op.base, op.off0, op.off1, int(op.R), op.units, b->eb, psi, lam, gr,
+                          op.aux != 0, b->sms, b->stream);
         break;
     case zxh::BOP_DIAG_ADJ:
         e = zxh::run_adj_diag(psi, lam, int(op.m), b->eb,
@@ -356,6 +360,9 @@ int launch_op(zxh_batch *b, const BatchOp &op)
 int build(zxh_batch *b)
 {
     if (int rc = compile(b)) return rc;
+    b->real = true;
+    for (const BatchOp &op : b->ops)
+        if ((op.kind == zxh::BOP_GROW || op.kind == zxh::BOP_GROW_ADJ) && !op.aux) b->real = false;
     make_tasks(b);
     return upload(b);
 }

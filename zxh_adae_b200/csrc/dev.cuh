@@ -84,6 +84,17 @@ __device__ __forceinline__ double2 phase_factor(const double2 *tab, int64_t th)
     return make_double2(t.x * c - t.y * s, t.x * s + t.y * c);
 }
 
+// a * x + b * y for real a, b: complex64 amplitudes as (re, im) pairs take paired
+// FP32 FMAs (two lanes of work per instruction).
+__device__ __forceinline__ float2 rmad2(float a, float2 x, float b, float2 y)
+{
+    return __ffma2_rn(make_float2(b, b), y, __fmul2_rn(make_float2(a, a), x));
+}
+__device__ __forceinline__ double2 rmad2(double a, double2 x, double b, double2 y)
+{
+    return make_double2(fma(b, y.x, a * x.x), fma(b, y.y, a * x.y));
+}
+
 template <typename E>
 __device__ __forceinline__ E cmul(E a, E b)
 {

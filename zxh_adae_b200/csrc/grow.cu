@@ -39,44 +39,52 @@ namespace {
 
 using namespace gdev;
 
-template <typename E, int R, bool ADJ>
+template <typename E, int R, bool ADJ, bool REAL>
 __global__ void __launch_bounds__(kThreads, 2) grow_kernel(const uint8_t *__restrict__ blob, uint64_t poff,
                                                             uint64_t toff, E *__restrict__ psi, E *__restrict__ lam,
                                                             double *grads, uint64_t nitems)
 {
     __shared__ GrowShared<E> sm;
     constexpr int WARPS = kThreads / 32;
-    grow_body<E, R, ADJ>(blob, poff, toff, psi, lam, grads, uint64_t(blockIdx.x) * WARPS, uint64_t(gridDim.x) * WARPS,
-                         nitems, sm);
+    grow_body<E, R, ADJ, REAL>(blob, poff, toff, psi, lam, grads, uint64_t(blockIdx.x) * WARPS,
+                               uint64_t(gridDim.x) * WARPS, nitems, sm);
 }
 
-template <typename E, int R, bool ADJ>
+template <typename E, int R, bool ADJ, bool REAL>
 cudaError_t launch_grow(const uint8_t *dblob, uint64_t poff, uint64_t toff, uint64_t nitems, E *psi, E *lam,
                         double *grads, int sms, cudaStream_t st)
 {
     int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grow_kernel<E, R, ADJ>, kThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grow_kernel<E, R, ADJ, REAL>, kThreads, 0);
     if (per_sm < 1) per_sm = 1;
     const uint64_t ctas = (nitems + kThreads / 32 - 1) / (kThreads / 32);
     const unsigned grid = unsigned(std::max<uint64_t>(1, std::min<uint64_t>(ctas, uint64_t(sms) * uint64_t(per_sm))));
-    grow_kernel<E, R, ADJ><<<grid, kThreads, 0, st>>>(dblob, poff, toff, psi, lam, grads, nitems);
+    grow_kernel<E, R, ADJ, REAL><<<grid, kThreads, 0, st>>>(dblob, poff, toff, psi, lam, grads, nitems);
     return cudaGetLastError();
 }
 
-template <typename E, bool ADJ>
+template <typename E, bool ADJ, bool REAL>
 cudaError_t grow_typed(int R, const uint8_t *dblob, uint64_t poff, uint64_t toff, uint64_t nitems, E *psi, E *lam,
                        double *grads, int sms, cudaStream_t st)
 {
     switch (R) {
-    case 0: return launch_grow<E, 0, ADJ>(dblob, poff, toff, nitems, psi, lam, grads, sms, st);
-    case 1: return launch_grow<E, 1, ADJ>(dblob, poff, toff, nitems, psi, lam, grads, sms, st);
-    case 2: return launch_grow<E, 2, ADJ>(dblob, poff, toff, nitems, psi, lam, grads, sms, st);
-    case 3: return launch_grow<E, 3, ADJ>(dblob, poff, toff, nitems, psi, lam, grads, sms, st);
+    case 0: return launch_grow<E, 0, ADJ, REAL>(dblob, poff, toff, nitems, psi, lam, grads, sms, st);
+    case 1: return launch_grow<E, 1, ADJ, REAL>(dblob, poff, toff, nitems, psi, lam, grads, sms, st);
+    case 2: return launch_grow<E, 2, ADJ, REAL>(dblob, poff, toff, nitems, psi, lam, grads, sms, st);
+    case 3: return launch_grow<E, 3, ADJ, REAL>(dblob, poff, toff, nitems, psi, lam, grads, sms, st);
     case 4:
-        if constexpr (!ADJ) return launch_grow<E, 4, ADJ>(dblob, poff, toff, nitems, psi, lam, grads, sms, st);
+        if constexpr (!ADJ) return launch_grow<E, 4, ADJ, REAL>(dblob, poff, toff, nitems, psi, lam, grads, sms, st);
         return cudaErrorInvalidValue;
     default: return cudaErrorInvalidValue;
     }
+}
+
+template <typename E, bool ADJ>
+cudaError_t grow_real(bool real, int R, const uint8_t *dblob, uint64_t poff, uint64_t toff, uint64_t nitems, E *psi,
+                      E *lam, double *grads, int sms, cudaStream_t st)
+{
+    return real ? grow_typed<E, ADJ, true>(R, dblob, poff, toff, nitems, psi, lam, grads, sms, st)
+                : grow_typed<E, ADJ, false>(R, dblob, poff, toff, nitems, psi, lam, grads, sms, st);
 }
 
 }  // namespace
@@ -92,19 +100,19 @@ int grow_fixed_bits(int elem_bytes) { return elem_bytes == 8 ? 6 : 5; }
 int grow_adjoint_gates() { return kGrowAdjGates; }
 
 cudaError_t run_grow(const uint8_t *dblob, uint64_t poff, uint64_t toff, int R, uint64_t nitems, int elem_bytes,
-                     void *psi, void *lam, double *grads, int sms, cudaStream_t st)
+                     void *psi, void *lam, double *grads, bool real, int sms, cudaStream_t st)
 {
     const bool adj = lam != nullptr;
     if (elem_bytes == 8) {
         auto *a = static_cast<float2 *>(psi);
         auto *b = static_cast<float2 *>(lam);
-        return adj ? grow_typed<float2, true>(R, dblob, poff, toff, nitems, a, b, grads, sms, st)
-                   : grow_typed<float2, false>(R, dblob, poff, toff, nitems, a, b, grads, sms, st);
+        return adj ? grow_real<float2, true>(real, R, dblob, poff, toff, nitems, a, b, grads, sms, st)
+                   : grow_real<float2, false>(real, R, dblob, poff, toff, nitems, a, b, grads, sms, st);
     }
     auto *a = static_cast<double2 *>(psi);
     auto *b = static_cast<double2 *>(lam);
-    return adj ? grow_typed<double2, true>(R, dblob, poff, toff, nitems, a, b, grads, sms, st)
-               : grow_typed<double2, false>(R, dblob, poff, toff, nitems, a, b, grads, sms, st);
+    return adj ? grow_real<double2, true>(real, R, dblob, poff, toff, nitems, a, b, grads, sms, st)
+               : grow_real<double2, false>(real, R, dblob, poff, toff, nitems, a, b, grads, sms, st);
 }
 
 }  // namespace zxh

@@ -82,8 +82,9 @@ __device__ __forceinline__ void grow_store(E *s, uint64_t a, int lane, typename 
     }
 }
 
-// Register gate on coordinate RR: rows j (bit RR clear) and j | 2^RR.
-template <int RR, int NR, int V, bool ADJ, typename VT, typename RT>
+// Register gate on coordinate RR: rows j (bit RR clear) and j | 2^RR. REAL: the
+// matrix has no imaginary parts (RY and the like), half the multiply-adds.
+template <int RR, int NR, int V, bool ADJ, bool REAL, typename VT, typename RT>
 __device__ __forceinline__ void grow_reg_gate(VT (&x)[NR], VT (&y)[NR], const RT (&m)[V][8], uint32_t orient,
                                               uint32_t gen, double &acc)
 {
@@ -104,25 +105,35 @@ __device__ __forceinline__ void grow_reg_gate(VT (&x)[NR], VT (&y)[NR], const RT
                 } else if (gen == 2) {  // Im<l|X|p> = Im(conj(l0) p1 + conj(l1) p0)
                     part += (llo.x * hi.y - llo.y * hi.x) + (lhi.x * lo.y - lhi.y * lo.x);
                 }
-                vset(y[j], v, mad2(&m[v][0], llo, lhi));
-                vset(y[j | B], v, mad2(&m[v][4], llo, lhi));
+                if constexpr (REAL) {
+                    vset(y[j], v, rmad2(m[v][0], llo, m[v][2], lhi));
+                    vset(y[j | B], v, rmad2(m[v][4], llo, m[v][6], lhi));
+                } else {
+                    vset(y[j], v, mad2(&m[v][0], llo, lhi));
+                    vset(y[j | B], v, mad2(&m[v][4], llo, lhi));
+                }
             }
-            vset(x[j], v, mad2(&m[v][0], lo, hi));
-            vset(x[j | B], v, mad2(&m[v][4], lo, hi));
+            if constexpr (REAL) {
+                vset(x[j], v, rmad2(m[v][0], lo, m[v][2], hi));
+                vset(x[j | B], v, rmad2(m[v][4], lo, m[v][6], hi));
+            } else {
+                vset(x[j], v, mad2(&m[v][0], lo, hi));
+                vset(x[j | B], v, mad2(&m[v][4], lo, hi));
+            }
         }
     }
     if constexpr (ADJ) acc += double(part);
 }
 
-template <int R, int NR, int V, bool ADJ, typename VT, typename RT>
+template <int R, int NR, int V, bool ADJ, bool REAL, typename VT, typename RT>
 __device__ __forceinline__ void grow_reg_dispatch(int rr, VT (&x)[NR], VT (&y)[NR], const RT (&m)[V][8],
                                                   uint32_t orient, uint32_t gen, double &acc)
 {
     switch (rr) {
-    case 0: if constexpr (R > 0) grow_reg_gate<0, NR, V, ADJ>(x, y, m, orient, gen, acc); break;
-    case 1: if constexpr (R > 1) grow_reg_gate<(R > 1 ? 1 : 0), NR, V, ADJ>(x, y, m, orient, gen, acc); break;
-    case 2: if constexpr (R > 2) grow_reg_gate<(R > 2 ? 2 : 0), NR, V, ADJ>(x, y, m, orient, gen, acc); break;
-    case 3: if constexpr (R > 3) grow_reg_gate<(R > 3 ? 3 : 0), NR, V, ADJ>(x, y, m, orient, gen, acc); break;
+    case 0: if constexpr (R > 0) grow_reg_gate<0, NR, V, ADJ, REAL>(x, y, m, orient, gen, acc); break;
+    case 1: if constexpr (R > 1) grow_reg_gate<(R > 1 ? 1 : 0), NR, V, ADJ, REAL>(x, y, m, orient, gen, acc); break;
+    case 2: if constexpr (R > 2) grow_reg_gate<(R > 2 ? 2 : 0), NR, V, ADJ, REAL>(x, y, m, orient, gen, acc); break;
+    case 3: if constexpr (R > 3) grow_reg_gate<(R > 3 ? 3 : 0), NR, V, ADJ, REAL>(x, y, m, orient, gen, acc); break;
     default: break;
     }
 }
@@ -442,8 +453,9 @@ __device__ __forceinline__ void adj_window_grad(const VT (&x)[1 << R], const VT 
 
 // One general strided pass (or the part of it made of items first + warp,
 // first + warp + step, ... below end) on the calling CTA. Every thread of the CTA
-// calls it; it synchronises the CTA on entry and exit.
-template <typename E, int R, bool ADJ>
+// calls it; it synchronises the CTA on entry and exit. REAL: every gate of the
+// pass has a real matrix.
+template <typename E, int R, bool ADJ, bool REAL = false>
 __device__ __forceinline__ void grow_body(const uint8_t *__restrict__ blob, uint64_t poff, uint64_t toff,
                                           E *__restrict__ psi, E *__restrict__ lam, double *grads, uint64_t first,
                                           uint64_t step, uint64_t end, GrowShared<E> &sm)
@@ -598,7 +610,7 @@ __device__ __forceinline__ void grow_body(const uint8_t *__restrict__ blob, uint
                 for (int i = 0; i < 8; i++) m[v][i] = s_u[g][(orient >> v) & 1][i];
             double ga = 0.0;
             if ((kr & 0xff) == 0) {
-                grow_reg_dispatch<R, NR, V, ADJ>(int(kr >> 8), x, y, m, orient, gen, ga);
+                grow_reg_dispatch<R, NR, V, ADJ, REAL>(int(kr >> 8), x, y, m, orient, gen, ga);
             } else {
                 using EE = decltype(vget(x[0], 0));
                 const int lx = int(s_g[g][1]), vx = int(s_g[g][2]);
@@ -611,7 +623,8 @@ __device__ __forceinline__ void grow_body(const uint8_t *__restrict__ blob, uint
                         const EE own = vget(x[j], v);
                         const EE src = vget(x[j], v ^ (V == 2 ? vx : 0));
                         const EE pt = lx ? shfl_xor_c(src, lx) : src;
-                        nx[v] = mad2(&m[v][0], own, pt);
+                        if constexpr (REAL) nx[v] = rmad2(m[v][0], own, m[v][2], pt);
+                        else nx[v] = mad2(&m[v][0], own, pt);
                         if constexpr (ADJ) {
                             const EE lown = vget(y[j], v);
                             const EE lsrc = vget(y[j], v ^ (V == 2 ? vx : 0));
@@ -622,7 +635,8 @@ __device__ __forceinline__ void grow_body(const uint8_t *__restrict__ blob, uint
                             } else if (gen == 2) {
                                 gpart += lown.x * pt.y - lown.y * pt.x;
                             }
-                            ny[v] = mad2(&m[v][0], lown, lpt);
+                            if constexpr (REAL) ny[v] = rmad2(m[v][0], lown, m[v][2], lpt);
+                            else ny[v] = mad2(&m[v][0], lown, lpt);
                         }
                     }
 #pragma unroll

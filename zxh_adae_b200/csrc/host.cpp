@@ -666,6 +666,13 @@ int GrowBuild::selector(const Sel &s)
     return int(sels.size()) - 1;
 }
 
+bool GrowBuild::all_real() const
+{
+    for (const GrowGateDev &g : gates)
+        if (g.u[1] != 0.0 || g.u[3] != 0.0 || g.u[5] != 0.0 || g.u[7] != 0.0) return false;
+    return true;
+}
+
 bool GrowBuild::add_gate(const U3Op &u, uint32_t gen, uint32_t slot, bool adjoint_matrix)
 {
     if (gates.size() >= size_t(kGrowMaxGates) || u.has_ctrl || !u.delta) return false;

@@ -84,6 +84,7 @@ struct GrowBuild {
     // kinds and slots and inverse = true (the inverse phase is applied).
     bool add_window(int which, const std::vector<DiagTerm> &w, const std::vector<uint32_t> *gk = nullptr,
                     const std::vector<uint32_t> *slot = nullptr, bool inverse = false);
+    bool all_real() const;  // every gate matrix has zero imaginary parts
 };
 
 struct Pass {

@@ -156,17 +156,6 @@ __device__ __forceinline__ E cmad2(RT ar, RT ai, E x, RT br, RT bi, E y)
     return o;
 }
 
-// a * x + b * y for real a, b: complex64 amplitudes as (re, im) pairs take paired
-// FP32 FMAs (two lanes of work per instruction).
-__device__ __forceinline__ float2 rmad2(float a, float2 x, float b, float2 y)
-{
-    return __ffma2_rn(make_float2(b, b), y, __fmul2_rn(make_float2(a, a), x));
-}
-__device__ __forceinline__ double2 rmad2(double a, double2 x, double b, double2 y)
-{
-    return make_double2(fma(b, y.x, a * x.x), fma(b, y.y, a * x.y));
-}
-
 // 2x2 gate on register bit RR of every row pair: compile-time positions keep the
 // amplitudes in registers. REAL: the matrix has no imaginary parts (a rotation
 // split off a U3 by the planner), half the multiply-adds.
