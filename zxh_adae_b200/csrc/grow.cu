@@ -19,7 +19,7 @@
 //   per-thread constant, the third is nonzero only for the pass's own register
 //   qubits. Gate orientation and window phases follow from these bits; a
 //   window's phase over a thread's rows is a polynomial in the row bits (constant,
-//   linear, pairwise) walked in Gray-code order.
+//   linear, pairwise), summed per row at compile-time positions.
 // * Adjoint mode (two states psi, lambda): each gate's gradient Im<lambda|G|psi>
 //   is reduced in FP64 right before its U^dagger is applied to both states; the
 //   pass's gates act on distinct qubits and commute, so that is the gradient at

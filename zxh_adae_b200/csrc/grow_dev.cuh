@@ -142,12 +142,20 @@ __device__ __forceinline__ void grow_reg_dispatch(int rr, VT (&x)[NR], VT (&y)[N
 // k_i w_i + sum_{i<j} k_i k_j q_ij. Term classes (sorted on the host): [0, n1)
 // single selector without row dependence, [n1, n2) two selectors without row
 // dependence, [n2, n) the rest.
+// pair coefficients q_ij, i < j, stored row by row
 template <int R>
 struct WinPoly {
+    static constexpr int NQ = R * (R - 1) / 2 > 0 ? R * (R - 1) / 2 : 1;
     int64_t K;
-    int64_t w[R];
-    int64_t q[R][R];
+    int64_t w[R > 0 ? R : 1];
+    int64_t q[NQ];
 };
+
+template <int R>
+__host__ __device__ constexpr int qidx(int i, int j)  // i < j
+{
+    return i * (2 * R - i - 1) / 2 + (j - i - 1);
+}
 
 template <int R>
 __device__ __forceinline__ void add_w(WinPoly<R> &P, int kb, int64_t val)
@@ -165,7 +173,7 @@ __device__ __forceinline__ void add_q(WinPoly<R> &P, int a, int b, int64_t val)
     for (int ii = 0; ii < R; ii++)
 #pragma unroll
         for (int jj = ii + 1; jj < R; jj++)
-            if (ii == i && jj == j) P.q[ii][jj] += val;
+            if (ii == i && jj == j) P.q[qidx<R>(ii, jj)] += val;
 }
 
 template <int R>
@@ -174,11 +182,9 @@ __device__ __forceinline__ void window_poly(WinPoly<R> &P, const GrowTermDev *t,
 {
     P.K = 0;
 #pragma unroll
-    for (int i = 0; i < R; i++) {
-        P.w[i] = 0;
+    for (int i = 0; i < R; i++) P.w[i] = 0;
 #pragma unroll
-        for (int j = 0; j < R; j++) P.q[i][j] = 0;
-    }
+    for (int i = 0; i < WinPoly<R>::NQ; i++) P.q[i] = 0;
     for (uint32_t q = 0; q < n1; q++)
         if ((c >> t[q].s0) & 1) P.K += t[q].coef;
     for (uint32_t q = n1; q < n2; q++)
@@ -212,8 +218,8 @@ __device__ __forceinline__ void window_poly(WinPoly<R> &P, const GrowTermDev *t,
 template <int R>
 struct WinPoly32 {
     uint32_t K;
-    uint32_t w[R];
-    uint32_t q[R][R];
+    uint32_t w[R > 0 ? R : 1];
+    uint32_t q[WinPoly<R>::NQ];
 };
 
 template <int R>
@@ -222,43 +228,34 @@ __device__ __forceinline__ WinPoly32<R> to32(const WinPoly<R> &P)
     WinPoly32<R> o;
     o.K = turns32(P.K);
 #pragma unroll
-    for (int i = 0; i < R; i++) {
-        o.w[i] = turns32(P.w[i]);
+    for (int i = 0; i < R; i++) o.w[i] = turns32(P.w[i]);
 #pragma unroll
-        for (int j = 0; j < R; j++) o.q[i][j] = j > i ? turns32(P.q[i][j]) : 0u;
-    }
+    for (int i = 0; i < WinPoly<R>::NQ; i++) o.q[i] = turns32(P.q[i]);
     return o;
 }
 
-// complex64: the window's phase in 32-bit turns per amplitude; applied to x and,
-// when given, to y (adjoint passes: psi and lambda get the same phase)
+// complex64: the window's phase in 32-bit turns per amplitude, summed per row from
+// the row's bits (compile-time, so the polynomial stays in registers); applied to
+// x and, when given, to y (adjoint passes: psi and lambda get the same phase)
 template <int R, typename VT>
 __device__ __forceinline__ void apply_poly32(VT (&x)[1 << R], const WinPoly32<R> (&P)[2], const float2 *s_exp,
                                              VT *y = nullptr)
 {
     constexpr int NR = 1 << R;
-    constexpr int V = 2;
-    uint32_t acc[V];
 #pragma unroll
-    for (int v = 0; v < V; v++) acc[v] = P[v].K;
+    for (int g = 0; g < NR; g++) {
 #pragma unroll
-    for (int jj = 0; jj < NR; jj++) {
-        const int g = jj ^ (jj >> 1);
-        if (jj > 0) {
-            const int fb = ctz_const(jj);
-            const bool up = (g >> fb) & 1;
+        for (int v = 0; v < 2; v++) {
+            uint32_t a = P[v].K;
 #pragma unroll
-            for (int v = 0; v < V; v++) {
-                uint32_t d = P[v].w[fb];
+            for (int i = 0; i < R; i++) {
+                if (!((g >> i) & 1)) continue;
+                a += P[v].w[i];
 #pragma unroll
-                for (int o = 0; o < R; o++)
-                    if (o != fb && ((g >> o) & 1)) d += (o < fb) ? P[v].q[o][fb] : P[v].q[fb][o];
-                acc[v] += up ? d : 0u - d;
+                for (int j = i + 1; j < R; j++)
+                    if ((g >> j) & 1) a += P[v].q[qidx<R>(i, j)];
             }
-        }
-#pragma unroll
-        for (int v = 0; v < V; v++) {
-            const float2 ph = phase_factor32(s_exp, acc[v]);
+            const float2 ph = phase_factor32(s_exp, a);
             vset(x[g], v, cmul(vget(x[g], v), ph));
             if (y) vset(y[g], v, cmul(vget(y[g], v), ph));
         }
@@ -270,31 +267,22 @@ __device__ __forceinline__ void apply_poly(VT (&x)[1 << R], const WinPoly<R> (&P
                                            VT *y = nullptr)
 {
     constexpr int NR = 1 << R;
-    {
-        int64_t acc[V];
 #pragma unroll
-        for (int v = 0; v < V; v++) acc[v] = P[v].K;
+    for (int g = 0; g < NR; g++) {
 #pragma unroll
-        for (int jj = 0; jj < NR; jj++) {
-            const int g = jj ^ (jj >> 1);
-            if (jj > 0) {
-                const int fb = ctz_const(jj);
-                const bool up = (g >> fb) & 1;
+        for (int v = 0; v < V; v++) {
+            int64_t a = P[v].K;
 #pragma unroll
-                for (int v = 0; v < V; v++) {
-                    int64_t d = P[v].w[fb];
+            for (int i = 0; i < R; i++) {
+                if (!((g >> i) & 1)) continue;
+                a += P[v].w[i];
 #pragma unroll
-                    for (int o = 0; o < R; o++)
-                        if (o != fb && ((g >> o) & 1)) d += (o < fb) ? P[v].q[o][fb] : P[v].q[fb][o];
-                    acc[v] += up ? d : -d;
-                }
+                for (int j = i + 1; j < R; j++)
+                    if ((g >> j) & 1) a += P[v].q[qidx<R>(i, j)];
             }
-#pragma unroll
-            for (int v = 0; v < V; v++) {
-                const E ph = phase_factor(s_exp, acc[v]);
-                vset(x[g], v, cmul(vget(x[g], v), ph));
-                if (y) vset(y[g], v, cmul(vget(y[g], v), ph));
-            }
+            const E ph = phase_factor(s_exp, a);
+            vset(x[g], v, cmul(vget(x[g], v), ph));
+            if (y) vset(y[g], v, cmul(vget(y[g], v), ph));
         }
     }
 }
