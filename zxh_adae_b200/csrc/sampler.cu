@@ -6,8 +6,9 @@
 // level structure (segments of 2^12 amplitudes, then an offset inside the segment),
 // and returns shots grouped by segment in the reference's output order. The
 // machinery is new:
-//   seg_scan_kernel      one read of the state: per-segment FP64 |amp|^2 mass and a
-//                        single-pass decoupled-lookback inclusive scan over segments
+//   seg_mass_kernel      one streaming read of the state: per-segment FP64 |amp|^2
+//                        mass, one warp per segment.
+//   seg_scan_kernel      single-pass decoupled-lookback inclusive scan of the masses
 //                        (the reference runs segment_mass_kernel + a CUB scan).
 //   count_kernel         shot -> segment by binary search, warp-aggregated atomics.
 //   offsets (3 kernels)  exclusive scan of the per-segment counts.
@@ -75,12 +76,22 @@ __device__ __forceinline__ double seg_partial(const float2 *seg, uint32_t seglen
     const uint32_t nv = seglen / 2;
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
     uint32_t k = uint32_t(lane);
+    auto sq = [](const float4 &x) { return double(x.x) * x.x + double(x.y) * x.y + double(x.z) * x.z + double(x.w) * x.w; };
+    for (; k + 224 < nv; k += 256) {  // 8 loads in flight per lane
+        float4 x[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) x[i] = __ldcs(v + k + 32 * i);
+        a0 += sq(x[0]) + sq(x[4]);
+        a1 += sq(x[1]) + sq(x[5]);
+        a2 += sq(x[2]) + sq(x[6]);
+        a3 += sq(x[3]) + sq(x[7]);
+    }
     for (; k + 96 < nv; k += 128) {
         const float4 x0 = __ldg(v + k), x1 = __ldg(v + k + 32), x2 = __ldg(v + k + 64), x3 = __ldg(v + k + 96);
-        a0 += double(x0.x) * x0.x + double(x0.y) * x0.y + double(x0.z) * x0.z + double(x0.w) * x0.w;
-        a1 += double(x1.x) * x1.x + double(x1.y) * x1.y + double(x1.z) * x1.z + double(x1.w) * x1.w;
-        a2 += double(x2.x) * x2.x + double(x2.y) * x2.y + double(x2.z) * x2.z + double(x2.w) * x2.w;
-        a3 += double(x3.x) * x3.x + double(x3.y) * x3.y + double(x3.z) * x3.z + double(x3.w) * x3.w;
+        a0 += sq(x0);
+        a1 += sq(x1);
+        a2 += sq(x2);
+        a3 += sq(x3);
     }
     for (; k < nv; k += 32) {
         const float4 x = __ldg(v + k);
@@ -132,9 +143,23 @@ __device__ __forceinline__ double range_mass(const double2 *seg, uint32_t lo, ui
 
 // ---------------------------------------------------------------------------
 
+// Per-segment FP64 mass, one warp per segment: a plain streaming read of the state.
 template <typename E>
-__global__ void __launch_bounds__(kThreads) seg_scan_kernel(const E *__restrict__ state, uint64_t nseg, uint32_t seglen,
-                                                            double *__restrict__ segcdf, double *agg_val,
+__global__ void __launch_bounds__(kThreads) seg_mass_kernel(const E *__restrict__ state, uint64_t nseg, uint32_t seglen,
+                                                            double *__restrict__ mass)
+{
+    const int lane = threadIdx.x & 31;
+    const uint64_t w0 = (uint64_t(blockIdx.x) * kThreads + threadIdx.x) >> 5;
+    const uint64_t nw = (uint64_t(gridDim.x) * kThreads) >> 5;
+    for (uint64_t sg = w0; sg < nseg; sg += nw) {
+        const double acc = warp_sum_f64(seg_partial(state + sg * seglen, seglen, lane));
+        if (lane == 0) mass[sg] = acc;
+    }
+}
+
+// Inclusive scan of the segment masses (read from segcdf, which seg_mass_kernel
+// filled, and overwritten in place chunk by chunk) with decoupled lookback.
+__global__ void __launch_bounds__(kThreads) seg_scan_kernel(uint64_t nseg, double *segcdf, double *agg_val,
                                                             uint32_t *agg_flag, double *inc_val, uint32_t *inc_flag,
                                                             uint32_t *ticket, DevStatus *status)
 {
@@ -142,7 +167,7 @@ __global__ void __launch_bounds__(kThreads) seg_scan_kernel(const E *__restrict_
     __shared__ double s_mass[kSegsPerChunk];
     __shared__ double s_prefix;
     __shared__ int s_abort;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x;
     const uint64_t nchunks = (nseg + kSegsPerChunk - 1) / kSegsPerChunk;
     if (tid == 0) s_abort = 0;
     for (;;) {
@@ -153,11 +178,7 @@ __global__ void __launch_bounds__(kThreads) seg_scan_kernel(const E *__restrict_
         if (chunk >= nchunks || s_abort) break;
         const uint64_t base = chunk * kSegsPerChunk;
         const int nloc = int((nseg - base < uint64_t(kSegsPerChunk) ? nseg - base : uint64_t(kSegsPerChunk)));
-        for (int sl = warp; sl < nloc; sl += kThreads / 32) {
-            const E *seg = state + (base + uint64_t(sl)) * seglen;
-            const double acc = warp_sum_f64(seg_partial(seg, seglen, lane));
-            if (lane == 0) s_mass[sl] = acc;
-        }
+        if (tid < nloc) s_mass[tid] = segcdf[base + uint64_t(tid)];
         __syncthreads();
         if (tid == 0) {
             double run = 0.0;
@@ -528,14 +549,15 @@ cudaError_t run_sampler(const void *state, int elem_bytes, int m, uint64_t shots
     e = cudaMemcpyAsync(sc.coltab, host_coltab, 8 * 256 * 8, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return e;
     const unsigned gs = unsigned(std::max<uint64_t>(1, std::min<uint64_t>(nchunks, uint64_t(sms) * 4)));
+    const unsigned gmass = unsigned(std::max<uint64_t>(1, std::min<uint64_t>((nseg * 32 + kThreads - 1) / kThreads,
+                                                                             uint64_t(sms) * 8)));
     if (elem_bytes == 8)
-        seg_scan_kernel<float2><<<gs, kThreads, 0, st>>>(static_cast<const float2 *>(state), nseg, seglen, sc.segcdf,
-                                                        sc.agg_val, sc.agg_flag, sc.inc_val, sc.inc_flag, sc.ticket,
-                                                        status);
+        seg_mass_kernel<float2><<<gmass, kThreads, 0, st>>>(static_cast<const float2 *>(state), nseg, seglen, sc.segcdf);
     else
-        seg_scan_kernel<double2><<<gs, kThreads, 0, st>>>(static_cast<const double2 *>(state), nseg, seglen, sc.segcdf,
-                                                         sc.agg_val, sc.agg_flag, sc.inc_val, sc.inc_flag, sc.ticket,
-                                                         status);
+        seg_mass_kernel<double2><<<gmass, kThreads, 0, st>>>(static_cast<const double2 *>(state), nseg, seglen,
+                                                            sc.segcdf);
+    seg_scan_kernel<<<gs, kThreads, 0, st>>>(nseg, sc.segcdf, sc.agg_val, sc.agg_flag, sc.inc_val, sc.inc_flag,
+                                             sc.ticket, status);
     const unsigned gc = unsigned(std::max<uint64_t>(1, std::min<uint64_t>((shots + kThreads - 1) / kThreads, uint64_t(sms) * 8)));
     count_kernel<<<gc, kThreads, 0, st>>>(sc.segcdf, nseg, stream_seed, shots, sc.counts);
     block_sum_kernel<<<unsigned(nblk), kThreads, 0, st>>>(sc.counts, nseg, sc.bsum);
@@ -563,7 +585,7 @@ cudaError_t run_sampler(const void *state, int elem_bytes, int m, uint64_t shots
                                                                sc.heavy_count);
     const unsigned gm = unsigned(std::max<uint64_t>(1, std::min<uint64_t>((shots + kThreads - 1) / kThreads, uint64_t(sms) * 8)));
     map_kernel<<<gm, kThreads, 0, st>>>(sc.real, shots, sc.coltab, b, sc.words);
-    kernels += 8;
+    kernels += 9;
     return cudaGetLastError();
 }
 
@@ -580,14 +602,15 @@ cudaError_t run_sampler_real(const void *state, int elem_bytes, int m, uint64_t 
     const uint64_t nblk = (nseg + kScanBlock - 1) / kScanBlock;
     const uint64_t stream2 = mix_seed_host(stream_seed, 1);
     const unsigned gs = unsigned(std::max<uint64_t>(1, std::min<uint64_t>(nchunks, uint64_t(sms) * 4)));
+    const unsigned gmass = unsigned(std::max<uint64_t>(1, std::min<uint64_t>((nseg * 32 + kThreads - 1) / kThreads,
+                                                                             uint64_t(sms) * 8)));
     if (elem_bytes == 8)
-        seg_scan_kernel<float2><<<gs, kThreads, 0, st>>>(static_cast<const float2 *>(state), nseg, seglen, sc.segcdf,
-                                                        sc.agg_val, sc.agg_flag, sc.inc_val, sc.inc_flag, sc.ticket,
-                                                        status);
+        seg_mass_kernel<float2><<<gmass, kThreads, 0, st>>>(static_cast<const float2 *>(state), nseg, seglen, sc.segcdf);
     else
-        seg_scan_kernel<double2><<<gs, kThreads, 0, st>>>(static_cast<const double2 *>(state), nseg, seglen, sc.segcdf,
-                                                         sc.agg_val, sc.agg_flag, sc.inc_val, sc.inc_flag, sc.ticket,
-                                                         status);
+        seg_mass_kernel<double2><<<gmass, kThreads, 0, st>>>(static_cast<const double2 *>(state), nseg, seglen,
+                                                            sc.segcdf);
+    seg_scan_kernel<<<gs, kThreads, 0, st>>>(nseg, sc.segcdf, sc.agg_val, sc.agg_flag, sc.inc_val, sc.inc_flag,
+                                             sc.ticket, status);
     const unsigned gc = unsigned(std::max<uint64_t>(1, std::min<uint64_t>((shots + kThreads - 1) / kThreads, uint64_t(sms) * 8)));
     count_kernel<<<gc, kThreads, 0, st>>>(sc.segcdf, nseg, stream_seed, shots, sc.counts);
     block_sum_kernel<<<unsigned(nblk), kThreads, 0, st>>>(sc.counts, nseg, sc.bsum);
