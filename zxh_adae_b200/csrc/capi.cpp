@@ -415,10 +415,10 @@ int zxh_measure(zxh_sim *s, size_t shots)
     const uint64_t local = 1ULL << m;
     const uint64_t seglen = std::min<uint64_t>(4096, local);
     const uint64_t nseg = local / seglen;
-    const size_t need = zxh::SamplerScratch::need_bytes(nseg, shots);
+    const size_t need = zxh::SamplerScratch::need_bytes(nseg, shots, true);
     if (int rc = ensure_dev(s, reinterpret_cast<void **>(&s->d_samp), s->samp_cap, need, "cudaMalloc(sampler)"))
         return rc;
-    s->sc.carve(s->d_samp, nseg, shots);
+    s->sc.carve(s->d_samp, nseg, shots, true);
     static thread_local uint64_t tab[8][256];
     column_tables(s->ws.map, tab);
     CK(s, cudaMemsetAsync(s->d_status, 0, sizeof(zxh::DevStatus), s->stream), "reset status");

@@ -68,54 +68,6 @@ __device__ __forceinline__ uint32_t ld_flag(const uint32_t *p)
 
 __device__ __forceinline__ double ld_val(const double *p) { return *reinterpret_cast<const volatile double *>(p); }
 
-// A lane's share of a segment's |amp|^2 mass: 16-byte loads, four independent
-// accumulators (more loads in flight per warp).
-__device__ __forceinline__ double seg_partial(const float2 *seg, uint32_t seglen, int lane)
-{
-    const float4 *v = reinterpret_cast<const float4 *>(seg);
-    const uint32_t nv = seglen / 2;
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-    uint32_t k = uint32_t(lane);
-    auto sq = [](const float4 &x) { return double(x.x) * x.x + double(x.y) * x.y + double(x.z) * x.z + double(x.w) * x.w; };
-    for (; k + 224 < nv; k += 256) {  // 8 loads in flight per lane
-        float4 x[8];
-#pragma unroll
-        for (int i = 0; i < 8; i++) x[i] = __ldcs(v + k + 32 * i);
-        a0 += sq(x[0]) + sq(x[4]);
-        a1 += sq(x[1]) + sq(x[5]);
-        a2 += sq(x[2]) + sq(x[6]);
-        a3 += sq(x[3]) + sq(x[7]);
-    }
-    for (; k + 96 < nv; k += 128) {
-        const float4 x0 = __ldg(v + k), x1 = __ldg(v + k + 32), x2 = __ldg(v + k + 64), x3 = __ldg(v + k + 96);
-        a0 += sq(x0);
-        a1 += sq(x1);
-        a2 += sq(x2);
-        a3 += sq(x3);
-    }
-    for (; k < nv; k += 32) {
-        const float4 x = __ldg(v + k);
-        a0 += double(x.x) * x.x + double(x.y) * x.y + double(x.z) * x.z + double(x.w) * x.w;
-    }
-    if ((seglen & 1) && lane == 0) a1 += prob(seg[seglen - 1]);
-    return (a0 + a1) + (a2 + a3);
-}
-
-__device__ __forceinline__ double seg_partial(const double2 *seg, uint32_t seglen, int lane)
-{
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-    uint32_t k = uint32_t(lane);
-    for (; k + 96 < seglen; k += 128) {
-        const double2 x0 = __ldg(seg + k), x1 = __ldg(seg + k + 32), x2 = __ldg(seg + k + 64), x3 = __ldg(seg + k + 96);
-        a0 += x0.x * x0.x + x0.y * x0.y;
-        a1 += x1.x * x1.x + x1.y * x1.y;
-        a2 += x2.x * x2.x + x2.y * x2.y;
-        a3 += x3.x * x3.x + x3.y * x3.y;
-    }
-    for (; k < seglen; k += 32) a0 += prob(seg[k]);
-    return (a0 + a1) + (a2 + a3);
-}
-
 // |amp|^2 mass of seg[lo, hi), in order; complex64 ranges with even bounds use
 // 16-byte loads.
 __device__ __forceinline__ double range_mass(const float2 *seg, uint32_t lo, uint32_t hi)
@@ -143,17 +95,37 @@ __device__ __forceinline__ double range_mass(const double2 *seg, uint32_t lo, ui
 
 // ---------------------------------------------------------------------------
 
-// Per-segment FP64 mass, one warp per segment: a plain streaming read of the state.
+// Lane l of a warp owns amplitudes [l p, (l + 1) p) of a segment, p = seglen / 32
+// rounded up; its mass and the warp's inclusive prefix over lanes. The segment
+// kernel and the resolve kernel both use this order, so a segment's total and its
+// lane prefixes are the same numbers in both.
+__device__ __forceinline__ double lane_prefix(double part, int lane)
+{
+    double incl = part;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    return incl;
+}
+
+// Per-segment FP64 mass, one warp per segment: one streaming read of the state.
+// With parts, every lane's range mass is kept for the resolve step.
 template <typename E>
 __global__ void __launch_bounds__(kThreads) seg_mass_kernel(const E *__restrict__ state, uint64_t nseg, uint32_t seglen,
-                                                            double *__restrict__ mass)
+                                                            double *__restrict__ mass, double *__restrict__ parts)
 {
     const int lane = threadIdx.x & 31;
     const uint64_t w0 = (uint64_t(blockIdx.x) * kThreads + threadIdx.x) >> 5;
     const uint64_t nw = (uint64_t(gridDim.x) * kThreads) >> 5;
+    const uint32_t per_lane = (seglen + 31) / 32;
+    const uint32_t lo = min(seglen, uint32_t(lane) * per_lane), hi = min(seglen, lo + per_lane);
     for (uint64_t sg = w0; sg < nseg; sg += nw) {
-        const double acc = warp_sum_f64(seg_partial(state + sg * seglen, seglen, lane));
-        if (lane == 0) mass[sg] = acc;
+        const double part = range_mass(state + sg * seglen, lo, hi);
+        if (parts) parts[sg * 32 + uint64_t(lane)] = part;
+        const double total = __shfl_sync(0xffffffffu, lane_prefix(part, lane), 31);
+        if (lane == 0) mass[sg] = total;
     }
 }
 
@@ -325,7 +297,8 @@ __global__ void __launch_bounds__(kThreads) resolve_warp_kernel(const E *__restr
                                                                 uint32_t seglen, const unsigned long long *counts,
                                                                 const unsigned long long *offsets, uint64_t stream2,
                                                                 uint64_t *__restrict__ real_out,
-                                                                uint32_t *heavy_list, uint32_t *heavy_count)
+                                                                uint32_t *heavy_list, uint32_t *heavy_count,
+                                                                const double *__restrict__ parts)
 {
     const int lane = threadIdx.x & 31;
     const uint64_t gwarp = (uint64_t(blockIdx.x) * kThreads + threadIdx.x) >> 5;
@@ -344,16 +317,12 @@ __global__ void __launch_bounds__(kThreads) resolve_warp_kernel(const E *__restr
             const unsigned long long cnt = __shfl_sync(0xffffffffu, cl, src);
             const unsigned long long off = offsets[g];
             const E *seg = state + g * seglen;
-            // lane range [lane*per_lane, (lane+1)*per_lane)
-            const uint32_t lo = uint32_t(lane) * per_lane;
+            // lane range [lane*per_lane, (lane+1)*per_lane): its mass from the
+            // segment kernel when kept, else read again
+            const uint32_t lo = min(seglen, uint32_t(lane) * per_lane);
             const uint32_t hi = min(seglen, lo + per_lane);
-            const double part = range_mass(seg, lo, hi);
-            double incl = part;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const double v = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += v;
-            }
+            const double part = parts ? parts[g * 32 + uint64_t(lane)] : range_mass(seg, lo, hi);
+            const double incl = lane_prefix(part, lane);
             const double total = __shfl_sync(0xffffffffu, incl, 31);
             const double excl = incl - part;
             // this lane's shot
@@ -481,7 +450,7 @@ __global__ void __launch_bounds__(kThreads) map_kernel(const uint64_t *__restric
 
 // One layout routine serves both the size query and the carving, so the two can
 // never disagree.
-static size_t layout(SamplerScratch *sc, uint8_t *base, uint64_t nseg, uint64_t shots)
+static size_t layout(SamplerScratch *sc, uint8_t *base, uint64_t nseg, uint64_t shots, bool with_parts)
 {
     const uint64_t nchunks = (nseg + kSegsPerChunk - 1) / kSegsPerChunk;
     const uint64_t nblk = (nseg + kScanBlock - 1) / kScanBlock;
@@ -506,7 +475,9 @@ static size_t layout(SamplerScratch *sc, uint8_t *base, uint64_t nseg, uint64_t 
     uint8_t *real = take(shots * 8);
     uint8_t *words = take(shots * 8);
     uint8_t *coltab = take(8 * 256 * 8);
+    uint8_t *parts = with_parts ? take(nseg * 32 * 8) : nullptr;
     if (sc) {
+        sc->parts = reinterpret_cast<double *>(parts);
         sc->segcdf = reinterpret_cast<double *>(segcdf);
         sc->flags_begin = fb;
         sc->agg_val = reinterpret_cast<double *>(agg_val);
@@ -527,9 +498,15 @@ static size_t layout(SamplerScratch *sc, uint8_t *base, uint64_t nseg, uint64_t 
     return b;
 }
 
-size_t SamplerScratch::need_bytes(uint64_t nseg, uint64_t shots) { return layout(nullptr, nullptr, nseg, shots); }
+size_t SamplerScratch::need_bytes(uint64_t nseg, uint64_t shots, bool parts)
+{
+    return layout(nullptr, nullptr, nseg, shots, parts);
+}
 
-void SamplerScratch::carve(uint8_t *base, uint64_t nseg, uint64_t shots) { layout(this, base, nseg, shots); }
+void SamplerScratch::carve(uint8_t *base, uint64_t nseg, uint64_t shots, bool parts)
+{
+    layout(this, base, nseg, shots, parts);
+}
 
 cudaError_t run_sampler(const void *state, int elem_bytes, int m, uint64_t shots, uint64_t stream_seed,
                         const uint64_t *host_coltab, uint64_t b, SamplerScratch &sc, DevStatus *status, int sms,
@@ -552,10 +529,11 @@ cudaError_t run_sampler(const void *state, int elem_bytes, int m, uint64_t shots
     const unsigned gmass = unsigned(std::max<uint64_t>(1, std::min<uint64_t>((nseg * 32 + kThreads - 1) / kThreads,
                                                                              uint64_t(sms) * 8)));
     if (elem_bytes == 8)
-        seg_mass_kernel<float2><<<gmass, kThreads, 0, st>>>(static_cast<const float2 *>(state), nseg, seglen, sc.segcdf);
+        seg_mass_kernel<float2><<<gmass, kThreads, 0, st>>>(static_cast<const float2 *>(state), nseg, seglen, sc.segcdf,
+                                                            sc.parts);
     else
         seg_mass_kernel<double2><<<gmass, kThreads, 0, st>>>(static_cast<const double2 *>(state), nseg, seglen,
-                                                            sc.segcdf);
+                                                            sc.segcdf, sc.parts);
     seg_scan_kernel<<<gs, kThreads, 0, st>>>(nseg, sc.segcdf, sc.agg_val, sc.agg_flag, sc.inc_val, sc.inc_flag,
                                              sc.ticket, status);
     const unsigned gc = unsigned(std::max<uint64_t>(1, std::min<uint64_t>((shots + kThreads - 1) / kThreads, uint64_t(sms) * 8)));
@@ -568,11 +546,12 @@ cudaError_t run_sampler(const void *state, int elem_bytes, int m, uint64_t shots
                                                                           uint64_t(sms) * 8)));
     if (elem_bytes == 8)
         resolve_warp_kernel<float2><<<gw, kThreads, 0, st>>>(static_cast<const float2 *>(state), nseg, seglen, sc.counts,
-                                                            sc.offsets, stream2, sc.real, sc.heavy_list, sc.heavy_count);
+                                                            sc.offsets, stream2, sc.real, sc.heavy_list, sc.heavy_count,
+                                                            sc.parts);
     else
         resolve_warp_kernel<double2><<<gw, kThreads, 0, st>>>(static_cast<const double2 *>(state), nseg, seglen,
                                                              sc.counts, sc.offsets, stream2, sc.real, sc.heavy_list,
-                                                             sc.heavy_count);
+                                                             sc.heavy_count, sc.parts);
     const size_t smem = size_t(seglen) * 8;
     const unsigned gh = unsigned(sms) * 2;
     if (elem_bytes == 8)
@@ -605,10 +584,11 @@ cudaError_t run_sampler_real(const void *state, int elem_bytes, int m, uint64_t 
     const unsigned gmass = unsigned(std::max<uint64_t>(1, std::min<uint64_t>((nseg * 32 + kThreads - 1) / kThreads,
                                                                              uint64_t(sms) * 8)));
     if (elem_bytes == 8)
-        seg_mass_kernel<float2><<<gmass, kThreads, 0, st>>>(static_cast<const float2 *>(state), nseg, seglen, sc.segcdf);
+        seg_mass_kernel<float2><<<gmass, kThreads, 0, st>>>(static_cast<const float2 *>(state), nseg, seglen, sc.segcdf,
+                                                            sc.parts);
     else
         seg_mass_kernel<double2><<<gmass, kThreads, 0, st>>>(static_cast<const double2 *>(state), nseg, seglen,
-                                                            sc.segcdf);
+                                                            sc.segcdf, sc.parts);
     seg_scan_kernel<<<gs, kThreads, 0, st>>>(nseg, sc.segcdf, sc.agg_val, sc.agg_flag, sc.inc_val, sc.inc_flag,
                                              sc.ticket, status);
     const unsigned gc = unsigned(std::max<uint64_t>(1, std::min<uint64_t>((shots + kThreads - 1) / kThreads, uint64_t(sms) * 8)));
@@ -621,11 +601,12 @@ cudaError_t run_sampler_real(const void *state, int elem_bytes, int m, uint64_t 
                                                                           uint64_t(sms) * 8)));
     if (elem_bytes == 8)
         resolve_warp_kernel<float2><<<gw, kThreads, 0, st>>>(static_cast<const float2 *>(state), nseg, seglen, sc.counts,
-                                                            sc.offsets, stream2, real_out, sc.heavy_list, sc.heavy_count);
+                                                            sc.offsets, stream2, real_out, sc.heavy_list, sc.heavy_count,
+                                                            sc.parts);
     else
         resolve_warp_kernel<double2><<<gw, kThreads, 0, st>>>(static_cast<const double2 *>(state), nseg, seglen,
                                                              sc.counts, sc.offsets, stream2, real_out, sc.heavy_list,
-                                                             sc.heavy_count);
+                                                             sc.heavy_count, sc.parts);
     const size_t smem = size_t(seglen) * 8;
     const unsigned gh = unsigned(sms) * 2;
     if (elem_bytes == 8)

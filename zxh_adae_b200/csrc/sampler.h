@@ -17,9 +17,10 @@ struct SamplerScratch {
     uint32_t *heavy_list = nullptr;
     uint64_t *real = nullptr, *words = nullptr;
     uint64_t *coltab = nullptr;
+    double *parts = nullptr;  // optional: the 32 lane-range masses of every segment
 
-    static size_t need_bytes(uint64_t nseg, uint64_t shots);
-    void carve(uint8_t *base, uint64_t nseg, uint64_t shots);
+    static size_t need_bytes(uint64_t nseg, uint64_t shots, bool parts = false);
+    void carve(uint8_t *base, uint64_t nseg, uint64_t shots, bool parts = false);
 };
 
 uint64_t mix_seed_host(uint64_t base, uint64_t salt);
