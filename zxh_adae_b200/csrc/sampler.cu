@@ -7,9 +7,10 @@
 // and returns shots grouped by segment in the reference's output order. The
 // machinery is new:
 //   seg_mass_kernel      one streaming read of the state: per-segment FP64 |amp|^2
-//                        mass, one warp per segment.
-//   seg_scan_kernel      single-pass decoupled-lookback inclusive scan of the masses
-//                        (the reference runs segment_mass_kernel + a CUB scan).
+//                        mass, one warp per segment (and the 32 lane-range masses of
+//                        each segment, kept for the resolve step).
+//   mass scan (3 kernels) inclusive FP64 scan of the masses: the segment CDF (the
+//                        reference runs segment_mass_kernel + a CUB scan).
 //   count_kernel         shot -> segment by binary search, warp-aggregated atomics.
 //   offsets (3 kernels)  exclusive scan of the per-segment counts.
 //   resolve_warp_kernel  segments hit by <= 32 shots: one warp streams the segment
@@ -19,7 +20,7 @@
 //   resolve_cta_kernel   heavier segments, one per CTA (round robin): the CTA builds
 //                        the segment CDF in shared memory and binary-searches it.
 //   map_kernel           real index -> packed virtual bits (measure_cuda.cu:315-338).
-// Every spin on a predecessor flag is bounded and reports ZXH_ERR_TIMEOUT.
+// No kernel waits on another CTA.
 #include "core.h"
 #include "dev.cuh"
 #include "sampler.h"
@@ -33,7 +34,6 @@ namespace {
 
 constexpr uint64_t kSeedShot = 0x510e527fade682d1ULL;    // measure_cuda.cu:427
 constexpr uint64_t kSeedOffset = 0x9b05688c2b3e6c1fULL;  // measure_cuda.cu:499
-constexpr int kSegsPerChunk = 32;
 constexpr int kWarpMax = 32;
 constexpr uint32_t kCtaShots = 16384;
 constexpr int kScanBlock = 4096;
@@ -61,12 +61,6 @@ __device__ __forceinline__ double prob(const E &a)
     return re * re + im * im;
 }
 
-__device__ __forceinline__ uint32_t ld_flag(const uint32_t *p)
-{
-    return *reinterpret_cast<const volatile uint32_t *>(p);
-}
-
-__device__ __forceinline__ double ld_val(const double *p) { return *reinterpret_cast<const volatile double *>(p); }
 
 // |amp|^2 mass of seg[lo, hi), in order; complex64 ranges with even bounds use
 // 16-byte loads.
@@ -129,76 +123,6 @@ __global__ void __launch_bounds__(kThreads) seg_mass_kernel(const E *__restrict_
     }
 }
 
-// Inclusive scan of the segment masses (read from segcdf, which seg_mass_kernel
-// filled, and overwritten in place chunk by chunk) with decoupled lookback.
-__global__ void __launch_bounds__(kThreads) seg_scan_kernel(uint64_t nseg, double *segcdf, double *agg_val,
-                                                            uint32_t *agg_flag, double *inc_val, uint32_t *inc_flag,
-                                                            uint32_t *ticket, DevStatus *status)
-{
-    __shared__ uint32_t s_chunk;
-    __shared__ double s_mass[kSegsPerChunk];
-    __shared__ double s_prefix;
-    __shared__ int s_abort;
-    const int tid = threadIdx.x;
-    const uint64_t nchunks = (nseg + kSegsPerChunk - 1) / kSegsPerChunk;
-    if (tid == 0) s_abort = 0;
-    for (;;) {
-        __syncthreads();
-        if (tid == 0) s_chunk = atomicAdd(ticket, 1u);
-        __syncthreads();
-        const uint64_t chunk = s_chunk;
-        if (chunk >= nchunks || s_abort) break;
-        const uint64_t base = chunk * kSegsPerChunk;
-        const int nloc = int((nseg - base < uint64_t(kSegsPerChunk) ? nseg - base : uint64_t(kSegsPerChunk)));
-        if (tid < nloc) s_mass[tid] = segcdf[base + uint64_t(tid)];
-        __syncthreads();
-        if (tid == 0) {
-            double run = 0.0;
-            for (int i = 0; i < nloc; i++) {
-                run += s_mass[i];
-                s_mass[i] = run;
-            }
-            const double agg = run;
-            double excl = 0.0;
-            if (chunk == 0) {
-                inc_val[0] = agg;
-                __threadfence();
-                atomicExch(&inc_flag[0], 1u);
-            } else {
-                agg_val[chunk] = agg;
-                __threadfence();
-                atomicExch(&agg_flag[chunk], 1u);
-                int64_t p = int64_t(chunk) - 1;
-                const long long t0 = clock64();
-                while (p >= 0) {
-                    if (ld_flag(&inc_flag[p])) {
-                        __threadfence();
-                        excl += ld_val(&inc_val[p]);
-                        break;
-                    }
-                    if (ld_flag(&agg_flag[p])) {
-                        __threadfence();
-                        excl += ld_val(&agg_val[p]);
-                        p--;
-                        continue;
-                    }
-                    if (clock64() - t0 > (1LL << 31)) {
-                        report(status, kErrTimeout, 2, chunk);
-                        s_abort = 1;
-                        break;
-                    }
-                }
-                inc_val[chunk] = excl + agg;
-                __threadfence();
-                atomicExch(&inc_flag[chunk], 1u);
-            }
-            s_prefix = excl;
-        }
-        __syncthreads();
-        if (tid < nloc) segcdf[base + uint64_t(tid)] = s_prefix + s_mass[tid];
-    }
-}
-
 __device__ __forceinline__ uint64_t upper_index(const double *cdf, uint64_t n, double tau)
 {
     uint64_t lo = 0, hi = n;
@@ -231,63 +155,70 @@ __global__ void __launch_bounds__(kThreads) count_kernel(const double *__restric
 }
 
 // exclusive scan of counts: block sums, scan of block sums, block scans
-__global__ void __launch_bounds__(kThreads) block_sum_kernel(const unsigned long long *__restrict__ counts, uint64_t n,
-                                                             unsigned long long *__restrict__ bsum)
+// Scan of n values in blocks of kScanBlock: per-block sums, one small scan over
+// them, then each block's scan plus its offset. T = unsigned long long for the
+// shot counts (exclusive offsets), double for the segment masses (inclusive CDF,
+// written over the masses).
+template <typename T>
+__global__ void __launch_bounds__(kThreads) block_sum_kernel(const T *__restrict__ v, uint64_t n, T *__restrict__ bsum)
 {
-    __shared__ unsigned long long sh[kThreads / 32];
+    __shared__ T sh[kThreads / 32];
     const uint64_t b0 = uint64_t(blockIdx.x) * kScanBlock;
-    unsigned long long acc = 0;
-    for (uint64_t i = b0 + threadIdx.x; i < (n < b0 + kScanBlock ? n : b0 + kScanBlock); i += kThreads) acc += counts[i];
+    T acc = 0;
+    for (uint64_t i = b0 + threadIdx.x; i < (n < b0 + kScanBlock ? n : b0 + kScanBlock); i += kThreads) acc += v[i];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
     __syncthreads();
     if (threadIdx.x == 0) {
-        unsigned long long t = 0;
+        T t = 0;
         for (int w = 0; w < kThreads / 32; w++) t += sh[w];
         bsum[blockIdx.x] = t;
     }
 }
 
-__global__ void scan_small_kernel(unsigned long long *v, uint64_t n)
+template <typename T>
+__global__ void scan_small_kernel(T *v, uint64_t n)
 {
-    // single thread; n is at most a few thousand block sums
+    // single thread, exclusive; n is at most a few thousand block sums
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    unsigned long long run = 0;
+    T run = 0;
     for (uint64_t i = 0; i < n; i++) {
-        const unsigned long long x = v[i];
+        const T x = v[i];
         v[i] = run;
         run += x;
     }
 }
 
-__global__ void __launch_bounds__(kThreads) block_scan_kernel(const unsigned long long *__restrict__ counts, uint64_t n,
-                                                              const unsigned long long *__restrict__ boff,
-                                                              unsigned long long *__restrict__ offsets)
+// in and out may be the same array (every thread reads its own values first)
+template <typename T, bool INCL>
+__global__ void __launch_bounds__(kThreads) block_scan_kernel(const T *in, uint64_t n, const T *__restrict__ boff,
+                                                              T *out)
 {
-    constexpr int PER = kScanBlock / kThreads;  // 16 consecutive counts per thread
-    __shared__ unsigned long long sh[kThreads];
+    constexpr int PER = kScanBlock / kThreads;  // 16 consecutive values per thread
+    __shared__ T sh[kThreads];
     const uint64_t b0 = uint64_t(blockIdx.x) * kScanBlock + uint64_t(threadIdx.x) * PER;
-    unsigned long long loc[PER];
-    unsigned long long acc = 0;
+    T loc[PER];
+    T acc = 0;
 #pragma unroll
     for (int k = 0; k < PER; k++) {
-        loc[k] = (b0 + k < n) ? counts[b0 + k] : 0ULL;
+        loc[k] = (b0 + k < n) ? in[b0 + k] : T(0);
         acc += loc[k];
     }
     sh[threadIdx.x] = acc;
     __syncthreads();
     for (int o = 1; o < kThreads; o <<= 1) {
-        const unsigned long long v = threadIdx.x >= unsigned(o) ? sh[threadIdx.x - o] : 0ULL;
+        const T x = threadIdx.x >= unsigned(o) ? sh[threadIdx.x - o] : T(0);
         __syncthreads();
-        sh[threadIdx.x] += v;
+        sh[threadIdx.x] += x;
         __syncthreads();
     }
-    unsigned long long run = boff[blockIdx.x] + sh[threadIdx.x] - acc;
+    T run = boff[blockIdx.x] + (sh[threadIdx.x] - acc);
 #pragma unroll
     for (int k = 0; k < PER; k++) {
-        if (b0 + k < n) offsets[b0 + k] = run;
-        run += loc[k];
+        if (INCL) run += loc[k];
+        if (b0 + k < n) out[b0 + k] = run;
+        if (!INCL) run += loc[k];
     }
 }
 
@@ -452,7 +383,6 @@ __global__ void __launch_bounds__(kThreads) map_kernel(const uint64_t *__restric
 // never disagree.
 static size_t layout(SamplerScratch *sc, uint8_t *base, uint64_t nseg, uint64_t shots, bool with_parts)
 {
-    const uint64_t nchunks = (nseg + kSegsPerChunk - 1) / kSegsPerChunk;
     const uint64_t nblk = (nseg + kScanBlock - 1) / kScanBlock;
     size_t b = 0;
     auto take = [&](size_t x) {
@@ -462,11 +392,7 @@ static size_t layout(SamplerScratch *sc, uint8_t *base, uint64_t nseg, uint64_t 
     };
     uint8_t *segcdf = take(nseg * 8);
     uint8_t *fb = base ? base + b : nullptr;
-    uint8_t *agg_val = take(nchunks * 8);
-    uint8_t *inc_val = take(nchunks * 8);
-    uint8_t *agg_flag = take(nchunks * 4);
-    uint8_t *inc_flag = take(nchunks * 4);
-    uint8_t *ticket = take(16);
+    uint8_t *heavy_count = take(16);
     uint8_t *fe = base ? base + b : nullptr;
     uint8_t *counts = take(nseg * 8);
     uint8_t *offsets = take(nseg * 8);
@@ -480,12 +406,7 @@ static size_t layout(SamplerScratch *sc, uint8_t *base, uint64_t nseg, uint64_t 
         sc->parts = reinterpret_cast<double *>(parts);
         sc->segcdf = reinterpret_cast<double *>(segcdf);
         sc->flags_begin = fb;
-        sc->agg_val = reinterpret_cast<double *>(agg_val);
-        sc->inc_val = reinterpret_cast<double *>(inc_val);
-        sc->agg_flag = reinterpret_cast<uint32_t *>(agg_flag);
-        sc->inc_flag = reinterpret_cast<uint32_t *>(inc_flag);
-        sc->ticket = reinterpret_cast<uint32_t *>(ticket);
-        sc->heavy_count = sc->ticket + 1;
+        sc->heavy_count = reinterpret_cast<uint32_t *>(heavy_count);
         sc->flags_end = fe;
         sc->counts = reinterpret_cast<unsigned long long *>(counts);
         sc->offsets = reinterpret_cast<unsigned long long *>(offsets);
@@ -515,7 +436,6 @@ cudaError_t run_sampler(const void *state, int elem_bytes, int m, uint64_t shots
     const uint64_t local = 1ULL << m;
     const uint32_t seglen = uint32_t(std::min<uint64_t>(4096, local));
     const uint64_t nseg = local / seglen;
-    const uint64_t nchunks = (nseg + kSegsPerChunk - 1) / kSegsPerChunk;
     const uint64_t nblk = (nseg + kScanBlock - 1) / kScanBlock;
     const uint64_t stream2 = mix_seed_host(stream_seed, 1);
     cudaError_t e;
@@ -525,7 +445,6 @@ cudaError_t run_sampler(const void *state, int elem_bytes, int m, uint64_t shots
     if (e != cudaSuccess) return e;
     e = cudaMemcpyAsync(sc.coltab, host_coltab, 8 * 256 * 8, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return e;
-    const unsigned gs = unsigned(std::max<uint64_t>(1, std::min<uint64_t>(nchunks, uint64_t(sms) * 4)));
     const unsigned gmass = unsigned(std::max<uint64_t>(1, std::min<uint64_t>((nseg * 32 + kThreads - 1) / kThreads,
                                                                              uint64_t(sms) * 8)));
     if (elem_bytes == 8)
@@ -534,13 +453,16 @@ cudaError_t run_sampler(const void *state, int elem_bytes, int m, uint64_t shots
     else
         seg_mass_kernel<double2><<<gmass, kThreads, 0, st>>>(static_cast<const double2 *>(state), nseg, seglen,
                                                             sc.segcdf, sc.parts);
-    seg_scan_kernel<<<gs, kThreads, 0, st>>>(nseg, sc.segcdf, sc.agg_val, sc.agg_flag, sc.inc_val, sc.inc_flag,
-                                             sc.ticket, status);
+    double *bsum_d = reinterpret_cast<double *>(sc.bsum);  // the counts' scan reuses it afterwards
+    block_sum_kernel<double><<<unsigned(nblk), kThreads, 0, st>>>(sc.segcdf, nseg, bsum_d);
+    scan_small_kernel<double><<<1, 32, 0, st>>>(bsum_d, nblk);
+    block_scan_kernel<double, true><<<unsigned(nblk), kThreads, 0, st>>>(sc.segcdf, nseg, bsum_d, sc.segcdf);
     const unsigned gc = unsigned(std::max<uint64_t>(1, std::min<uint64_t>((shots + kThreads - 1) / kThreads, uint64_t(sms) * 8)));
     count_kernel<<<gc, kThreads, 0, st>>>(sc.segcdf, nseg, stream_seed, shots, sc.counts);
-    block_sum_kernel<<<unsigned(nblk), kThreads, 0, st>>>(sc.counts, nseg, sc.bsum);
-    scan_small_kernel<<<1, 32, 0, st>>>(sc.bsum, nblk);
-    block_scan_kernel<<<unsigned(nblk), kThreads, 0, st>>>(sc.counts, nseg, sc.bsum, sc.offsets);
+    block_sum_kernel<unsigned long long><<<unsigned(nblk), kThreads, 0, st>>>(sc.counts, nseg, sc.bsum);
+    scan_small_kernel<unsigned long long><<<1, 32, 0, st>>>(sc.bsum, nblk);
+    block_scan_kernel<unsigned long long, false><<<unsigned(nblk), kThreads, 0, st>>>(sc.counts, nseg, sc.bsum,
+                                                                                     sc.offsets);
     const uint64_t warps_needed = (nseg + 31) / 32;
     const unsigned gw = unsigned(std::max<uint64_t>(1, std::min<uint64_t>((warps_needed * 32 + kThreads - 1) / kThreads,
                                                                           uint64_t(sms) * 8)));
@@ -564,7 +486,8 @@ cudaError_t run_sampler(const void *state, int elem_bytes, int m, uint64_t shots
                                                                sc.heavy_count);
     const unsigned gm = unsigned(std::max<uint64_t>(1, std::min<uint64_t>((shots + kThreads - 1) / kThreads, uint64_t(sms) * 8)));
     map_kernel<<<gm, kThreads, 0, st>>>(sc.real, shots, sc.coltab, b, sc.words);
-    kernels += 9;
+    kernels += 11;
+    (void)status;  // no step of the draw waits on another CTA
     return cudaGetLastError();
 }
 
@@ -577,10 +500,8 @@ cudaError_t run_sampler_real(const void *state, int elem_bytes, int m, uint64_t 
     const uint64_t local = 1ULL << m;
     const uint32_t seglen = uint32_t(std::min<uint64_t>(4096, local));
     const uint64_t nseg = local / seglen;
-    const uint64_t nchunks = (nseg + kSegsPerChunk - 1) / kSegsPerChunk;
     const uint64_t nblk = (nseg + kScanBlock - 1) / kScanBlock;
     const uint64_t stream2 = mix_seed_host(stream_seed, 1);
-    const unsigned gs = unsigned(std::max<uint64_t>(1, std::min<uint64_t>(nchunks, uint64_t(sms) * 4)));
     const unsigned gmass = unsigned(std::max<uint64_t>(1, std::min<uint64_t>((nseg * 32 + kThreads - 1) / kThreads,
                                                                              uint64_t(sms) * 8)));
     if (elem_bytes == 8)
@@ -589,13 +510,16 @@ cudaError_t run_sampler_real(const void *state, int elem_bytes, int m, uint64_t 
     else
         seg_mass_kernel<double2><<<gmass, kThreads, 0, st>>>(static_cast<const double2 *>(state), nseg, seglen,
                                                             sc.segcdf, sc.parts);
-    seg_scan_kernel<<<gs, kThreads, 0, st>>>(nseg, sc.segcdf, sc.agg_val, sc.agg_flag, sc.inc_val, sc.inc_flag,
-                                             sc.ticket, status);
+    double *bsum_d = reinterpret_cast<double *>(sc.bsum);  // the counts' scan reuses it afterwards
+    block_sum_kernel<double><<<unsigned(nblk), kThreads, 0, st>>>(sc.segcdf, nseg, bsum_d);
+    scan_small_kernel<double><<<1, 32, 0, st>>>(bsum_d, nblk);
+    block_scan_kernel<double, true><<<unsigned(nblk), kThreads, 0, st>>>(sc.segcdf, nseg, bsum_d, sc.segcdf);
     const unsigned gc = unsigned(std::max<uint64_t>(1, std::min<uint64_t>((shots + kThreads - 1) / kThreads, uint64_t(sms) * 8)));
     count_kernel<<<gc, kThreads, 0, st>>>(sc.segcdf, nseg, stream_seed, shots, sc.counts);
-    block_sum_kernel<<<unsigned(nblk), kThreads, 0, st>>>(sc.counts, nseg, sc.bsum);
-    scan_small_kernel<<<1, 32, 0, st>>>(sc.bsum, nblk);
-    block_scan_kernel<<<unsigned(nblk), kThreads, 0, st>>>(sc.counts, nseg, sc.bsum, sc.offsets);
+    block_sum_kernel<unsigned long long><<<unsigned(nblk), kThreads, 0, st>>>(sc.counts, nseg, sc.bsum);
+    scan_small_kernel<unsigned long long><<<1, 32, 0, st>>>(sc.bsum, nblk);
+    block_scan_kernel<unsigned long long, false><<<unsigned(nblk), kThreads, 0, st>>>(sc.counts, nseg, sc.bsum,
+                                                                                     sc.offsets);
     const uint64_t warps_needed = (nseg + 31) / 32;
     const unsigned gw = unsigned(std::max<uint64_t>(1, std::min<uint64_t>((warps_needed * 32 + kThreads - 1) / kThreads,
                                                                           uint64_t(sms) * 8)));
@@ -617,6 +541,7 @@ cudaError_t run_sampler_real(const void *state, int elem_bytes, int m, uint64_t 
         resolve_cta_kernel<double2><<<gh, kThreads, smem, st>>>(static_cast<const double2 *>(state), seglen, sc.counts,
                                                                sc.offsets, stream2, real_out, sc.heavy_list,
                                                                sc.heavy_count);
+    (void)status;  // no step of the draw waits on another CTA
     return cudaGetLastError();
 }
 

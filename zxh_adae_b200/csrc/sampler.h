@@ -9,9 +9,7 @@ namespace zxh {
 
 struct SamplerScratch {
     double *segcdf = nullptr;
-    double *agg_val = nullptr, *inc_val = nullptr;
-    uint32_t *agg_flag = nullptr, *inc_flag = nullptr;
-    uint32_t *ticket = nullptr, *heavy_count = nullptr;
+    uint32_t *heavy_count = nullptr;
     void *flags_begin = nullptr, *flags_end = nullptr;  // region zeroed before every draw
     unsigned long long *counts = nullptr, *offsets = nullptr, *bsum = nullptr;
     uint32_t *heavy_list = nullptr;
