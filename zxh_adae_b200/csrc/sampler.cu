@@ -89,6 +89,38 @@ __device__ __forceinline__ double range_mass(const double2 *seg, uint32_t lo, ui
 
 // ---------------------------------------------------------------------------
 
+// Mass of lane l's range [l p, (l + 1) p) of a full 4096-amplitude segment, p =
+// 128, read coalesced: in step g the warp reads 32 consecutive 16-byte vectors,
+// which all belong to range g / G (G steps per range), and the range's mass is
+// the warp's sum of them; lane l keeps range l. The same code runs in the segment
+// pass and in the resolve step's fallback, so both see the same numbers.
+__device__ __forceinline__ double vec_mass(const float4 &x)
+{
+    return (double(x.x) * x.x + double(x.y) * x.y) + (double(x.z) * x.z + double(x.w) * x.w);
+}
+__device__ __forceinline__ double vec_mass(const double2 &x) { return x.x * x.x + x.y * x.y; }
+
+template <typename E>
+__device__ __forceinline__ double lane_range_mass(const E *seg, int lane)
+{
+    using VT = typename ET<E>::VT;
+    constexpr int G = 4096 / ET<E>::V / 32 / 32;  // steps per range: 2 (complex64), 4 (complex128)
+    const VT *v = reinterpret_cast<const VT *>(seg);
+    double mine = 0.0;
+#pragma unroll 4
+    for (int r = 0; r < 32; r++) {
+        VT x[G];
+#pragma unroll
+        for (int i = 0; i < G; i++) x[i] = __ldcs(v + (r * G + i) * 32 + lane);
+        double t = 0.0;
+#pragma unroll
+        for (int i = 0; i < G; i++) t += vec_mass(x[i]);
+        t = warp_sum_f64(t);
+        if (lane == r) mine = t;
+    }
+    return mine;
+}
+
 // Lane l of a warp owns amplitudes [l p, (l + 1) p) of a segment, p = seglen / 32
 // rounded up; its mass and the warp's inclusive prefix over lanes. The segment
 // kernel and the resolve kernel both use this order, so a segment's total and its
@@ -116,7 +148,8 @@ __global__ void __launch_bounds__(kThreads) seg_mass_kernel(const E *__restrict_
     const uint32_t per_lane = (seglen + 31) / 32;
     const uint32_t lo = min(seglen, uint32_t(lane) * per_lane), hi = min(seglen, lo + per_lane);
     for (uint64_t sg = w0; sg < nseg; sg += nw) {
-        const double part = range_mass(state + sg * seglen, lo, hi);
+        const double part = seglen == 4096 ? lane_range_mass(state + sg * seglen, lane)
+                                           : range_mass(state + sg * seglen, lo, hi);
         if (parts) parts[sg * 32 + uint64_t(lane)] = part;
         const double total = __shfl_sync(0xffffffffu, lane_prefix(part, lane), 31);
         if (lane == 0) mass[sg] = total;
@@ -252,7 +285,8 @@ __global__ void __launch_bounds__(kThreads) resolve_warp_kernel(const E *__restr
             // segment kernel when kept, else read again
             const uint32_t lo = min(seglen, uint32_t(lane) * per_lane);
             const uint32_t hi = min(seglen, lo + per_lane);
-            const double part = parts ? parts[g * 32 + uint64_t(lane)] : range_mass(seg, lo, hi);
+            const double part = parts ? parts[g * 32 + uint64_t(lane)]
+                                      : seglen == 4096 ? lane_range_mass(seg, lane) : range_mass(seg, lo, hi);
             const double incl = lane_prefix(part, lane);
             const double total = __shfl_sync(0xffffffffu, incl, 31);
             const double excl = incl - part;
