@@ -270,7 +270,9 @@ def _run_knobs(n, gates, dtype, knobs):
 
 @pytest.mark.parametrize("dtype", DTYPES)
 @pytest.mark.parametrize("knobs", [{"low_pass": 0}, {"low_regs_c64": 0, "low_regs_c128": 0},
-                                   {"low_regs_c64": 2, "low_regs_c128": 3}, {"real_split": 0}, {}])
+                                   {"low_regs_c64": 2, "low_regs_c128": 3}, {"real_split": 0}, {},
+                                   {"row_wide_c64": 0}, {"row_wide_c64": 0, "real_split": 0},
+                                   {"row_wide_c64": 0, "low_regs_c64": 3}, {"low_regs_c64": 5, "low_regs_c128": 4}])
 @pytest.mark.parametrize("n", [10, 12, 13, 18])
 def test_low_pass_forms(dtype, knobs, n):
     # TMA fast pass + strided passes, and the strided low pass (lane bits swapped

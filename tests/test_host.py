@@ -28,17 +28,17 @@ def test_diag_batch_is_one_pass():
 def test_u3_layer_splits_into_low_and_strided_passes():
     rng = np.random.default_rng(0)
     lay = zx.as_records([(zx._core.U3, 0, q, *rng.uniform(0, 6.28, 3)) for q in range(30)])
-    # one low pass (complex64: the 6 lane / vector bits + 4 register bits;
-    # complex128: 5 lane bits + 4) and strided passes of 4 gates
+    # one low pass (complex64: the 5 lane bits + 5 register bits, then strided
+    # passes of 5 gates; complex128: 5 lane bits + 4, then passes of 4 gates)
     st = plan_stats(30, np.concatenate([wl.h_all(30), lay]), dtype="complex64")
-    assert st["fast"] == 0 and st["row"] == 6 and st["passes"] == 6
+    assert st["fast"] == 0 and st["row"] == 5 and st["passes"] == 5
     st = plan_stats(30, np.concatenate([wl.h_all(30), lay]), dtype="complex128")
     assert st["fast"] == 0 and st["row"] == 7 and st["passes"] == 7
 
 
 def test_small_windows_fuse_into_u3_passes():
     st = plan_stats(20, wl.plain_layers(20, 10, 1))
-    assert st["diagonal"] == 0 and st["passes"] == 40  # 10 layers x (1 low + 3 strided), cp chains fused
+    assert st["diagonal"] == 0 and st["passes"] == 30  # 10 layers x (1 low + 2 strided), cp chains fused
     st = plan_stats(20, wl.plain_layers(20, 10, 1), dtype="complex128")
     assert st["diagonal"] == 0 and st["passes"] == 40  # 10 layers x (1 low + 3 strided)
 

@@ -592,7 +592,7 @@ int zxh_set_param(zxh_sim *s, const char *name, int value)
         {"row_wide_c64", &s->pp.row_wide_c64, 0, 1},
         {"row_wide_c128", &s->pp.row_wide_c128, 0, 1},
         {"low_pass", &s->pp.low_pass, 0, 1},
-        {"low_regs_c64", &s->pp.low_regs_c64, 0, 4},
+        {"low_regs_c64", &s->pp.low_regs_c64, 0, 5},
         {"low_regs_c128", &s->pp.low_regs_c128, 0, 4},
         {"real_split", &s->pp.real_split, 0, 1},
         {"diag_prefetch_c64", &s->pp.diag_prefetch_c64, 0, 1},

@@ -40,11 +40,13 @@ struct PlanParams {
     int fast_fuse_quad = 32;    // largest in-tile quadratic term count of a window fused into a fast pass
     int fast_contig_c64 = 4;    // contiguous low bits of a fast tile that also spans high bits (complex64)
     int fast_contig_c128 = 3;   // same for complex128
-    int row_wide_c64 = 0;       // strided high-qubit pass shape, complex64: 0 = 16-byte lanes x 16 rows, 1 = 8-byte x 32
+    int row_wide_c64 = 1;       // strided pass shape, complex64: 0 = 16-byte lanes x 16 rows (4 register bits),
+                                // 1 = 8-byte lanes x 32 rows (5 register bits: a 30-qubit U3 layer in 5 passes)
     int row_wide_c128 = 1;      // complex128: 0 = 8 rows, 1 = 16 rows
     int low_pass = 1;           // 1: gates on the lane / vector bits ride in a strided low pass (lane bits
                                 // swapped into registers) instead of the TMA fast pass
-    int low_regs_c64 = 4;       // gates on register bits that join the low pass, complex64 (0..4)
+    int low_regs_c64 = 5;       // gates on register bits that join the low pass, complex64 (0..5; at most
+                                // the shape's register bits)
     int low_regs_c128 = 4;      // same for complex128
     int real_split = 1;         // 1: in all-strided U3 batches each gate runs as a real rotation; its phases
                                 // ride in the windows before / after the batch (half the multiply-adds)
@@ -119,7 +121,7 @@ int fast_tile_bits(int elem_bytes);
 int fast_reg_bits(int elem_bytes);
 int row_reg_bits(int elem_bytes, int wide);
 int row_fixed_bits(int elem_bytes, int wide);
-bool row_low_ok(int elem_bytes, int wide);  // the shape has the 16 rows of 16 bytes the low pass swaps
+bool row_low_ok(int elem_bytes, int wide);  // the shape's lane bits can swap with its rows (the low pass)
 
 int plan(const std::vector<Op> &ops, int elem_bytes, const PlanParams &pp, const WalkState &start, Plan &out,
          std::string &err);

@@ -615,28 +615,42 @@ __device__ __forceinline__ void from_f4(double2 &v, const float4 &t)
 // rows, 16 of them) through the warp's 16 x 32 shared-memory slots: slot of (lane
 // l, row j) = j * 32 + (l ^ (j & 7)), conflict-free both ways. Afterwards thread
 // L's row j holds what lane (L & 16) | j had in row L & 15. back = true undoes it.
-template <typename VT>
-__device__ __forceinline__ void lane_row_transpose(VT (&x)[16], float4 *tb, int lane, bool back)
+// With 32 rows of 8 bytes all 5 lane bits swap with the 5 register bits: slot of
+// (lane l, row j) = j * 32 + (l ^ j); thread L's row j then holds lane j's row L.
+template <typename VT, int NR>
+__device__ __forceinline__ void lane_row_transpose(VT (&x)[NR], void *tbv, int lane, bool back)
 {
-    const int jr = lane & 15, hi = lane & 16;
+    if constexpr (NR == 32) {
+        static_assert(sizeof(VT) == 8, "32 rows of 8 bytes");
+        VT *tb = static_cast<VT *>(tbv);
 #pragma unroll
-    for (int j = 0; j < 16; j++) {
-        const int slot = back ? jr * 32 + (hi | (j ^ (jr & 7))) : j * 32 + (lane ^ (j & 7));
-        tb[slot] = as_f4(x[j]);
-    }
-    __syncwarp();
+        for (int j = 0; j < 32; j++) tb[back ? lane * 32 + (j ^ lane) : j * 32 + (lane ^ j)] = x[j];
+        __syncwarp();
 #pragma unroll
-    for (int j = 0; j < 16; j++) {
-        const int slot = back ? j * 32 + (lane ^ (j & 7)) : jr * 32 + (hi | (j ^ (jr & 7)));
-        from_f4(x[j], tb[slot]);
+        for (int j = 0; j < 32; j++) x[j] = tb[back ? j * 32 + (lane ^ j) : lane * 32 + (j ^ lane)];
+    } else {
+        static_assert(NR == 16, "16 rows of 16 bytes or 32 rows of 8 bytes");
+        float4 *tb = static_cast<float4 *>(tbv);
+        const int jr = lane & 15, hi = lane & 16;
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            const int slot = back ? jr * 32 + (hi | (j ^ (jr & 7))) : j * 32 + (lane ^ (j & 7));
+            tb[slot] = as_f4(x[j]);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            const int slot = back ? j * 32 + (lane ^ (j & 7)) : jr * 32 + (hi | (j ^ (jr & 7)));
+            from_f4(x[j], tb[slot]);
+        }
     }
 }
 
-// XP (the low pass): the pass also owns the lowest bits. Gates on lane bits 0..3
+// XP (the low pass): the pass also owns the lowest bits. Gates on lane bits 0..R-1
 // run as register updates after lane_row_transpose (a second transpose restores
-// the layout before the store); the top lane bit keeps its shfl.xor gate. One pass
-// then applies gates on the F lowest bits and on 4 more with one read and one
-// write of every amplitude.
+// the layout before the store); with 16-byte rows the top lane bit keeps its
+// shfl.xor gate. One pass then applies gates on the F lowest bits and on R more
+// with one read and one write of every amplitude.
 template <typename E, int W, bool XP, bool REAL, bool WIN>
 __global__ void __launch_bounds__(kThreads, 2) row_pass_kernel(const uint8_t *__restrict__ blob, uint64_t poff,
                                                             uint64_t toff, E *__restrict__ state)
@@ -649,8 +663,9 @@ __global__ void __launch_bounds__(kThreads, 2) row_pass_kernel(const uint8_t *__
     constexpr int R = RowCfg<E, W>::R;
     constexpr int NR = 1 << R;
     constexpr int WARPS = kThreads / 32;
-    static_assert(!XP || (R == 4 && sizeof(VT) == 16), "the low pass swaps 4 lane bits with 16 rows of 16 bytes");
-    extern __shared__ __align__(16) float4 s_xp[];  // XP: 16 x 32 slots per warp
+    static_assert(!XP || (R == 4 && sizeof(VT) == 16) || (R == 5 && sizeof(VT) == 8),
+                  "the low pass swaps lane bits with 16 rows of 16 bytes or 32 rows of 8 bytes");
+    extern __shared__ __align__(16) float4 s_xp[];  // XP: NR x 32 row slots per warp
 
     const RowPassDev &p = *reinterpret_cast<const RowPassDev *>(blob + poff);
     const FastGateDev *gates = reinterpret_cast<const FastGateDev *>(blob + p.off_gates);
@@ -761,7 +776,7 @@ __global__ void __launch_bounds__(kThreads, 2) row_pass_kernel(const uint8_t *__
         if constexpr (WIN) {
             if (offw0) window(0, offw0);
         }
-        float4 *tb = s_xp + warp * (NR * 32);
+        void *tb = reinterpret_cast<unsigned char *>(s_xp) + size_t(warp) * NR * 32 * sizeof(VT);
         if constexpr (REAL) {
             // dense table (real passes): slot i holds the gate of coordinate C0 + i
             // (identity where the pass has none), so the loop unrolls with
@@ -828,14 +843,16 @@ int row_fixed_bits(int elem_bytes, int wide)
     return 5 + (v == 2 ? 1 : 0);
 }
 
-bool row_low_ok(int elem_bytes, int wide) { return row_reg_bits(elem_bytes, wide) == 4; }
+// the shapes the low pass supports: 16 rows of 16 bytes, or (complex64, wide) 32
+// rows of 8 bytes
+bool row_low_ok(int elem_bytes, int wide) { return elem_bytes == 8 || row_reg_bits(elem_bytes, wide) == 4; }
 
 template <typename E, int W, bool XP, bool REAL, bool WIN>
 static cudaError_t launch_row(const uint8_t *dblob, uint64_t poff, uint64_t toff, uint64_t nitems, void *state,
                               int sms, cudaStream_t st)
 {
     auto kern = row_pass_kernel<E, W, XP, REAL, WIN>;
-    const size_t smem = XP ? size_t(kThreads / 32) * 16 * 32 * sizeof(float4) : 0;
+    const size_t smem = XP ? size_t(kThreads / 32) * (size_t(1) << RowCfg<E, W>::R) * 32 * sizeof(typename RowCfg<E, W>::VT) : 0;
     if (XP) {
         const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         if (e != cudaSuccess) return e;
@@ -857,7 +874,7 @@ static cudaError_t launch_row_win(const uint8_t *dblob, uint64_t poff, uint64_t 
                : launch_row<E, W, XP, REAL, false>(dblob, poff, toff, nitems, state, sms, st);
 }
 
-// The low-pass shapes (16 rows of 16 bytes) also run with real gates.
+// The low-pass shapes also run with real gates.
 template <typename E, int W>
 static cudaError_t launch_row_low(const uint8_t *dblob, uint64_t poff, uint64_t toff, uint64_t nitems, bool low,
                                   bool real, bool win, void *state, int sms, cudaStream_t st)
@@ -871,12 +888,13 @@ static cudaError_t launch_row_low(const uint8_t *dblob, uint64_t poff, uint64_t 
 cudaError_t run_row_pass(const uint8_t *dblob, uint64_t poff, uint64_t toff, uint64_t nitems, int elem_bytes,
                          int wide, bool low, bool real, bool win, void *state, int sms, cudaStream_t st)
 {
-    if (row_low_ok(elem_bytes, wide)) {
-        if (elem_bytes == 8) return launch_row_low<float2, 0>(dblob, poff, toff, nitems, low, real, win, state, sms, st);
-        return launch_row_low<double2, 1>(dblob, poff, toff, nitems, low, real, win, state, sms, st);
-    }
+    // the wide complex64 shape always takes the instance with the window code:
+    // ptxas spills far less there (the windows are skipped at run time)
+    if (elem_bytes == 8)
+        return wide ? launch_row_low<float2, 1>(dblob, poff, toff, nitems, low, real, true, state, sms, st)
+                    : launch_row_low<float2, 0>(dblob, poff, toff, nitems, low, real, win, state, sms, st);
+    if (wide) return launch_row_low<double2, 1>(dblob, poff, toff, nitems, low, real, win, state, sms, st);
     if (low || real) return cudaErrorInvalidValue;
-    if (elem_bytes == 8) return launch_row_win<float2, 1, false, false>(dblob, poff, toff, nitems, win, state, sms, st);
     return launch_row_win<double2, 0, false, false>(dblob, poff, toff, nitems, win, state, sms, st);
 }
 
