@@ -65,7 +65,7 @@ REF_SAMPLE_QUBITS = 18
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)  # ~0.3 s timed: several clock samples land inside
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--qubits", type=int, default=N_QUBITS)
@@ -128,8 +128,12 @@ class Clocks:
         try:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=self.fh, stderr=subprocess.DEVNULL)
+            # the timed region starts once the sampler is up (its first line written)
+            t0 = time.perf_counter()
+            while time.perf_counter() - t0 < 2.0 and self.path.stat().st_size == 0:
+                time.sleep(0.02)
         except Exception:
             self.proc = None
         return self
