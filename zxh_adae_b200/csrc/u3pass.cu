@@ -485,10 +485,6 @@ struct RowCfg<double2, 1> {
 };
 
 
-// Phases of a window fused into a strided pass, at one thread's amplitudes. Tile
-// coordinates are [0, F) = vector and lane bits, then F + r = register bit r;
-// base holds the item's out-of-tile bits. apply(row, v, turns) is called for every
-// row (in Gray-code order) and vector slot v.
 // A window with linear terms only: the phase is K(item) + A(lane, vector slot) +
 // B(row), so each amplitude takes one product of two factors: e^{i (K + A)} per
 // thread and item, e^{i B} per row from rowf (per CTA, shared). apply(row, v,
@@ -521,9 +517,13 @@ __device__ __forceinline__ void row_window_linear(const uint8_t *blob, const Dia
     }
 }
 
-template <int F, int LV, int R, int V, typename Apply>
-__device__ __forceinline__ void row_window(const uint8_t *blob, const DiagDev &dd, const int64_t *qreg, uint64_t base,
-                                           int lane, Apply &&apply)
+// Phases of a window fused into a strided pass, at one thread's amplitudes. Tile
+// coordinates are [0, F) = vector and lane bits, then F + r = register bit r;
+// base holds the item's out-of-tile bits. apply(row, v, factor) is called for
+// every row (in Gray-code order) and vector slot v with the phase factor.
+template <int F, int LV, int R, int V, typename E, typename Apply>
+__device__ __forceinline__ void row_window(const uint8_t *blob, const DiagDev &dd, const int64_t *qreg,
+                                           const E *s_exp, uint64_t base, int lane, Apply &&apply)
 {
     constexpr int T = F + R;
     constexpr int NR = 1 << R;
@@ -584,17 +584,42 @@ __device__ __forceinline__ void row_window(const uint8_t *blob, const DiagDev &d
 #pragma unroll
         for (int v = 0; v < V; v++) w[r][v] += dk;
     }
+    if constexpr (sizeof(E) == 8) {
+        // complex64: the walk in 32-bit turns (2 pi / 2^32 resolution) and the
+        // table-plus-Taylor factor without an integer-to-float conversion
+        uint32_t a32[V], w32[R][V];
 #pragma unroll
-    for (int jj = 0; jj < NR; jj++) {
-        const int gj = jj ^ (jj >> 1);
-        if (jj > 0) {
-            const int fb = ctz_const(jj);
+        for (int v = 0; v < V; v++) {
+            a32[v] = turns32(acc[v]);
 #pragma unroll
-            for (int v = 0; v < V; v++) acc[v] += ((gj >> fb) & 1) ? w[fb][v] : -w[fb][v];
+            for (int r = 0; r < R; r++) w32[r][v] = turns32(w[r][v]);
         }
-        const int64_t qr = qreg[gj];
 #pragma unroll
-        for (int v = 0; v < V; v++) apply(gj, v, acc[v] + qr);
+        for (int jj = 0; jj < NR; jj++) {
+            const int gj = jj ^ (jj >> 1);
+            if (jj > 0) {
+                const int fb = ctz_const(jj);
+#pragma unroll
+                for (int v = 0; v < V; v++) a32[v] += ((gj >> fb) & 1) ? w32[fb][v] : 0u - w32[fb][v];
+            }
+            const uint32_t qr = turns32(qreg[gj]);
+#pragma unroll
+            for (int v = 0; v < V; v++)
+                apply(gj, v, phase_factor32(reinterpret_cast<const float2 *>(s_exp), a32[v] + qr));
+        }
+    } else {
+#pragma unroll
+        for (int jj = 0; jj < NR; jj++) {
+            const int gj = jj ^ (jj >> 1);
+            if (jj > 0) {
+                const int fb = ctz_const(jj);
+#pragma unroll
+                for (int v = 0; v < V; v++) acc[v] += ((gj >> fb) & 1) ? w[fb][v] : -w[fb][v];
+            }
+            const int64_t qr = qreg[gj];
+#pragma unroll
+            for (int v = 0; v < V; v++) apply(gj, v, phase_factor(s_exp, acc[v] + qr));
+        }
     }
 }
 
@@ -769,8 +794,8 @@ __global__ void __launch_bounds__(kThreads, 2) row_pass_kernel(const uint8_t *__
                     vset(x[j], v, cmul(vget(x[j], v), f));
                 });
             else
-                row_window<F, LV, R, V>(blob, dd, s_qreg[d], base, lane, [&](int j, int v, int64_t th) {
-                    vset(x[j], v, cmul(vget(x[j], v), phase_factor(s_exp, th)));
+                row_window<F, LV, R, V>(blob, dd, s_qreg[d], s_exp, base, lane, [&](int j, int v, E f) {
+                    vset(x[j], v, cmul(vget(x[j], v), f));
                 });
         };
         if constexpr (WIN) {
