@@ -301,6 +301,7 @@ struct GrowShared {
     uint8_t s_mu[kGrowMaxSel];                     // selector bits inside the lane / vector bits
     uint64_t s_bmask;                              // selector betas
     double s_tacc[kThreads / 32][kGrowMaxTerms];   // adjoint windows: per-warp term gradients
+    double s_gacc[kThreads / 32][kGrowAdjGates][32];  // adjoint gates: per-lane gradient sums (off the registers)
 };
 
 // Adjoint window gradients of one item, before the inverse phases are applied.
@@ -506,6 +507,8 @@ __device__ __forceinline__ void grow_body(const uint8_t *__restrict__ blob, uint
     }
     if constexpr (ADJ) {
         for (uint32_t i = uint32_t(tid); i < uint32_t(WARPS) * kGrowMaxTerms; i += kThreads) (&sm.s_tacc[0][0])[i] = 0.0;
+        for (uint32_t i = uint32_t(tid); i < uint32_t(WARPS) * kGrowAdjGates * 32; i += kThreads)
+            (&sm.s_gacc[0][0][0])[i] = 0.0;
     }
     // lane part of every selector (with beta), per vector slot
     uint64_t lb[V];
@@ -518,9 +521,6 @@ __device__ __forceinline__ void grow_body(const uint8_t *__restrict__ blob, uint
     }
     __syncthreads();
 
-    double acc[ADJ ? kGrowAdjGates : 1];
-#pragma unroll
-    for (int g = 0; g < (ADJ ? kGrowAdjGates : 1); g++) acc[g] = 0.0;
 
     for (uint64_t item = first + uint64_t(warp); item < end; item += step) {
         uint64_t r0 = item << F;
@@ -636,9 +636,7 @@ __device__ __forceinline__ void grow_body(const uint8_t *__restrict__ blob, uint
                 if constexpr (ADJ) ga += double(gpart);
             }
             if constexpr (ADJ) {
-#pragma unroll
-                for (int i = 0; i < kGrowAdjGates; i++)
-                    if (uint32_t(i) == g) acc[i] += ga;
+                if (g < uint32_t(kGrowAdjGates)) sm.s_gacc[warp][g][lane] += ga;  // this lane's own slot
             }
         }
         if constexpr (!ADJ) {
@@ -682,7 +680,7 @@ __device__ __forceinline__ void grow_body(const uint8_t *__restrict__ blob, uint
 #pragma unroll
         for (int g = 0; g < kGrowAdjGates; g++) {
             if (uint32_t(g) >= ngates) break;
-            const double v = warp_sum_f64(acc[g]);
+            const double v = warp_sum_f64(sm.s_gacc[warp][g][lane]);
             if (lane == 0) sm.s_tacc[warp][g] = v;
         }
         __syncthreads();
