@@ -328,3 +328,57 @@ def test_load_circuit_through_the_host_compiler(dtype, seed):
     ph = got[k] / ref[k]
     ph /= abs(ph)
     assert float(np.max(np.abs(got - ph * ref))) <= TOL[dtype] * 10
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_empty_barrier_only_and_single_qubit_circuits(dtype):
+    for n in (1, 2, 7):
+        for gates in ([], [(zx._core.BARRIER, 0, 0)]):
+            s = zx.ZXH(n, dtype=dtype)
+            s.push_gates(zx.as_records(gates))
+            s.execute()
+            st = s.get_state().astype(np.complex128)
+            assert st[0] == 1 and not np.any(st[1:])
+            s.apply(zx.as_records([]))
+            assert np.array_equal(s.get_state().astype(np.complex128), st)
+    for seed in range(6):
+        gates = wl.random_circuit(1, 40, 8800 + seed)
+        o, s = run_pair(1, gates, dtype)
+        assert max_err(s, o) <= TOL[dtype]
+
+
+def _inverse_records(recs):
+    """The inverse circuit: gates in reverse order, each inverted (U3(t, l, p)^-1 =
+    U3(-t, -p, -l); P / CP / RZ negate the angle; H, X, CX are their own inverses)."""
+    C = zx._core
+    out = []
+    for r in reversed(zx.as_records(recs).tolist()):
+        t, cq, q, _res, th, la, ph = r
+        if t == C.U3:
+            out.append((t, cq, q, -th, -ph, -la))
+        elif t in (C.P, C.CP, C.RZ, C.CRZ, C.RX):
+            out.append((t, cq, q, -th))
+        else:
+            out.append((t, cq, q))
+    return zx.as_records(out)
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_large_state_round_trip(dtype):
+    # size-independent check at 26 qubits: layers of U3 + cp chains, X-flipped
+    # selectors and their inverse bring |+>^n back; the norm stays 1
+    n = 26 if dtype == "complex64" else 25
+    layers = _layers_with_x(n, 3, seed=123)
+    h = len(wl.h_all(n))
+    body = layers[h:]
+    s = zx.ZXH(n, dtype=dtype)
+    s.push_gates(layers)
+    s.execute()
+    st = s.get_state().astype(np.complex128)
+    assert abs(np.vdot(st, st).real - 1.0) < (1e-5 if dtype == "complex64" else 1e-12)
+    s.apply(_inverse_records(body))
+    back = s.get_state().astype(np.complex128)
+    k = int(np.argmax(np.abs(back)))
+    ph = back[k] / abs(back[k])
+    amp = 2.0 ** (-n / 2)
+    assert np.max(np.abs(back - ph * amp)) < (1e-4 if dtype == "complex64" else 1e-10) * amp
