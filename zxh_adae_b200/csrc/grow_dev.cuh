@@ -48,11 +48,6 @@ __device__ __forceinline__ E mad2(const RT *m, E a, E b)  // m[0..3] = (x re, x 
     return o;
 }
 
-template <typename E>
-__device__ __forceinline__ double re_cj(E a, E b) { return double(a.x) * double(b.x) + double(a.y) * double(b.y); }
-template <typename E>
-__device__ __forceinline__ double im_cj(E a, E b) { return double(a.x) * double(b.y) - double(a.y) * double(b.x); }
-
 // One row vector of the state at amplitude address a (zeros in the lane bits);
 // complex64 vectors hold two amplitudes whose order follows bit 0 of a. Loads and
 // stores go through L2 only (.cg): in the persistent batch kernel another SM may
