@@ -246,7 +246,7 @@ int zxh_batch_run(zxh_batch *batch, int mode, double *energies, double *grads, s
 int zxh_batch_set(zxh_batch *batch, const char *name, int value);
 int zxh_batch_get(const zxh_batch *batch, const char *name, int *value);
 /* Times the persistent launch over grow_regs in {2, 3, 4} x task_items in {32,
- * 128, 512} (task_elems = 1024 x task_items; reps timed runs each after one
+ * 128, 512, 2048} (task_elems = 1024 x task_items; reps timed runs each after one
  * warm-up) and keeps the fastest. */
 int zxh_batch_tune(zxh_batch *batch, int reps);
 /* ops and tasks of the compiled batch, device ms of the last run, and the

@@ -552,7 +552,7 @@ int zxh_batch_tune(zxh_batch *b, int reps)
     const size_t ngr = b->grad_off.back();
     std::vector<double> e(b->n.size()), g(std::max<size_t>(ngr, 1));
     const int regs_c[] = {2, 3, 4};
-    const int items_c[] = {32, 128, 512};
+    const int items_c[] = {32, 128, 512, 2048};
     double best = 1e300;
     int best_r = b->grow_regs, best_i = b->task_items;
     for (int r : regs_c) {
