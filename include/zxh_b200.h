@@ -287,6 +287,8 @@ int zxh_optimize_gates(size_t n, int level, const zxh_gate *gates, size_t count,
  * strided passes after a |0...0> init, the pass set of the batched launch; needs
  * eager_expand_all), adj_windows (1: the adjoint sweep undoes diagonal gates
  * inside its general strided passes, 0: in separate diagonal-group passes),
+ * adj_regs (1..4: gates with high deltas per reverse strided pass; 4 runs at one
+ * CTA per SM),
  * low_pass (1: gates on the lane / vector bits ride in a strided low pass with
  * lane bits swapped into registers, 0: the TMA fast tile pass), low_regs_c64,
  * low_regs_c128 (0..4: register-bit gates that join the low pass), real_split

@@ -208,7 +208,8 @@ int reverse_program(zxh_sim *s, const std::vector<size_t> &ends, AffineMap A, st
     const size_t count = s->gates.size();
     long open = -1;                    // diagonal group being filled (states too small for strided passes)
     size_t next_ck = ends.size() - 1;  // checkpoints are restored from the last one down
-    const int F = zxh::grow_fixed_bits(s->elem_bytes), R = zxh::grow_reg_bits(s->elem_bytes, true);
+    const int F = zxh::grow_fixed_bits(s->elem_bytes);
+    const int R = std::max(1, std::min(s->pp.adj_regs, zxh::grow_reg_bits(s->elem_bytes, true)));
     const int maxg = zxh::grow_adjoint_gates();
     const bool fuse = N >= F && s->pp.adj_windows;  // diagonal gates ride in the general strided passes
     PairGroup pg;

@@ -130,6 +130,7 @@ int compile(zxh_batch *b)
     zxh::PlanParams pp;
     pp.grow_only = 1;
     pp.grow_regs = b->grow_regs;
+    pp.adj_regs = 3;  // the persistent kernel runs reverse passes of at most 3 register coordinates
     std::vector<uint8_t> etab;
     zxh::exp_table(b->eb, etab);
     const uint64_t exp_off = append(b->blob, etab.data(), etab.size());

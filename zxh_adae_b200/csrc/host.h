@@ -57,6 +57,7 @@ struct PlanParams {
     int grow_regs = 4;          // register coordinates (gates with high deltas) per general strided pass
     int grow_only = 0;          // 1: only INIT and general strided passes (the persistent batch kernel's set)
     int adj_windows = 1;        // adjoint sweep: diagonal gates ride in the general strided passes as windows
+    int adj_regs = 4;           // adjoint sweep: gates with high deltas per strided pass (4 runs at one CTA per SM)
     int diag_prefetch_c64 = 1;  // diagonal pass: each warp stages its next tile with a TMA bulk copy
     int diag_prefetch_c128 = 0; // same for complex128 (no gain measured there)
     int diag_chunk_bits = -1;   // log2 tiles a warp walks in Gray-code order in a diagonal pass (-1: chosen
