@@ -288,7 +288,10 @@ int zxh_optimize_gates(size_t n, int level, const zxh_gate *gates, size_t count,
  * eager_expand_all), adj_windows (1: the adjoint sweep undoes diagonal gates
  * inside its general strided passes, 0: in separate diagonal-group passes),
  * adj_regs (1..4: gates with high deltas per reverse strided pass; 4 runs at one
- * CTA per SM),
+ * CTA per SM), grow_staged (0..7, bit mask: general strided passes whose warps
+ * stage their next item in shared memory with TMA bulk copies; 1 = the adjoint
+ * sweep's in complex64, 2 = the forward ones, 4 = the adjoint sweep's in
+ * complex128),
  * low_pass (1: gates on the lane / vector bits ride in a strided low pass with
  * lane bits swapped into registers, 0: the TMA fast tile pass), low_regs_c64,
  * low_regs_c128 (0..4: register-bit gates that join the low pass), real_split

@@ -50,12 +50,14 @@ def test_expectation_drops_x_terms_outside_the_state():
 
 @pytest.mark.parametrize("n,seed", [(4, 0), (7, 1), (10, 2)])
 @pytest.mark.parametrize("adj_regs", [3, 4])
-def test_adjoint_matches_oracle_differences(n, seed, adj_regs):
+@pytest.mark.parametrize("staged", [0, 7])
+def test_adjoint_matches_oracle_differences(n, seed, adj_regs, staged):
     circ = mixed_circuit(n, seed) if seed else ad.hardware_efficient_ansatz(n, 3)
     terms = random_terms(n, seed) if seed else ad.tfim_terms(n)
     p = _params(circ, seed)
     s = _core.ZXH(n)
     s.set_param("adj_regs", adj_regs)  # high-delta gates per reverse strided pass
+    s.set_param("grow_staged", staged)  # strided passes staging their next item in shared memory
     e, g = ad.adjoint(s, circ, p, terms)
     assert abs(e - ob.oracle_energy(n, circ.records(p), terms)) < 1e-11
     fd = ob.oracle_central_difference(n, circ, p, terms)

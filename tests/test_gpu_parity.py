@@ -110,6 +110,12 @@ def test_general_strided_pass_after_cx_transport(dtype, n, seed):
     s2.push_gates(gates)
     s2.execute()
     assert max_err(s2, o) <= TOL[dtype]
+    for staged in (0, 7):  # rows loaded straight into registers / staged one item ahead in shared memory
+        s3 = zx.ZXH(n, dtype=dtype)
+        s3.set_param("grow_staged", staged)
+        s3.push_gates(gates)
+        s3.execute()
+        assert max_err(s3, o) <= TOL[dtype], staged
 
 
 @pytest.mark.parametrize("seed", range(24))

@@ -476,6 +476,7 @@ int zxh_adjoint_gradient(zxh_sim *s, const zxh_term *terms, size_t nterms, size_
     }
 
     // reverse sweep
+    CK(s, cudaMemsetAsync(s->d_status, 0, sizeof(zxh::DevStatus), s->stream), "reset status");
     CK(s, cudaEventRecord(s->ev0, s->stream), "event");
     CK(s, cudaMemcpyAsync(s->d_psi, s->d_state, bytes, cudaMemcpyDeviceToDevice, s->stream), "copy state");
     CK(s, zxh::run_lambda(s->d_psi, s->d_lam, N, s->elem_bytes, d_terms, uint32_t(dt.size()), d_energy, s->sms,
@@ -496,7 +497,9 @@ int zxh_adjoint_gradient(zxh_sim *s, const zxh_term *terms, size_t nterms, size_
             break;
         case RevStep::GROW:
             CK(s, zxh::run_grow(s->d_adj + L.grow, r.off, r.toff, int(r.gb.regs.size()), r.gb.dev.nitems, s->elem_bytes,
-                                s->d_psi, s->d_lam, d_grads, r.gb.all_real(), s->sms, s->stream),
+                                s->d_psi, s->d_lam, d_grads, r.gb.all_real(),
+                                (s->pp.grow_staged & (s->elem_bytes == 8 ? 1 : 4)) != 0,
+                                s->d_status, s->sms, s->stream),
                "adjoint strided launch");
             kernels++;
             break;
@@ -509,11 +512,16 @@ int zxh_adjoint_gradient(zxh_sim *s, const zxh_term *terms, size_t nterms, size_
         }
     }
     CK(s, cudaEventRecord(s->ev1, s->stream), "event");
+    CK(s, cudaMemcpyAsync(s->h_status, s->d_status, sizeof(zxh::DevStatus), cudaMemcpyDeviceToHost, s->stream),
+       "read status");
     CK(s, cudaMemcpyAsync(value, d_energy, sizeof(double), cudaMemcpyDeviceToHost, s->stream), "read energy");
     if (count)
         CK(s, cudaMemcpyAsync(grads, d_grads, count * sizeof(double), cudaMemcpyDeviceToHost, s->stream),
            "read gradients");
     CK(s, cudaStreamSynchronize(s->stream), "adjoint sweep");
+    if (s->h_status->code != 0)
+        return fail(s, int(s->h_status->code),
+                    "device wait gave up (site " + std::to_string(s->h_status->where) + ")");
     float rev_ms = 0.0f;
     CK(s, cudaEventElapsedTime(&rev_ms, s->ev0, s->ev1), "event time");
     s->last_ms = float(fwd_ms + double(rev_ms));

@@ -336,7 +336,7 @@ int launch_op(zxh_batch *b, const BatchOp &op)
         break;
     case zxh::BOP_GROW:
         e = zxh::run_grow(b->d_blob + op.base, op.off0, op.off1, int(op.R), op.units, b->eb, psi, nullptr, nullptr,
-                          op.aux != 0, b->sms, b->stream);
+                          op.aux != 0, (zxh::PlanParams().grow_staged & 2) != 0, b->d_status, b->sms, b->stream);
         break;
     case zxh::BOP_LAMBDA:
         e = zxh::run_lambda(psi, lam, int(op.m), b->eb, reinterpret_cast<const zxh::TermDev *>(b->d_blob + op.off0),
@@ -344,7 +344,8 @@ int launch_op(zxh_batch *b, const BatchOp &op)
         break;
     case zxh::BOP_GROW_ADJ:
         e = zxh::run_grow(b->d_blob + op.base, op.off0, op.off1, int(op.R), op.units, b->eb, psi, lam, gr,
-                          op.aux != 0, b->sms, b->stream);
+                          op.aux != 0, (zxh::PlanParams().grow_staged & (b->eb == 8 ? 1 : 4)) != 0, b->d_status,
+                          b->sms, b->stream);
         break;
     case zxh::BOP_DIAG_ADJ:
         e = zxh::run_adj_diag(psi, lam, int(op.m), b->eb,

@@ -597,6 +597,7 @@ int zxh_set_param(zxh_sim *s, const char *name, int value)
         {"real_split", &s->pp.real_split, 0, 1},
         {"diag_prefetch_c64", &s->pp.diag_prefetch_c64, 0, 1},
         {"adj_regs", &s->pp.adj_regs, 1, 4},
+        {"grow_staged", &s->pp.grow_staged, 0, 7},
         {"diag_prefetch_c128", &s->pp.diag_prefetch_c128, 0, 1},
         {"diag_chunk_bits", &s->pp.diag_chunk_bits, -1, 8},
         {"grow", &s->pp.grow, 0, 1},

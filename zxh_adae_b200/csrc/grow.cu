@@ -40,51 +40,62 @@ namespace {
 using namespace gdev;
 
 // The adjoint pass with 4 register coordinates holds 16 rows of both states: one
-// CTA per SM (twice the rows in flight per warp, the same bytes per SM).
-template <typename E, int R, bool ADJ, bool REAL>
-__global__ void __launch_bounds__(kThreads, (ADJ && R == 4) ? 1 : 2) grow_kernel(const uint8_t *__restrict__ blob, uint64_t poff,
-                                                            uint64_t toff, E *__restrict__ psi, E *__restrict__ lam,
-                                                            double *grads, uint64_t nitems)
+// CTA per SM (twice the rows in flight per warp, the same bytes per SM). PF: the
+// staged form (next item's rows copied into shared memory during the current one).
+template <typename E, int R, bool ADJ, bool REAL, bool PF>
+__global__ void __launch_bounds__(kThreads, (ADJ && R == 4) ? 1 : 2)
+    grow_kernel(const uint8_t *__restrict__ blob, uint64_t poff, uint64_t toff, E *__restrict__ psi,
+                E *__restrict__ lam, double *grads, uint64_t nitems, DevStatus *status)
 {
     __shared__ GrowShared<E> sm;
+    extern __shared__ __align__(128) uint8_t stage[];
     constexpr int WARPS = kThreads / 32;
-    grow_body<E, R, ADJ, REAL>(blob, poff, toff, psi, lam, grads, uint64_t(blockIdx.x) * WARPS,
-                               uint64_t(gridDim.x) * WARPS, nitems, sm);
+    grow_body<E, R, ADJ, REAL, PF>(blob, poff, toff, psi, lam, grads, uint64_t(blockIdx.x) * WARPS,
+                                   uint64_t(gridDim.x) * WARPS, nitems, sm, stage, status);
 }
 
-template <typename E, int R, bool ADJ, bool REAL>
+template <typename E, int R, bool ADJ, bool REAL, bool PF>
 cudaError_t launch_grow(const uint8_t *dblob, uint64_t poff, uint64_t toff, uint64_t nitems, E *psi, E *lam,
-                        double *grads, int sms, cudaStream_t st)
+                        double *grads, DevStatus *status, int sms, cudaStream_t st)
 {
+    auto kern = grow_kernel<E, R, ADJ, REAL, PF>;
+    const size_t smem = PF ? grow_stage_bytes<R, ADJ>() : 0;
+    if (PF) {
+        const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        if (e != cudaSuccess) return e;
+    }
     int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grow_kernel<E, R, ADJ, REAL>, kThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem);
     if (per_sm < 1) per_sm = 1;
     const uint64_t ctas = (nitems + kThreads / 32 - 1) / (kThreads / 32);
     const unsigned grid = unsigned(std::max<uint64_t>(1, std::min<uint64_t>(ctas, uint64_t(sms) * uint64_t(per_sm))));
-    grow_kernel<E, R, ADJ, REAL><<<grid, kThreads, 0, st>>>(dblob, poff, toff, psi, lam, grads, nitems);
+    kern<<<grid, kThreads, smem, st>>>(dblob, poff, toff, psi, lam, grads, nitems, status);
     return cudaGetLastError();
 }
 
-template <typename E, bool ADJ, bool REAL>
+template <typename E, bool ADJ, bool REAL, bool PF>
 cudaError_t grow_typed(int R, const uint8_t *dblob, uint64_t poff, uint64_t toff, uint64_t nitems, E *psi, E *lam,
-                       double *grads, int sms, cudaStream_t st)
+                       double *grads, DevStatus *status, int sms, cudaStream_t st)
 {
     switch (R) {
-    case 0: return launch_grow<E, 0, ADJ, REAL>(dblob, poff, toff, nitems, psi, lam, grads, sms, st);
-    case 1: return launch_grow<E, 1, ADJ, REAL>(dblob, poff, toff, nitems, psi, lam, grads, sms, st);
-    case 2: return launch_grow<E, 2, ADJ, REAL>(dblob, poff, toff, nitems, psi, lam, grads, sms, st);
-    case 3: return launch_grow<E, 3, ADJ, REAL>(dblob, poff, toff, nitems, psi, lam, grads, sms, st);
-    case 4: return launch_grow<E, 4, ADJ, REAL>(dblob, poff, toff, nitems, psi, lam, grads, sms, st);
+    case 0: return launch_grow<E, 0, ADJ, REAL, PF>(dblob, poff, toff, nitems, psi, lam, grads, status, sms, st);
+    case 1: return launch_grow<E, 1, ADJ, REAL, PF>(dblob, poff, toff, nitems, psi, lam, grads, status, sms, st);
+    case 2: return launch_grow<E, 2, ADJ, REAL, PF>(dblob, poff, toff, nitems, psi, lam, grads, status, sms, st);
+    case 3: return launch_grow<E, 3, ADJ, REAL, PF>(dblob, poff, toff, nitems, psi, lam, grads, status, sms, st);
+    case 4: return launch_grow<E, 4, ADJ, REAL, PF>(dblob, poff, toff, nitems, psi, lam, grads, status, sms, st);
     default: return cudaErrorInvalidValue;
     }
 }
 
 template <typename E, bool ADJ>
-cudaError_t grow_real(bool real, int R, const uint8_t *dblob, uint64_t poff, uint64_t toff, uint64_t nitems, E *psi,
-                      E *lam, double *grads, int sms, cudaStream_t st)
+cudaError_t grow_real(bool real, bool staged, int R, const uint8_t *dblob, uint64_t poff, uint64_t toff,
+                      uint64_t nitems, E *psi, E *lam, double *grads, DevStatus *status, int sms, cudaStream_t st)
 {
-    return real ? grow_typed<E, ADJ, true>(R, dblob, poff, toff, nitems, psi, lam, grads, sms, st)
-                : grow_typed<E, ADJ, false>(R, dblob, poff, toff, nitems, psi, lam, grads, sms, st);
+    if (staged)
+        return real ? grow_typed<E, ADJ, true, true>(R, dblob, poff, toff, nitems, psi, lam, grads, status, sms, st)
+                    : grow_typed<E, ADJ, false, true>(R, dblob, poff, toff, nitems, psi, lam, grads, status, sms, st);
+    return real ? grow_typed<E, ADJ, true, false>(R, dblob, poff, toff, nitems, psi, lam, grads, status, sms, st)
+                : grow_typed<E, ADJ, false, false>(R, dblob, poff, toff, nitems, psi, lam, grads, status, sms, st);
 }
 
 }  // namespace
@@ -100,19 +111,21 @@ int grow_fixed_bits(int elem_bytes) { return elem_bytes == 8 ? 6 : 5; }
 int grow_adjoint_gates() { return kGrowAdjGates; }
 
 cudaError_t run_grow(const uint8_t *dblob, uint64_t poff, uint64_t toff, int R, uint64_t nitems, int elem_bytes,
-                     void *psi, void *lam, double *grads, bool real, int sms, cudaStream_t st)
+                     void *psi, void *lam, double *grads, bool real, bool staged, DevStatus *status, int sms,
+                     cudaStream_t st)
 {
     const bool adj = lam != nullptr;
+    staged = staged && status != nullptr;
     if (elem_bytes == 8) {
         auto *a = static_cast<float2 *>(psi);
         auto *b = static_cast<float2 *>(lam);
-        return adj ? grow_real<float2, true>(real, R, dblob, poff, toff, nitems, a, b, grads, sms, st)
-                   : grow_real<float2, false>(real, R, dblob, poff, toff, nitems, a, b, grads, sms, st);
+        return adj ? grow_real<float2, true>(real, staged, R, dblob, poff, toff, nitems, a, b, grads, status, sms, st)
+                   : grow_real<float2, false>(real, staged, R, dblob, poff, toff, nitems, a, b, grads, status, sms, st);
     }
     auto *a = static_cast<double2 *>(psi);
     auto *b = static_cast<double2 *>(lam);
-    return adj ? grow_real<double2, true>(real, R, dblob, poff, toff, nitems, a, b, grads, sms, st)
-               : grow_real<double2, false>(real, R, dblob, poff, toff, nitems, a, b, grads, sms, st);
+    return adj ? grow_real<double2, true>(real, staged, R, dblob, poff, toff, nitems, a, b, grads, status, sms, st)
+               : grow_real<double2, false>(real, staged, R, dblob, poff, toff, nitems, a, b, grads, status, sms, st);
 }
 
 }  // namespace zxh

@@ -439,10 +439,28 @@ __device__ __forceinline__ void adj_window_grad(const VT (&x)[1 << R], const VT 
 // first + warp + step, ... below end) on the calling CTA. Every thread of the CTA
 // calls it; it synchronises the CTA on entry and exit. REAL: every gate of the
 // pass has a real matrix.
-template <typename E, int R, bool ADJ, bool REAL = false>
+// Bytes of one row of a warp (32 lanes x 16-byte vectors), the unit of a staged copy.
+constexpr uint32_t kGrowRowBytes = 512;
+
+// Shared memory of the staged form: one mbarrier per warp (padded to 128 bytes),
+// then per warp the rows of one item of each state.
+template <int R, bool ADJ>
+__host__ __device__ constexpr size_t grow_stage_bytes()
+{
+    return 128 + size_t(kThreads / 32) * (ADJ ? 2 : 1) * (size_t(1) << R) * kGrowRowBytes;
+}
+
+// PF (staged form): every warp keeps the rows of its next item on their way into
+// shared memory (one TMA bulk copy per row, completing on the warp's mbarrier)
+// while it works on the current one, so the loads of one item overlap the
+// arithmetic and stores of the previous one without holding registers. stage is
+// the dynamic shared memory laid out as grow_stage_bytes; a wait that gives up
+// (after about a second) records kErrTimeout in status and ends the warp's loop.
+template <typename E, int R, bool ADJ, bool REAL = false, bool PF = false>
 __device__ __forceinline__ void grow_body(const uint8_t *__restrict__ blob, uint64_t poff, uint64_t toff,
                                           E *__restrict__ psi, E *__restrict__ lam, double *grads, uint64_t first,
-                                          uint64_t step, uint64_t end, GrowShared<E> &sm)
+                                          uint64_t step, uint64_t end, GrowShared<E> &sm, uint8_t *stage = nullptr,
+                                          DevStatus *status = nullptr)
 {
     using VT = typename GrowCfg<E>::VT;
     using RT = typename ET<E>::R;
@@ -514,21 +532,80 @@ __device__ __forceinline__ void grow_body(const uint8_t *__restrict__ blob, uint
         for (uint32_t s = 0; s < nsel; s++)
             lb[v] |= uint64_t(par64(sels[s].alpha & e) ^ int(sels[s].beta & 1)) << s;
     }
+    // staged form: this warp's barrier and row buffers
+    constexpr int NS = ADJ ? 2 : 1;
+    [[maybe_unused]] uint64_t *wbar = nullptr;
+    [[maybe_unused]] VT *wbuf = nullptr;
+    if constexpr (PF) {
+        wbar = reinterpret_cast<uint64_t *>(stage) + warp;
+        wbuf = reinterpret_cast<VT *>(stage + 128) + size_t(warp) * NS * NR * 32;
+        if (lane == 0) mbar_init(wbar, 1);
+        fence_mbar_init();
+    }
     __syncthreads();
 
-
-    for (uint64_t item = first + uint64_t(warp); item < end; item += step) {
+    // first amplitude address of an item: the item's bits spread around the pivots
+    auto item_base = [&](uint64_t item) {
         uint64_t r0 = item << F;
 #pragma unroll
         for (int i = 0; i < R; i++) {
             const uint32_t b = p.piv[i];
             r0 = ((r0 >> b) << (b + 1)) | (r0 & ((1ULL << b) - 1ULL));
         }
+        return r0;
+    };
+    // staged form: start the copies of an item's rows (lane j < NS * NR copies row
+    // j % NR of state j / NR: the 512 contiguous bytes its lanes' vectors lie in)
+    [[maybe_unused]] auto stage_item = [&](uint64_t item) {
+        const uint64_t b0 = item_base(item);
+        if (lane == 0) mbar_arrive_expect_tx(wbar, uint32_t(NS * NR) * kGrowRowBytes);
+        __syncwarp();
+        if (lane < NS * NR) {
+            const int k = lane & (NR - 1);
+            const E *src = (lane >= NR) ? lam : psi;
+            const VT *row = reinterpret_cast<const VT *>(src) + (((b0 ^ s_D[k]) >> LV) & ~uint64_t(31));
+            bulk_g2s(wbuf + size_t(lane) * 32, row, kGrowRowBytes, wbar);
+        }
+    };
+    uint32_t taken = 0;  // items this warp has taken (the barrier's phase)
+    if constexpr (PF) {
+        if (first + uint64_t(warp) < end) stage_item(first + uint64_t(warp));
+    }
+
+    for (uint64_t item = first + uint64_t(warp); item < end; item += step, taken++) {
+        const uint64_t r0 = item_base(item);
         VT x[NR], y[NR];
+        if constexpr (PF) {
+            if (!__all_sync(0xffffffffu, mbar_wait_bounded(wbar, taken & 1u))) {
+                if (lane == 0) report(status, kErrTimeout, 9, item);
+                (void)mbar_wait_bounded(wbar, taken & 1u);  // the copies may still be in flight
+                break;
+            }
 #pragma unroll
-        for (int k = 0; k < NR; k++) {
-            x[k] = grow_load(psi, r0 ^ s_D[k], lane);
-            if constexpr (ADJ) y[k] = grow_load(lam, r0 ^ s_D[k], lane);
+            for (int k = 0; k < NR; k++) {
+                const uint64_t a = r0 ^ s_D[k];
+                const uint32_t slot = uint32_t((a >> LV) ^ uint64_t(lane)) & 31u;
+                VT t = wbuf[k * 32 + slot];
+                if constexpr (V == 2) {
+                    if (a & 1) t = make_float4(t.z, t.w, t.x, t.y);
+                }
+                x[k] = t;
+                if constexpr (ADJ) {
+                    VT u = wbuf[(NR + k) * 32 + slot];
+                    if constexpr (V == 2) {
+                        if (a & 1) u = make_float4(u.z, u.w, u.x, u.y);
+                    }
+                    y[k] = u;
+                }
+            }
+            __syncwarp();  // every lane has read the buffer before it is refilled
+            if (item + step < end) stage_item(item + step);
+        } else {
+#pragma unroll
+            for (int k = 0; k < NR; k++) {
+                x[k] = grow_load(psi, r0 ^ s_D[k], lane);
+                if constexpr (ADJ) y[k] = grow_load(lam, r0 ^ s_D[k], lane);
+            }
         }
         // selector bits of this item: lane s takes selectors s and s + 32
         const bool p0 = lane < int(nsel) && par64(s_alpha[lane] & r0);

@@ -1482,6 +1482,7 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
             gb.dev.off_terms[0] = put_vec(out.blob, gb.terms[0]);
             gb.dev.off_terms[1] = put_vec(out.blob, gb.terms[1]);
             ps.off = put(out.blob, gb.dev);
+            ps.prefetch = (pp.grow_staged & 2) ? 1 : 0;
             continue;
         }
         if (ps.kind == Pass::ROW) {

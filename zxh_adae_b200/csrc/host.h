@@ -58,6 +58,10 @@ struct PlanParams {
     int grow_only = 0;          // 1: only INIT and general strided passes (the persistent batch kernel's set)
     int adj_windows = 1;        // adjoint sweep: diagonal gates ride in the general strided passes as windows
     int adj_regs = 4;           // adjoint sweep: gates with high deltas per strided pass (4 runs at one CTA per SM)
+    int grow_staged = 1;        // general strided passes whose warps stage their next item in shared memory
+                                // (TMA bulk copies): bit 0 the adjoint sweep's in complex64, bit 1 the
+                                // forward ones, bit 2 the adjoint sweep's in complex128 (measured on the
+                                // 24-qubit ansatz: -2 % complex64 adjoint, +3 % complex128, +3 % forward)
     int diag_prefetch_c64 = 1;  // diagonal pass: each warp stages its next tile with a TMA bulk copy
     int diag_prefetch_c128 = 0; // same for complex128 (no gain measured there)
     int diag_chunk_bits = -1;   // log2 tiles a warp walks in Gray-code order in a diagonal pass (-1: chosen
@@ -104,7 +108,8 @@ struct Pass {
     int real = 0;                        // ROW: every gate matrix is real
     int chunk_bits = -1;                 // DIAG: tiles per Gray-code chunk (log2, -1 = automatic)
     int row_bits = 0;                    // DIAG: log2 rows of a warp tile
-    int prefetch = 0;                    // DIAG: tiles staged one ahead by TMA bulk copies
+    int prefetch = 0;                    // DIAG: tiles staged one ahead by TMA bulk copies; GROW: the
+                                         // staged form (next item in shared memory)
     std::vector<FastGateDev> fgates;     // FAST
     GrowBuild gb;                        // GROW
 };

@@ -549,7 +549,7 @@ cudaError_t run_passes(const std::vector<Pass> &passes, const uint8_t *dblob, vo
             if (e == cudaSuccess) e = run_set_one(state, elem_bytes, st);
         } else if (ps.kind == Pass::GROW) {
             e = run_grow(dblob, ps.off, ps.off2, int(ps.gb.regs.size()), ps.gb.dev.nitems, elem_bytes, state, nullptr,
-                         nullptr, ps.gb.all_real(), sms, st);
+                         nullptr, ps.gb.all_real(), ps.prefetch != 0, status, sms, st);
         } else if (ps.kind == Pass::DIAG) {
             e = run_diag(dblob, ps.off, ps.off2, ps.m, elem_bytes, ps.row_bits, ps.chunk_bits, ps.prefetch != 0, state, status,
                          sms, st);

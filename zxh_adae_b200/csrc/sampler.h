@@ -52,9 +52,12 @@ cudaError_t run_row_pass(const uint8_t *dblob, uint64_t poff, uint64_t toff, uin
 cudaError_t run_set_one(void *state, int elem_bytes, cudaStream_t st);
 // General strided pass (grow.cu): lam == nullptr applies the pass to psi; otherwise
 // the adjoint form on psi and lam with gradients added to grads[slot]. real: every
-// gate of the pass has a real matrix (GrowBuild::all_real).
+// gate of the pass has a real matrix (GrowBuild::all_real). staged: the form whose
+// warps copy their next item into shared memory during the current one (needs
+// status, where a wait that gives up is recorded).
 cudaError_t run_grow(const uint8_t *dblob, uint64_t poff, uint64_t toff, int R, uint64_t nitems, int elem_bytes,
-                     void *psi, void *lam, double *grads, bool real, int sms, cudaStream_t st);
+                     void *psi, void *lam, double *grads, bool real, bool staged, DevStatus *status, int sms,
+                     cudaStream_t st);
 int grow_reg_bits(int elem_bytes, bool adjoint);
 int grow_fixed_bits(int elem_bytes);
 int grow_adjoint_gates();
