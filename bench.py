@@ -494,13 +494,26 @@ def sampler_leg(local: int, n: int = N_QUBITS, shots: int = 1_000_000, steps: in
         sim.measure(shots)
         ms.append(sim.last_stats()[2])
     kernels = sim.last_stats()[0]
+    # counts of the last draw: on the device (zxh_counts: only the distinct
+    # outcomes cross to the host) vs every shot copied and np.unique'd on the host
+    cw, hw = [], []
+    for k in range(3):
+        t0 = time.perf_counter()
+        words, cnt = sim.counts_words()
+        cw.append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        hk, hc = np.unique(sim.results_words(), return_counts=True)
+        hw.append(time.perf_counter() - t0)
+    same = bool(np.array_equal(words, hk) and np.array_equal(cnt, hc.astype(np.uint64)))
     sim.close()
     t = statistics.median(ms)
     peak, kind = peaks()
     gbps = (1 << n) * 8 / (t / 1e3) / 1e9
     return {"workload": f"{shots} shots from a {n}-qubit complex64 state (H all + one U3 layer)", "ms": t,
             "shots_per_s": shots / (t / 1e3), "state_read_GBps": gbps, "frac_of_peak": gbps / peak,
-            "kernels": kernels, "bytes": "one read of the state"}
+            "kernels": kernels, "bytes": "one read of the state",
+            "counts": {"distinct": int(len(words)), "device_counts_wall_ms": min(cw) * 1e3,
+                       "host_unique_wall_ms": min(hw) * 1e3, "identical": same}}
 
 
 def timed_applies(sim, batches, warmup, steps, pg, local):

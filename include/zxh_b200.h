@@ -134,6 +134,18 @@ int zxh_measure(zxh_sim *sim, size_t shots);
  * (measure_result_pack.h:24-44 layout). */
 int zxh_get_results(zxh_sim *sim, uint64_t *words, size_t shots);
 
+/* The distinct outcomes of the last zxh_measure and how often each was drawn,
+ * counted on the device (the reference's sample_counts unpacks every shot on the
+ * host into a std::map, bindings.cpp:36-54 / zxh.cpp:842-871). words[i] (same
+ * layout as zxh_get_results) was drawn counts[i] times, i < *n_unique, in
+ * increasing order of the state's real index (not sorted by word). A word
+ * repeats only where the affine map is singular (a CX whose control equals its
+ * target, which the reference also accepts: zxh.cpp:282-287). words NULL:
+ * only *n_unique is set (a size query; the counting done for it is kept for the
+ * next call). ZXH_ERR_LIMIT if capacity < *n_unique. No draw since the last
+ * zxh_execute / zxh_apply: *n_unique = 0. */
+int zxh_counts(zxh_sim *sim, uint64_t *words, uint64_t *counts, size_t capacity, size_t *n_unique);
+
 /* Replaces ZXH::measured_count (zxh.cpp:566-569). */
 int zxh_measured_count(const zxh_sim *sim, size_t *out);
 

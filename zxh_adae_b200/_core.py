@@ -81,6 +81,7 @@ _sig("zxh_apply", [_P, _P, _SZ])
 _sig("zxh_measure", [_P, _SZ])
 _sig("zxh_get_results", [_P, _P, _SZ])
 _sig("zxh_measured_count", [_P, ctypes.POINTER(_SZ)])
+_sig("zxh_counts", [_P, _P, _P, _SZ, ctypes.POINTER(_SZ)])
 _sig("zxh_get_state", [_P, _P, _SZ, ctypes.c_int])
 _sig("zxh_get_state_device", [_P, _P, _SZ, ctypes.c_int])
 _sig("zxh_required_M", [_P, ctypes.POINTER(_SZ)])
@@ -340,12 +341,28 @@ class ZXH:
         self.measure(shots)
         return self._rows(self.results_words(shots))
 
+    def counts_words(self) -> tuple:
+        """(words, counts) of the last measure(): its distinct outcomes, counted on
+        the device, sorted by word (bit q = qubit q)."""
+        nu = _SZ(0)
+        self._ck(_lib.zxh_counts(self._h, None, None, 0, ctypes.byref(nu)))
+        k = int(nu.value)
+        words = np.zeros(max(k, 1), np.uint64)
+        cnt = np.zeros(max(k, 1), np.uint64)
+        self._ck(_lib.zxh_counts(self._h, words.ctypes.data, cnt.ctypes.data, k, ctypes.byref(nu)))
+        order = np.argsort(words[:k], kind="stable")
+        words, cnt = words[:k][order], cnt[:k][order]
+        if k > 1 and np.any(words[1:] == words[:-1]):  # a singular map (CX with control = target)
+            words, inv = np.unique(words, return_inverse=True)
+            cnt = np.bincount(inv, weights=cnt.astype(np.float64)).astype(np.uint64)
+        return words, cnt
+
     def sample_counts(self, shots: int) -> dict:
-        """Counts keyed by bitstrings with qubit n-1 first (bindings.cpp:36-54)."""
+        """Counts keyed by bitstrings with qubit n-1 first (bindings.cpp:36-54), in
+        increasing key order as the reference's std::map."""
         self.measure(shots)
-        words = self.results_words(shots)
+        keys, cnt = self.counts_words()
         n = self._n
-        keys, cnt = np.unique(words, return_counts=True)  # sorted, as the reference's std::map
         return {format(k, f"0{n}b"): c for k, c in zip(keys.tolist(), cnt.tolist())}
 
     def get_state(self, order: int = ORDER_REFERENCE) -> np.ndarray:

@@ -222,6 +222,7 @@ int zxh_destroy(zxh_sim *s)
     if (s->d_status) cudaFree(s->d_status);
     if (s->h_status) cudaFreeHost(s->h_status);
     if (s->d_samp) cudaFree(s->d_samp);
+    if (s->d_cnt) cudaFree(s->d_cnt);
     if (s->d_out) cudaFree(s->d_out);
     if (s->d_psi) cudaFree(s->d_psi);
     if (s->d_lam) cudaFree(s->d_lam);
@@ -436,6 +437,8 @@ int zxh_measure(zxh_sim *s, size_t shots)
     s->stat_passes = 2;
     if (s->h_status->code != 0) return fail(s, int(s->h_status->code), "sampler device wait gave up");
     s->measured = shots;
+    s->measured_m = m;
+    s->cnt_ready = false;
     return ZXH_OK;
 }
 
@@ -449,6 +452,62 @@ int zxh_get_results(zxh_sim *s, uint64_t *words, size_t shots)
     CK(s, cudaMemcpyAsync(words, s->sc.words, shots * sizeof(uint64_t), cudaMemcpyDeviceToHost, s->stream),
        "copy results");
     CK(s, cudaStreamSynchronize(s->stream), "copy results");
+    return ZXH_OK;
+}
+
+int zxh_counts(zxh_sim *s, uint64_t *words, uint64_t *counts, size_t capacity, size_t *n_unique)
+{
+    if (!s || !n_unique) return ZXH_ERR_ARG;
+    *n_unique = 0;
+    if (s->measured == 0) return ZXH_OK;
+    if (words && !counts) return fail(s, ZXH_ERR_ARG, "counts: counts is null");
+    if (int rc = use_device(s)) return rc;
+    const int m = s->measured_m;
+    const uint64_t nseg = (1ULL << m) / std::min<uint64_t>(4096, 1ULL << m);
+    const size_t seg_bytes = (nseg * 8 + 255) & ~size_t(255);
+    const size_t shot_bytes = (s->measured * 8 + 255) & ~size_t(255);
+    const size_t need = 2 * seg_bytes + 256 + 2 * shot_bytes;
+    uint64_t kernels = 0;
+    if (!s->cnt_ready) {
+        if (int rc = ensure_dev(s, reinterpret_cast<void **>(&s->d_cnt), s->cnt_cap, need, "cudaMalloc(counts)"))
+            return rc;
+    }
+    auto *nuniq = reinterpret_cast<unsigned long long *>(s->d_cnt);
+    auto *uoff = reinterpret_cast<unsigned long long *>(s->d_cnt + seg_bytes);
+    auto *total = reinterpret_cast<unsigned long long *>(s->d_cnt + 2 * seg_bytes);
+    auto *dwords = reinterpret_cast<uint64_t *>(s->d_cnt + 2 * seg_bytes + 256);
+    auto *dhits = reinterpret_cast<uint64_t *>(s->d_cnt + 2 * seg_bytes + 256 + shot_bytes);
+    CK(s, cudaEventRecord(s->ev0, s->stream), "event");
+    if (!s->cnt_ready) {
+        CK(s, zxh::run_counts(s->sc, m, s->ws.map.b(), nuniq, uoff, total, dwords, dhits, 1, s->sms, s->stream,
+                              kernels),
+           "counts launch");
+        CK(s, cudaMemcpyAsync(&s->cnt_total, total, sizeof(uint64_t), cudaMemcpyDeviceToHost, s->stream),
+           "read count total");
+        CK(s, cudaStreamSynchronize(s->stream), "counts");
+        s->cnt_ready = true;
+    }
+    *n_unique = size_t(s->cnt_total);
+    if (!words) {
+        CK(s, cudaEventRecord(s->ev1, s->stream), "event");
+        CK(s, cudaStreamSynchronize(s->stream), "counts");
+        CK(s, cudaEventElapsedTime(&s->last_ms, s->ev0, s->ev1), "event time");
+        s->stat_kernels = kernels;
+        s->stat_passes = 0;
+        return ZXH_OK;
+    }
+    if (capacity < s->cnt_total) return fail(s, ZXH_ERR_LIMIT, "counts: capacity below the number of distinct outcomes");
+    CK(s, zxh::run_counts(s->sc, m, s->ws.map.b(), nuniq, uoff, total, dwords, dhits, 2, s->sms, s->stream, kernels),
+       "counts launch");
+    CK(s, cudaEventRecord(s->ev1, s->stream), "event");
+    CK(s, cudaMemcpyAsync(words, dwords, s->cnt_total * sizeof(uint64_t), cudaMemcpyDeviceToHost, s->stream),
+       "copy count words");
+    CK(s, cudaMemcpyAsync(counts, dhits, s->cnt_total * sizeof(uint64_t), cudaMemcpyDeviceToHost, s->stream),
+       "copy counts");
+    CK(s, cudaStreamSynchronize(s->stream), "counts");
+    CK(s, cudaEventElapsedTime(&s->last_ms, s->ev0, s->ev1), "event time");
+    s->stat_kernels = kernels;
+    s->stat_passes = 0;
     return ZXH_OK;
 }
 

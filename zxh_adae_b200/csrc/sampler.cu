@@ -411,7 +411,190 @@ __global__ void __launch_bounds__(kThreads) map_kernel(const uint64_t *__restric
     }
 }
 
+// ---------------------------------------------------------------------------
+// Counts: the distinct outcomes of a draw and how often each came up, without
+// copying the shots to the host. The draw leaves every shot's real index grouped
+// by segment (segments in increasing order), so counting is per segment: a
+// segment with at most kWarpMax shots sorts its offsets in one warp (bitonic
+// network over the lanes) and run-length encodes them; a heavier segment (the
+// sampler's heavy list) builds a histogram of its 2^12 offsets in shared memory.
+// Pass 1 writes each segment's number of distinct outcomes, a scan of those gives
+// every segment's first output slot, and pass 2 repeats the work and writes the
+// (virtual word, count) pairs there, in increasing real index.
+
+__device__ __forceinline__ uint32_t warp_sort32(uint32_t v, int lane)
+{
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1)
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const uint32_t o = __shfl_xor_sync(0xffffffffu, v, j);
+            const bool up = (lane & k) == 0;
+            const bool low = (lane & j) == 0;
+            v = (low == up) ? min(v, o) : max(v, o);
+        }
+    return v;
+}
+
+__device__ __forceinline__ uint64_t map_word(const uint64_t (*tab)[256], uint64_t b, uint64_t r)
+{
+    uint64_t v = b;
+#pragma unroll
+    for (int k = 0; k < 8; k++) v ^= tab[k][(r >> (8 * k)) & 255];
+    return v;
+}
+
+template <bool WRITE>
+__global__ void __launch_bounds__(kThreads) count_light_kernel(const uint64_t *__restrict__ real, uint64_t nseg,
+                                                               uint32_t seglen, const unsigned long long *counts,
+                                                               const unsigned long long *offsets,
+                                                               unsigned long long *nuniq,
+                                                               const unsigned long long *uoff,
+                                                               const uint64_t *__restrict__ coltab, uint64_t b,
+                                                               uint64_t *__restrict__ words,
+                                                               uint64_t *__restrict__ hits)
+{
+    __shared__ uint64_t tab[WRITE ? 8 : 1][256];
+    if constexpr (WRITE) {
+        for (int i = threadIdx.x; i < 8 * 256; i += kThreads) tab[i >> 8][i & 255] = coltab[i];
+        __syncthreads();
+    }
+    const int lane = threadIdx.x & 31;
+    const uint64_t gwarp = (uint64_t(blockIdx.x) * kThreads + threadIdx.x) >> 5;
+    const uint64_t nwarps = (uint64_t(gridDim.x) * kThreads) >> 5;
+    for (uint64_t g0 = gwarp * 32; g0 < nseg; g0 += nwarps * 32) {
+        const uint64_t gl = g0 + uint64_t(lane);
+        const unsigned long long cl = gl < nseg ? counts[gl] : 0ULL;
+        if (!WRITE && gl < nseg && cl == 0) nuniq[gl] = 0;
+        unsigned todo = __ballot_sync(0xffffffffu, cl != 0 && cl <= kWarpMax);
+        while (todo) {
+            const int src = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const uint64_t g = g0 + uint64_t(src);
+            const uint32_t cnt = uint32_t(__shfl_sync(0xffffffffu, cl, src));
+            const uint64_t base = g * seglen;
+            const unsigned long long off = offsets[g];
+            uint32_t key = 0xffffffffu;  // padding sorts last
+            if (uint32_t(lane) < cnt) key = uint32_t(real[off + uint64_t(lane)] - base);
+            key = warp_sort32(key, lane);
+            const uint32_t prev = __shfl_up_sync(0xffffffffu, key, 1);
+            const bool first = uint32_t(lane) < cnt && (lane == 0 || key != prev);
+            const unsigned starts = __ballot_sync(0xffffffffu, first);
+            if constexpr (!WRITE) {
+                if (lane == 0) nuniq[g] = __popc(starts);
+            } else if (first) {
+                const unsigned above = starts & ~((2u << lane) - 1u);  // lane 31: 2u << 31 wraps to 0, nothing above
+                const uint32_t next = above ? uint32_t(__ffs(above) - 1) : cnt;
+                const uint64_t slot = uoff[g] + uint64_t(__popc(starts & ((1u << lane) - 1u)));
+                words[slot] = map_word(tab, b, base + key);
+                hits[slot] = next - uint32_t(lane);
+            }
+        }
+    }
+}
+
+// heavy segment h goes to CTA h mod grid (shared histogram of seglen bins)
+template <bool WRITE>
+__global__ void __launch_bounds__(kThreads) count_heavy_kernel(const uint64_t *__restrict__ real, uint32_t seglen,
+                                                               const unsigned long long *counts,
+                                                               const unsigned long long *offsets,
+                                                               const uint32_t *heavy_list,
+                                                               const uint32_t *heavy_count,
+                                                               unsigned long long *nuniq,
+                                                               const unsigned long long *uoff,
+                                                               const uint64_t *__restrict__ coltab, uint64_t b,
+                                                               uint64_t *__restrict__ words,
+                                                               uint64_t *__restrict__ hits)
+{
+    __shared__ uint32_t hist[4096];
+    __shared__ uint32_t s_warp[kThreads / 32];
+    __shared__ uint64_t tab[WRITE ? 8 : 1][256];
+    if constexpr (WRITE) {
+        for (int i = threadIdx.x; i < 8 * 256; i += kThreads) tab[i >> 8][i & 255] = coltab[i];
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t nh = *heavy_count;
+    const uint32_t per = (seglen + kThreads - 1) / kThreads;  // bins of a thread (16 for full segments)
+    for (uint32_t h = blockIdx.x; h < nh; h += gridDim.x) {
+        const uint64_t g = heavy_list[h];
+        const unsigned long long cnt = counts[g], off = offsets[g];
+        const uint64_t base = g * seglen;
+        for (uint32_t k = threadIdx.x; k < seglen; k += kThreads) hist[k] = 0;
+        __syncthreads();
+        for (uint64_t j = threadIdx.x; j < cnt; j += kThreads) atomicAdd(&hist[uint32_t(real[off + j] - base)], 1u);
+        __syncthreads();
+        const uint32_t lo = min(seglen, uint32_t(threadIdx.x) * per), hi = min(seglen, lo + per);
+        uint32_t mine = 0;
+        for (uint32_t k = lo; k < hi; k++) mine += hist[k] != 0;
+        // block exclusive scan of the per-thread distinct counts
+        uint32_t incl = mine;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        if (lane == 31) s_warp[warp] = incl;
+        __syncthreads();
+        uint32_t before = 0, total = 0;
+        for (int w = 0; w < kThreads / 32; w++) {
+            before += w < warp ? s_warp[w] : 0;
+            total += s_warp[w];
+        }
+        if constexpr (!WRITE) {
+            if (threadIdx.x == 0) nuniq[g] = total;
+        } else {
+            uint64_t slot = uoff[g] + before + incl - mine;
+            for (uint32_t k = lo; k < hi; k++)
+                if (hist[k]) {
+                    words[slot] = map_word(tab, b, base + k);
+                    hits[slot] = hist[k];
+                    slot++;
+                }
+        }
+        __syncthreads();  // hist and s_warp are reused by the next heavy segment
+    }
+}
+
+__global__ void count_total_kernel(const unsigned long long *nuniq, const unsigned long long *uoff, uint64_t nseg,
+                                   unsigned long long *total)
+{
+    *total = uoff[nseg - 1] + nuniq[nseg - 1];
+}
+
 }  // namespace
+
+cudaError_t run_counts(const SamplerScratch &sc, int m, uint64_t b, unsigned long long *nuniq,
+                       unsigned long long *uoff, unsigned long long *total, uint64_t *words, uint64_t *hits,
+                       int pass, int sms, cudaStream_t st, uint64_t &kernels)
+{
+    const uint64_t local = 1ULL << m;
+    const uint32_t seglen = uint32_t(std::min<uint64_t>(4096, local));
+    const uint64_t nseg = local / seglen;
+    const uint64_t nblk = (nseg + kScanBlock - 1) / kScanBlock;
+    const uint64_t warps_needed = (nseg + 31) / 32;
+    const unsigned gw = unsigned(std::max<uint64_t>(1, std::min<uint64_t>((warps_needed * 32 + kThreads - 1) / kThreads,
+                                                                          uint64_t(sms) * 8)));
+    const unsigned gh = unsigned(sms) * 4;
+    if (pass == 1) {
+        count_light_kernel<false><<<gw, kThreads, 0, st>>>(sc.real, nseg, seglen, sc.counts, sc.offsets, nuniq,
+                                                           nullptr, nullptr, b, nullptr, nullptr);
+        count_heavy_kernel<false><<<gh, kThreads, 0, st>>>(sc.real, seglen, sc.counts, sc.offsets, sc.heavy_list,
+                                                           sc.heavy_count, nuniq, nullptr, nullptr, b, nullptr,
+                                                           nullptr);
+        block_sum_kernel<unsigned long long><<<unsigned(nblk), kThreads, 0, st>>>(nuniq, nseg, sc.bsum);
+        scan_small_kernel<unsigned long long><<<1, 32, 0, st>>>(sc.bsum, nblk);
+        block_scan_kernel<unsigned long long, false><<<unsigned(nblk), kThreads, 0, st>>>(nuniq, nseg, sc.bsum, uoff);
+        count_total_kernel<<<1, 1, 0, st>>>(nuniq, uoff, nseg, total);
+        kernels += 6;
+    } else {
+        count_light_kernel<true><<<gw, kThreads, 0, st>>>(sc.real, nseg, seglen, sc.counts, sc.offsets, nuniq, uoff,
+                                                          sc.coltab, b, words, hits);
+        count_heavy_kernel<true><<<gh, kThreads, 0, st>>>(sc.real, seglen, sc.counts, sc.offsets, sc.heavy_list,
+                                                          sc.heavy_count, nuniq, uoff, sc.coltab, b, words, hits);
+        kernels += 2;
+    }
+    return cudaGetLastError();
+}
 
 // One layout routine serves both the size query and the carving, so the two can
 // never disagree.

@@ -29,6 +29,14 @@ cudaError_t run_sampler(const void *state, int elem_bytes, int m, uint64_t shots
                         const uint64_t *host_coltab, uint64_t b, SamplerScratch &sc, DevStatus *status, int sms,
                         cudaStream_t st, uint64_t &kernels);
 
+// Counts of the draw left in sc by run_sampler on a 2^m-amplitude state (map
+// offset b): pass 1 writes every segment's number of distinct outcomes (nuniq),
+// their exclusive scan (uoff) and the total; pass 2 writes the distinct outcomes'
+// virtual words and counts at uoff, in increasing real index.
+cudaError_t run_counts(const SamplerScratch &sc, int m, uint64_t b, unsigned long long *nuniq,
+                       unsigned long long *uoff, unsigned long long *total, uint64_t *words, uint64_t *hits,
+                       int pass, int sms, cudaStream_t st, uint64_t &kernels);
+
 // run_sampler's draw up to real indices, into a caller buffer (noalloc.cu).
 cudaError_t run_sampler_real(const void *state, int elem_bytes, int m, uint64_t shots, uint64_t stream_seed,
                              uint64_t *real_out, SamplerScratch &sc, DevStatus *status, int sms, cudaStream_t st);

@@ -40,6 +40,14 @@ struct zxh_sim {
     size_t samp_cap = 0;
     zxh::SamplerScratch sc;
     size_t measured = 0;
+    int measured_m = 0;  // log2 amplitudes of the state the last draw read
+
+    // counts of the last draw (zxh_counts): per-segment distinct outcomes and
+    // their scan, the total, then the (word, count) pairs
+    uint8_t *d_cnt = nullptr;
+    size_t cnt_cap = 0;
+    bool cnt_ready = false;  // pass 1 ran for the current draw
+    uint64_t cnt_total = 0;
 
     void *d_out = nullptr;
     size_t out_cap = 0;
