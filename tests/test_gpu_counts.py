@@ -157,3 +157,45 @@ def test_sample_counts_matches_sampling():
     rows = s.Sampling(5000)
     assert counts == dict(Counter("".join("1" if b else "0" for b in reversed(r)) for r in rows))
     assert list(counts) == sorted(counts)
+
+
+class _Inst:
+    def __init__(self, name, qubits, params=()):
+        self.operation = type("Op", (), {"name": name, "params": list(params)})()
+        self.qubits = list(qubits)
+
+
+class _Circuit:
+    def __init__(self, n, insts):
+        self.num_qubits = n
+        self.data = insts
+
+    def find_bit(self, q):
+        return type("Bit", (), {"index": q})()
+
+
+def test_backend_run_on_the_gpu():
+    # the zxh backend's run path (seed, clear, load, execute, sample_counts)
+    b = zx.make_zxh_backend()
+    bell = _Circuit(2, [_Inst("h", [0]), _Inst("cx", [0, 1]), _Inst("measure", [0]), _Inst("measure", [1])])
+    counts = b.run(bell, shots=4000, seed_simulator=11).result().get_counts()
+    assert set(counts) == {"00", "11"} and sum(counts.values()) == 4000
+    assert abs(counts["00"] - 2000) < 200
+    again = b.run(bell, shots=4000, seed_simulator=11).result().get_counts()
+    assert again == counts
+    # the same draw through the simulator directly
+    s = zx.ZXH(2)
+    s.set_seed(11)
+    s.push_gates([(_core.H, 0, 0), (_core.CX, 0, 1)])
+    s.execute()
+    assert s.sample_counts(4000) == counts
+    # frontend gates through the host compiler
+    n = 5
+    insts = [_Inst("h", [q]) for q in range(n)] + [_Inst("swap", [0, 4]), _Inst("ccx", [1, 2, 3]),
+                                                   _Inst("ry", [2], [0.4]), _Inst("rzz", [0, 1], [0.3])]
+    b5 = zx.make_zxh_backend(dtype="complex64")
+    res = b5.run([_Circuit(n, insts)] * 2, shots=3000, seed_simulator=5, optimize_level=2).result()
+    c0, c1 = res.get_counts()
+    assert c0 == c1 and sum(c0.values()) == 3000 and all(len(k) == n for k in c0)
+    b.close()
+    b5.close()

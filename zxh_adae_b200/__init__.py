@@ -3,7 +3,8 @@
 Drop-in for the reference's ``zxhsim`` package entry points on the single-GPU
 path (src/zxh/zxhsim/__init__.py of ZXH-Sim): ``ZXH``, ``init``, ``finalize``,
 ``active``, ``rank``, ``nprocs``, ``PrintRes``, ``load_circuit`` (with the host
-circuit compiler, ``optimize_records``) and ``load_circuit_transpiled``.
+circuit compiler, ``optimize_records``), ``load_circuit_transpiled`` and
+``make_zxh_backend`` (the ``zxh`` backend's run path without Qiskit).
 """
 from __future__ import annotations
 
@@ -21,6 +22,7 @@ from ._core import (
     rank,
     version,
 )
+from .backend import make_zxh_backend
 from .loader import compile_circuit, load_circuit, load_circuit_transpiled
 
 __version__ = _core.__version__
@@ -40,4 +42,5 @@ __all__ = [
     "load_circuit",
     "compile_circuit",
     "optimize_records",
+    "make_zxh_backend",
 ]
