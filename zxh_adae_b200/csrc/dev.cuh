@@ -105,7 +105,15 @@ __device__ __forceinline__ E cmul(E a, E b)
 }
 
 // Trailing zeros of a compile-time constant (index arithmetic in unrolled loops).
-__host__ __device__ constexpr int ctz_const(int x) { return (x & 1) ? 0 : 1 + ctz_const(x >> 1); }
+// Trailing zeros of x > 0. Not recursive, so it is inlined and, inside a fully
+// unrolled loop, folds to a constant (register arrays indexed by it then stay in
+// registers; a recursive form stays a call and forces them into local memory).
+__host__ __device__ __forceinline__ constexpr int ctz_const(int x)
+{
+    int n = 0;
+    while (n < 31 && !((x >> n) & 1)) n++;
+    return n;
+}
 
 __device__ __forceinline__ int par64(uint64_t x) { return __popcll(x) & 1; }
 

@@ -126,7 +126,7 @@ __device__ __forceinline__ void apply_window(E (&x)[1 << R], const E *s_exp, int
     for (int jj = 0; jj < (1 << R); jj++) {
         const int gj = jj ^ (jj >> 1);
         if (jj > 0) {
-            const int fb = ctz_const(jj);
+            const int fb = __ffs(jj) - 1;  // a run-time index: w stays in local memory, off the registers
             acc += ((gj >> fb) & 1) ? w[fb] : -w[fb];
         }
         x[gj] = cmul(x[gj], phase_factor(s_exp, acc + qreg[gj]));
@@ -598,7 +598,7 @@ __device__ __forceinline__ void row_window(const uint8_t *blob, const DiagDev &d
         for (int jj = 0; jj < NR; jj++) {
             const int gj = jj ^ (jj >> 1);
             if (jj > 0) {
-                const int fb = ctz_const(jj);
+                const int fb = __ffs(jj) - 1;  // a run-time index: w stays in local memory, off the registers
 #pragma unroll
                 for (int v = 0; v < V; v++) a32[v] += ((gj >> fb) & 1) ? w32[fb][v] : 0u - w32[fb][v];
             }
@@ -612,7 +612,7 @@ __device__ __forceinline__ void row_window(const uint8_t *blob, const DiagDev &d
         for (int jj = 0; jj < NR; jj++) {
             const int gj = jj ^ (jj >> 1);
             if (jj > 0) {
-                const int fb = ctz_const(jj);
+                const int fb = __ffs(jj) - 1;  // a run-time index: w stays in local memory, off the registers
 #pragma unroll
                 for (int v = 0; v < V; v++) acc[v] += ((gj >> fb) & 1) ? w[fb][v] : -w[fb][v];
             }
