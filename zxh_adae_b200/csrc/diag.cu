@@ -63,6 +63,14 @@ __global__ void __launch_bounds__(kThreads) diag_kernel(const uint8_t *__restric
     __shared__ int64_t s_cross[kDiagTileMax][kDiagOut];  // [tile bit][out bit]
     __shared__ int64_t s_quad[kDiagOut][kDiagOut];       // symmetric, zero diagonal
     __shared__ int64_t s_lin[kDiagOut];
+    // complex64: the walk runs in 32-bit turns. Per out bit o: the change of every
+    // lane's (and vector slot's) lane-bit phase, of each row weight, and of each
+    // out bit's coefficient when bit o flips; and the row-only quadratic parts.
+    constexpr int C32 = (V == 2) ? kDiagOut : 1;
+    __shared__ uint32_t s_cd32[C32][32][2];           // [out bit][lane][slot]
+    __shared__ uint32_t s_cr32[C32][ROWB];            // [out bit][row bit]
+    __shared__ uint32_t s_quad32[C32][kDiagOut];      // [out bit][out bit]
+    __shared__ uint32_t s_qi32[V == 2 ? ROWS : 1];
     // PF: two tile buffers per warp, filled by TMA bulk copies one tile ahead
     extern __shared__ __align__(128) unsigned char s_tiles[];
     __shared__ __align__(8) uint64_t s_bar[WARPS][2];
@@ -127,6 +135,23 @@ __global__ void __launch_bounds__(kThreads) diag_kernel(const uint8_t *__restric
             if (int(t.i) >= F && ((tid >> (t.i - F)) & 1) && ((tid >> (t.j - F)) & 1)) acc += t.coef;
         }
         s_qi[tid] = acc;
+        if constexpr (V == 2) s_qi32[tid] = turns32(acc);
+    }
+    if constexpr (V == 2) {
+        __syncthreads();  // s_cross and s_quad are complete
+        for (int i = tid; i < kDiagOut * 64; i += kThreads) {
+            const int o = i >> 6, l = (i >> 1) & 31, v = i & 1;
+            const uint32_t e = uint32_t(v) | (uint32_t(l) << LV);
+            int64_t c = 0;
+            for (int kk = 0; kk < F && kk < kDiagTileMax; kk++)
+                if ((e >> kk) & 1) c += s_cross[kk][o];
+            s_cd32[o][l][v] = turns32(c);
+        }
+        for (int i = tid; i < kDiagOut * ROWB; i += kThreads) {
+            const int o = i / ROWB, l = i % ROWB;
+            s_cr32[o][l] = F + l < kDiagTileMax ? turns32(s_cross[F + l][o]) : 0u;
+        }
+        for (int i = tid; i < kDiagOut * kDiagOut; i += kThreads) (&s_quad32[0][0])[i] = turns32((&s_quad[0][0])[i]);
     }
     __syncthreads();
 
@@ -157,6 +182,36 @@ __global__ void __launch_bounds__(kThreads) diag_kernel(const uint8_t *__restric
             h = ((t0 >> lane) & 1) ? h + s_lin[lane] : 0;
         }
         int64_t kp = warp_sum_i64(h) + d.c0;
+        // complex64: the walk state in 32-bit turns, updated per tile from the
+        // shared 32-bit tables (no shuffles of 64-bit coefficients per tile): kp32
+        // the out-bit part, g32 this lane's out-bit coefficient, lp32 this lane's
+        // lane-bit part (both vector slots, with its tile-constant terms), w32 the
+        // row weights
+        [[maybe_unused]] uint32_t kp32 = 0, g32 = 0, lp32[V], w32[ROWB][V];
+        if constexpr (V == 2) {
+            kp32 = turns32(kp);
+            g32 = turns32(g);
+            int64_t lp[V];
+#pragma unroll
+            for (int v = 0; v < V; v++) lp[v] = qf[v] + linf[v];
+#pragma unroll
+            for (int kk = 0; kk < F; kk++) {
+                const int64_t dk = __shfl_sync(0xffffffffu, da, kk);
+#pragma unroll
+                for (int v = 0; v < V; v++) {
+                    const uint32_t e = uint32_t(v) | (uint32_t(lane) << LV);
+                    if ((e >> kk) & 1) lp[v] += dk;
+                }
+            }
+#pragma unroll
+            for (int v = 0; v < V; v++) lp32[v] = turns32(lp[v]);
+#pragma unroll
+            for (int l = 0; l < ROWB; l++) {
+                const int64_t dk = __shfl_sync(0xffffffffu, da, (F + l) & 31);
+#pragma unroll
+                for (int v = 0; v < V; v++) w32[l][v] = (l < IB) ? turns32(d.lin_in[F + l] + dk + rho[l][v]) : 0u;
+            }
+        }
 
     for (uint32_t it_t = 0; it_t < (1u << cb); it_t++, k++) {
         const uint64_t tile = t0 | uint64_t(it_t ^ (it_t >> 1));
@@ -200,10 +255,26 @@ __global__ void __launch_bounds__(kThreads) diag_kernel(const uint8_t *__restric
         if (it_t > 0) {
             const int o = __ffs(it_t) - 1;
             const bool up = (tile >> o) & 1;
-            const int64_t go = __shfl_sync(0xffffffffu, g, o);
-            kp += up ? go : -go;
-            if (lane < int(nout)) g += up ? s_quad[o][lane] : -s_quad[o][lane];
-            if (lane < int(T)) da += up ? s_cross[lane][o] : -s_cross[lane][o];
+            if constexpr (V == 2) {
+                const uint32_t go = __shfl_sync(0xffffffffu, g32, o);
+                kp32 += up ? go : 0u - go;
+                const uint32_t dq = s_quad32[o][lane];  // zero for lanes past the out bits
+                g32 += up ? dq : 0u - dq;
+                const uint2 dc = *reinterpret_cast<const uint2 *>(&s_cd32[o][lane][0]);
+                lp32[0] += up ? dc.x : 0u - dc.x;
+                lp32[1] += up ? dc.y : 0u - dc.y;
+#pragma unroll
+                for (int l = 0; l < ROWB; l++) {
+                    const uint32_t dr = s_cr32[o][l];  // zero for row bits outside the tile
+#pragma unroll
+                    for (int v = 0; v < V; v++) w32[l][v] += up ? dr : 0u - dr;
+                }
+            } else {
+                const int64_t go = __shfl_sync(0xffffffffu, g, o);
+                kp += up ? go : -go;
+                if (lane < int(nout)) g += up ? s_quad[o][lane] : -s_quad[o][lane];
+                if (lane < int(T)) da += up ? s_cross[lane][o] : -s_cross[lane][o];
+            }
         }
         if (ngen) {
             for (uint32_t q = uint32_t(lane); q < ngen; q += 32) {
@@ -212,36 +283,14 @@ __global__ void __launch_bounds__(kThreads) diag_kernel(const uint8_t *__restric
             }
             __syncwarp();
         }
-        int64_t acc[V], w[ROWB][V];
-#pragma unroll
-        for (int v = 0; v < V; v++) acc[v] = kp + qf[v] + linf[v];
-#pragma unroll
-        for (int k = 0; k < F; k++) {
-            const int64_t dk = __shfl_sync(0xffffffffu, da, k);
-#pragma unroll
-            for (int v = 0; v < V; v++) {
-                const uint32_t e = uint32_t(v) | (uint32_t(lane) << LV);
-                if ((e >> k) & 1) acc[v] += dk;
-            }
-        }
-#pragma unroll
-        for (int l = 0; l < ROWB; l++) {
-            const int64_t dk = __shfl_sync(0xffffffffu, da, (F + l) & 31);
-#pragma unroll
-            for (int v = 0; v < V; v++) w[l][v] = (l < IB) ? (d.lin_in[F + l] + dk + rho[l][v]) : 0;
-        }
-
         // 3. rows in Gray-code order: one add per amplitude walks the row bits.
         //    complex64 carries the per-amplitude phase in 32-bit turns (2 pi / 2^32
-        //    resolution, a few ulp of rounding per amplitude).
+        //    resolution; every coefficient is rounded once to that grid, so a phase
+        //    is off by at most half a step per term it sums).
         if constexpr (V == 2) {
-            uint32_t a32[V], w32[ROWB][V];
+            uint32_t a32[V];
 #pragma unroll
-            for (int v = 0; v < V; v++) {
-                a32[v] = turns32(acc[v]);
-#pragma unroll
-                for (int l = 0; l < ROWB; l++) w32[l][v] = turns32(w[l][v]);
-            }
+            for (int v = 0; v < V; v++) a32[v] = kp32 + lp32[v];
 #pragma unroll
             for (int it = 0; it < ROWS; it++) {
                 const uint32_t gi = uint32_t(it ^ (it >> 1));
@@ -253,7 +302,7 @@ __global__ void __launch_bounds__(kThreads) diag_kernel(const uint8_t *__restric
                 }
                 const uint32_t e0 = (uint32_t(lane) << LV) | (gi << F);
                 if (it >= NI || e0 >= tile_elems) continue;
-                const uint32_t qrow = turns32(s_qi[gi]);
+                const uint32_t qrow = s_qi32[gi];
                 VT x = data[it];
 #pragma unroll
                 for (int v = 0; v < V; v++) {
@@ -270,6 +319,24 @@ __global__ void __launch_bounds__(kThreads) diag_kernel(const uint8_t *__restric
                 __stcs(reinterpret_cast<VT *>(base + e0), x);
             }
         } else {
+        int64_t acc[V], w[ROWB][V];
+#pragma unroll
+        for (int v = 0; v < V; v++) acc[v] = kp + qf[v] + linf[v];
+#pragma unroll
+        for (int kk = 0; kk < F; kk++) {
+            const int64_t dk = __shfl_sync(0xffffffffu, da, kk);
+#pragma unroll
+            for (int v = 0; v < V; v++) {
+                const uint32_t e = uint32_t(v) | (uint32_t(lane) << LV);
+                if ((e >> kk) & 1) acc[v] += dk;
+            }
+        }
+#pragma unroll
+        for (int l = 0; l < ROWB; l++) {
+            const int64_t dk = __shfl_sync(0xffffffffu, da, (F + l) & 31);
+#pragma unroll
+            for (int v = 0; v < V; v++) w[l][v] = (l < IB) ? (d.lin_in[F + l] + dk + rho[l][v]) : 0;
+        }
 #pragma unroll
         for (int it = 0; it < ROWS; it++) {
             const uint32_t gi = uint32_t(it ^ (it >> 1));
