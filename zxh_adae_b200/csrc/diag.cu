@@ -38,7 +38,9 @@ constexpr int kDiagGen = 32;  // general terms handled per window (more are spli
 constexpr int kDiagOut = 32;  // out-of-tile bits of the incremental walk (2^(32 + T) amplitudes at most)
 constexpr int kDiagTileMax = 10;
 
-template <typename E, int ROWB, bool PF>
+// FULL: the tile spans all its rows (T = F + ROWB, every state of at least that
+// many bits), so no row needs a bounds check.
+template <typename E, int ROWB, bool PF, bool FULL>
 __global__ void __launch_bounds__(kThreads) diag_kernel(const uint8_t *__restrict__ blob, uint64_t doff, uint64_t toff,
                                                         uint32_t T, uint32_t nout, uint32_t cb, E *__restrict__ state,
                                                         DevStatus *status)
@@ -245,7 +247,7 @@ __global__ void __launch_bounds__(kThreads) diag_kernel(const uint8_t *__restric
         for (int it = 0; it < ROWS; it++) {
             const uint32_t gi = uint32_t(it ^ (it >> 1));
             const uint32_t e0 = (uint32_t(lane) << LV) | (gi << F);
-            if (it < NI && e0 < tile_elems) {
+            if (FULL || (it < NI && e0 < tile_elems)) {
                 if constexpr (PF) data[it] = *reinterpret_cast<const VT *>(src + e0);
                 else data[it] = __ldcs(reinterpret_cast<const VT *>(src + e0));
             }
@@ -301,21 +303,27 @@ __global__ void __launch_bounds__(kThreads) diag_kernel(const uint8_t *__restric
                     for (int v = 0; v < V; v++) a32[v] += up ? w32[fb][v] : 0u - w32[fb][v];
                 }
                 const uint32_t e0 = (uint32_t(lane) << LV) | (gi << F);
-                if (it >= NI || e0 >= tile_elems) continue;
+                if (!FULL && (it >= NI || e0 >= tile_elems)) continue;
                 const uint32_t qrow = s_qi32[gi];
                 VT x = data[it];
+                uint32_t th[V];
 #pragma unroll
-                for (int v = 0; v < V; v++) {
-                    uint32_t th = a32[v] + qrow;
-                    const uint32_t e = e0 | uint32_t(v);
-                    for (uint32_t q = 0; q < ngen; q++) {
-                        const uint32_t bb = s_gb[warp][q];
-                        const int s1 = par64(gt[q].a1_t & e) ^ int(bb & 1);
-                        const int s2 = par64(gt[q].a2_t & e) ^ int(bb >> 1);
-                        if (s1 & s2) th += turns32(gt[q].coef);
+                for (int v = 0; v < V; v++) th[v] = a32[v] + qrow;
+                if (ngen) {
+#pragma unroll
+                    for (int v = 0; v < V; v++) {
+                        const uint32_t e = e0 | uint32_t(v);
+                        for (uint32_t q = 0; q < ngen; q++) {
+                            const uint32_t bb = s_gb[warp][q];
+                            const int s1 = par64(gt[q].a1_t & e) ^ int(bb & 1);
+                            const int s2 = par64(gt[q].a2_t & e) ^ int(bb >> 1);
+                            if (s1 & s2) th[v] += turns32(gt[q].coef);
+                        }
                     }
-                    vset(x, v, cmul(vget(x, v), phase_factor32(reinterpret_cast<const float2 *>(s_exp), th)));
                 }
+#pragma unroll
+                for (int v = 0; v < V; v++)
+                    vset(x, v, cmul(vget(x, v), phase_factor32(reinterpret_cast<const float2 *>(s_exp), th[v])));
                 __stcs(reinterpret_cast<VT *>(base + e0), x);
             }
         } else {
@@ -347,7 +355,7 @@ __global__ void __launch_bounds__(kThreads) diag_kernel(const uint8_t *__restric
                 for (int v = 0; v < V; v++) acc[v] += up ? w[fb][v] : -w[fb][v];
             }
             const uint32_t e0 = (uint32_t(lane) << LV) | (gi << F);
-            if (it >= NI || e0 >= tile_elems) continue;
+            if (!FULL && (it >= NI || e0 >= tile_elems)) continue;
             const int64_t qrow = s_qi[gi];
             VT x = data[it];
 #pragma unroll
@@ -374,7 +382,7 @@ __global__ void __launch_bounds__(kThreads) diag_kernel(const uint8_t *__restric
 
 namespace {
 
-template <typename E, int ROWB, bool PF>
+template <typename E, int ROWB, bool PF, bool FULL>
 cudaError_t launch_diag(const uint8_t *dblob, uint64_t doff, uint64_t toff, int m, int chunk_bits, E *state,
                         DevStatus *status, int sms, cudaStream_t st)
 {
@@ -382,7 +390,7 @@ cudaError_t launch_diag(const uint8_t *dblob, uint64_t doff, uint64_t toff, int 
     const int T = std::min(m, Tfull);
     const int nout = m - T;
     if (nout > kDiagOut) return cudaErrorInvalidValue;
-    auto kern = diag_kernel<E, ROWB, PF>;
+    auto kern = diag_kernel<E, ROWB, PF, FULL>;
     const size_t smem = PF ? size_t(kThreads / 32) * 2 * (sizeof(E) << T) : 0;
     if (PF) {
         const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
@@ -408,8 +416,12 @@ template <typename E, int ROWB>
 cudaError_t launch_diag_pf(const uint8_t *dblob, uint64_t doff, uint64_t toff, int m, int chunk_bits, bool pf,
                            E *state, DevStatus *status, int sms, cudaStream_t st)
 {
-    return pf ? launch_diag<E, ROWB, true>(dblob, doff, toff, m, chunk_bits, state, status, sms, st)
-              : launch_diag<E, ROWB, false>(dblob, doff, toff, m, chunk_bits, state, status, sms, st);
+    const bool full = m >= (ET<E>::V == 2 ? 6 : 5) + ROWB;
+    if (full)
+        return pf ? launch_diag<E, ROWB, true, true>(dblob, doff, toff, m, chunk_bits, state, status, sms, st)
+                  : launch_diag<E, ROWB, false, true>(dblob, doff, toff, m, chunk_bits, state, status, sms, st);
+    return pf ? launch_diag<E, ROWB, true, false>(dblob, doff, toff, m, chunk_bits, state, status, sms, st)
+              : launch_diag<E, ROWB, false, false>(dblob, doff, toff, m, chunk_bits, state, status, sms, st);
 }
 
 }  // namespace

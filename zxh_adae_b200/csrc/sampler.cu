@@ -35,7 +35,6 @@ namespace {
 constexpr uint64_t kSeedShot = 0x510e527fade682d1ULL;    // measure_cuda.cu:427
 constexpr uint64_t kSeedOffset = 0x9b05688c2b3e6c1fULL;  // measure_cuda.cu:499
 constexpr int kWarpMax = 32;
-constexpr uint32_t kCtaShots = 16384;
 constexpr int kScanBlock = 4096;
 
 __device__ __forceinline__ uint64_t splitmix64(uint64_t x)
@@ -341,6 +340,21 @@ __global__ void __launch_bounds__(kThreads) resolve_warp_kernel(const E *__restr
     }
 }
 
+// Shared CDF of a heavy segment: entry k at k + k / 16, so the 16 consecutive
+// entries a thread scans sit in distinct banks across the warp.
+__device__ __forceinline__ uint32_t cdf_slot(uint32_t k) { return k + (k >> 4); }
+
+__device__ __forceinline__ uint64_t upper_index_padded(const double *cdf, uint64_t n, double tau)
+{
+    uint64_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint64_t mid = lo + (hi - lo) / 2;
+        if (cdf[cdf_slot(uint32_t(mid))] <= tau) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo >= n ? n - 1 : lo;
+}
+
 template <typename E>
 __global__ void __launch_bounds__(kThreads) resolve_cta_kernel(const E *__restrict__ state, uint32_t seglen,
                                                                const unsigned long long *counts,
@@ -349,49 +363,44 @@ __global__ void __launch_bounds__(kThreads) resolve_cta_kernel(const E *__restri
                                                                const uint32_t *heavy_list,
                                                                const uint32_t *heavy_count)
 {
-    extern __shared__ double cdf[];
-    __shared__ double s_tot[kThreads];
+    extern __shared__ double cdf[];  // cdf_slot(seglen) entries
+    __shared__ double s_warp[kThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t nh = *heavy_count;
     // heavy segment h goes to CTA h mod grid, which places all of its shots
     for (uint32_t h = blockIdx.x; h < nh; h += gridDim.x) {
         const uint64_t g = heavy_list[h];
         const unsigned long long cnt = counts[g], off = offsets[g];
-        const uint64_t nchunks = (cnt + kCtaShots - 1) / kCtaShots;
-        const uint64_t c0 = 0;
-        // build the segment CDF once for all of its shots
+        // build the segment CDF once for all of its shots: coalesced loads, a serial
+        // scan of each thread's consecutive range, a block scan of the range totals
         const E *seg = state + g * seglen;
         const uint32_t per = (seglen + kThreads - 1) / kThreads;
-        const uint32_t lo = threadIdx.x * per, hi = min(seglen, lo + per);
-        for (uint32_t k = threadIdx.x; k < seglen; k += kThreads) cdf[k] = prob(__ldg(seg + k));  // coalesced
+        const uint32_t lo = min(seglen, threadIdx.x * per), hi = min(seglen, lo + per);
+        for (uint32_t k = threadIdx.x; k < seglen; k += kThreads) cdf[cdf_slot(k)] = prob(__ldg(seg + k));
         __syncthreads();
         double run = 0.0;
         for (uint32_t k = lo; k < hi; k++) {
-            run += cdf[k];
-            cdf[k] = run;
+            run += cdf[cdf_slot(k)];
+            cdf[cdf_slot(k)] = run;
         }
-        s_tot[threadIdx.x] = run;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double acc = 0.0;
-            for (int t = 0; t < kThreads; t++) {
-                const double v = s_tot[t];
-                s_tot[t] = acc;
-                acc += v;
-            }
+        double incl = run;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
         }
+        if (lane == 31) s_warp[warp] = incl;
         __syncthreads();
-        const double add = s_tot[threadIdx.x];
-        for (uint32_t k = lo; k < hi; k++) cdf[k] += add;
+        double add = incl - run;
+        for (int w = 0; w < warp; w++) add += s_warp[w];
+        for (uint32_t k = lo; k < hi; k++) cdf[cdf_slot(k)] += add;
         __syncthreads();
-        const double total = cdf[seglen - 1];
-        for (uint64_t c = c0; c < nchunks; c++) {
-            const uint64_t j0 = c * kCtaShots, j1 = (cnt < j0 + kCtaShots ? cnt : j0 + kCtaShots);
-            for (uint64_t j = j0 + threadIdx.x; j < j1; j += kThreads) {
-                const double tau = uniform_open01(stream2 ^ (kSeedOffset + off + j)) * total;
-                real_out[off + j] = g * seglen + upper_index(cdf, seglen, tau);
-            }
+        const double total = cdf[cdf_slot(seglen - 1)];
+        for (uint64_t j = threadIdx.x; j < cnt; j += kThreads) {
+            const double tau = uniform_open01(stream2 ^ (kSeedOffset + off + j)) * total;
+            real_out[off + j] = g * seglen + upper_index_padded(cdf, seglen, tau);
         }
-        __syncthreads();
+        __syncthreads();  // cdf and s_warp are reused by the next heavy segment
     }
 }
 
@@ -691,7 +700,7 @@ cudaError_t run_sampler(const void *state, int elem_bytes, int m, uint64_t shots
         resolve_warp_kernel<double2><<<gw, kThreads, 0, st>>>(static_cast<const double2 *>(state), nseg, seglen,
                                                              sc.counts, sc.offsets, stream2, sc.real, sc.heavy_list,
                                                              sc.heavy_count, sc.parts);
-    const size_t smem = size_t(seglen) * 8;
+    const size_t smem = size_t(seglen + seglen / 16 + 1) * 8;
     const unsigned gh = unsigned(sms) * 2;
     if (elem_bytes == 8)
         resolve_cta_kernel<float2><<<gh, kThreads, smem, st>>>(static_cast<const float2 *>(state), seglen, sc.counts,
@@ -748,7 +757,7 @@ cudaError_t run_sampler_real(const void *state, int elem_bytes, int m, uint64_t 
         resolve_warp_kernel<double2><<<gw, kThreads, 0, st>>>(static_cast<const double2 *>(state), nseg, seglen,
                                                              sc.counts, sc.offsets, stream2, real_out, sc.heavy_list,
                                                              sc.heavy_count, sc.parts);
-    const size_t smem = size_t(seglen) * 8;
+    const size_t smem = size_t(seglen + seglen / 16 + 1) * 8;
     const unsigned gh = unsigned(sms) * 2;
     if (elem_bytes == 8)
         resolve_cta_kernel<float2><<<gh, kThreads, smem, st>>>(static_cast<const float2 *>(state), seglen, sc.counts,
