@@ -292,6 +292,68 @@ __global__ void __launch_bounds__(kThreads) resolve_warp_kernel(const E *__restr
             // this lane's shot
             double tau = 0.0;
             if (uint64_t(lane) < cnt) tau = uniform_open01(stream2 ^ (kSeedOffset + off + uint64_t(lane))) * total;
+            if (seglen == 4096) {
+                // full segments: the owner range is 128 amplitudes, 4 per lane; they
+                // are loaded at once and kept in registers, and the next shot's are
+                // on their way while this shot is placed (the sums run in the same
+                // order as the general path below, so the draws are the same)
+                E cur[4], nxt[4];
+                double t = __shfl_sync(0xffffffffu, tau, 0);
+                int owner = __popc(__ballot_sync(0xffffffffu, incl <= t));
+                if (owner < 32) {
+#pragma unroll
+                    for (int i = 0; i < 4; i++) cur[i] = __ldg(seg + uint32_t(owner) * 128u + uint32_t(lane) * 4u + i);
+                }
+#pragma unroll 1
+                for (int j = 0; j < int(cnt); j++) {
+                    double tn = 0.0;
+                    int on = 32;
+                    if (j + 1 < int(cnt)) {
+                        tn = __shfl_sync(0xffffffffu, tau, j + 1);
+                        on = __popc(__ballot_sync(0xffffffffu, incl <= tn));
+                        if (on < 32) {
+#pragma unroll
+                            for (int i = 0; i < 4; i++)
+                                nxt[i] = __ldg(seg + uint32_t(on) * 128u + uint32_t(lane) * 4u + i);
+                        }
+                    }
+                    uint64_t hit = seglen - 1;
+                    if (owner < 32) {
+                        const double obase = __shfl_sync(0xffffffffu, excl, owner);
+                        double p[4], sp = 0.0;
+#pragma unroll
+                        for (int i = 0; i < 4; i++) {
+                            p[i] = prob(cur[i]);
+                            sp += p[i];
+                        }
+                        double sincl = sp;
+#pragma unroll
+                        for (int o = 1; o < 32; o <<= 1) {
+                            const double v = __shfl_up_sync(0xffffffffu, sincl, o);
+                            if (lane >= o) sincl += v;
+                        }
+                        const int sl = __popc(__ballot_sync(0xffffffffu, obase + sincl <= t));
+                        uint32_t found = 4;  // past this lane's sub-range
+                        if (sl < 32 && lane == sl) {
+                            double run = obase + sincl - sp;
+#pragma unroll
+                            for (int i = 0; i < 4; i++) {
+                                run += p[i];
+                                if (found == 4 && run > t) found = uint32_t(i);
+                            }
+                        }
+                        const uint32_t fs = __shfl_sync(0xffffffffu, found, sl < 32 ? sl : 0);
+                        hit = uint64_t(owner) * 128u + (sl < 32 ? uint32_t(sl) * 4u + fs : 128u);
+                        if (hit >= seglen) hit = seglen - 1;
+                    }
+                    if (lane == 0) real_out[off + uint64_t(j)] = g * seglen + hit;
+                    t = tn;
+                    owner = on;
+#pragma unroll
+                    for (int i = 0; i < 4; i++) cur[i] = nxt[i];
+                }
+                continue;
+            }
             for (int j = 0; j < int(cnt); j++) {
                 const double t = __shfl_sync(0xffffffffu, tau, j);
                 // owner lane: first lane whose inclusive prefix exceeds t
