@@ -123,6 +123,21 @@ int zxh_execute(zxh_sim *sim);
  * execute() always restarts from |0...0>, zxh.cpp:329-338). */
 int zxh_apply(zxh_sim *sim, const zxh_gate *gates, size_t count);
 
+/* zxh_apply without waiting: plans the batch on the host, queues its upload
+ * (from one of two pinned program slots), its passes and the read-back of its
+ * status word on the handle's stream, and returns. The next call plans while this
+ * batch runs on the GPU. A step whose device wait gave up is reported by the next
+ * zxh_sync, or by the next call of any other entry point that uses the device
+ * (each settles the work in flight first). zxh_state_view / zxh_stream users
+ * order their own work after it (same stream) or call zxh_sync. zxh_last_stats
+ * reports the launches and passes of the last batch and 0 ms. No counterpart in
+ * the reference. */
+int zxh_apply_async(zxh_sim *sim, const zxh_gate *gates, size_t count);
+
+/* Waits for the zxh_apply_async work in flight; ZXH_ERR_TIMEOUT if a step's device
+ * wait gave up. ZXH_OK at once when nothing is in flight. */
+int zxh_sync(zxh_sim *sim);
+
 /* Replaces ZXH::measure (zxh.cpp:555-559, measure_common.cpp:73-92): draws shots
  * outcomes with the reference GPU sampler's uniform stream
  * (src/zxh/src/measure/measure_cuda.cu:387-516,642-691) and keeps them on the

@@ -388,3 +388,36 @@ def test_large_state_round_trip(dtype):
     ph = back[k] / abs(back[k])
     amp = 2.0 ** (-n / 2)
     assert np.max(np.abs(back - ph * amp)) < (1e-4 if dtype == "complex64" else 1e-10) * amp
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_apply_async_matches_apply(dtype):
+    # the same batches through zxh_apply and zxh_apply_async give the same state
+    # bit for bit (same plans, same kernels); a growing program forces the pinned
+    # slots and the device program to grow between steps; measure and get_state
+    # settle the work in flight themselves
+    n = 16
+    batches = [wl.diag_batch(n, 64 << (k % 4), seed=900 + k) for k in range(6)]
+    batches += [wl.u3_layer(n, seed=950 + k) for k in range(3)]
+    batches += [wl.random_circuit(n, 200, 990)]
+    a = zx.ZXH(n, dtype=dtype)
+    b = zx.ZXH(n, dtype=dtype)
+    for s in (a, b):
+        s.push_gates(wl.h_all(n))
+        s.execute()
+    for bt in batches:
+        a.apply(bt)
+        b.apply_async(bt)
+    b.sync()
+    b.sync()  # nothing in flight: returns at once
+    assert np.array_equal(a.get_state(), b.get_state())
+    for bt in batches[:3]:
+        b.apply_async(bt)
+        a.apply(bt)
+    a.set_seed(4)
+    b.set_seed(4)
+    a.measure(2000)
+    b.measure(2000)  # settles the queued batches first
+    assert np.array_equal(a.results_words(), b.results_words())
+    st = b.last_stats()
+    assert st[0] > 0

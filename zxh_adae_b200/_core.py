@@ -78,6 +78,8 @@ _sig("zxh_rx", [_P, _SZ, _D])
 _sig("zxh_push_gates", [_P, _P, _SZ])
 _sig("zxh_execute", [_P])
 _sig("zxh_apply", [_P, _P, _SZ])
+_sig("zxh_apply_async", [_P, _P, _SZ])
+_sig("zxh_sync", [_P])
 _sig("zxh_measure", [_P, _SZ])
 _sig("zxh_get_results", [_P, _P, _SZ])
 _sig("zxh_measured_count", [_P, ctypes.POINTER(_SZ)])
@@ -312,6 +314,16 @@ class ZXH:
         """Applies more gates to the current state without recording them."""
         rec = as_records(gates)
         self._ck(_lib.zxh_apply(self._h, rec.ctypes.data, len(rec)))
+
+    def apply_async(self, gates) -> None:
+        """apply() without waiting for the GPU: the next call plans while this batch
+        runs; errors surface at sync() or at the next other call."""
+        rec = as_records(gates)
+        self._ck(_lib.zxh_apply_async(self._h, rec.ctypes.data, len(rec)))
+
+    def sync(self) -> None:
+        """Waits for the apply_async work in flight."""
+        self._ck(_lib.zxh_sync(self._h))
 
     def measure(self, shots: int) -> None:
         self._ck(_lib.zxh_measure(self._h, int(shots)))

@@ -41,7 +41,7 @@ int cuda_fail(zxh_sim *s, cudaError_t e, const char *what)
 int use_device(zxh_sim *s)
 {
     CK(s, cudaSetDevice(s->device), "cudaSetDevice");
-    return ZXH_OK;
+    return zxh_sync(s);
 }
 
 int ensure_dev(zxh_sim *s, void **p, size_t &cap, size_t need, const char *what)
@@ -223,6 +223,10 @@ int zxh_destroy(zxh_sim *s)
     if (s->h_status) cudaFreeHost(s->h_status);
     if (s->d_samp) cudaFree(s->d_samp);
     if (s->d_cnt) cudaFree(s->d_cnt);
+    for (int j = 0; j < 2; j++) {
+        if (s->h_async[j]) cudaFreeHost(s->h_async[j]);
+        if (s->async_ev[j]) cudaEventDestroy(s->async_ev[j]);
+    }
     if (s->d_out) cudaFree(s->d_out);
     if (s->d_psi) cudaFree(s->d_psi);
     if (s->d_lam) cudaFree(s->d_lam);
@@ -378,25 +382,99 @@ int zxh_execute(zxh_sim *s)
     return ZXH_OK;
 }
 
+// Host planning of one batch (zxh_apply and zxh_apply_async): the plan and the
+// walk state after it.
+static int plan_batch(zxh_sim *s, const zxh_gate *gates, size_t count, zxh::Plan &pl, zxh::WalkState &ws)
+{
+    std::vector<Gate> tmp;
+    for (size_t i = 0; i < count; i++)
+        if (int rc = lower(s, gates[i], tmp)) return rc;
+    zxh::WalkState start = s->ws;
+    ws = s->ws;
+    std::vector<zxh::Op> ops;
+    std::string err;
+    if (int rc = zxh::walk(tmp.data(), tmp.size(), s->disable_x, s->M, ws, ops, err)) return fail(s, rc, err);
+    if (int rc = zxh::plan(ops, s->elem_bytes, s->pp, start, pl, err)) return fail(s, rc, err);
+    return ZXH_OK;
+}
+
 int zxh_apply(zxh_sim *s, const zxh_gate *gates, size_t count)
 {
     if (!s) return ZXH_ERR_ARG;
     if (!s->executed) return fail(s, ZXH_ERR_STATE, "zxh_apply requires zxh_execute first");
     if (count && !gates) return fail(s, ZXH_ERR_ARG, "gates is null");
     if (int rc = use_device(s)) return rc;
-    std::vector<Gate> tmp;
-    for (size_t i = 0; i < count; i++)
-        if (int rc = lower(s, gates[i], tmp)) return rc;
-    zxh::WalkState start = s->ws;
-    zxh::WalkState ws = s->ws;
-    std::vector<zxh::Op> ops;
-    std::string err;
-    if (int rc = zxh::walk(tmp.data(), tmp.size(), s->disable_x, s->M, ws, ops, err)) return fail(s, rc, err);
     zxh::Plan pl;
-    if (int rc = zxh::plan(ops, s->elem_bytes, s->pp, start, pl, err)) return fail(s, rc, err);
+    zxh::WalkState ws;
+    if (int rc = plan_batch(s, gates, count, pl, ws)) return rc;
     if (int rc = run_plan(s, pl)) return rc;
     s->ws = ws;
     s->measured = 0;
+    return ZXH_OK;
+}
+
+int zxh_apply_async(zxh_sim *s, const zxh_gate *gates, size_t count)
+{
+    if (!s) return ZXH_ERR_ARG;
+    if (!s->executed) return fail(s, ZXH_ERR_STATE, "zxh_apply_async requires zxh_execute first");
+    if (count && !gates) return fail(s, ZXH_ERR_ARG, "gates is null");
+    CK(s, cudaSetDevice(s->device), "cudaSetDevice");
+    zxh::Plan pl;
+    zxh::WalkState ws;
+    if (int rc = plan_batch(s, gates, count, pl, ws)) return rc;  // overlaps the steps in flight
+    const size_t bytes = std::max<size_t>(pl.blob.size(), 16);
+    if (bytes > s->async_cap || bytes > s->blob_cap) {
+        // growing a buffer that queued work may still read: settle first
+        if (int rc = zxh_sync(s)) return rc;
+        if (bytes > s->async_cap) {
+            for (int j = 0; j < 2; j++) {
+                if (s->h_async[j]) cudaFreeHost(s->h_async[j]);
+                s->h_async[j] = nullptr;
+            }
+            s->async_cap = 0;
+            for (int j = 0; j < 2; j++)
+                CK(s, cudaMallocHost(reinterpret_cast<void **>(&s->h_async[j]), bytes * 2), "cudaMallocHost(program)");
+            s->async_cap = bytes * 2;
+        }
+        if (int rc = ensure_dev(s, reinterpret_cast<void **>(&s->d_blob), s->blob_cap, bytes * 2,
+                                "cudaMalloc(program)"))
+            return rc;
+    }
+    const int j = s->async_slot;
+    if (!s->async_ev[j]) CK(s, cudaEventCreateWithFlags(&s->async_ev[j], cudaEventDisableTiming), "event");
+    CK(s, cudaEventSynchronize(s->async_ev[j]), "program slot");  // the upload that last read slot j has run
+    std::memcpy(s->h_async[j], pl.blob.data(), pl.blob.size());
+    if (!s->async_pending)  // a step's failure stays recorded until zxh_sync reads it
+        CK(s, cudaMemsetAsync(s->d_status, 0, sizeof(zxh::DevStatus), s->stream), "reset status");
+    CK(s, cudaMemcpyAsync(s->d_blob, s->h_async[j], pl.blob.size(), cudaMemcpyHostToDevice, s->stream),
+       "upload program");
+    CK(s, cudaEventRecord(s->async_ev[j], s->stream), "event");
+    uint64_t kernels = 0;
+    CK(s, zxh::run_passes(pl.passes, s->d_blob, s->d_state, s->elem_bytes, s->d_status, s->sms, s->stream, kernels),
+       "launch");
+    CK(s, cudaMemcpyAsync(s->h_status, s->d_status, sizeof(zxh::DevStatus), cudaMemcpyDeviceToHost, s->stream),
+       "read status");
+    s->async_slot ^= 1;
+    s->async_pending = true;
+    s->stat_kernels = kernels;
+    s->stat_passes = 0;
+    for (const zxh::Pass &p : pl.passes)
+        if (p.kind != zxh::Pass::PRODUCT) s->stat_passes++;
+    s->last_ms = 0.0f;
+    s->ws = ws;
+    s->measured = 0;
+    return ZXH_OK;
+}
+
+int zxh_sync(zxh_sim *s)
+{
+    if (!s) return ZXH_ERR_ARG;
+    if (!s->async_pending) return ZXH_OK;
+    s->async_pending = false;
+    CK(s, cudaStreamSynchronize(s->stream), "apply_async");
+    if (s->h_status->code != 0)
+        return fail(s, int(s->h_status->code),
+                    "device wait gave up (site " + std::to_string(s->h_status->where) + ")");
     return ZXH_OK;
 }
 

@@ -52,6 +52,14 @@ struct zxh_sim {
     void *d_out = nullptr;
     size_t out_cap = 0;
 
+    // zxh_apply_async: two pinned program slots (each reused once the upload that
+    // last read it has run, an event per slot) and whether work is in flight
+    uint8_t *h_async[2] = {nullptr, nullptr};
+    size_t async_cap = 0;
+    cudaEvent_t async_ev[2] = {nullptr, nullptr};
+    int async_slot = 0;
+    bool async_pending = false;
+
     uint64_t stat_kernels = 0, stat_passes = 0;
     float last_ms = 0.0f;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -73,6 +81,8 @@ constexpr double kPi = 3.14159265358979323846;
 // Records msg as the handle's (or the thread's, for a null handle) last error.
 int fail(zxh_sim *s, int code, const std::string &msg);
 int cuda_fail(zxh_sim *s, cudaError_t e, const char *what);
+// Makes the handle's device current and settles zxh_apply_async work in flight
+// (waits for it and returns the error a step recorded, if any).
 int use_device(zxh_sim *s);
 // Grows a device allocation to at least need bytes (contents are not kept).
 int ensure_dev(zxh_sim *s, void **p, size_t &cap, size_t need, const char *what);
