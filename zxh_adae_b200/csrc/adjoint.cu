@@ -5,7 +5,7 @@
 // map, a virtual X_q flips the real address by delta_q (A delta_q = e_q).
 //
 //   lambda_kernel     lambda = H psi for a sum of Z, ZZ and X terms, and <psi|H|psi>
-//                     reduced in FP64 in the same pass.
+//                     reduced in FP64 in the same pass (lambda_dev.cuh).
 //   adj_pair_kernel   one rotation (or any 2x2 gate) of the reverse sweep: its
 //                     gradient Im<lambda|G|psi> reduced in FP64, then psi and
 //                     lambda uncomputed with U^dagger, one read-modify-write of both.
@@ -15,6 +15,7 @@
 #include "adjoint.h"
 #include "core.h"
 #include "dev.cuh"
+#include "lambda_dev.cuh"
 
 #include <cuda_runtime.h>
 
@@ -48,50 +49,12 @@ __global__ void __launch_bounds__(kThreads) lambda_kernel(const E *__restrict__ 
                                                           const TermDev *__restrict__ terms, uint32_t nterms,
                                                           double *energy)
 {
-    using R = typename ET<E>::R;
-    __shared__ TermDev st[kMaxTerms];
+    __shared__ ldev::LamTables<E> t;
     __shared__ double sh[kThreads / 32];
-    __shared__ uint32_t s_nx;
-    for (uint32_t i = threadIdx.x; i < nterms; i += kThreads) st[i] = terms[i];
-    if (threadIdx.x == 0) {  // X terms come first (the host sorts them)
-        uint32_t k = 0;
-        while (k < nterms && terms[k].kind == 3) k++;
-        s_nx = k;
-    }
-    __syncthreads();
-    const uint32_t nx = s_nx;
-    // lambda is accumulated in the state's precision (it is stored in it); the
-    // energy <psi|lambda> is reduced in FP64
-    double en = 0.0;
-    for (uint64_t r = uint64_t(blockIdx.x) * kThreads + threadIdx.x; r < n; r += uint64_t(gridDim.x) * kThreads) {
-        const E p = psi[r];
-        R dg = 0, xr = 0, xi = 0;
-        uint32_t t = 0;
-        for (; t + 4 <= nx; t += 4) {  // four gathers in flight
-            const E q0 = psi[r ^ st[t].delta], q1 = psi[r ^ st[t + 1].delta];
-            const E q2 = psi[r ^ st[t + 2].delta], q3 = psi[r ^ st[t + 3].delta];
-            xr += R(st[t].coef) * q0.x + R(st[t + 1].coef) * q1.x + R(st[t + 2].coef) * q2.x + R(st[t + 3].coef) * q3.x;
-            xi += R(st[t].coef) * q0.y + R(st[t + 1].coef) * q1.y + R(st[t + 2].coef) * q2.y + R(st[t + 3].coef) * q3.y;
-        }
-        for (; t < nterms; t++) {
-            const TermDev &tm = st[t];
-            const R cf = R(tm.coef);
-            if (tm.kind == 3) {
-                const E q = psi[r ^ tm.delta];
-                xr += cf * q.x;
-                xi += cf * q.y;
-            } else {
-                int s = par64(r & tm.a0) ^ int(tm.b0);
-                if (tm.kind == 2) s ^= par64(r & tm.a1) ^ int(tm.b1);
-                dg += s ? -cf : cf;
-            }
-        }
-        E l;
-        l.x = dg * p.x + xr;
-        l.y = dg * p.y + xi;
-        if (WRITE) lam[r] = l;
-        en += double(p.x) * double(l.x) + double(p.y) * double(l.y);  // Re(conj(psi) lambda)
-    }
+    ldev::lam_load(t, terms, nterms);
+    const uint64_t gw = uint64_t(blockIdx.x) * (kThreads / 32) + (threadIdx.x >> 5);
+    const uint64_t nw = uint64_t(gridDim.x) * (kThreads / 32);
+    double en = ldev::lam_rows<E, WRITE, false>(psi, lam, 0, n, t, gw, nw);
     en = block_sum(en, sh);
     if (threadIdx.x == 0) atomicAdd(energy, en);
 }
@@ -201,7 +164,8 @@ cudaError_t run_lambda(const void *psi, void *lam, int m, int elem_bytes, const 
                        double *energy, int sms, cudaStream_t st)
 {
     const uint64_t n = 1ULL << m;
-    const unsigned grid = grid_for(n, sms);
+    // a warp takes 256 amplitudes at a time (8 per lane)
+    const unsigned grid = unsigned(std::max<uint64_t>(1, std::min<uint64_t>((n + 2047) / 2048, uint64_t(sms) * 8)));
     if (elem_bytes == 8) {
         auto p = static_cast<const float2 *>(psi);
         auto l = static_cast<float2 *>(lam);

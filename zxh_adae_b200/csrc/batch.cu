@@ -13,6 +13,7 @@
 #include "batch.h"
 #include "dev.cuh"
 #include "grow_dev.cuh"
+#include "lambda_dev.cuh"
 
 #include <algorithm>
 #include <cuda_runtime.h>
@@ -28,7 +29,7 @@ constexpr long long kSpinLimit = 1LL << 31;  // cycles a task waits for its depe
 
 template <typename E>
 struct LamShared {
-    TermDev t[kMaxTerms];
+    ldev::LamTables<E> t;
     double red[kWarps];
 };
 
@@ -80,33 +81,9 @@ template <typename E>
 __device__ __forceinline__ void lambda_body(const E *psi, E *lam, uint64_t b, uint64_t e, const TermDev *terms,
                                             uint32_t nterms, double *energy, LamShared<E> &sm)
 {
-    using R = typename ET<E>::R;
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < nterms; i += kThreads) sm.t[i] = terms[i];
-    __syncthreads();
-    double en = 0.0;
-    for (uint64_t r = b + threadIdx.x; r < e; r += kThreads) {
-        const E p = __ldcg(psi + r);
-        R dg = 0, xr = 0, xi = 0;  // lambda in the state's precision, the energy in FP64
-        for (uint32_t t = 0; t < nterms; t++) {
-            const TermDev &tm = sm.t[t];
-            const R cf = R(tm.coef);
-            if (tm.kind == 3) {
-                const E q = __ldcg(psi + (r ^ tm.delta));
-                xr += cf * q.x;
-                xi += cf * q.y;
-            } else {
-                int s = par64(r & tm.a0) ^ int(tm.b0);
-                if (tm.kind == 2) s ^= par64(r & tm.a1) ^ int(tm.b1);
-                dg += s ? -cf : cf;
-            }
-        }
-        E l;
-        l.x = dg * p.x + xr;
-        l.y = dg * p.y + xi;
-        __stcg(lam + r, l);
-        en += double(p.x) * double(l.x) + double(p.y) * double(l.y);
-    }
+    __syncthreads();  // the shared tables may still be read by a previous op
+    ldev::lam_load(sm.t, terms, nterms);
+    double en = ldev::lam_rows<E, true, true>(psi, lam, b, e, sm.t, threadIdx.x >> 5, kWarps);
     en = cta_sum(en, sm.red);
     if (threadIdx.x == 0) atomicAdd(energy, en);
 }
