@@ -483,12 +483,24 @@ int zxh_adjoint_gradient(zxh_sim *s, const zxh_term *terms, size_t nterms, size_
                           s->stream),
        "lambda launch");
     kernels++;
+    // A checkpoint is not copied back into psi: the next general strided pass
+    // reads psi from it (and writes psi); any other kernel gets the copy first.
+    const void *psi_from = nullptr;
+    auto settle_restore = [&]() -> int {
+        if (psi_from) {
+            CK(s, cudaMemcpyAsync(s->d_psi, psi_from, bytes, cudaMemcpyDeviceToDevice, s->stream),
+               "restore checkpoint");
+            psi_from = nullptr;
+        }
+        return ZXH_OK;
+    };
     for (const RevStep &r : steps) {
+        if (r.kind != RevStep::GROW && r.kind != RevStep::RESTORE)
+            if (int rc = settle_restore()) return rc;
         switch (r.kind) {
         case RevStep::RESTORE:
-            CK(s, cudaMemcpyAsync(s->d_psi, static_cast<uint8_t *>(s->d_ckpt) + r.ckpt * bytes, bytes,
-                                  cudaMemcpyDeviceToDevice, s->stream),
-               "restore checkpoint");
+            if (int rc = settle_restore()) return rc;
+            psi_from = static_cast<uint8_t *>(s->d_ckpt) + r.ckpt * bytes;
             break;
         case RevStep::PAIR:
             CK(s, zxh::run_adj_pair(s->d_psi, s->d_lam, s->elem_bytes, r.pair, d_grads + r.slot, s->sms, s->stream),
@@ -499,8 +511,9 @@ int zxh_adjoint_gradient(zxh_sim *s, const zxh_term *terms, size_t nterms, size_
             CK(s, zxh::run_grow(s->d_adj + L.grow, r.off, r.toff, int(r.gb.regs.size()), r.gb.dev.nitems, s->elem_bytes,
                                 s->d_psi, s->d_lam, d_grads, r.gb.all_real(),
                                 (s->pp.grow_staged & (s->elem_bytes == 8 ? 1 : 4)) != 0,
-                                s->d_status, s->sms, s->stream),
+                                s->d_status, s->sms, s->stream, psi_from),
                "adjoint strided launch");
+            psi_from = nullptr;
             kernels++;
             break;
         case RevStep::DIAG:
@@ -511,6 +524,7 @@ int zxh_adjoint_gradient(zxh_sim *s, const zxh_term *terms, size_t nterms, size_
             break;
         }
     }
+    if (int rc = settle_restore()) return rc;  // psi ends as the sweep's last state
     CK(s, cudaEventRecord(s->ev1, s->stream), "event");
     CK(s, cudaMemcpyAsync(s->h_status, s->d_status, sizeof(zxh::DevStatus), cudaMemcpyDeviceToHost, s->stream),
        "read status");

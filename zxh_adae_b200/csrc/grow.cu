@@ -45,18 +45,18 @@ using namespace gdev;
 template <typename E, int R, bool ADJ, bool REAL, bool PF>
 __global__ void __launch_bounds__(kThreads, (ADJ && R == 4) ? 1 : 2)
     grow_kernel(const uint8_t *__restrict__ blob, uint64_t poff, uint64_t toff, E *__restrict__ psi,
-                E *__restrict__ lam, double *grads, uint64_t nitems, DevStatus *status)
+                E *__restrict__ lam, double *grads, uint64_t nitems, DevStatus *status, const E *psi_src)
 {
     __shared__ GrowShared<E> sm;
     extern __shared__ __align__(128) uint8_t stage[];
     constexpr int WARPS = kThreads / 32;
     grow_body<E, R, ADJ, REAL, PF>(blob, poff, toff, psi, lam, grads, uint64_t(blockIdx.x) * WARPS,
-                                   uint64_t(gridDim.x) * WARPS, nitems, sm, stage, status);
+                                   uint64_t(gridDim.x) * WARPS, nitems, sm, stage, status, psi_src);
 }
 
 template <typename E, int R, bool ADJ, bool REAL, bool PF>
 cudaError_t launch_grow(const uint8_t *dblob, uint64_t poff, uint64_t toff, uint64_t nitems, E *psi, E *lam,
-                        double *grads, DevStatus *status, int sms, cudaStream_t st)
+                        double *grads, DevStatus *status, const E *psi_src, int sms, cudaStream_t st)
 {
     auto kern = grow_kernel<E, R, ADJ, REAL, PF>;
     const size_t smem = PF ? grow_stage_bytes<R, ADJ>() : 0;
@@ -69,33 +69,34 @@ cudaError_t launch_grow(const uint8_t *dblob, uint64_t poff, uint64_t toff, uint
     if (per_sm < 1) per_sm = 1;
     const uint64_t ctas = (nitems + kThreads / 32 - 1) / (kThreads / 32);
     const unsigned grid = unsigned(std::max<uint64_t>(1, std::min<uint64_t>(ctas, uint64_t(sms) * uint64_t(per_sm))));
-    kern<<<grid, kThreads, smem, st>>>(dblob, poff, toff, psi, lam, grads, nitems, status);
+    kern<<<grid, kThreads, smem, st>>>(dblob, poff, toff, psi, lam, grads, nitems, status, psi_src);
     return cudaGetLastError();
 }
 
 template <typename E, bool ADJ, bool REAL, bool PF>
 cudaError_t grow_typed(int R, const uint8_t *dblob, uint64_t poff, uint64_t toff, uint64_t nitems, E *psi, E *lam,
-                       double *grads, DevStatus *status, int sms, cudaStream_t st)
+                       double *grads, DevStatus *status, const E *psi_src, int sms, cudaStream_t st)
 {
     switch (R) {
-    case 0: return launch_grow<E, 0, ADJ, REAL, PF>(dblob, poff, toff, nitems, psi, lam, grads, status, sms, st);
-    case 1: return launch_grow<E, 1, ADJ, REAL, PF>(dblob, poff, toff, nitems, psi, lam, grads, status, sms, st);
-    case 2: return launch_grow<E, 2, ADJ, REAL, PF>(dblob, poff, toff, nitems, psi, lam, grads, status, sms, st);
-    case 3: return launch_grow<E, 3, ADJ, REAL, PF>(dblob, poff, toff, nitems, psi, lam, grads, status, sms, st);
-    case 4: return launch_grow<E, 4, ADJ, REAL, PF>(dblob, poff, toff, nitems, psi, lam, grads, status, sms, st);
+    case 0: return launch_grow<E, 0, ADJ, REAL, PF>(dblob, poff, toff, nitems, psi, lam, grads, status, psi_src, sms, st);
+    case 1: return launch_grow<E, 1, ADJ, REAL, PF>(dblob, poff, toff, nitems, psi, lam, grads, status, psi_src, sms, st);
+    case 2: return launch_grow<E, 2, ADJ, REAL, PF>(dblob, poff, toff, nitems, psi, lam, grads, status, psi_src, sms, st);
+    case 3: return launch_grow<E, 3, ADJ, REAL, PF>(dblob, poff, toff, nitems, psi, lam, grads, status, psi_src, sms, st);
+    case 4: return launch_grow<E, 4, ADJ, REAL, PF>(dblob, poff, toff, nitems, psi, lam, grads, status, psi_src, sms, st);
     default: return cudaErrorInvalidValue;
     }
 }
 
 template <typename E, bool ADJ>
 cudaError_t grow_real(bool real, bool staged, int R, const uint8_t *dblob, uint64_t poff, uint64_t toff,
-                      uint64_t nitems, E *psi, E *lam, double *grads, DevStatus *status, int sms, cudaStream_t st)
+                      uint64_t nitems, E *psi, E *lam, double *grads, DevStatus *status, const E *src, int sms,
+                      cudaStream_t st)
 {
     if (staged)
-        return real ? grow_typed<E, ADJ, true, true>(R, dblob, poff, toff, nitems, psi, lam, grads, status, sms, st)
-                    : grow_typed<E, ADJ, false, true>(R, dblob, poff, toff, nitems, psi, lam, grads, status, sms, st);
-    return real ? grow_typed<E, ADJ, true, false>(R, dblob, poff, toff, nitems, psi, lam, grads, status, sms, st)
-                : grow_typed<E, ADJ, false, false>(R, dblob, poff, toff, nitems, psi, lam, grads, status, sms, st);
+        return real ? grow_typed<E, ADJ, true, true>(R, dblob, poff, toff, nitems, psi, lam, grads, status, src, sms, st)
+                    : grow_typed<E, ADJ, false, true>(R, dblob, poff, toff, nitems, psi, lam, grads, status, src, sms, st);
+    return real ? grow_typed<E, ADJ, true, false>(R, dblob, poff, toff, nitems, psi, lam, grads, status, src, sms, st)
+                : grow_typed<E, ADJ, false, false>(R, dblob, poff, toff, nitems, psi, lam, grads, status, src, sms, st);
 }
 
 }  // namespace
@@ -112,20 +113,22 @@ int grow_adjoint_gates() { return kGrowAdjGates; }
 
 cudaError_t run_grow(const uint8_t *dblob, uint64_t poff, uint64_t toff, int R, uint64_t nitems, int elem_bytes,
                      void *psi, void *lam, double *grads, bool real, bool staged, DevStatus *status, int sms,
-                     cudaStream_t st)
+                     cudaStream_t st, const void *psi_src)
 {
     const bool adj = lam != nullptr;
     staged = staged && status != nullptr;
     if (elem_bytes == 8) {
         auto *a = static_cast<float2 *>(psi);
         auto *b = static_cast<float2 *>(lam);
-        return adj ? grow_real<float2, true>(real, staged, R, dblob, poff, toff, nitems, a, b, grads, status, sms, st)
-                   : grow_real<float2, false>(real, staged, R, dblob, poff, toff, nitems, a, b, grads, status, sms, st);
+        auto *c = static_cast<const float2 *>(psi_src);
+        return adj ? grow_real<float2, true>(real, staged, R, dblob, poff, toff, nitems, a, b, grads, status, c, sms, st)
+                   : grow_real<float2, false>(real, staged, R, dblob, poff, toff, nitems, a, b, grads, status, c, sms, st);
     }
     auto *a = static_cast<double2 *>(psi);
     auto *b = static_cast<double2 *>(lam);
-    return adj ? grow_real<double2, true>(real, staged, R, dblob, poff, toff, nitems, a, b, grads, status, sms, st)
-               : grow_real<double2, false>(real, staged, R, dblob, poff, toff, nitems, a, b, grads, status, sms, st);
+    auto *c = static_cast<const double2 *>(psi_src);
+    return adj ? grow_real<double2, true>(real, staged, R, dblob, poff, toff, nitems, a, b, grads, status, c, sms, st)
+               : grow_real<double2, false>(real, staged, R, dblob, poff, toff, nitems, a, b, grads, status, c, sms, st);
 }
 
 }  // namespace zxh

@@ -456,12 +456,16 @@ __host__ __device__ constexpr size_t grow_stage_bytes()
 // arithmetic and stores of the previous one without holding registers. stage is
 // the dynamic shared memory laid out as grow_stage_bytes; a wait that gives up
 // (after about a second) records kErrTimeout in status and ends the warp's loop.
+// psi_src (optional): psi is read from there and written to psi (the adjoint
+// sweep's first pass after a checkpoint reads the checkpoint instead of copying
+// it back first); every amplitude is read before it is written, by its own warp.
 template <typename E, int R, bool ADJ, bool REAL = false, bool PF = false>
 __device__ __forceinline__ void grow_body(const uint8_t *__restrict__ blob, uint64_t poff, uint64_t toff,
                                           E *__restrict__ psi, E *__restrict__ lam, double *grads, uint64_t first,
                                           uint64_t step, uint64_t end, GrowShared<E> &sm, uint8_t *stage = nullptr,
-                                          DevStatus *status = nullptr)
+                                          DevStatus *status = nullptr, const E *psi_src = nullptr)
 {
+    const E *ps = psi_src ? psi_src : psi;
     using VT = typename GrowCfg<E>::VT;
     using RT = typename ET<E>::R;
     constexpr int V = GrowCfg<E>::V;
@@ -562,7 +566,7 @@ __device__ __forceinline__ void grow_body(const uint8_t *__restrict__ blob, uint
         __syncwarp();
         if (lane < NS * NR) {
             const int k = lane & (NR - 1);
-            const E *src = (lane >= NR) ? lam : psi;
+            const E *src = (lane >= NR) ? lam : ps;
             const VT *row = reinterpret_cast<const VT *>(src) + (((b0 ^ s_D[k]) >> LV) & ~uint64_t(31));
             bulk_g2s(wbuf + size_t(lane) * 32, row, kGrowRowBytes, wbar);
         }
@@ -603,7 +607,7 @@ __device__ __forceinline__ void grow_body(const uint8_t *__restrict__ blob, uint
         } else {
 #pragma unroll
             for (int k = 0; k < NR; k++) {
-                x[k] = grow_load(psi, r0 ^ s_D[k], lane);
+                x[k] = grow_load(ps, r0 ^ s_D[k], lane);
                 if constexpr (ADJ) y[k] = grow_load(lam, r0 ^ s_D[k], lane);
             }
         }

@@ -63,9 +63,10 @@ cudaError_t run_set_one(void *state, int elem_bytes, cudaStream_t st);
 // gate of the pass has a real matrix (GrowBuild::all_real). staged: the form whose
 // warps copy their next item into shared memory during the current one (needs
 // status, where a wait that gives up is recorded).
+// psi_src: read psi from there (written to psi).
 cudaError_t run_grow(const uint8_t *dblob, uint64_t poff, uint64_t toff, int R, uint64_t nitems, int elem_bytes,
                      void *psi, void *lam, double *grads, bool real, bool staged, DevStatus *status, int sms,
-                     cudaStream_t st);
+                     cudaStream_t st, const void *psi_src = nullptr);
 int grow_reg_bits(int elem_bytes, bool adjoint);
 int grow_fixed_bits(int elem_bytes);
 int grow_adjoint_gates();
