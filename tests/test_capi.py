@@ -44,3 +44,22 @@ def test_create_rejects_bad_arguments_without_abort():
     assert b"1..63" in lib.zxh_last_error(None)
     assert lib.zxh_create(ctypes.byref(h), 4, 0, 0, 7, 0) == 1  # ZXH_ERR_ARG
     assert lib.zxh_create(None, 4, 0, 0, 2, 0) == 1
+
+
+def test_null_handles_are_argument_errors():
+    # every handle-taking entry point answers a null handle with ZXH_ERR_ARG before
+    # touching a device, so a caller's bookkeeping slip is an error code, not a crash
+    lib = ctypes.CDLL(str(LIB))
+    nu = ctypes.c_size_t(7)
+    calls = {
+        "zxh_execute": (None,),
+        "zxh_apply": (None, None, ctypes.c_size_t(0)),
+        "zxh_apply_async": (None, None, ctypes.c_size_t(0)),
+        "zxh_sync": (None,),
+        "zxh_measure": (None, ctypes.c_size_t(10)),
+        "zxh_get_results": (None, None, ctypes.c_size_t(1)),
+        "zxh_counts": (None, None, None, ctypes.c_size_t(0), ctypes.byref(nu)),
+        "zxh_measured_count": (None, ctypes.byref(nu)),
+    }
+    for name, args in calls.items():
+        assert getattr(lib, name)(*args) == 1, name  # ZXH_ERR_ARG
