@@ -178,24 +178,75 @@ int forward_segments(zxh_sim *s, const std::vector<size_t> &ends, double &ms, ui
     ws.init_bits = N;
     ms = 0.0;
     kernels = 0;
-    size_t a = 0;
+    // every segment is planned on the host first, its program uploaded in one
+    // copy, then all passes and checkpoint saves are queued and waited for once
+    std::vector<zxh::Plan> plans(ends.size());
+    std::vector<size_t> boff(ends.size());
+    size_t total = 0, a = 0;
     for (size_t k = 0; k < ends.size(); k++) {
         const zxh::WalkState start = ws;
         std::vector<zxh::Op> ops;
         std::string err;
         if (int rc = zxh::walk(s->gates.data() + a, ends[k] - a, false, N, ws, ops, err)) return fail(s, rc, err);
-        zxh::Plan pl;
-        if (int rc = zxh::plan(ops, s->elem_bytes, s->pp, start, pl, err)) return fail(s, rc, err);
-        if (int rc = run_plan(s, pl)) return rc;
+        if (int rc = zxh::plan(ops, s->elem_bytes, s->pp, start, plans[k], err)) return fail(s, rc, err);
         ws.fresh = false;
-        ms += double(s->last_ms);
-        kernels += s->stat_kernels;
-        if (k < nck)
-            CK(s, cudaMemcpyAsync(static_cast<uint8_t *>(s->d_ckpt) + k * bytes, s->d_state, bytes,
-                                  cudaMemcpyDeviceToDevice, s->stream),
-               "save checkpoint");
+        boff[k] = total;
+        total += (plans[k].blob.size() + 255) & ~size_t(255);
         a = ends[k];
     }
+    total = std::max<size_t>(total, 256);
+    if (total > s->stage_cap) {
+        if (s->h_stage) cudaFreeHost(s->h_stage);
+        s->h_stage = nullptr;
+        s->stage_cap = 0;
+        CK(s, cudaMallocHost(reinterpret_cast<void **>(&s->h_stage), total * 2), "cudaMallocHost(program)");
+        s->stage_cap = total * 2;
+    }
+    if (int rc = ensure_dev(s, reinterpret_cast<void **>(&s->d_blob), s->blob_cap, s->stage_cap, "cudaMalloc(program)"))
+        return rc;
+    for (size_t k = 0; k < ends.size(); k++) std::memcpy(s->h_stage + boff[k], plans[k].blob.data(), plans[k].blob.size());
+    CK(s, cudaMemcpyAsync(s->d_blob, s->h_stage, total, cudaMemcpyHostToDevice, s->stream), "upload programs");
+    CK(s, cudaMemsetAsync(s->d_status, 0, sizeof(zxh::DevStatus), s->stream), "reset status");
+    CK(s, cudaEventRecord(s->ev0, s->stream), "event");
+    // cur: where the state after the segments so far lives (the state buffer or a
+    // checkpoint slot); a general strided pass at a segment's end writes straight
+    // into the slot and the next segment's first one reads from it
+    auto ckpt = [&](size_t k) { return static_cast<void *>(static_cast<uint8_t *>(s->d_ckpt) + k * bytes); };
+    void *cur = s->d_state;
+    auto to_state = [&]() -> int {
+        if (cur != s->d_state)
+            CK(s, cudaMemcpyAsync(s->d_state, cur, bytes, cudaMemcpyDeviceToDevice, s->stream), "load checkpoint");
+        cur = s->d_state;
+        return ZXH_OK;
+    };
+    for (size_t k = 0; k < ends.size(); k++) {
+        const std::vector<zxh::Pass> &P = plans[k].passes;
+        if (!P.empty()) {
+            const void *src = nullptr;
+            if (cur != s->d_state) {
+                if (P.front().kind == zxh::Pass::GROW) src = cur;
+                else if (int rc = to_state()) return rc;
+            }
+            void *dst = (k < nck && P.back().kind == zxh::Pass::GROW) ? ckpt(k) : nullptr;
+            if (dst == src && dst) dst = nullptr;  // never in place on a slot it reads whole
+            CK(s, zxh::run_passes(P, s->d_blob + boff[k], s->d_state, s->elem_bytes, s->d_status, s->sms, s->stream,
+                                  kernels, src, dst),
+               "launch");
+            cur = dst ? dst : s->d_state;
+        }
+        if (k < nck && cur != ckpt(k))
+            CK(s, cudaMemcpyAsync(ckpt(k), cur, bytes, cudaMemcpyDeviceToDevice, s->stream), "save checkpoint");
+    }
+    if (int rc = to_state()) return rc;  // the forward output stays in the state buffer
+    CK(s, cudaEventRecord(s->ev1, s->stream), "event");
+    CK(s, cudaMemcpyAsync(s->h_status, s->d_status, sizeof(zxh::DevStatus), cudaMemcpyDeviceToHost, s->stream),
+       "read status");
+    CK(s, cudaStreamSynchronize(s->stream), "forward");
+    float fms = 0.0f;
+    CK(s, cudaEventElapsedTime(&fms, s->ev0, s->ev1), "event time");
+    ms = double(fms);
+    if (s->h_status->code != 0)
+        return fail(s, int(s->h_status->code), "device wait gave up (site " + std::to_string(s->h_status->where) + ")");
     s->executed = true;
     return ZXH_OK;
 }

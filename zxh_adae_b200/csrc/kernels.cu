@@ -516,9 +516,11 @@ cudaError_t run_set_one(void *state, int elem_bytes, cudaStream_t st)
 }
 
 cudaError_t run_passes(const std::vector<Pass> &passes, const uint8_t *dblob, void *state, int elem_bytes,
-                       DevStatus *status, int sms, cudaStream_t st, uint64_t &kernels)
+                       DevStatus *status, int sms, cudaStream_t st, uint64_t &kernels, const void *first_src,
+                       void *last_dst)
 {
-    for (const Pass &ps : passes) {
+    for (size_t i = 0; i < passes.size(); i++) {
+        const Pass &ps = passes[i];
         cudaError_t e = cudaSuccess;
         if (ps.kind == Pass::PRODUCT) {
             const uint64_t nvec = std::max<uint64_t>(1, (1ULL << ps.m) / (16 / elem_bytes));
@@ -548,8 +550,12 @@ cudaError_t run_passes(const std::vector<Pass> &passes, const uint8_t *dblob, vo
             e = cudaMemsetAsync(state, 0, bytes, st);
             if (e == cudaSuccess) e = run_set_one(state, elem_bytes, st);
         } else if (ps.kind == Pass::GROW) {
-            e = run_grow(dblob, ps.off, ps.off2, int(ps.gb.regs.size()), ps.gb.dev.nitems, elem_bytes, state, nullptr,
-                         nullptr, ps.gb.all_real(), ps.prefetch != 0, status, sms, st);
+            // out of place at the ends when asked: read the first pass from first_src,
+            // write the last pass to last_dst (reading state)
+            void *dst = (i + 1 == passes.size() && last_dst) ? last_dst : state;
+            const void *src = (i == 0 && first_src) ? first_src : (dst != state ? state : nullptr);
+            e = run_grow(dblob, ps.off, ps.off2, int(ps.gb.regs.size()), ps.gb.dev.nitems, elem_bytes, dst, nullptr,
+                         nullptr, ps.gb.all_real(), ps.prefetch != 0, status, sms, st, src);
         } else if (ps.kind == Pass::DIAG) {
             e = run_diag(dblob, ps.off, ps.off2, ps.m, elem_bytes, ps.row_bits, ps.chunk_bits, ps.prefetch != 0, state, status,
                          sms, st);

@@ -43,8 +43,12 @@ cudaError_t run_sampler_real(const void *state, int elem_bytes, int m, uint64_t 
 
 // Pass runner and get_state scatter (kernels.cu).
 struct Pass;
+// first_src / last_dst (only where the first / last pass is a general strided
+// pass): that pass reads psi from first_src / writes it to last_dst instead of
+// working on state in place.
 cudaError_t run_passes(const std::vector<Pass> &passes, const uint8_t *dblob, void *state, int elem_bytes,
-                       DevStatus *status, int sms, cudaStream_t st, uint64_t &kernels);
+                       DevStatus *status, int sms, cudaStream_t st, uint64_t &kernels, const void *first_src = nullptr,
+                       void *last_dst = nullptr);
 // prefetch: each warp stages the next tile in shared memory with a TMA bulk copy
 // while it works on the current one (waits bounded; a timeout sets status).
 cudaError_t run_diag(const uint8_t *dblob, uint64_t doff, uint64_t toff, int m, int elem_bytes, int row_bits,
