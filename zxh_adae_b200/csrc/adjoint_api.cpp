@@ -157,7 +157,9 @@ std::vector<uint8_t> pack_grow(std::vector<RevStep> &steps)
 
 // Forward pass in segments [0, ends[0]), [ends[0], ends[1]), ... with every qubit
 // expanded; the state after segment k < ends.size() - 1 is saved as checkpoint k.
-int forward_segments(zxh_sim *s, const std::vector<size_t> &ends, double &ms, uint64_t &kernels)
+// wait = false: returns once everything is queued (the caller waits, reads the
+// status word, which stays set for it, and the time between evf0 and evf1).
+int forward_segments(zxh_sim *s, const std::vector<size_t> &ends, double &ms, uint64_t &kernels, bool wait = true)
 {
     const int N = int(s->n);
     const size_t bytes = size_t(s->elem_bytes) << N;
@@ -206,8 +208,10 @@ int forward_segments(zxh_sim *s, const std::vector<size_t> &ends, double &ms, ui
         return rc;
     for (size_t k = 0; k < ends.size(); k++) std::memcpy(s->h_stage + boff[k], plans[k].blob.data(), plans[k].blob.size());
     CK(s, cudaMemcpyAsync(s->d_blob, s->h_stage, total, cudaMemcpyHostToDevice, s->stream), "upload programs");
+    if (!s->evf0) CK(s, cudaEventCreate(&s->evf0), "event");
+    if (!s->evf1) CK(s, cudaEventCreate(&s->evf1), "event");
     CK(s, cudaMemsetAsync(s->d_status, 0, sizeof(zxh::DevStatus), s->stream), "reset status");
-    CK(s, cudaEventRecord(s->ev0, s->stream), "event");
+    CK(s, cudaEventRecord(s->evf0, s->stream), "event");
     // cur: where the state after the segments so far lives (the state buffer or a
     // checkpoint slot); a general strided pass at a segment's end writes straight
     // into the slot and the next segment's first one reads from it
@@ -238,12 +242,16 @@ int forward_segments(zxh_sim *s, const std::vector<size_t> &ends, double &ms, ui
             CK(s, cudaMemcpyAsync(ckpt(k), cur, bytes, cudaMemcpyDeviceToDevice, s->stream), "save checkpoint");
     }
     if (int rc = to_state()) return rc;  // the forward output stays in the state buffer
-    CK(s, cudaEventRecord(s->ev1, s->stream), "event");
+    CK(s, cudaEventRecord(s->evf1, s->stream), "event");
+    if (!wait) {
+        s->executed = true;
+        return ZXH_OK;
+    }
     CK(s, cudaMemcpyAsync(s->h_status, s->d_status, sizeof(zxh::DevStatus), cudaMemcpyDeviceToHost, s->stream),
        "read status");
     CK(s, cudaStreamSynchronize(s->stream), "forward");
     float fms = 0.0f;
-    CK(s, cudaEventElapsedTime(&fms, s->ev0, s->ev1), "event time");
+    CK(s, cudaEventElapsedTime(&fms, s->evf0, s->evf1), "event time");
     ms = double(fms);
     if (s->h_status->code != 0)
         return fail(s, int(s->h_status->code), "device wait gave up (site " + std::to_string(s->h_status->where) + ")");
@@ -490,7 +498,9 @@ int zxh_adjoint_gradient(zxh_sim *s, const zxh_term *terms, size_t nterms, size_
     ends.push_back(count);
     double fwd_ms = 0.0;
     uint64_t kernels = 0;
-    if (int rc = forward_segments(s, ends, fwd_ms, kernels)) return rc;
+    // queued, not waited for: the reverse program is planned on the host while
+    // the forward passes run
+    if (int rc = forward_segments(s, ends, fwd_ms, kernels, false)) return rc;
 
     // reverse program
     AffineMap A = s->ws.map;
@@ -526,8 +536,8 @@ int zxh_adjoint_gradient(zxh_sim *s, const zxh_term *terms, size_t nterms, size_
            "upload phase table");
     }
 
-    // reverse sweep
-    CK(s, cudaMemsetAsync(s->d_status, 0, sizeof(zxh::DevStatus), s->stream), "reset status");
+    // reverse sweep (the status word was reset before the forward passes and
+    // keeps a forward failure)
     CK(s, cudaEventRecord(s->ev0, s->stream), "event");
     CK(s, cudaMemcpyAsync(s->d_psi, s->d_state, bytes, cudaMemcpyDeviceToDevice, s->stream), "copy state");
     CK(s, zxh::run_lambda(s->d_psi, s->d_lam, N, s->elem_bytes, d_terms, uint32_t(dt.size()), d_energy, s->sms,
@@ -587,8 +597,10 @@ int zxh_adjoint_gradient(zxh_sim *s, const zxh_term *terms, size_t nterms, size_
     if (s->h_status->code != 0)
         return fail(s, int(s->h_status->code),
                     "device wait gave up (site " + std::to_string(s->h_status->where) + ")");
-    float rev_ms = 0.0f;
+    float rev_ms = 0.0f, f_ms = 0.0f;
     CK(s, cudaEventElapsedTime(&rev_ms, s->ev0, s->ev1), "event time");
+    CK(s, cudaEventElapsedTime(&f_ms, s->evf0, s->evf1), "event time");
+    fwd_ms = double(f_ms);
     s->last_ms = float(fwd_ms + double(rev_ms));
     s->stat_kernels = kernels;
     s->stat_passes = steps.size() + 1;

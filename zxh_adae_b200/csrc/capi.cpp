@@ -233,6 +233,8 @@ int zxh_destroy(zxh_sim *s)
     if (s->d_ckpt) cudaFree(s->d_ckpt);
     if (s->d_adj) cudaFree(s->d_adj);
     if (s->ev0) cudaEventDestroy(s->ev0);
+    if (s->evf0) cudaEventDestroy(s->evf0);
+    if (s->evf1) cudaEventDestroy(s->evf1);
     if (s->ev1) cudaEventDestroy(s->ev1);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;

@@ -63,6 +63,7 @@ struct zxh_sim {
     uint64_t stat_kernels = 0, stat_passes = 0;
     float last_ms = 0.0f;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t evf0 = nullptr, evf1 = nullptr;  // the adjoint sweep's forward part
     zxh::PlanParams pp;
 
     // adjoint sweep: the reverse copy of the state, lambda, forward checkpoints,
