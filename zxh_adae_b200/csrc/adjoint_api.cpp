@@ -499,7 +499,13 @@ int zxh_adjoint_gradient(zxh_sim *s, const zxh_term *terms, size_t nterms, size_
     double fwd_ms = 0.0;
     uint64_t kernels = 0;
     // queued, not waited for: the reverse program is planned on the host while
-    // the forward passes run
+    // the forward passes run. Every return from here on waits for the stream
+    // first, so an early error never leaves queued work reading the pinned
+    // program buffer that the next call refills.
+    struct WaitOnExit {
+        zxh_sim *s;
+        ~WaitOnExit() { cudaStreamSynchronize(s->stream); }
+    } wait_on_exit{s};
     if (int rc = forward_segments(s, ends, fwd_ms, kernels, false)) return rc;
 
     // reverse program
