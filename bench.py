@@ -21,8 +21,17 @@ as one read-modify-write pass of the state. The state (8 GiB) is larger than L2
                into oracle/_ref) on a bounded sample: the same B = 4096 batch
                distribution on an 18-qubit complex128 state, timed with the
                reference's header-subtraction method, GB/s at 16 B/amplitude.
+* config2      configuration 2 in full: B in {64, 256, 1024, 4096} random p/cp and
+               the 435-pair cp cascade at 30 qubits, complex64 and complex128:
+               gates/s, passes/s, GB/s, fraction of the HBM peak, the complex64
+               fidelity error against complex128.
 * u3_layer     the U3-batch half of the 30-qubit target: one layer of U3 on every
-               qubit of the same complex64 state, its passes and GB/s per pass.
+               qubit of the same complex64 state, its passes and GB/s per pass
+               (u3_layer_c128: the same in complex128).
+* sampler      10^6 shots from the 30-qubit state (sampler_c128: complex128).
+* config1      configuration 1 (20 qubits, complex128 and complex64, 1024 shots).
+* config3      configuration 3 (32 qubits complex64: 40 x [U3 all; cz matching],
+               4 layers against complex128, the hidden-string circuit, 10^6 shots).
 * batch        configuration 5: energies and adjoint gradients of 512 uneven
                circuits, every pass as its own launch vs one persistent launch vs
                its CUDA-graph replay (autotuned), and the plain per-circuit API.
@@ -33,14 +42,23 @@ as one read-modify-write pass of the state. The state (8 GiB) is larger than L2
                (complex64 state, FP64 reductions, checkpoint every 48 parameters)
                against gradients/s of parameter shift (864 energies on the plain
                forward path, complex64), both timed on the host through the public
-               API, and the max |error| of both against FP64 central differences
-               (step 1e-6) on the complex128 forward path. Rank 0 at N = 1 only.
+               API and as summed kernel time, and the max |error| of both against
+               FP64 central differences (step 1e-6) on the complex128 forward path.
+* gpu_baseline the reference's own GPU path (its CUDA backend compiled for sm_100a
+               from its sources) timed on the same GPU on configuration 2's
+               batches, one U3 layer and 10^6 shots at 30 qubits (complex128, the
+               reference's header-subtraction method), beside this library's times
+               for the same work, and the two complex128 states compared on the
+               device. Like cpu_baseline it is a baseline leg: it runs the
+               reference, never this library's path through the oracle.
+Rank 0 at N = 1 only, for every leg after the headline.
 
-``--workload u3|adjoint|batch`` time those legs alone (the commands the
-ncu summaries under profiles/ were taken with). ``--impl reference`` runs the
-reference CPU backend alone and prints its line. Multi-GPU (``torchrun``): the
-path does not shard, each rank runs an independent replica; value is the sum over
-ranks, times are the max over ranks.
+``--workload u3|adjoint|batch|sample|config2|config3`` time those legs alone (the
+commands the ncu summaries under profiles/ were taken with). ``--impl reference``
+runs the reference CPU backend alone and prints its line; that process imports
+the workload generators without loading this library. Multi-GPU (``torchrun``):
+the path does not shard, each rank runs an independent replica; value is the sum
+over ranks, times are the max over ranks.
 """
 from __future__ import annotations
 
@@ -74,11 +92,13 @@ def parse():
     ap.add_argument("--qubits", type=int, default=N_QUBITS)
     ap.add_argument("--batch", type=int, default=BATCH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="diag", choices=["diag", "u3", "adjoint", "batch", "sample", "config3"])
+    ap.add_argument("--workload", default="diag",
+                    choices=["diag", "u3", "adjoint", "batch", "sample", "config2", "config3"])
     ap.add_argument("--no-tune", action="store_true", help="batch workload: skip the autotuner")
     ap.add_argument("--batch-count", type=int, default=512, help="batch workload: circuits")
     ap.add_argument("--no-extras", action="store_true", help="skip the U3-layer and adjoint legs of the diag line")
     ap.add_argument("--no-adjoint-checks", action="store_true", help="adjoint workload: skip parameter shift and FD")
+    ap.add_argument("--no-gpu-baseline", action="store_true", help="skip timing the reference CUDA backend")
     return ap.parse_args()
 
 
@@ -189,12 +209,33 @@ def profile_traffic(name: str):
 # --------------------------------------------------------------------------- reference CPU
 
 
+def standalone_workloads():
+    """zxh_adae_b200.workloads and the pure-numpy records module it uses, imported
+    without running the package's __init__ (which loads libzxhb200.so): the
+    reference arm generates the same gate lists but must not load this library.
+    Where the package is already imported, that module is returned."""
+    import importlib
+    import types
+
+    name = "zxh_adae_b200"
+    if name in sys.modules:
+        return importlib.import_module(name + ".workloads")
+    stub = types.ModuleType(name)
+    stub.__path__ = [str(ROOT / name)]
+    sys.modules[name] = stub
+    try:
+        return importlib.import_module(name + ".workloads")
+    finally:
+        del sys.modules[name]  # a later `import zxh_adae_b200` runs the real package
+
+
 def ref_cpu_sample(steps: int, warmup: int, batch: int):
     """Reference OpenMP backend, diag batch on a REF_SAMPLE_QUBITS-qubit state,
     header-subtracted as the reference's diag microbenchmark does
     (benchmarks/runners/diag_batch_microbench.py:209-231), 16 B/amplitude."""
     from oracle.bridge import Reference, ref_available
-    from zxh_adae_b200 import workloads as wl
+
+    wl = standalone_workloads()
 
     if not ref_available("omp"):
         return None
@@ -303,8 +344,9 @@ def adjoint_leg(local: int, n: int = 24, reps: int = 8, checkpoint_every: int = 
     }
     if checks:
         ad.energy(s64, circ, p, terms)  # warm-up of the forward path
+        ps_dev = []
         t0 = time.perf_counter()
-        g_ps = ad.parameter_shift(s64, circ, p, terms)
+        g_ps = ad.parameter_shift(s64, circ, p, terms, device_ms=ps_dev)
         t_ps = time.perf_counter() - t0
         s128 = zx.ZXH(n, dtype="complex128", device=local)
         e128 = ad.energy(s128, circ, p, terms)
@@ -314,6 +356,11 @@ def adjoint_leg(local: int, n: int = 24, reps: int = 8, checkpoint_every: int = 
             "param_shift_s": t_ps,
             "param_shift_grads_per_s": circ.nparams / t_ps,
             "speedup": t_ps / t_adj,
+            # kernel time only (execute + expectation of each of the 864 energies vs
+            # the adjoint call's kernels): the share of the speed-up that is not host work
+            "param_shift_energies": len(ps_dev),
+            "param_shift_device_s": sum(ps_dev) / 1e3,
+            "speedup_device": (sum(ps_dev) / 1e3) / (statistics.mean(dev) / 1e3),
             "energy_err_vs_c128": abs(e - e128),
             "max_abs_err_vs_fp64_fd": float(np.max(np.abs(g - fd))),
             "param_shift_max_abs_err_vs_fp64_fd": float(np.max(np.abs(g_ps - fd))),
@@ -381,34 +428,92 @@ def batch_leg(local: int, count: int = 512, seed: int = 2025, tune: bool = True,
     return d
 
 
-def fidelity_err(sim_a, sim_b) -> float:
-    """1 - |<a|b>|^2 / (<a|a><b|b>) of two simulators' states (same map and size),
-    computed on the device in FP64, chunked."""
+def _device_state(ptr: int, m: int, eb: int):
     import torch
 
     class _CAI:
-        def __init__(self, ptr, n, ts):
-            self.__cuda_array_interface__ = {"shape": (n,), "typestr": ts, "data": (ptr, False), "version": 3}
+        def __init__(self):
+            self.__cuda_array_interface__ = {"shape": (1 << m,), "typestr": "<c8" if eb == 8 else "<c16",
+                                             "data": (ptr, False), "version": 3}
 
-    def view(s):
-        ptr, m, eb, g = s.state_view()
-        return torch.as_tensor(_CAI(ptr, 1 << m, "<c8" if eb == 8 else "<c16"), device="cuda"), g
+    return torch.as_tensor(_CAI(), device="cuda")
 
-    a, ga = view(sim_a)
-    b, gb = view(sim_b)
+
+def compare_states(a, phase_a: complex, b, phase_b: complex) -> dict:
+    """max |phase_a a - phase_b b| and 1 - |<a|b>|^2 / (<a|a><b|b>) of two device
+    states (torch views, real-address order), in FP64 on the device, chunked."""
+    import torch
+
     if a.numel() != b.numel():
-        return float("nan")
+        return {"max_abs": float("nan"), "fidelity_err": float("nan")}
+    pa = torch.tensor(phase_a, dtype=torch.complex128, device="cuda")
+    pb = torch.tensor(phase_b, dtype=torch.complex128, device="cuda")
+    mx = torch.zeros((), dtype=torch.float64, device="cuda")
     acc = torch.zeros((), dtype=torch.complex128, device="cuda")
     na = torch.zeros((), dtype=torch.float64, device="cuda")
     nb = torch.zeros((), dtype=torch.float64, device="cuda")
     step = 1 << 26
     for i in range(0, a.numel(), step):
-        x = a[i:i + step].to(torch.complex128)
-        y = b[i:i + step].to(torch.complex128)
+        x = a[i:i + step].to(torch.complex128) * pa
+        y = b[i:i + step].to(torch.complex128) * pb
+        mx = torch.maximum(mx, (x - y).abs().max())
         acc += torch.vdot(y, x)
         na += (x.abs() ** 2).sum()
         nb += (y.abs() ** 2).sum()
-    return float(1.0 - abs(complex(acc)) ** 2 / (float(na) * float(nb)))
+    return {"max_abs": float(mx), "fidelity_err": float(1.0 - abs(complex(acc)) ** 2 / (float(na) * float(nb)))}
+
+
+def fidelity_err(sim_a, sim_b) -> float:
+    """1 - |<a|b>|^2 / (<a|a><b|b>) of two simulators' states (same map and size)."""
+    pa, ma, ea, ga = sim_a.state_view()
+    pb, mb, eb, gb = sim_b.state_view()
+    if ma != mb:
+        return float("nan")
+    return compare_states(_device_state(pa, ma, ea), ga, _device_state(pb, mb, eb), gb)["fidelity_err"]
+
+
+CONFIG2_BATCHES = (64, 256, 1024, 4096)
+
+
+def config2_leg(local: int, n: int = N_QUBITS, steps: int = 5, warmup: int = 2) -> dict:
+    """Configuration 2 at n qubits: an H-prepared state, then per step one batch of
+    B random p/cp gates (B in 64, 256, 1024, 4096; 50/50, angles uniform [0, 2 pi))
+    or the full controlled-phase cascade (every pair j > i, angle pi / 2^(j - i)), in
+    complex64 and complex128. Per batch: device ms (CUDA events on the library's
+    stream), ms through the blocking API (host planning included), gates/s,
+    passes/s, GB/s at 2 x state bytes per pass and the fraction of the measured HBM
+    peak; then the fidelity error of the complex64 state against the complex128
+    one after all the same batches."""
+    import zxh_adae_b200 as zx
+    from zxh_adae_b200 import workloads as wl
+
+    peak, kind = peaks()
+    keys = list(CONFIG2_BATCHES) + ["cascade"]
+    batches = {B: [wl.diag_batch(n, B, seed=7000 + 10 * B + k) for k in range(warmup + steps)]
+               for B in CONFIG2_BATCHES}
+    batches["cascade"] = [wl.cp_cascade(n)] * (warmup + steps)
+    rows = {k: {"batch": k, "gates": int(len(batches[k][0]))} for k in keys}
+    sims = {}
+    for dtype, eb in (("complex64", 8), ("complex128", 16)):
+        sim = zx.ZXH(n, dtype=dtype, device=local)
+        sim.push_gates(wl.h_all(n))
+        sim.execute()
+        for k in keys:
+            dev_ms, launches, passes, wall, _ = timed_applies(sim, batches[k], warmup, steps, None, local)
+            ms = sum(dev_ms) / steps
+            pps = passes / steps
+            gbps = pps * 2 * (1 << n) * eb / (ms / 1e3) / 1e9
+            rows[k]["c64" if eb == 8 else "c128"] = {
+                "ms": ms, "api_ms": 1e3 * wall / steps, "passes": pps, "kernels": launches / steps,
+                "gates_per_s": rows[k]["gates"] / (ms / 1e3), "passes_per_s": pps / (ms / 1e3),
+                "GBps": gbps, "frac_of_peak": gbps / peak}
+        sims[dtype] = sim
+    fid = fidelity_err(sims["complex64"], sims["complex128"])
+    for s in sims.values():
+        s.close()
+    return {"workload": f"{n}q H-prepared; per step B random p/cp (50/50) or the {n * (n - 1) // 2}-pair cp cascade",
+            "peak": peak, "peak_kind": kind, "rows": [rows[k] for k in keys],
+            "complex64_fidelity_err_vs_complex128": fid, "steps": steps, "warmup": warmup}
 
 
 def config1_leg(local: int, seed: int = 2024) -> dict:
@@ -480,43 +585,50 @@ def config3_leg(local: int, seed: int = 33) -> dict:
     return out
 
 
-def sampler_leg(local: int, n: int = N_QUBITS, shots: int = 1_000_000, steps: int = 5) -> dict:
-    """10^6 multinomial shots from an n-qubit complex64 state (H on all + one U3
-    layer); roofline = one read of the state (2^n x 8 B)."""
+def sampler_leg(local: int, n: int = N_QUBITS, shots: int = 1_000_000, steps: int = 5,
+                dtype: str = "complex64") -> dict:
+    """10^6 multinomial shots from an n-qubit state (H on all + one U3 layer);
+    roofline = one read of the state (2^n x 8 or 16 B). Device ms (CUDA events)
+    and the wall time of the measure call."""
     import zxh_adae_b200 as zx
     from zxh_adae_b200 import workloads as wl
 
-    sim = zx.ZXH(n, dtype="complex64", device=local)
+    eb = 8 if dtype == "complex64" else 16
+    sim = zx.ZXH(n, dtype=dtype, device=local)
     sim.push_gates(np.concatenate([wl.h_all(n), wl.u3_layer(n, seed=5)]))
     sim.execute()
     sim.set_seed(11)
     sim.measure(shots)
-    ms = []
+    ms, wall = [], []
     for k in range(steps):
         sim.set_seed(100 + k)
+        t0 = time.perf_counter()
         sim.measure(shots)
+        wall.append(time.perf_counter() - t0)
         ms.append(sim.last_stats()[2])
     kernels = sim.last_stats()[0]
-    # counts of the last draw: on the device (zxh_counts: only the distinct
-    # outcomes cross to the host) vs every shot copied and np.unique'd on the host
-    cw, hw = [], []
-    for k in range(3):
-        t0 = time.perf_counter()
-        words, cnt = sim.counts_words()
-        cw.append(time.perf_counter() - t0)
-        t0 = time.perf_counter()
-        hk, hc = np.unique(sim.results_words(), return_counts=True)
-        hw.append(time.perf_counter() - t0)
-    same = bool(np.array_equal(words, hk) and np.array_equal(cnt, hc.astype(np.uint64)))
+    out = {}
+    if dtype == "complex64":
+        # counts of the last draw: on the device (zxh_counts: only the distinct
+        # outcomes cross to the host) vs every shot copied and np.unique'd on the host
+        cw, hw = [], []
+        for k in range(3):
+            t0 = time.perf_counter()
+            words, cnt = sim.counts_words()
+            cw.append(time.perf_counter() - t0)
+            t0 = time.perf_counter()
+            hk, hc = np.unique(sim.results_words(), return_counts=True)
+            hw.append(time.perf_counter() - t0)
+        same = bool(np.array_equal(words, hk) and np.array_equal(cnt, hc.astype(np.uint64)))
+        out["counts"] = {"distinct": int(len(words)), "device_counts_wall_ms": min(cw) * 1e3,
+                         "host_unique_wall_ms": min(hw) * 1e3, "identical": same}
     sim.close()
     t = statistics.median(ms)
     peak, kind = peaks()
-    gbps = (1 << n) * 8 / (t / 1e3) / 1e9
-    return {"workload": f"{shots} shots from a {n}-qubit complex64 state (H all + one U3 layer)", "ms": t,
-            "shots_per_s": shots / (t / 1e3), "state_read_GBps": gbps, "frac_of_peak": gbps / peak,
-            "kernels": kernels, "bytes": "one read of the state",
-            "counts": {"distinct": int(len(words)), "device_counts_wall_ms": min(cw) * 1e3,
-                       "host_unique_wall_ms": min(hw) * 1e3, "identical": same}}
+    gbps = (1 << n) * eb / (t / 1e3) / 1e9
+    return {"workload": f"{shots} shots from a {n}-qubit {dtype} state (H all + one U3 layer)", "ms": t,
+            "api_ms": 1e3 * statistics.median(wall), "shots_per_s": shots / (t / 1e3), "state_read_GBps": gbps,
+            "frac_of_peak": gbps / peak, "kernels": kernels, "bytes": "one read of the state", **out}
 
 
 def timed_applies(sim, batches, warmup, steps, pg, local):
@@ -564,31 +676,137 @@ def timed_async(n, dtype, local, batches, warmup, steps, pg) -> float:
     return wall
 
 
-def u3_leg(local: int, n: int = N_QUBITS, steps: int = 5, warmup: int = 3) -> dict:
-    """One U3 layer (U3 on every qubit) per step on the n-qubit complex64 state."""
+def u3_leg(local: int, n: int = N_QUBITS, steps: int = 5, warmup: int = 3, dtype: str = "complex64") -> dict:
+    """One U3 layer (U3 on every qubit) per step on the n-qubit state; complex64
+    also reports its fidelity error against the same layers in complex128."""
     import zxh_adae_b200 as zx
     from zxh_adae_b200 import workloads as wl
 
-    sim = zx.ZXH(n, dtype="complex64", device=local)
+    eb = 8 if dtype == "complex64" else 16
+    sim = zx.ZXH(n, dtype=dtype, device=local)
     sim.push_gates(wl.h_all(n))
     sim.execute()
     layers = [wl.u3_layer(n, seed=500 + k) for k in range(warmup + steps)]
     dev_ms, launches, passes, wall, _ = timed_applies(sim, layers, warmup, steps, None, local)
-    ref = zx.ZXH(n, dtype="complex128", device=local)
-    ref.push_gates(np.concatenate([wl.h_all(n)] + layers))
-    ref.execute()
-    fid = fidelity_err(sim, ref)
-    ref.close()
+    fid = None
+    if dtype == "complex64":
+        ref = zx.ZXH(n, dtype="complex128", device=local)
+        ref.push_gates(np.concatenate([wl.h_all(n)] + layers))
+        ref.execute()
+        fid = fidelity_err(sim, ref)
+        ref.close()
     sim.close()
-    state = (1 << n) * 8
+    state = (1 << n) * eb
     ms = sum(dev_ms) / steps
     gbps = (passes / steps) * 2 * state / (ms / 1e3) / 1e9
     peak, kind = peaks()
-    return {"workload": f"U3 on all {n} qubits of a complex64 state, random angles, one layer per step",
-            "ms_per_layer": ms, "passes_per_layer": passes / steps, "kernels_per_layer": launches / steps,
-            "gates_per_s": n / (ms / 1e3), "passes_per_s": (passes / steps) / (ms / 1e3),
-            "pass_GBps": gbps, "frac_of_peak": gbps / peak, "peak": peak, "peak_kind": kind,
-            "fidelity_err_vs_complex128": fid, "bytes": "2 x state per pass (one read and one write)"}
+    return {"workload": f"U3 on all {n} qubits of a {dtype} state, random angles, one layer per step",
+            "ms_per_layer": ms, "api_ms_per_layer": 1e3 * wall / steps, "passes_per_layer": passes / steps,
+            "kernels_per_layer": launches / steps, "gates_per_s": n / (ms / 1e3),
+            "passes_per_s": (passes / steps) / (ms / 1e3), "pass_GBps": gbps, "frac_of_peak": gbps / peak,
+            "layer_GBps": 2 * state / (ms / 1e3) / 1e9, "layer_frac_of_peak": 2 * state / (ms / 1e3) / 1e9 / peak,
+            "peak": peak, "peak_kind": kind, "fidelity_err_vs_complex128": fid,
+            "bytes": "2 x state per pass (one read and one write)"}
+
+
+def gpu_baseline_leg(local: int, ours: dict, n: int = N_QUBITS, seed: int = 4242) -> dict:
+    """The reference's own GPU path, timed on this GPU: ZXH-Sim's CUDA backend
+    (kernel_cuda.cu / measure_cuda.cu, compiled for sm_100a from the reference's
+    sources into oracle/_ref; complex128 only) on configuration 2's batches, one
+    U3 layer on all n qubits and 10^6 shots, n = 30. Its execute() ends with a
+    device synchronize (zxh.cpp:550-551), so each item is timed on the host with
+    the reference's header-subtraction method (diag_batch_microbench.py:209-231):
+    an H-on-all header run and the header + item run, alternated H F F H, and
+    the item's time is the mean of the two differences. Beside each item: this
+    library's complex128 and complex64 times for the same work (device and
+    through the blocking API, from the legs above) and the ratios. After the
+    B = 4096 and U3-layer items, the reference's state and this library's
+    complex128 state for the same gate list are compared on the device."""
+    from oracle.bridge import Reference, ref_available
+    from zxh_adae_b200 import workloads as wl
+    import zxh_adae_b200 as zx
+
+    if not ref_available("cuda"):
+        return {"unavailable": "reference CUDA backend not built (oracle/_ref/libzxhref_cuda.so)"}
+    out = {"backend": "reference cuda (kernel_cuda.cu, measure_cuda.cu), sm_100a, complex128",
+           "method": "header-subtracted execute() wall time, H F F H", "qubits": n, "items": []}
+    header = wl.h_all(n)
+    hs = Reference(n, backend="cuda")
+    hs.push(header)
+    hs.execute()
+
+    def ex(sim):
+        t0 = time.perf_counter()
+        sim.execute()
+        return time.perf_counter() - t0
+
+    def item(name, gates, ours_c128, ours_c64, compare=False):
+        fs = Reference(n, backend="cuda")
+        fs.push(np.concatenate([header, gates]))
+        fs.execute()  # first run: allocation and first launches
+        h1, f1, f2, h2 = ex(hs), ex(fs), ex(fs), ex(hs)
+        t = max(1e-9, 0.5 * ((f1 - h1) + (f2 - h2)))
+        rec = {"item": name, "gates": int(len(gates)), "reference_ms": 1e3 * t,
+               "reference_GBps": 2 * (1 << n) * 16 / t / 1e9}
+        for tag, d in (("c128", ours_c128), ("c64", ours_c64)):
+            if d:
+                rec[f"ours_{tag}_ms"] = d["ms"]
+                rec[f"ours_{tag}_api_ms"] = d["api_ms"]
+                rec[f"speedup_{tag}_device"] = 1e3 * t / d["ms"]
+                rec[f"speedup_{tag}_api"] = 1e3 * t / d["api_ms"]
+        if compare:  # parity at full size: the same gate list through this library
+            s = zx.ZXH(n, dtype="complex128", device=local)
+            s.push_gates(np.concatenate([header, gates]))
+            s.execute()
+            ptr, m, eb, g = s.state_view()
+            found = fs.device_state()
+            if found is None:
+                rec["parity"] = "reference state probe failed its layout checks"
+            else:
+                rptr, rm, rg = found
+                rec["parity_live_bits_equal"] = bool(rm == m)
+                if rm == m:
+                    rec["parity_vs_ours_c128"] = compare_states(_device_state(ptr, m, eb), g,
+                                                                _device_state(rptr, rm, 16), rg)
+            s.close()
+        return fs, rec
+
+    rows = {r["batch"]: r for r in ours.get("config2", {}).get("rows", [])}
+    for B in CONFIG2_BATCHES:
+        r = rows.get(B, {})
+        fs, rec = item(f"diag B={B}", wl.diag_batch(n, B, seed=seed + B), r.get("c128"), r.get("c64"),
+                       compare=(B == 4096))
+        out["items"].append(rec)
+        del fs
+    r = rows.get("cascade", {})
+    fs, rec = item("cp cascade", wl.cp_cascade(n), r.get("c128"), r.get("c64"))
+    out["items"].append(rec)
+    del fs
+    u64, u128 = ours.get("u3_layer"), ours.get("u3_layer_c128")
+    conv = (lambda d: {"ms": d["ms_per_layer"], "api_ms": d["api_ms_per_layer"]} if d else None)
+    fs, rec = item("U3 layer", wl.u3_layer(n, seed=seed), conv(u128), conv(u64), compare=True)
+    out["items"].append(rec)
+    # 10^6 shots from the U3-layer state: the reference's measure() (draw + result
+    # copy to the host) on the host clock, against this library's measure call
+    shots = 1_000_000
+    fs.measure(1, shots)
+    walls = []
+    for k in range(3):
+        t0 = time.perf_counter()
+        fs.measure(100 + k, shots)
+        fs.device_sync()
+        walls.append(time.perf_counter() - t0)
+    rec = {"item": f"{shots} shots", "reference_ms": 1e3 * min(walls)}
+    for tag, key in (("c128", "sampler_c128"), ("c64", "sampler")):
+        d = ours.get(key)
+        if d:
+            rec[f"ours_{tag}_ms"] = d["ms"]
+            rec[f"ours_{tag}_api_ms"] = d["api_ms"]
+            rec[f"speedup_{tag}_device"] = rec["reference_ms"] / d["ms"]
+            rec[f"speedup_{tag}_api"] = rec["reference_ms"] / d["api_ms"]
+    out["items"].append(rec)
+    del fs, hs
+    return out
 
 
 def run_ours(args):
@@ -604,6 +822,10 @@ def run_ours(args):
     if args.workload == "config3":
         if rank == 0:
             print(json.dumps({"metric": METRIC, "workload": "config3", **config3_leg(local)}))
+        return
+    if args.workload == "config2":
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "workload": "config2", **config2_leg(local, n)}))
         return
     if args.workload == "sample":
         if rank == 0:
@@ -661,11 +883,17 @@ def run_ours(args):
             if cpu is not None:
                 cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
         if not args.no_extras and args.workload == "diag":
+            extras["config2"] = config2_leg(local, n)
             extras["u3_layer"] = u3_leg(local, n)
+            extras["u3_layer_c128"] = u3_leg(local, n, dtype="complex128")
             extras["sampler"] = sampler_leg(local, n)
+            extras["sampler_c128"] = sampler_leg(local, n, dtype="complex128")
             extras["config1"] = config1_leg(local)
+            extras["config3"] = config3_leg(local)
             extras["adjoint"] = adjoint_leg(local)
             extras["batch"] = batch_leg(local)
+            if not args.no_gpu_baseline:
+                extras["gpu_baseline"] = gpu_baseline_leg(local, extras, n)
     if rank != 0:
         return
     line = {

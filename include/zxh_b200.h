@@ -190,9 +190,10 @@ int zxh_stream(zxh_sim *sim, void **stream);
 int zxh_last_stats(const zxh_sim *sim, uint64_t *kernels, uint64_t *passes, double *device_ms);
 
 /* Multinomial sampler that allocates nothing, for callers that cannot call
- * cudaMalloc (inside a CUDA graph capture region, in a process whose device
- * memory is reserved once up front, or on a latency path that must not take the
- * allocator's locks). No counterpart in the reference. It draws shots outcomes
+ * cudaMalloc (a process whose device memory is reserved once up front, a
+ * framework whose own allocator owns the device, or a latency path that must not
+ * take the CUDA allocator's locks). No counterpart in the reference: it has no
+ * counterpart to replace. It draws shots outcomes
  * from the 2^m_bits-amplitude device state `state` (dtype ZXH_C64 or ZXH_C128,
  * interleaved re/im, real-address order) with the same uniform stream and the
  * same output order as zxh_measure after zxh_set_seed(seed), and writes the
@@ -203,8 +204,9 @@ int zxh_last_stats(const zxh_sim *sim, uint64_t *kernels, uint64_t *passes, doub
  * working memory is one 2.25 MiB file-scope device array that every GPU loading
  * the library holds until exit and that all calls on a device share: calls that
  * overlap on the GPU race and must be serialised by the caller. The first call on
- * a device resolves that array's address (cudaGetSymbolAddress); make it before
- * any stream capture. Errors are reported through zxh_last_error(NULL). */
+ * a device resolves that array's address (cudaGetSymbolAddress) and keeps it for
+ * the process; make that first call before any stream capture, and make no call
+ * after a cudaDeviceReset. Errors are reported through zxh_last_error(NULL). */
 int zxh_sample_noalloc(const void *state, int dtype, size_t m_bits, uint64_t seed, size_t shots, uint64_t *real_out,
                        void *stream);
 
@@ -269,7 +271,11 @@ int zxh_batch_gradient_offsets(const zxh_batch *batch, size_t *offsets);
 int zxh_batch_run(zxh_batch *batch, int mode, double *energies, double *grads, size_t ngrads);
 /* Knobs: grow_regs (1..4, gates with high deltas per general strided pass),
  * task_items (pass items per task), task_elems (amplitudes per task of the
- * element-wise passes). Setting one recompiles the batch. */
+ * element-wise passes); setting one of these recompiles the batch.
+ * wait_limit_log2 (0..31, default 31): a persistent task waits at most
+ * 2^wait_limit_log2 SM clocks for the previous pass of its circuit, then the run
+ * ends early and zxh_batch_run returns ZXH_ERR_TIMEOUT; the handle stays usable
+ * (the next run starts from scratch). Small values exist to test that path. */
 int zxh_batch_set(zxh_batch *batch, const char *name, int value);
 int zxh_batch_get(const zxh_batch *batch, const char *name, int *value);
 /* Times the persistent launch over grow_regs in {2, 3, 4} x task_items in {32,

@@ -158,6 +158,11 @@ class Reference:
             L.zxhref_required_M.restype = _SZ
             L.zxhref_get_state.argtypes = [_P, _P]
             L.zxhref_sample.argtypes = [_P, ctypes.c_uint64, _SZ, _P]
+            L.zxhref_measure.argtypes = [_P, ctypes.c_uint64, _SZ]
+            if backend == "cuda":
+                L.zxhref_device_state.argtypes = [_P, ctypes.POINTER(_P), ctypes.POINTER(_SZ),
+                                                  ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+                L.zxhref_device_sync.restype = ctypes.c_int
             cls._libs[backend] = L
         return cls._libs[backend]
 
@@ -187,6 +192,25 @@ class Reference:
         out = np.zeros(1 << self.n, np.complex128)
         self.L.zxhref_get_state(self.h, out.ctypes.data)
         return out
+
+    def measure(self, seed: int, shots: int) -> None:
+        """set_seed + measure only (the draw stays in the reference's cache)."""
+        self.L.zxhref_measure(self.h, seed, shots)
+
+    def device_state(self):
+        """cuda backend: (device pointer, live real-address bits m, global phase) of the
+        state after execute(); the 2^m complex128 amplitudes are in real-address order.
+        None when the probe's layout checks fail."""
+        ptr, m = _P(), _SZ(0)
+        re, im = ctypes.c_double(), ctypes.c_double()
+        if self.L.zxhref_device_state(self.h, ctypes.byref(ptr), ctypes.byref(m), ctypes.byref(re),
+                                      ctypes.byref(im)) != 0:
+            return None
+        return int(ptr.value), int(m.value), complex(re.value, im.value)
+
+    def device_sync(self) -> None:
+        if self.L.zxhref_device_sync() != 0:
+            raise RuntimeError("reference device synchronize failed")
 
     def sample(self, seed: int, shots: int) -> np.ndarray:
         wc = (self.n + 63) // 64

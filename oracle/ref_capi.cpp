@@ -91,6 +91,14 @@ void zxhref_get_state(void *h, double *out)
     std::memcpy(out, st.data(), st.size() * sizeof(val_t));
 }
 
+// set_seed + measure alone (zxh.cpp:216-220,555-559): the draw, for timing.
+void zxhref_measure(void *h, uint64_t seed, size_t shots)
+{
+    ZXH &s = *static_cast<ZXH *>(h);
+    s.set_seed(seed);
+    s.measure(shots);
+}
+
 // set_seed + measure + get_results (zxh.cpp:216-220,555-564); packs each result
 // into ceil(n/64) words, bit q = virtual qubit q.
 void zxhref_sample(void *h, uint64_t seed, size_t shots, uint64_t *words)

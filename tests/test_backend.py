@@ -129,5 +129,6 @@ def test_reset_clears_recorded_gates():
 def test_make_zxh_backend_exported():
     import zxh_adae_b200 as zx
     b = zx.make_zxh_backend(disable_x=True, dtype="complex64")
-    assert isinstance(b, bk.Backend) and b.name == "zxh" and b._disable_x and b._dtype == "complex64"
+    assert isinstance(b, bk.Backend) and b.name == "zxh"
+    assert b._build["disable_x"] and b._build["dtype"] == "complex64"
     assert _core.ZXH.clear_seed  # the seed path the backend prefers exists on the simulator

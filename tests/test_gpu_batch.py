@@ -59,6 +59,40 @@ def test_batch_energies_match_oracle():
         assert abs(e[k] - ob.oracle_energy(n, rec, terms)) < 1e-11
 
 
+def _param_circuit(n, rec):
+    """The records as an adjoint.Circuit whose parameters are the angles of the
+    parameterised records (P, CP, RZ, RY = U3(theta, 0, 0)), one each."""
+    from zxh_adae_b200 import adjoint as ad
+    par, vals = [], []
+    for r in rec:
+        t = int(r["type"])
+        ry = t == _core.U3 and r["lam"] == 0.0 and r["phi"] == 0.0
+        if t in (_core.P, _core.CP, _core.RZ) or ry:
+            par.append(len(vals))
+            vals.append(float(r["theta"]))
+        else:
+            par.append(-1)
+    return ad.Circuit(n, rec, par), np.array(vals)
+
+
+@pytest.mark.parametrize("dtype,tol", [("complex128", 1e-6), ("complex64", 1e-5)])
+def test_batch_gradients_match_oracle_central_differences(dtype, tol):
+    circ = wl.batch_tfim(3, 8, nmin=6, nmax=8, layers=2)
+    c8 = mixed_circuit(8, 71)
+    p8 = np.random.default_rng(71).uniform(-math.pi, math.pi, c8.nparams)
+    circ.append((8, c8.records(p8), random_terms(8, 72)))
+    b = Batch([(c[0], c[1], c[2]) for c in circ], dtype=dtype)
+    e, g = b.run("persistent")
+    per = b.gradients(g)
+    for k, (n, rec, terms, *_) in enumerate(circ):
+        c, p = (c8, p8) if k == len(circ) - 1 else _param_circuit(n, rec)
+        which = sorted({0, 1, c.nparams // 3, c.nparams // 2, c.nparams - 2, c.nparams - 1})
+        fd = ob.oracle_central_difference(n, c, p, terms, 1e-6, which)
+        got = c.gradient(per[k])
+        assert abs(e[k] - ob.oracle_energy(n, c.records(p), terms)) < (1e-11 if dtype == "complex128" else 1e-5)
+        assert np.max(np.abs(got[which] - fd[which])) < tol, (k, got[which], fd[which])
+
+
 def test_batch_complex64_against_complex128():
     circ = small_batch(seed=5)
     e_ref, g_ref = per_circuit(circ)
@@ -107,3 +141,32 @@ def test_batch_pass_set_on_one_simulator(dtype):
         s.execute()
         err = np.max(np.abs(s.get_state().astype(np.complex128) - o.get_state()))
         assert err <= (1e-12 if dtype == "complex128" else 1e-6)
+
+
+def test_batch_task_wait_gives_up_and_the_handle_recovers():
+    # The persistent kernel's bounded wait (a task waiting for the previous pass of
+    # its circuit) capped at 2^0 SM clocks: the first task that finds its
+    # predecessor unfinished gives up at once, records a timeout in the status
+    # word and its CTA ends; the others give up the same way when they reach a
+    # task whose predecessor will not finish. Nothing faults; the call returns
+    # ZXH_ERR_TIMEOUT and the next run, with the limit restored, is exact.
+    circ = wl.batch_tfim(4, 9, nmin=10, nmax=12, layers=3)
+    b = Batch([(c[0], c[1], c[2]) for c in circ], dtype="complex128")
+    e0, g0 = b.run("persistent")
+    b.set("wait_limit_log2", 0)
+    assert b.get("wait_limit_log2") == 0
+    gave_up = 0
+    for _ in range(4):  # a wait is met on the first run in practice; a few tries make it certain
+        try:
+            b.run("persistent")
+        except RuntimeError as ex:
+            assert "gave up" in str(ex)
+            gave_up += 1
+            break
+    assert gave_up == 1
+    b.set("wait_limit_log2", 31)
+    for mode in ("persistent", "graph"):
+        e1, g1 = b.run(mode)
+        assert np.max(np.abs(e1 - e0)) < 1e-12 and np.max(np.abs(g1 - g0)) < 1e-12
+    with pytest.raises(ValueError):
+        b.set("wait_limit_log2", 32)

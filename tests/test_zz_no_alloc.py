@@ -1,10 +1,10 @@
 """The allocation-free sampler entry point, zxh_sample_noalloc, through the C ABI.
 
-Callers that cannot allocate device memory (code inside a CUDA graph capture
-region, services whose device memory is reserved once up front, latency paths
-that must not take the allocator's locks) pass their own device state and output
-buffers to zxh_sample_noalloc, which keeps its working memory in one static
-device array. Its draws must equal those of the allocating sampler (zxh_measure)
+Callers that cannot allocate device memory (services whose device memory is
+reserved once up front, frameworks whose own allocator owns the device, latency
+paths that must not take the CUDA allocator's locks) pass their own device state
+and output buffers to zxh_sample_noalloc, which keeps its working memory in one
+static device array. Its draws must equal those of the allocating sampler (zxh_measure)
 for the same seed: same uniform stream, same output order, so the tolerance is
 zero. Each case makes two calls in a row, so the second one runs on the scratch
 the first one left behind.

@@ -34,13 +34,11 @@ if not _LIB_PATH.is_file():
 
 _lib = ctypes.CDLL(str(_LIB_PATH))
 
-GATE_DTYPE = np.dtype(
-    [("type", "<u4"), ("cq", "<u4"), ("q", "<u4"), ("reserved", "<u4"),
-     ("theta", "<f8"), ("lam", "<f8"), ("phi", "<f8")]
+from .records import (  # noqa: F401  (re-exported: the record layouts of include/zxh_b200.h)
+    BARRIER, CP, CRZ, CX, GATE_DTYPE, RX, RZ, TERM_DTYPE, TERM_X, TERM_Z, TERM_ZZ, U3, H, P, X, Z, as_records,
+    as_terms,
 )
 
-# gate codes (include/zxh_b200.h)
-BARRIER, Z, RZ, P, CRZ, CP, X, CX, H, U3, RX = 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11
 C64, C128 = 1, 2
 ORDER_REFERENCE, ORDER_QUBIT = 0, 1
 
@@ -122,35 +120,6 @@ def version() -> str:
 def _raise(rc: int, handle) -> None:
     msg = _lib.zxh_last_error(handle).decode(errors="replace")
     raise _ERRORS.get(rc, RuntimeError)(msg or f"zxh error {rc}")
-
-
-def as_records(gates) -> np.ndarray:
-    """Gate records from a structured array or an iterable of
-    ``(type, cq, q[, theta, lambda, phi])`` tuples."""
-    if isinstance(gates, np.ndarray) and gates.dtype == GATE_DTYPE:
-        return np.ascontiguousarray(gates)
-    rows = list(gates)
-    rec = np.zeros(len(rows), GATE_DTYPE)
-    for i, g in enumerate(rows):
-        t, cq, q, th, la, ph = (list(g) + [0.0] * 6)[:6]
-        rec[i] = (t, cq, q, 0, th, la, ph)
-    return rec
-
-
-# observable terms (include/zxh_b200.h zxh_term)
-TERM_DTYPE = np.dtype([("kind", "<u4"), ("q0", "<u4"), ("q1", "<u4"), ("reserved", "<u4"), ("coef", "<f8")])
-TERM_Z, TERM_ZZ, TERM_X = 1, 2, 3
-
-
-def as_terms(terms) -> np.ndarray:
-    """Observable terms from a structured array or ``(kind, q0, q1, coef)`` tuples."""
-    if isinstance(terms, np.ndarray) and terms.dtype == TERM_DTYPE:
-        return np.ascontiguousarray(terms)
-    rows = list(terms)
-    out = np.zeros(len(rows), TERM_DTYPE)
-    for i, (k, q0, q1, c) in enumerate(rows):
-        out[i] = (k, q0, q1, 0, c)
-    return out
 
 
 PASS_KINDS = ("product", "expand", "tile", "pair", "diagonal", "fast", "row", "grow")

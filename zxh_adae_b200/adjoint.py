@@ -107,12 +107,18 @@ def hardware_efficient_ansatz(n: int, reps: int = 8) -> Circuit:
     return Circuit(n, rec, par)
 
 
-def energy(sim, circ: Circuit, params, terms) -> float:
-    """<H> through the plain forward path: execute, then the expectation pass."""
+def energy(sim, circ: Circuit, params, terms, device_ms: list | None = None) -> float:
+    """<H> through the plain forward path: execute, then the expectation pass.
+    device_ms, if given, receives the kernel milliseconds of both (CUDA events on
+    the simulator's stream)."""
     sim.clear_gates()
     sim.push_gates(circ.records(params))
     sim.execute()
-    return sim.expectation(terms)
+    ms = sim.last_stats()[2]
+    e = sim.expectation(terms)
+    if device_ms is not None:
+        device_ms.append(ms + sim.last_stats()[2])
+    return e
 
 
 def adjoint(sim, circ: Circuit, params, terms, checkpoint_every: int = 0):
@@ -123,14 +129,14 @@ def adjoint(sim, circ: Circuit, params, terms, checkpoint_every: int = 0):
     return e, circ.gradient(g)
 
 
-def _shifted(sim, circ, params, terms, s, which):
+def _shifted(sim, circ, params, terms, s, which, device_ms=None):
     p = np.asarray(params, np.float64)
     ks = range(p.size) if which is None else which
     g = np.full(p.size, np.nan)
     for k in ks:
         d = np.zeros_like(p)
         d[k] = s
-        g[k] = energy(sim, circ, p + d, terms) - energy(sim, circ, p - d, terms)
+        g[k] = energy(sim, circ, p + d, terms, device_ms) - energy(sim, circ, p - d, terms, device_ms)
     return g
 
 
@@ -140,12 +146,13 @@ def finite_difference(sim, circ: Circuit, params, terms, step: float = 1e-6, whi
     return _shifted(sim, circ, params, terms, step, which) / (2 * step)
 
 
-def parameter_shift(sim, circ: Circuit, params, terms, which=None) -> np.ndarray:
+def parameter_shift(sim, circ: Circuit, params, terms, which=None, device_ms: list | None = None) -> np.ndarray:
     """(E(p + pi/2 e_k) - E(p - pi/2 e_k)) / 2: exact for RY, RZ, RX, P and CP
-    parameters that feed one gate each (each is a single-frequency rotation)."""
+    parameters that feed one gate each (each is a single-frequency rotation).
+    device_ms, if given, receives the kernel milliseconds of every energy."""
     if len(np.unique(circ.param)) != len(circ.param) or np.any(circ.coef != 1.0):
         raise ValueError("parameter shift needs every parameter on exactly one gate with coefficient 1")
-    return _shifted(sim, circ, params, terms, math.pi / 2, which) / 2
+    return _shifted(sim, circ, params, terms, math.pi / 2, which, device_ms) / 2
 
 
 try:

@@ -20,7 +20,6 @@ compiler, the work the reference's transpiler stage ``zxh_post`` does
 """
 from __future__ import annotations
 
-import secrets
 import time
 import uuid
 from collections.abc import Iterable
@@ -36,7 +35,7 @@ class JobError(RuntimeError):
 class ExperimentResult:
     """Outcome of one circuit: counts keyed by bitstrings, qubit n-1 first."""
 
-    def __init__(self, counts: dict, shots: int, seed, sample_time: float) -> None:
+    def __init__(self, counts: dict, sample_time: float, *, shots: int, seed) -> None:
         self.counts = counts
         self.shots = shots
         self.seed = seed
@@ -61,7 +60,42 @@ class Result:
         return [r.counts for r in self.results]
 
 
+class _SimulatorSlot:
+    """The one simulator a backend keeps between circuits. It is created at the
+    width of the first circuit; a circuit of another width is refused, because
+    the simulator's width is fixed at creation (the reference backend keeps one
+    cached instance the same way, qiskit_backend.py:256-271)."""
+
+    def __init__(self, factory) -> None:
+        self._factory = factory
+        self.sim = None
+
+    def for_width(self, num_qubits: int):
+        if self.sim is None:
+            self.sim = self._factory(num_qubits)
+        elif self.sim.num_qubits() != num_qubits:
+            raise JobError("ZXH backend caches a single simulator instance. "
+                           f"Expected num_qubits={self.sim.num_qubits()}, got num_qubits={num_qubits}.")
+        return self.sim
+
+    def release(self) -> None:
+        if self.sim is not None:
+            self.sim.close()
+        self.sim = None
+
+
+def _reseed(sim, seed) -> None:
+    # no seed: the draw stream is whatever the simulator takes without one
+    if seed is None:
+        sim.clear_seed()
+    else:
+        sim.set_seed(int(seed))
+
+
 class Job:
+    """Runs its circuits when submitted (the reference's job does the same,
+    qiskit_backend.py:150-214); result() afterwards."""
+
     def __init__(self, backend: "Backend", circuits: list, options: dict) -> None:
         self._backend = backend
         self._circuits = circuits
@@ -75,29 +109,26 @@ class Job:
     def backend(self) -> "Backend":
         return self._backend
 
+    def status(self) -> str:
+        return "INITIALIZING" if self._result is None else "DONE"
+
     def submit(self) -> None:
         if self._result is not None:
             raise JobError("Job already submitted")
-        self._result = self._run_job()
-
-    def status(self) -> str:
-        return "DONE" if self._result is not None else "INITIALIZING"
+        opts = self._options
+        shots, seed = int(opts.get("shots", 1)), opts.get("seed_simulator")
+        experiments = [
+            ExperimentResult(*self._backend._run_circuit(c, shots=shots, seed_simulator=seed,
+                                                         optimize_level=opts.get("optimize_level")),
+                             shots=shots, seed=seed)
+            for c in self._circuits
+        ]
+        self._result = Result(self._backend.name, self._job_id, experiments)
 
     def result(self) -> Result:
         if self._result is None:
             raise JobError("Job not submitted")
         return self._result
-
-    def _run_job(self) -> Result:
-        shots = int(self._options.get("shots", 1))
-        seed = self._options.get("seed_simulator")
-        level = self._options.get("optimize_level")
-        results = []
-        for circuit in self._circuits:
-            counts, sample_time = self._backend._run_circuit(circuit, shots=shots, seed_simulator=seed,
-                                                             optimize_level=level)
-            results.append(ExperimentResult(counts, shots, seed, sample_time))
-        return Result(self._backend.name, self._job_id, results)
 
 
 class Backend:
@@ -105,14 +136,14 @@ class Backend:
 
     name = "zxh"
     description = "ZXH backend (B200)"
+    # simulator construction parameters; run() must not be given them
+    _BUILD_ONLY = ("disable_x", "eager_expand_all")
 
     def __init__(self, *, disable_x: bool = False, eager_expand_all: bool = False, dtype: str = "complex128",
                  device: int = 0) -> None:
-        self._disable_x = disable_x
-        self._eager_expand_all = eager_expand_all
-        self._dtype = dtype
-        self._device = device
-        self._sim = None
+        self._build = {"disable_x": disable_x, "eager_expand_all": eager_expand_all, "dtype": dtype,
+                       "device": device}
+        self._slot = _SimulatorSlot(self._make_sim)
         self.options = {"shots": 1, "seed_simulator": None, "optimize_level": None}
 
     @property
@@ -129,51 +160,34 @@ class Backend:
         return sorted(FRONTEND_GATES)
 
     def _make_sim(self, num_qubits: int):
-        return _core.ZXH(num_qubits, disable_x=self._disable_x, eager_expand_all=self._eager_expand_all,
-                         dtype=self._dtype, device=self._device)
-
-    def _get_or_create_sim(self, num_qubits: int):
-        if self._sim is None:
-            self._sim = self._make_sim(num_qubits)
-            return self._sim
-        if self._sim.num_qubits() != num_qubits:
-            raise JobError("ZXH backend caches a single simulator instance. "
-                           f"Expected num_qubits={self._sim.num_qubits()}, got num_qubits={num_qubits}.")
-        return self._sim
+        return _core.ZXH(num_qubits, **self._build)
 
     def _run_circuit(self, circuit, *, shots: int, seed_simulator, optimize_level=None) -> tuple:
-        sim = self._get_or_create_sim(circuit.num_qubits)
-        if seed_simulator is None:
-            clear_seed = getattr(sim, "clear_seed", None)
-            if clear_seed is not None:
-                clear_seed()
-            else:
-                sim.set_seed(secrets.randbits(64))
-        else:
-            sim.set_seed(int(seed_simulator))
+        """One circuit on the cached simulator: (counts, seconds spent sampling)."""
+        sim = self._slot.for_width(circuit.num_qubits)
+        _reseed(sim, seed_simulator)
         sim.clear_gates()
         if optimize_level is None:
             load_circuit_transpiled(sim, circuit)
         else:
             load_circuit(sim, circuit, int(optimize_level))
         sim.execute()
-        t0 = time.perf_counter()
-        counts = {str(k): int(v) for k, v in sim.sample_counts(shots).items()}
-        return counts, time.perf_counter() - t0
+        started = time.perf_counter()
+        raw = sim.sample_counts(shots)
+        elapsed = time.perf_counter() - started
+        return {str(word): int(n) for word, n in raw.items()}, elapsed
 
     def run(self, run_input, **options) -> Job:
-        invalid = {"disable_x", "eager_expand_all"} & set(options)
-        if invalid:
-            raise JobError(f"{', '.join(sorted(invalid))} is a backend construction parameter for ZXH, "
+        misplaced = sorted(k for k in self._BUILD_ONLY if k in options)
+        if misplaced:
+            raise JobError(f"{', '.join(misplaced)} is a backend construction parameter for ZXH, "
                            "not a run() option.")
-        job = Job(self, _coerce_circuits(run_input), {**self.options, **options})
+        job = Job(self, _coerce_circuits(run_input), dict(self.options, **options))
         job.submit()
         return job
 
     def close(self) -> None:
-        if self._sim is not None and hasattr(self._sim, "close"):
-            self._sim.close()
-        self._sim = None
+        self._slot.release()
 
 
 def _is_circuit(obj) -> bool:

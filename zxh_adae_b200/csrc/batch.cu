@@ -25,7 +25,6 @@ namespace {
 using namespace gdev;
 
 constexpr int kWarps = kThreads / 32;
-constexpr long long kSpinLimit = 1LL << 31;  // cycles a task waits for its dependency
 
 template <typename E>
 struct LamShared {
@@ -177,7 +176,8 @@ __global__ void __launch_bounds__(kThreads, 2) batch_kernel(const uint8_t *__res
                                                              const BatchOp *__restrict__ ops,
                                                              const BatchTask *__restrict__ tasks, uint32_t ntasks,
                                                              uint32_t *next, uint32_t *remaining, E *arena,
-                                                             double *grads, double *energies, DevStatus *status)
+                                                             double *grads, double *energies, DevStatus *status,
+                                                             long long spin_limit)
 {
     __shared__ BatchShared<E> sm;
     __shared__ uint32_t s_task, s_abort;
@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(kThreads, 2) batch_kernel(const uint8_t *__res
         if (op.dep != kNoDep && threadIdx.x == 0) {
             const long long t0 = clock64();
             while (*reinterpret_cast<volatile uint32_t *>(&remaining[op.dep]) != 0u) {
-                if (clock64() - t0 > kSpinLimit) {
+                if (clock64() - t0 > spin_limit) {
                     report(status, kErrTimeout, 100 + op.kind, t);
                     s_abort = 1;
                     break;
@@ -218,38 +218,40 @@ __global__ void __launch_bounds__(kThreads, 2) batch_kernel(const uint8_t *__res
 template <typename E, bool REAL>
 cudaError_t persistent_typed(const uint8_t *blob, const BatchOp *ops, const BatchTask *tasks, uint32_t ntasks,
                              uint32_t *next, uint32_t *remaining, E *arena, double *grads, double *energies,
-                             DevStatus *status, int sms, cudaStream_t st)
+                             DevStatus *status, long long spin_limit, int sms, cudaStream_t st)
 {
     int per_sm = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<E, REAL>, kThreads, 0);
     if (per_sm < 1) per_sm = 1;
     batch_kernel<E, REAL><<<unsigned(sms * per_sm), kThreads, 0, st>>>(blob, ops, tasks, ntasks, next, remaining,
-                                                                       arena, grads, energies, status);
+                                                                       arena, grads, energies, status, spin_limit);
     return cudaGetLastError();
 }
 
 template <typename E>
 cudaError_t persistent_real(bool real, const uint8_t *blob, const BatchOp *ops, const BatchTask *tasks,
                             uint32_t ntasks, uint32_t *next, uint32_t *remaining, E *arena, double *grads,
-                            double *energies, DevStatus *status, int sms, cudaStream_t st)
+                            double *energies, DevStatus *status, long long spin_limit, int sms, cudaStream_t st)
 {
     return real ? persistent_typed<E, true>(blob, ops, tasks, ntasks, next, remaining, arena, grads, energies, status,
-                                            sms, st)
+                                            spin_limit, sms, st)
                 : persistent_typed<E, false>(blob, ops, tasks, ntasks, next, remaining, arena, grads, energies,
-                                             status, sms, st);
+                                             status, spin_limit, sms, st);
 }
 
 }  // namespace
 
 cudaError_t run_batch_persistent(const uint8_t *blob, const BatchOp *ops, const BatchTask *tasks, uint32_t ntasks,
                                  uint32_t *next, uint32_t *remaining, void *arena, double *grads, double *energies,
-                                 DevStatus *status, int elem_bytes, bool real, int sms, cudaStream_t st)
+                                 DevStatus *status, int elem_bytes, bool real, int wait_limit_log2, int sms,
+                                 cudaStream_t st)
 {
+    const long long spin_limit = 1LL << wait_limit_log2;
     if (elem_bytes == 8)
         return persistent_real(real, blob, ops, tasks, ntasks, next, remaining, static_cast<float2 *>(arena), grads,
-                               energies, status, sms, st);
+                               energies, status, spin_limit, sms, st);
     return persistent_real(real, blob, ops, tasks, ntasks, next, remaining, static_cast<double2 *>(arena), grads,
-                           energies, status, sms, st);
+                           energies, status, spin_limit, sms, st);
 }
 
 }  // namespace zxh

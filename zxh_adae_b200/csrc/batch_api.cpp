@@ -61,6 +61,7 @@ struct zxh_batch {
     cudaGraphExec_t gexec = nullptr;
 
     int grow_regs = 4, task_items = 128, task_elems = 1 << 17;
+    int wait_limit_log2 = 31;  // a task's wait for its predecessor: 2^31 SM clocks (about a second)
     uint64_t bytes = 0;  // algorithmic state bytes of one run
     bool real = false;   // every strided op has real gates: the persistent kernel's real-gate form
     float last_ms = 0.0f;
@@ -314,8 +315,8 @@ int enqueue_persistent(zxh_batch *b)
                            b->stream),
         "reset counters");
     BCK(b, zxh::run_batch_persistent(b->d_blob, b->d_ops, b->d_tasks, uint32_t(b->tasks.size()), b->d_next, b->d_rem,
-                                     b->d_arena, b->d_grads, b->d_energy, b->d_status, b->eb, b->real, b->sms,
-                                     b->stream),
+                                     b->d_arena, b->d_grads, b->d_energy, b->d_status, b->eb, b->real,
+                                     b->wait_limit_log2, b->sms, b->stream),
         "batch launch");
     return ZXH_OK;
 }
@@ -517,12 +518,18 @@ int zxh_batch_set(zxh_batch *b, const char *name, int value)
     if (!std::strcmp(name, "grow_regs")) field = &b->grow_regs, lo = 1, hi = 4;
     else if (!std::strcmp(name, "task_items")) field = &b->task_items, lo = 1, hi = 1 << 20;
     else if (!std::strcmp(name, "task_elems")) field = &b->task_elems, lo = 256, hi = 1 << 26;
+    else if (!std::strcmp(name, "wait_limit_log2")) field = &b->wait_limit_log2, lo = 0, hi = 31;
     else return bfail(b, ZXH_ERR_ARG, std::string("unknown batch parameter ") + name);
     if (value < lo || value > hi)
         return bfail(b, ZXH_ERR_ARG, std::string(name) + " must be in [" + std::to_string(lo) + ", " +
                                          std::to_string(hi) + "]");
     *field = value;
     BCK(b, cudaSetDevice(b->device), "cudaSetDevice");
+    if (field == &b->wait_limit_log2) {  // a launch argument: only the captured graph holds the old value
+        BCK(b, cudaStreamSynchronize(b->stream), "sync");
+        drop_graph(b);
+        return ZXH_OK;
+    }
     return field == &b->grow_regs ? build(b) : retask(b);
 }
 
@@ -532,6 +539,7 @@ int zxh_batch_get(const zxh_batch *b, const char *name, int *value)
     if (!std::strcmp(name, "grow_regs")) *value = b->grow_regs;
     else if (!std::strcmp(name, "task_items")) *value = b->task_items;
     else if (!std::strcmp(name, "task_elems")) *value = b->task_elems;
+    else if (!std::strcmp(name, "wait_limit_log2")) *value = b->wait_limit_log2;
     else return ZXH_ERR_ARG;
     return ZXH_OK;
 }

@@ -221,11 +221,18 @@ __global__ void __launch_bounds__(kThreads) diag_kernel(const uint8_t *__restric
         E *base = state + r;
 
         // 1. all rows in flight. PF: the tile is in shared memory (or on its way);
-        //    first start the copy of the next one into the other buffer, last read
-        //    by the previous tile (whose values every lane has consumed)
+        //    once it has landed, start the copy of the next one into the other
+        //    buffer, last read by the previous tile (whose values every lane has
+        //    consumed). The warp gives up as one; then only this tile's copy can
+        //    still be in flight, and it waits for that (bounded) before leaving.
         const E *src = base;
         if constexpr (PF) {
             __syncwarp();
+            if (!__all_sync(0xffffffffu, mbar_wait_bounded(&s_bar[warp][k & 1], (k >> 1) & 1))) {
+                if (lane == 0) report(status, kErrTimeout, 7, tile);
+                (void)mbar_wait_bounded(&s_bar[warp][k & 1], (k >> 1) & 1);
+                return;
+            }
             uint64_t nt = 0;
             bool has = true;
             if (it_t + 1 < (1u << cb)) nt = t0 | uint64_t((it_t + 1) ^ ((it_t + 1) >> 1));
@@ -235,10 +242,6 @@ __global__ void __launch_bounds__(kThreads) diag_kernel(const uint8_t *__restric
                 uint64_t *nb = &s_bar[warp][(k + 1) & 1];
                 mbar_arrive_expect_tx(nb, tile_bytes);
                 bulk_g2s(tbuf + size_t((k + 1) & 1) * tile_elems, state + (nt << T), tile_bytes, nb);
-            }
-            if (!mbar_wait_bounded(&s_bar[warp][k & 1], (k >> 1) & 1)) {
-                if (lane == 0) report(status, kErrTimeout, 7, tile);
-                return;
             }
             src = tbuf + size_t(k & 1) * tile_elems;
         }

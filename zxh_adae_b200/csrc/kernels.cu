@@ -299,8 +299,12 @@ __global__ void __launch_bounds__(kThreads) tile_kernel(const uint8_t *__restric
                     bufs[s][e] = state[chunk_base(g, S.r[s], e >> g.c) + (e & ((1u << g.c) - 1u))];
                 __syncthreads();
             }
-        } else if (!mbar_wait_bounded(&S.mbar[s], (k >> 1) & 1)) {
+        } else if (__syncthreads_or(!mbar_wait_bounded(&S.mbar[s], (k >> 1) & 1))) {
+            // the block gives up as one; this tile's copy and the next one's (issued
+            // above) may still be in flight: wait for both, bounded, before leaving
             if (tid == 0) report(status, kErrTimeout, 1, tidx);
+            (void)mbar_wait_bounded(&S.mbar[s], (k >> 1) & 1);
+            if (nxt < g.ntiles) (void)mbar_wait_bounded(&S.mbar[s ^ 1], ((k + 1) >> 1) & 1);
             if (warp == 0) bulk_wait0();
             return;
         }

@@ -1,13 +1,14 @@
 // noalloc.cu -- the multinomial sampler for callers that cannot allocate.
 //
-// Some callers of this library cannot call cudaMalloc: code running inside a CUDA
-// graph capture region (where allocation is not a capturable operation), code in
-// a memory pool that is sized once up front and must never grow (serving
-// processes that pre-reserve all device memory), and host threads that must not
-// take the allocator's locks on a latency-critical path. zxh_sample_noalloc gives
-// them the sampler of zxh_measure with no allocation at all: the caller owns the
-// state (a device pointer) and the output buffer (a device pointer), and every
-// piece of working memory lives in one file-scope __device__ array below.
+// Some callers of this library cannot call cudaMalloc: a serving process that
+// reserves all of its device memory once at start-up and must never grow it
+// afterwards, a framework whose own caching allocator owns the device and forbids
+// raw allocations next to it, and host threads on a latency-critical path that
+// must not take the CUDA allocator's locks or pay its first-touch costs.
+// zxh_sample_noalloc gives them the sampler of zxh_measure with no allocation at
+// all: the caller owns the state (a device pointer) and the output buffer (a
+// device pointer), and every piece of working memory lives in one file-scope
+// __device__ array below.
 //
 // Limits and sharing rules:
 //  * the array holds the scratch of states up to 2^28 amplitudes (2^16 segments
@@ -17,8 +18,10 @@
 //    GPU (different streams, or threads racing) corrupt each other's draws;
 //    serialise them. Each call clears the parts that must start at zero;
 //  * the first call on a device resolves the array's device address with
-//    cudaGetSymbolAddress (once per device, with that device current); make that
-//    first call before any stream capture begins.
+//    cudaGetSymbolAddress (once per device, with that device current) and keeps
+//    it for the life of the process; make that first call before any stream
+//    capture begins. The kept address belongs to the device's primary context:
+//    after cudaDeviceReset the process must not call this entry point again.
 #include "../../include/zxh_b200.h"
 #include "core.h"
 #include "sampler.h"
@@ -35,7 +38,6 @@ void set_thread_error(const std::string &msg);  // capi.cpp: message for zxh_las
 namespace {
 
 constexpr size_t kNoAllocScratchBytes = size_t(2304) << 10;  // 2.25 MiB
-constexpr size_t kStatusBytes = 256;                         // status word at the end
 constexpr int kMaxBits = 28;                                 // 2^28 amplitudes, 2^16 segments
 constexpr int kMaxDevices = 64;
 
@@ -88,29 +90,24 @@ extern "C" int zxh_sample_noalloc(const void *state, int dtype, size_t m_bits, u
     const uint64_t local = 1ULL << m;
     const uint64_t seglen = local < 4096 ? local : 4096;
     const uint64_t nseg = local / seglen;
-    if (zxh::SamplerScratch::need_bytes(nseg, 0) > kNoAllocScratchBytes - kStatusBytes)
+    if (zxh::SamplerScratch::need_bytes(nseg, 0) > kNoAllocScratchBytes)
         return fail(ZXH_ERR_LIMIT, "zxh_sample_noalloc: scratch layout exceeds the static array");
     zxh::SamplerScratch sc;
     sc.carve(base, nseg, 0);
-    zxh::DevStatus *status = reinterpret_cast<zxh::DevStatus *>(base + kNoAllocScratchBytes - kStatusBytes);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
 
     // the previous call's contents stay in the array: clear what starts at zero
     e = cudaMemsetAsync(sc.flags_begin, 0,
                         size_t(static_cast<uint8_t *>(sc.flags_end) - static_cast<uint8_t *>(sc.flags_begin)), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(sc.counts, 0, nseg * sizeof(unsigned long long), st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(status, 0, sizeof(zxh::DevStatus), st);
     if (e != cudaSuccess) return fail(ZXH_ERR_CUDA, std::string("clear scratch: ") + cudaGetErrorString(e));
 
     const uint64_t stream_seed = zxh::mix_seed_host(seed, 0);  // as zxh_measure with a set seed
-    e = zxh::run_sampler_real(state, dtype == ZXH_C64 ? 8 : 16, m, shots, stream_seed, real_out, sc, status,
+    // no step of the draw waits on another CTA, so there is no device status to read back
+    e = zxh::run_sampler_real(state, dtype == ZXH_C64 ? 8 : 16, m, shots, stream_seed, real_out, sc, nullptr,
                               g_scratch_sms[dev], st);
     if (e != cudaSuccess) return fail(ZXH_ERR_CUDA, std::string("sampler launch: ") + cudaGetErrorString(e));
     e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return fail(ZXH_ERR_CUDA, std::string("sampler: ") + cudaGetErrorString(e));
-    zxh::DevStatus hs;
-    e = cudaMemcpy(&hs, status, sizeof(hs), cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) return fail(ZXH_ERR_CUDA, std::string("read status: ") + cudaGetErrorString(e));
-    if (hs.code != 0) return fail(int(hs.code), "zxh_sample_noalloc: a bounded device wait gave up");
     return ZXH_OK;
 }

@@ -299,8 +299,11 @@ __global__ void __launch_bounds__(kThreads, 2) fast_tile_kernel(const uint8_t *_
         if (tidx >= g.ntiles) break;
         const int s = int(k & 1);
         const uint64_t nxt = tidx + gridDim.x;
-        if (!mbar_wait_bounded(&mbar[s], (k >> 1) & 1)) {
+        // the block gives up as one (no thread left behind at a barrier); only this
+        // tile's copy can be in flight then, and each thread waits for it (bounded)
+        if (__syncthreads_or(!mbar_wait_bounded(&mbar[s], (k >> 1) & 1))) {
             if (tid == 0) report(status, kErrTimeout, 3, tidx);
+            (void)mbar_wait_bounded(&mbar[s], (k >> 1) & 1);
             bulk_wait0();
             return;
         }

@@ -7,7 +7,8 @@ integer seed and draws from ``numpy.random.default_rng(seed)`` in a fixed order,
 so any run (ours, the oracle's, the reference's) sees the same gate list.
 
 Records use the 40-byte layout of include/zxh_b200.h; U3 records carry
-(theta, lambda, phi) in ZXH's argument order.
+(theta, lambda, phi) in ZXH's argument order. This module and ``records`` load
+no native code.
 """
 from __future__ import annotations
 
@@ -15,7 +16,7 @@ import math
 
 import numpy as np
 
-from ._core import BARRIER, CP, CX, H, P, RZ, U3, X, as_records
+from .records import BARRIER, CP, CX, H, P, RZ, U3, X, as_records
 
 TWO_PI = 2.0 * math.pi
 
@@ -146,7 +147,7 @@ def batch_tfim(count: int, seed: int, nmin: int = 10, nmax: int = 22, layers: in
     Returns a list of (n, records, terms, h).
     Draw order: n and h per circuit, then per layer (theta, phi, lambda) per qubit
     and the n - 1 alphas."""
-    from ._core import TERM_X, TERM_ZZ, as_terms
+    from .records import TERM_X, TERM_ZZ, as_terms
 
     rng = np.random.default_rng(seed)
     out = []
