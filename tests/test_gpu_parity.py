@@ -421,3 +421,63 @@ def test_apply_async_matches_apply(dtype):
     assert np.array_equal(a.results_words(), b.results_words())
     st = b.last_stats()
     assert st[0] > 0
+
+
+def _walsh_case(n, prefix, seed):
+    if prefix == "cx_chain":
+        pre = wl.cx_chain(n)
+    elif prefix == "cx_random":  # a dense map: random CX pairs, X flips (selector betas)
+        rng = np.random.default_rng(seed)
+        recs = []
+        for _ in range(3 * n):
+            c, t = (int(v) for v in rng.choice(n, 2, replace=False))
+            recs.append((zx._core.CX, c, t))
+            if rng.random() < 0.3:
+                recs.append((zx._core.X, 0, int(rng.integers(n))))
+        pre = zx.as_records(recs)
+    else:
+        pre = wl.h_all(n)[:0]
+    rz = zx.as_records([(zx._core.RZ, 0, q, 0.37 * q + 0.1) for q in range(0, n, 3)]
+                       + [(zx._core.Z, 0, 1)])
+    return np.concatenate([wl.h_all(n), pre, wl.diag_batch(n, 700, seed), rz, wl.cp_cascade(n)])
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+@pytest.mark.parametrize("prefix", ["cx_chain", "cx_random", "none"])
+@pytest.mark.parametrize("knobs", [{}, {"walsh_min_general": 0}, {"walsh": 0}],
+                         ids=["default", "walsh_always", "walsh_off"])
+@pytest.mark.parametrize("n", [10, 15])
+def test_walsh_window_pass(dtype, prefix, knobs, n):
+    # windows whose selectors are parities of several real bits (after CX / X
+    # transport) as one Walsh-sum pass; walsh_min_general = 0 also sends windows of
+    # single-bit selectors through it, walsh = 0 is the per-amplitude form
+    gates = _walsh_case(n, prefix, 40 + n)
+    o = Oracle(n)
+    o.push(gates)
+    o.execute()
+    s = zx.ZXH(n, dtype=dtype)
+    for k, v in knobs.items():
+        s.set_param(k, v)
+    s.push_gates(gates)
+    s.execute()
+    assert max_err(s, o) <= TOL[dtype]
+    if prefix != "none" and knobs.get("walsh", 1):
+        assert s.last_stats()[1] <= 3  # the window is one pass (the cascade's window may join it)
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_walsh_window_pass_through_apply(dtype):
+    n = 16
+    o = Oracle(n)
+    full = [wl.h_all(n), wl.cx_chain(n)]
+    s = zx.ZXH(n, dtype=dtype)
+    s.push_gates(np.concatenate(full))
+    s.execute()
+    for k in range(3):
+        b = wl.diag_batch(n, 1500, 900 + k)
+        s.apply(b)
+        assert s.last_stats()[1] == 1
+        full.append(b)
+    o.push(np.concatenate(full))
+    o.execute()
+    assert max_err(s, o) <= TOL[dtype]

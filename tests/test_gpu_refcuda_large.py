@@ -12,6 +12,7 @@ the global phases applied, in FP64:
 
 Shapes: configuration 2's diagonal batches (H on all, then B random p/cp with
 B in {64, 256, 1024, 4096}) and the full controlled-phase cascade at 28 qubits,
+a 4096-gate window after a CX chain (multi-bit selectors) at 26 qubits,
 configuration 3's U3 + cz matching layers at 26 qubits and its hidden-string
 circuit at 26+1 qubits, configuration 4's ansatz forward state at 24 qubits and
 configuration 1 at 20 qubits. A 16-qubit case also goes through get_state in
@@ -50,6 +51,9 @@ CASES = [
     ("config2_B1024_28q", 28, lambda: np.concatenate([wl.h_all(28), wl.diag_batch(28, 1024, 13)])),
     ("config2_B4096_28q", 28, lambda: np.concatenate([wl.h_all(28), wl.diag_batch(28, 4096, 14)])),
     ("config2_cascade_28q", 28, lambda: np.concatenate([wl.h_all(28), wl.cp_cascade(28)])),
+    # after a CX chain every selector is a prefix parity of the real bits: the
+    # window is one Walsh-sum pass here, single-gate sweeps in the reference
+    ("cxchain_B4096_26q", 26, lambda: np.concatenate([wl.h_all(26), wl.cx_chain(26), wl.diag_batch(26, 4096, 15)])),
     ("config3_u3cz4_26q", 26, lambda: wl.u3_matching_layers(26, 4, 33)),
     ("config3_hidden_27q", 27, lambda: wl.hidden_string(26, 34)[0]),
     ("config4_ansatz_24q", 24, _ansatz24),

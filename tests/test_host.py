@@ -25,6 +25,18 @@ def test_diag_batch_is_one_pass():
     assert st["M"] == 30 and st["product"] == 1 and st["passes"] == 1 and st["diagonal"] == 1
 
 
+def test_window_after_cx_chain_is_one_walsh_pass():
+    # after CX(i, i+1) on every i the selectors are prefix parities of the real
+    # bits: the whole 4096-gate window is one Walsh-sum pass, not 128 split passes
+    g = np.concatenate([wl.h_all(30), wl.cx_chain(30), wl.diag_batch(30, 4096, 1)])
+    for dtype in ("complex64", "complex128"):
+        st = plan_stats(30, g, dtype=dtype)
+        assert st["walsh"] == 1 and st["passes"] == 1 and st["diagonal"] == 0, st
+    # a window of single-bit selectors keeps the diagonal pass
+    st = plan_stats(30, np.concatenate([wl.h_all(30), wl.diag_batch(30, 4096, 1)]))
+    assert st["walsh"] == 0 and st["diagonal"] == 1
+
+
 def test_u3_layer_splits_into_low_and_strided_passes():
     rng = np.random.default_rng(0)
     lay = zx.as_records([(zx._core.U3, 0, q, *rng.uniform(0, 6.28, 3)) for q in range(30)])

@@ -138,6 +138,17 @@ struct DiagDev {
                         // those of coordinate k are [kidx[k], kidx[k+1])
 };
 
+// A diagonal window as a Walsh sum (walsh.cu): phase(r) = c0 + sum over terms of
+// w * (-1)^parity(mask & r), every term's mask split into its in-tile part g (the
+// low T bits) and out-of-tile part hi (mask >> T). Terms are sorted by g. Phases
+// are int64 fixed-point turns (wrapping modulo 2^64 = one turn).
+struct WalshTermDev { uint64_t hi; int64_t w; uint32_t g; uint32_t pad; };
+struct WalshDev {
+    int64_t c0;
+    uint32_t T, n_terms;
+    uint64_t off_terms;  // byte offset of WalshTermDev[n_terms] in the blob
+};
+
 // exp(2 pi i j / 1024), j = 0..1023: the coarse factor of a phase given in turns.
 constexpr int kExpTableBits = 10;
 

@@ -556,6 +556,62 @@ uint64_t compile_diag(std::vector<uint8_t> &blob, const std::vector<DiagTerm> &t
     return put(blob, d);
 }
 
+size_t count_general(const std::vector<DiagTerm> &w)
+{
+    size_t n = 0;
+    for (const DiagTerm &t : w) n += !(single_bit_or_zero(t.s0.alpha) && (!t.two || single_bit_or_zero(t.s1.alpha)));
+    return n;
+}
+
+// Compiles one window as a Walsh sum over tiles of 2^T amplitudes (walsh.cu): with
+// [S] = (1 - (-1)^S) / 2 and q = theta / 4 in turns,
+//   theta [S0]      = 2q - 2q s0 X(a0),
+//   theta [S0] [S1] = q - q s0 X(a0) - q s1 X(a1) + q s0 s1 X(a0 ^ a1),
+// s = (-1)^beta, X(a) = (-1)^parity(a & r); terms of equal mask merge and mask 0
+// is the constant. All sums wrap modulo 2^64 turns, and 4q equals theta's turns to
+// within rounding, so the phase of every amplitude is exact modulo a full turn.
+uint64_t compile_walsh(std::vector<uint8_t> &blob, const std::vector<DiagTerm> &terms, int T)
+{
+    std::vector<std::pair<uint64_t, uint64_t>> acc;  // (mask, coefficient)
+    acc.reserve(terms.size() * 4);
+    uint64_t c0 = 0;
+    auto add = [&](uint64_t mask, uint64_t v) {
+        if (mask) acc.emplace_back(mask, v);
+        else c0 += v;
+    };
+    for (const DiagTerm &t : terms) {
+        const uint64_t q = uint64_t(turns(t.theta * 0.25));
+        if (!t.two) {
+            const uint64_t h = q << 1;
+            add(0, h);
+            add(t.s0.alpha, t.s0.beta ? h : uint64_t(0) - h);
+            continue;
+        }
+        add(0, q);
+        add(t.s0.alpha, t.s0.beta ? q : uint64_t(0) - q);
+        add(t.s1.alpha, t.s1.beta ? q : uint64_t(0) - q);
+        add(t.s0.alpha ^ t.s1.alpha, t.s0.beta == t.s1.beta ? q : uint64_t(0) - q);
+    }
+    std::sort(acc.begin(), acc.end(), [](const std::pair<uint64_t, uint64_t> &a, const std::pair<uint64_t, uint64_t> &b) {
+        return a.first < b.first;
+    });
+    std::vector<WalshTermDev> out;
+    for (size_t i = 0; i < acc.size();) {
+        const uint64_t mask = acc[i].first;
+        uint64_t w = 0;
+        for (; i < acc.size() && acc[i].first == mask; i++) w += acc[i].second;
+        if (w) out.push_back(WalshTermDev{mask >> T, int64_t(w), uint32_t(mask & low_mask(T)), 0u});
+    }
+    std::stable_sort(out.begin(), out.end(), [](const WalshTermDev &a, const WalshTermDev &b) { return a.g < b.g; });
+    WalshDev d;
+    std::memset(&d, 0, sizeof(d));
+    d.c0 = int64_t(c0);
+    d.T = uint32_t(T);
+    d.n_terms = uint32_t(out.size());
+    d.off_terms = put_vec(blob, out);
+    return put(blob, d);
+}
+
 U3Dev compile_u3(const U3Op &u, const TileDev &g)
 {
     U3Dev d;
@@ -841,6 +897,10 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
             ngen += !(single_bit_or_zero(t.s0.alpha) && (!t.two || single_bit_or_zero(t.s1.alpha)));
         need_split = need_split || ngen > 32;
     }
+    // with the Walsh pass a window of any size stays whole: the passes that take at
+    // most 32 general terms (tile prologues / epilogues) refuse bigger ones, which
+    // then run standalone
+    need_split = need_split && !pp.walsh;
     std::vector<Op> split_ops;
     if (need_split) split_ops = split_windows(ops_in, 32);
     const std::vector<Op> &ops = need_split ? split_ops : ops_in;
@@ -991,19 +1051,42 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
                 return;
             }
         }
+        const size_t ngen = count_general(w);
+        if (pp.walsh && ngen >= size_t(pp.walsh_min_general) && mm >= walsh_tile_bits(elem_bytes)) {
+            Pass ps;
+            ps.kind = Pass::WALSH;
+            ps.m = mm;
+            ps.off = compile_walsh(out.blob, w, walsh_tile_bits(elem_bytes));
+            ps.off2 = exp_off;
+            out.passes.push_back(ps);
+            return;
+        }
         const int rb = elem_bytes == 8 ? pp.diag_row_bits_c64 : pp.diag_row_bits_c128;
         const int T = std::min(mm, diag_tile_bits(elem_bytes, rb));
         TileDev g = make_geom(mm, T, std::vector<int>());
-        Pass ps;
-        ps.kind = Pass::DIAG;
-        ps.m = mm;
-        ps.chunk_bits = pp.diag_chunk_bits;
-        ps.row_bits = rb;
-        ps.prefetch = elem_bytes == 8 ? pp.diag_prefetch_c64 : pp.diag_prefetch_c128;
-        ps.geom = g;
-        ps.off = compile_diag(out.blob, w, g);
-        ps.off2 = exp_off;
-        out.passes.push_back(ps);
+        // the diagonal pass evaluates at most 32 general terms per amplitude: a bigger
+        // window (only below the Walsh pass's tile size) runs as several passes
+        std::vector<Op> pieces;
+        if (ngen > 32) {
+            Op whole;
+            whole.kind = Op::DIAG;
+            whole.m = mm;
+            whole.diag = w;
+            pieces = split_windows(std::vector<Op>{whole}, 32);
+        }
+        const size_t npieces = pieces.empty() ? 1 : pieces.size();
+        for (size_t k = 0; k < npieces; k++) {
+            Pass ps;
+            ps.kind = Pass::DIAG;
+            ps.m = mm;
+            ps.chunk_bits = pp.diag_chunk_bits;
+            ps.row_bits = rb;
+            ps.prefetch = elem_bytes == 8 ? pp.diag_prefetch_c64 : pp.diag_prefetch_c128;
+            ps.geom = g;
+            ps.off = compile_diag(out.blob, pieces.empty() ? w : pieces[k].diag, g);
+            ps.off2 = exp_off;
+            out.passes.push_back(ps);
+        }
     };
 
     // Fuses a window into a fast pass as prologue (pre) or epilogue when it is
@@ -1333,7 +1416,7 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
                 last_tile_pass = -1;
             } else if (last_tile_pass >= 0 && out.passes[last_tile_pass].kind == Pass::TILE &&
                        out.passes[last_tile_pass].m == op.m &&
-                       out.passes[last_tile_pass].steps.size() < size_t(pp.max_steps)) {
+                       out.passes[last_tile_pass].steps.size() < size_t(pp.max_steps) && count_general(*wd) <= 32) {
                 attach_epilogue(last_tile_pass, *wd);
                 last_tile_pass = -1;  // keep one epilogue window per pass
             } else if (next_u3) {
@@ -1459,6 +1542,10 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
                 out.passes.push_back(ps);
             }
             last_tile_pass = -1;
+        }
+        if (held && count_general(*held) > 32) {  // more general terms than a tile step evaluates
+            standalone_diag(mm, *held);
+            held = nullptr;
         }
         for (size_t k = 0; k < groups.size(); k++) {
             const bool lowgrp = groups[k].first.empty();

@@ -67,6 +67,10 @@ struct PlanParams {
     int diag_chunk_bits = -1;   // log2 tiles a warp walks in Gray-code order in a diagonal pass (-1: chosen
                                 // per launch so every warp of a full grid gets at least 16 chunks)
     int product_table_bits = 12;
+    int walsh = 1;              // 1: windows with multi-bit selectors run as one Walsh-sum pass (walsh.cu)
+                                // instead of general terms evaluated per amplitude (split every 32 terms)
+    int walsh_min_general = 2;  // general (multi-bit selector) terms from which a standalone window takes the
+                                // Walsh pass; 0: every standalone window does
 };
 
 // General strided pass shape (grow.cu): fixed low bits and register coordinates.
@@ -95,7 +99,7 @@ struct GrowBuild {
 };
 
 struct Pass {
-    enum Kind { PRODUCT, EXPAND, TILE, PAIR, DIAG, FAST, ROW, GROW, INIT } kind;  // INIT: |0...0> (grow_only)
+    enum Kind { PRODUCT, EXPAND, TILE, PAIR, DIAG, FAST, ROW, GROW, INIT, WALSH } kind;  // INIT: |0...0> (grow_only)
     int m = 0;
     uint64_t off = 0;    // blob offset of the pass descriptor
     uint64_t off2 = 0;   // PRODUCT: lookup table; DIAG: exp table
@@ -120,9 +124,11 @@ struct Plan {
     void clear();
 };
 
-// Tile bits of the standalone diagonal pass (diag.cu) and of the fast U3 pass
-// (u3pass.cu), and the register bits of one fast-pass round.
+// Tile bits of the standalone diagonal pass (diag.cu), of the Walsh-sum window
+// pass (walsh.cu) and of the fast U3 pass (u3pass.cu), and the register bits of
+// one fast-pass round.
 int diag_tile_bits(int elem_bytes, int row_bits);
+int walsh_tile_bits(int elem_bytes);
 int fast_tile_bits(int elem_bytes);
 int fast_reg_bits(int elem_bytes);
 int row_reg_bits(int elem_bytes, int wide);

@@ -62,6 +62,13 @@ def diag_batch(n: int, batch: int, seed: int) -> np.ndarray:
     return as_records(recs)
 
 
+def cx_chain(n: int) -> np.ndarray:
+    """CX(i, i+1) for i = 0..n-2, in order (the adjoint ansatz's entangling chain).
+    After it every qubit's selector is the parity of a prefix of the real bits, so
+    the p/cp gates of a following window have multi-bit selectors."""
+    return as_records([(CX, i, i + 1) for i in range(n - 1)])
+
+
 def cp_cascade(n: int) -> np.ndarray:
     """Controlled-phase cascade over all pairs j > i with angle pi / 2^(j - i)."""
     recs = []
