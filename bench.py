@@ -93,7 +93,9 @@ def parse():
     ap.add_argument("--batch", type=int, default=BATCH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="diag",
-                    choices=["diag", "u3", "adjoint", "batch", "sample", "config2", "config3"])
+                    choices=["diag", "cxwindow", "u3", "adjoint", "batch", "sample", "config2", "config3"])
+    ap.add_argument("--dtype", default="complex64", choices=["complex64", "complex128"],
+                    help="diag / cxwindow / u3 workloads: the state's type")
     ap.add_argument("--no-tune", action="store_true", help="batch workload: skip the autotuner")
     ap.add_argument("--batch-count", type=int, default=512, help="batch workload: circuits")
     ap.add_argument("--no-extras", action="store_true", help="skip the U3-layer and adjoint legs of the diag line")
@@ -473,6 +475,7 @@ def fidelity_err(sim_a, sim_b) -> float:
 
 
 CONFIG2_BATCHES = (64, 256, 1024, 4096)
+CX_CHAIN_BATCHES = (256, 4096)  # the same windows after a CX chain (multi-bit selectors)
 
 
 def config2_leg(local: int, n: int = N_QUBITS, steps: int = 5, warmup: int = 2) -> dict:
@@ -488,17 +491,25 @@ def config2_leg(local: int, n: int = N_QUBITS, steps: int = 5, warmup: int = 2) 
     from zxh_adae_b200 import workloads as wl
 
     peak, kind = peaks()
-    keys = list(CONFIG2_BATCHES) + ["cascade"]
+    keys = list(CONFIG2_BATCHES) + ["cascade"] + [f"cx_chain+{B}" for B in CX_CHAIN_BATCHES]
     batches = {B: [wl.diag_batch(n, B, seed=7000 + 10 * B + k) for k in range(warmup + steps)]
                for B in CONFIG2_BATCHES}
     batches["cascade"] = [wl.cp_cascade(n)] * (warmup + steps)
+    for B in CX_CHAIN_BATCHES:
+        batches[f"cx_chain+{B}"] = [wl.diag_batch(n, B, seed=8000 + 10 * B + k) for k in range(warmup + steps)]
     rows = {k: {"batch": k, "gates": int(len(batches[k][0]))} for k in keys}
     sims = {}
     for dtype, eb in (("complex64", 8), ("complex128", 16)):
         sim = zx.ZXH(n, dtype=dtype, device=local)
         sim.push_gates(wl.h_all(n))
         sim.execute()
+        chained = False
         for k in keys:
+            if str(k).startswith("cx_chain") and not chained:
+                # CX(i, i+1) chain: map updates only; every later selector is a
+                # parity of several real bits (the Walsh-sum window pass)
+                sim.apply(wl.cx_chain(n))
+                chained = True
             dev_ms, launches, passes, wall, _ = timed_applies(sim, batches[k], warmup, steps, None, local)
             ms = sum(dev_ms) / steps
             pps = passes / steps
@@ -511,7 +522,8 @@ def config2_leg(local: int, n: int = N_QUBITS, steps: int = 5, warmup: int = 2) 
     fid = fidelity_err(sims["complex64"], sims["complex128"])
     for s in sims.values():
         s.close()
-    return {"workload": f"{n}q H-prepared; per step B random p/cp (50/50) or the {n * (n - 1) // 2}-pair cp cascade",
+    return {"workload": f"{n}q H-prepared; per step B random p/cp (50/50) or the {n * (n - 1) // 2}-pair cp cascade; "
+                        "then a CX chain and B random p/cp (selectors are parities of several real bits)",
             "peak": peak, "peak_kind": kind, "rows": [rows[k] for k in keys],
             "complex64_fidelity_err_vs_complex128": fid, "steps": steps, "warmup": warmup}
 
@@ -651,7 +663,7 @@ def timed_applies(sim, batches, warmup, steps, pg, local):
     return dev_ms, launches, passes, wall, clk.summary()
 
 
-def timed_async(n, dtype, local, batches, warmup, steps, pg) -> float:
+def timed_async(n, dtype, local, batches, warmup, steps, pg, prefix=None) -> float:
     """End-to-end wall time of K zxh_apply_async calls and the closing zxh_sync on a
     fresh H-prepared simulator: every step plans on the host, uploads its program
     from pinned memory and reads its status word back; step k + 1 is planned while
@@ -662,6 +674,8 @@ def timed_async(n, dtype, local, batches, warmup, steps, pg) -> float:
     sim = zx.ZXH(n, dtype=dtype, device=local)
     sim.push_gates(wl.h_all(n))
     sim.execute()
+    if prefix is not None:
+        sim.apply(prefix)
     for k in range(warmup):
         sim.apply_async(batches[k])
     sim.sync()
@@ -782,6 +796,14 @@ def gpu_baseline_leg(local: int, ours: dict, n: int = N_QUBITS, seed: int = 4242
     fs, rec = item("cp cascade", wl.cp_cascade(n), r.get("c128"), r.get("c64"))
     out["items"].append(rec)
     del fs
+    # a window after a CX chain: the reference runs every CP whose selector spans its
+    # lane and high bits as a full sweep of its own (kernel_cuda.cu:767-795,
+    # zxh.cpp:535-539); B = 256 keeps that run short
+    r = rows.get("cx_chain+256", {})
+    fs, rec = item("cx chain, then diag B=256", np.concatenate([wl.cx_chain(n), wl.diag_batch(n, 256, seed=seed + 1)]),
+                   r.get("c128"), r.get("c64"), compare=True)
+    out["items"].append(rec)
+    del fs
     u64, u128 = ours.get("u3_layer"), ours.get("u3_layer_c128")
     conv = (lambda d: {"ms": d["ms_per_layer"], "api_ms": d["api_ms_per_layer"]} if d else None)
     fs, rec = item("U3 layer", wl.u3_layer(n, seed=seed), conv(u128), conv(u64), compare=True)
@@ -815,8 +837,8 @@ def run_ours(args):
     from zxh_adae_b200 import workloads as wl
 
     n, B = args.qubits, args.batch
-    dtype = "complex64"
-    eb = 8
+    dtype = args.dtype
+    eb = 8 if dtype == "complex64" else 16
     state = (1 << n) * eb
     peak, peak_kind = peaks()
     if args.workload == "config3":
@@ -846,25 +868,35 @@ def run_ours(args):
     sim = zx.ZXH(n, dtype=dtype, device=local)
     sim.push_gates(wl.h_all(n))
     sim.execute()
+    tag = "c64" if dtype == "complex64" else "c128"
+    prefix = None
     if args.workload == "u3":
         batches = [wl.u3_layer(n, seed=rank * 100000 + k) for k in range(args.warmup + args.steps)]
-        desc = f"U3 layer on all {n} qubits, complex64, H-prepared, random angles per step"
-        dominant, traffic_file = "row_pass_kernel", f"row_pass_{n}q_c64.md"
+        desc = f"U3 layer on all {n} qubits, {dtype}, H-prepared, random angles per step"
+        dominant, traffic_file = "row_pass_kernel", f"row_pass_{n}q_{tag}.md"
+    elif args.workload == "cxwindow":
+        # a CX chain first (map updates only): every selector of the windows is then
+        # a parity of several real bits, and each window is one Walsh-sum pass
+        prefix = wl.cx_chain(n)
+        sim.apply(prefix)
+        batches = [wl.diag_batch(n, B, seed=rank * 100000 + k) for k in range(args.warmup + args.steps)]
+        desc = f"{n}q {dtype}, H-prepared, CX chain, then B={B} random p/cp (50/50) per step"
+        dominant, traffic_file = "walsh_kernel", f"walsh_pass_{n}q_{tag}.md"
     else:
         batches = [wl.diag_batch(n, B, seed=rank * 100000 + k) for k in range(args.warmup + args.steps)]
-        desc = f"diag-batch {n}q complex64, H-prepared, B={B} random p/cp (50/50) per step"
-        dominant, traffic_file = "diag_kernel", f"diag_pass_{n}q_c64.md"
+        desc = f"diag-batch {n}q {dtype}, H-prepared, B={B} random p/cp (50/50) per step"
+        dominant, traffic_file = "diag_kernel", f"diag_pass_{n}q_{tag}.md"
     dev_ms, launches, passes, wall, clocks = timed_applies(sim, batches, args.warmup, args.steps, pg, local)
     fid = None
     if rank == 0 and world == 1 and not args.no_extras:
         # the same gates in complex128, executed as one list: fidelity error of the timed complex64 state
         ref = zx.ZXH(n, dtype="complex128", device=local)
-        ref.push_gates(np.concatenate([wl.h_all(n)] + batches))
+        ref.push_gates(np.concatenate([wl.h_all(n)] + ([prefix] if prefix is not None else []) + batches))
         ref.execute()
         fid = fidelity_err(sim, ref)
         ref.close()
     sim.close()
-    wall_async = timed_async(n, dtype, local, batches, args.warmup, args.steps, pg)
+    wall_async = timed_async(n, dtype, local, batches, args.warmup, args.steps, pg, prefix)
     bytes_step = (passes / args.steps) * 2 * state
     dev_total_ms = max_over_ranks(pg, sum(dev_ms), local)
     wall = max_over_ranks(pg, wall, local)
@@ -907,14 +939,14 @@ def run_ours(args):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "c64",
+        "dtype": tag,
         "data": "synthetic",
         "config": {
             "workload": desc,
             "qubits": n,
-            "batch": B if args.workload == "diag" else n,
+            "batch": n if args.workload == "u3" else B,
             "passes_per_step": passes / args.steps,
-            "gates_per_s": (len(batches[0]) if args.workload == "diag" else n) / (dev_total_ms / args.steps / 1e3),
+            "gates_per_s": len(batches[0]) / (dev_total_ms / args.steps / 1e3),
             "passes_per_s": (passes / args.steps) / (dev_total_ms / args.steps / 1e3),
             "state_bytes": state,
             "l2": "state larger than L2, no flush" if state > 126 * 2**20 else "state fits in L2",

@@ -140,9 +140,11 @@ struct DiagDev {
 
 // A diagonal window as a Walsh sum (walsh.cu): phase(r) = c0 + sum over terms of
 // w * (-1)^parity(mask & r), every term's mask split into its in-tile part g (the
-// low T bits) and out-of-tile part hi (mask >> T). Terms are sorted by g. Phases
-// are int64 fixed-point turns (wrapping modulo 2^64 = one turn).
-struct WalshTermDev { uint64_t hi; int64_t w; uint32_t g; uint32_t pad; };
+// low T bits) and out-of-tile part hi (mask >> T). hi_g packs hi (bits 0..53: m <=
+// 63 and T >= 9) with g above it (bits 54..63). Terms are sorted by g. Phases are
+// int64 fixed-point turns (wrapping modulo 2^64 = one turn).
+constexpr int kWalshGShift = 54;
+struct WalshTermDev { uint64_t hi_g; int64_t w; };
 struct WalshDev {
     int64_t c0;
     uint32_t T, n_terms;

@@ -232,6 +232,13 @@ __device__ __forceinline__ void bulk_s2g(void *gdst, const void *smem_src, uint3
                  : "memory");
 }
 
+// Asks L2 to fetch [gsrc, gsrc + bytes) from memory (no destination, nothing to
+// wait for); both 16-byte aligned.
+__device__ __forceinline__ void bulk_prefetch_l2(const void *gsrc, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(gsrc), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 
 __device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }

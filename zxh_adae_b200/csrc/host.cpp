@@ -600,9 +600,11 @@ uint64_t compile_walsh(std::vector<uint8_t> &blob, const std::vector<DiagTerm> &
         const uint64_t mask = acc[i].first;
         uint64_t w = 0;
         for (; i < acc.size() && acc[i].first == mask; i++) w += acc[i].second;
-        if (w) out.push_back(WalshTermDev{mask >> T, int64_t(w), uint32_t(mask & low_mask(T)), 0u});
+        if (w) out.push_back(WalshTermDev{(mask >> T) | ((mask & low_mask(T)) << kWalshGShift), int64_t(w)});
     }
-    std::stable_sort(out.begin(), out.end(), [](const WalshTermDev &a, const WalshTermDev &b) { return a.g < b.g; });
+    std::stable_sort(out.begin(), out.end(), [](const WalshTermDev &a, const WalshTermDev &b) {
+        return (a.hi_g >> kWalshGShift) < (b.hi_g >> kWalshGShift);
+    });
     WalshDev d;
     std::memset(&d, 0, sizeof(d));
     d.c0 = int64_t(c0);
@@ -1057,6 +1059,7 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
             ps.kind = Pass::WALSH;
             ps.m = mm;
             ps.off = compile_walsh(out.blob, w, walsh_tile_bits(elem_bytes));
+            ps.row_bits = int(reinterpret_cast<const WalshDev *>(out.blob.data() + ps.off)->n_terms);
             ps.off2 = exp_off;
             out.passes.push_back(ps);
             return;

@@ -111,7 +111,7 @@ struct Pass {
     int low = 0;                         // ROW: the low pass (lane bits 0..3 swapped into registers)
     int real = 0;                        // ROW: every gate matrix is real
     int chunk_bits = -1;                 // DIAG: tiles per Gray-code chunk (log2, -1 = automatic)
-    int row_bits = 0;                    // DIAG: log2 rows of a warp tile
+    int row_bits = 0;                    // DIAG: log2 rows of a warp tile; WALSH: the window's term count
     int prefetch = 0;                    // DIAG: tiles staged one ahead by TMA bulk copies; GROW: the
                                          // staged form (next item in shared memory)
     std::vector<FastGateDev> fgates;     // FAST

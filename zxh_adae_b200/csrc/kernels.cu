@@ -564,7 +564,7 @@ cudaError_t run_passes(const std::vector<Pass> &passes, const uint8_t *dblob, vo
             e = run_diag(dblob, ps.off, ps.off2, ps.m, elem_bytes, ps.row_bits, ps.chunk_bits, ps.prefetch != 0, state, status,
                          sms, st);
         } else if (ps.kind == Pass::WALSH) {
-            e = run_walsh(dblob, ps.off, ps.off2, ps.m, elem_bytes, state, sms, st);
+            e = run_walsh(dblob, ps.off, ps.off2, ps.m, uint32_t(ps.row_bits), elem_bytes, state, sms, st);
         } else if (ps.kind == Pass::PAIR) {
             const uint64_t np = 1ULL << (ps.m - 1);
             const unsigned grid = unsigned(std::max<uint64_t>(1, std::min<uint64_t>((np + kThreads - 1) / kThreads,

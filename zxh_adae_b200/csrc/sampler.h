@@ -56,8 +56,9 @@ cudaError_t run_diag(const uint8_t *dblob, uint64_t doff, uint64_t toff, int m, 
 int diag_tile_bits(int elem_bytes, int row_bits);
 // The diagonal window as a Walsh sum (walsh.cu): one pass, cost per amplitude
 // independent of the window's size and of the affine map; needs m >= walsh_tile_bits.
-cudaError_t run_walsh(const uint8_t *dblob, uint64_t woff, uint64_t toff, int m, int elem_bytes, void *state, int sms,
-                      cudaStream_t st);
+// n_terms: the compiled window's term count (sizes the shared-memory stage).
+cudaError_t run_walsh(const uint8_t *dblob, uint64_t woff, uint64_t toff, int m, uint32_t n_terms, int elem_bytes,
+                      void *state, int sms, cudaStream_t st);
 int walsh_tile_bits(int elem_bytes);
 cudaError_t run_fast_tile(const uint8_t *dblob, uint64_t foff, uint64_t toff, uint64_t ntiles, int elem_bytes,
                           void *state, DevStatus *status, int sms, cudaStream_t st);
