@@ -289,10 +289,11 @@ int zxh_batch_stats(const zxh_batch *batch, uint64_t *ops, uint64_t *tasks, doub
 
 /* Host-only dry run of execute(): lowers the records, runs calc_mem, the
  * reference's execute() schedule and the pass planner, and launches nothing
- * (no CUDA call is made). out[12]: [0] M, [1] final real bits, [2..9] passes
+ * (no CUDA call is made). out[13]: [0] M, [1] final real bits, [2..9] passes
  * per kind (product, expand, tile, pair, diagonal, fast low-qubit, strided
  * high-qubit, general strided), [10] state passes (all but product and the
- * |0...0> init), [11] Walsh-sum window passes. No counterpart in the reference. */
+ * |0...0> init), [11] Walsh-sum window passes, [12] span passes. No
+ * counterpart in the reference. */
 int zxh_plan_stats(size_t n, int disable_x, int eager_expand_all, int dtype, const zxh_gate *gates, size_t count,
                    uint64_t *out);
 
@@ -334,7 +335,9 @@ int zxh_optimize_gates(size_t n, int level, const zxh_gate *gates, size_t count,
  * selectors are parities of several real bits runs as one Walsh-sum pass, its
  * cost per amplitude independent of the window's size; 0: general terms
  * evaluated per amplitude, 32 per pass), walsh_min_general (general terms from
- * which a standalone window takes the Walsh pass; 0 = every one). Takes effect at the next
+ * which a standalone window takes the Walsh pass; 0 = every one), span (1:
+ * complex64 U3 batches run as span passes, 13 gates on the low bits and up to 10
+ * high-bit gates per pass; 0: the register-row passes). Takes effect at the next
  * zxh_execute / zxh_apply. No counterpart in the reference. */
 int zxh_set_param(zxh_sim *sim, const char *name, int value);
 

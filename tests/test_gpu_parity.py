@@ -481,3 +481,59 @@ def test_walsh_window_pass_through_apply(dtype):
     o.push(np.concatenate(full))
     o.execute()
     assert max_err(s, o) <= TOL[dtype]
+
+
+def _span_case(n, kind, seed):
+    rng = np.random.default_rng(seed)
+    recs = [(zx._core.H, 0, q) for q in range(n)]
+    for layer in range(3):
+        if kind in ("flips", "mixed"):  # X gates: selectors with beta = 1 (the partner at bit 0 leads)
+            recs += [(zx._core.X, 0, int(q)) for q in rng.choice(n, n // 3, replace=False)]
+        recs += [(zx._core.U3, 0, q, *rng.uniform(0, 2 * np.pi, 3)) for q in range(n)]
+        if kind in ("cp", "mixed"):  # quadratic windows between the layers
+            recs += [(zx._core.CP, i, i + 1, float(rng.uniform(0, 2 * np.pi))) for i in range(n - 1)]
+            perm = rng.permutation(n)
+            recs += [(zx._core.CP, int(perm[2 * i]), int(perm[2 * i + 1]), np.pi) for i in range(n // 2)]
+    return zx.as_records(recs)
+
+
+@pytest.mark.parametrize("kind", ["plain", "flips", "cp", "mixed"])
+@pytest.mark.parametrize("n", [13, 14, 17, 23])
+@pytest.mark.parametrize("span", [1, 0])
+def test_span_passes(kind, n, span):
+    # complex64 U3 batches as span passes (13 gates on bits 0..12, up to 10 high-bit
+    # gates per strided pass), against the oracle; span = 0 is the row-pass plan
+    gates = _span_case(n, kind, 500 + n)
+    o = Oracle(n)
+    o.push(gates)
+    o.execute()
+    s = zx.ZXH(n, dtype="complex64")
+    s.set_param("span", span)
+    s.push_gates(gates)
+    s.execute()
+    assert max_err(s, o) <= TOL["complex64"]
+
+
+def test_span_pass_through_apply_round_trip():
+    # a 26-qubit U3 layer and its inverse through apply(): back to |+...+> (the
+    # layer runs as three span passes each way: 7 + 6 high-bit gates, 13 low)
+    n = 26
+    rng = np.random.default_rng(9)
+    ang = rng.uniform(0, 2 * np.pi, (n, 3))
+    fwd = zx.as_records([(zx._core.U3, 0, q, *ang[q]) for q in range(n)])
+    # U3(t, l, p)^-1 = U3(-t, -p, -l) (records carry theta, lambda, phi)
+    inv = zx.as_records([(zx._core.U3, 0, q, -ang[q][0], -ang[q][2], -ang[q][1]) for q in range(n)])
+    s = zx.ZXH(n, dtype="complex64")
+    s.push_gates(wl.h_all(n))
+    s.execute()
+    s.apply(fwd)
+    assert s.last_stats()[1] == 3
+    s.apply(inv)
+    ptr, m, eb, g = s.state_view()
+    import torch
+
+    class _CAI:
+        __cuda_array_interface__ = {"shape": (1 << m,), "typestr": "<c8", "data": (ptr, False), "version": 3}
+    st = torch.as_tensor(_CAI(), device="cuda").to(torch.complex128) * complex(g)
+    want = 2.0 ** (-n / 2)
+    assert float((st - want).abs().max()) < 1e-6

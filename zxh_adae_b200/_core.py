@@ -129,12 +129,12 @@ def plan_stats(n: int, gates, dtype: str = "complex64", disable_x: bool = False,
                eager_expand_all: bool = False) -> dict:
     """Host-only dry run of execute() (no GPU needed): state bits and pass counts."""
     rec = as_records(gates)
-    out = np.zeros(12, np.uint64)
+    out = np.zeros(13, np.uint64)
     rc = _lib.zxh_plan_stats(int(n), int(bool(disable_x)), int(bool(eager_expand_all)),
                              C64 if dtype == "complex64" else C128, rec.ctypes.data, len(rec), out.ctypes.data)
     if rc != 0:
         _raise(rc, None)
-    d = {"M": int(out[0]), "m": int(out[1]), "passes": int(out[10]), "walsh": int(out[11])}
+    d = {"M": int(out[0]), "m": int(out[1]), "passes": int(out[10]), "walsh": int(out[11]), "span": int(out[12])}
     d.update({k: int(out[2 + i]) for i, k in enumerate(PASS_KINDS)})
     return d
 

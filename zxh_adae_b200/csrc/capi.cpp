@@ -704,12 +704,12 @@ int zxh_plan_stats(size_t n, int disable_x, int eager_expand_all, int dtype, con
     if (int rc = zxh::walk(gl.data(), gl.size(), disable_x != 0, M, ws, ops, err)) return fail(nullptr, rc, err);
     zxh::Plan pl;
     if (int rc = zxh::plan(ops, eb, tmp.pp, start, pl, err)) return fail(nullptr, rc, err);
-    for (int k = 0; k < 12; k++) out[k] = 0;
+    for (int k = 0; k < 13; k++) out[k] = 0;
     out[0] = uint64_t(M);
     out[1] = uint64_t(ws.m);
     for (const zxh::Pass &p : pl.passes) {
-        if (p.kind == zxh::Pass::WALSH) {
-            out[11]++;
+        if (p.kind == zxh::Pass::WALSH || p.kind == zxh::Pass::SPAN) {
+            out[p.kind == zxh::Pass::WALSH ? 11 : 12]++;
             out[10]++;
             continue;
         }
@@ -745,6 +745,8 @@ int zxh_set_param(zxh_sim *s, const char *name, int value)
         {"diag_prefetch_c128", &s->pp.diag_prefetch_c128, 0, 1},
         {"walsh", &s->pp.walsh, 0, 1},
         {"walsh_min_general", &s->pp.walsh_min_general, 0, 1 << 20},
+        {"span", &s->pp.span, 0, 1},
+        {"span_min_run", &s->pp.span_min_run, 3, 8},
         {"diag_chunk_bits", &s->pp.diag_chunk_bits, -1, 8},
         {"grow", &s->pp.grow, 0, 1},
         {"grow_regs", &s->pp.grow_regs, 1, 4},

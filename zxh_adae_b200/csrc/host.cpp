@@ -1095,8 +1095,9 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
     // Fuses a window into a fast pass as prologue (pre) or epilogue when it is
     // small enough for per-thread evaluation; returns false otherwise.
     auto fuse_fast = [&](Pass &ps, const std::vector<DiagTerm> &w, bool pre) -> bool {
-        uint64_t &slot = ps.kind == Pass::ROW ? (pre ? ps.row.off_pre : ps.row.off_post)
-                                              : (pre ? ps.fast.off_pre : ps.fast.off_post);
+        uint64_t &slot = ps.kind == Pass::ROW    ? (pre ? ps.row.off_pre : ps.row.off_post)
+                         : ps.kind == Pass::SPAN ? (pre ? ps.span.off_pre : ps.span.off_post)
+                                                 : (pre ? ps.fast.off_pre : ps.fast.off_post);
         if (slot) return false;
         const size_t mark = out.blob.size();
         const uint64_t off = compile_diag(out.blob, w, ps.geom);
@@ -1116,8 +1117,9 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
         if (carry.empty()) return;
         const std::vector<DiagTerm> w = carry;
         carry.clear();
-        if (last_tile_pass >= 0 && out.passes[last_tile_pass].kind == Pass::ROW && out.passes[last_tile_pass].m == m &&
-            fuse_fast(out.passes[last_tile_pass], w, false)) {
+        if (last_tile_pass >= 0 &&
+            (out.passes[last_tile_pass].kind == Pass::ROW || out.passes[last_tile_pass].kind == Pass::SPAN) &&
+            out.passes[last_tile_pass].m == m && fuse_fast(out.passes[last_tile_pass], w, false)) {
             last_tile_pass = -1;
             return;
         }
@@ -1305,6 +1307,84 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
             std::vector<const U3Op *> gs;
             for (const U3Op &u : (split ? rot : op.u3)) gs.push_back(&u);
             std::sort(gs.begin(), gs.end(), [](const U3Op *a, const U3Op *b) { return a->delta < b->delta; });
+            if (split && elem_bytes == 8 && pp.span && mm >= span_tile_bits()) {
+                // span passes (span.cu): the gates on bits 0..T-1 in one low pass, the rest
+                // in as few strided passes as take T - 3 each, spread evenly (fewer gates
+                // per pass = longer contiguous runs, c = T - gates); the low pass runs
+                // last, like the row passes' (the windows then land on the strided passes)
+                const int T = span_tile_bits();
+                std::vector<const U3Op *> lowg, highg;
+                for (const U3Op *u : gs) (__builtin_ctzll(u->delta) < T ? lowg : highg).push_back(u);
+                const int first_pass = int(out.passes.size());
+                auto emit_span = [&](const std::vector<const U3Op *> &grp, bool low) {
+                    std::vector<int> dirs;
+                    if (!low)
+                        for (const U3Op *u : grp) dirs.push_back(__builtin_ctzll(u->delta));
+                    const int c = low ? T : T - int(dirs.size());
+                    Pass ps;
+                    ps.kind = Pass::SPAN;
+                    ps.m = mm;
+                    ps.low = low ? 1 : 0;
+                    ps.geom = make_geom(mm, c, dirs);
+                    std::memset(&ps.span, 0, sizeof(ps.span));
+                    ps.span.m = uint32_t(mm);
+                    ps.span.c = uint32_t(c);
+                    ps.span.low = low ? 1u : 0u;
+                    for (int k2 = 0; k2 < T; k2++) {
+                        ps.span.pos[k2] = ps.geom.pos[k2];
+                        ps.span.rot[k2][0] = 0.0f;
+                        ps.span.rot[k2][1] = 0.0f;
+                    }
+                    ps.span.tile_mask = ps.geom.tile_mask;
+                    ps.span.ntiles = ps.geom.ntiles;
+                    double scale = 1.0;
+                    for (const U3Op *u : grp) {
+                        const int b = __builtin_ctzll(u->delta);
+                        const int coord = int(std::find(ps.geom.pos, ps.geom.pos + T, uint8_t(b)) - ps.geom.pos);
+                        ps.span.gates |= 1u << coord;
+                        // R = [[c, -s], [s, c]]; with beta = 1 the partner at bit value 0
+                        // leads, which is R with s negated. One coefficient is factored out
+                        // (the larger of |c|, |s|), the factors multiply into scale.
+                        const double cc = u->u[0].real(), ss = u->sel.beta ? -u->u[2].real() : u->u[2].real();
+                        if (std::fabs(cc) >= std::fabs(ss)) {
+                            ps.span.rot[coord][0] = float(ss / cc);
+                            ps.span.rot[coord][1] = 0.0f;
+                            scale *= cc;
+                        } else {
+                            ps.span.rot[coord][0] = float(cc / ss);
+                            ps.span.rot[coord][1] = 1.0f;
+                            scale *= ss;
+                        }
+                    }
+                    ps.span.scale = float(scale);
+                    out.passes.push_back(ps);
+                    last_tile_pass = int(out.passes.size()) - 1;
+                };
+                const int H = int(highg.size());
+                const int per = T - std::max(3, std::min(8, pp.span_min_run));
+                const int np = (H + per - 1) / per;
+                size_t kk = 0;
+                for (int pi = 0; pi < np; pi++) {
+                    const size_t G = size_t(H / np + (pi < H % np ? 1 : 0));
+                    emit_span(std::vector<const U3Op *>(highg.begin() + long(kk), highg.begin() + long(kk + G)), false);
+                    kk += G;
+                }
+                if (!lowg.empty()) emit_span(lowg, true);
+                if (held) {
+                    if (!fuse_fast(out.passes[first_pass], *held, true)) {
+                        // not fusable: run it on its own, before the batch
+                        const std::vector<DiagTerm> w = *held;
+                        std::vector<Pass> batch(out.passes.begin() + first_pass, out.passes.end());
+                        out.passes.resize(first_pass);
+                        standalone_diag(mm, w);
+                        for (Pass &p2 : batch) out.passes.push_back(p2);
+                        last_tile_pass = int(out.passes.size()) - 1;
+                    }
+                    held = nullptr;
+                }
+                m = mm;
+                continue;
+            }
             auto emit_row = [&](const std::vector<const U3Op *> &fixed, const std::vector<const U3Op *> &grp, int low) {
                 std::vector<int> rb;
                 for (const U3Op *u : grp) rb.push_back(__builtin_ctzll(u->delta));
@@ -1408,7 +1488,8 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
             const bool next_u3 = i + 1 < ops.size() && ops[i + 1].kind == Op::U3BATCH && ops[i + 1].m == op.m;
             const bool spare_low = last_tile_pass >= 0 && out.passes[last_tile_pass].low && next_u3;
             if (!spare_low && last_tile_pass >= 0 &&
-                (out.passes[last_tile_pass].kind == Pass::FAST || out.passes[last_tile_pass].kind == Pass::ROW) &&
+                (out.passes[last_tile_pass].kind == Pass::FAST || out.passes[last_tile_pass].kind == Pass::ROW ||
+                 out.passes[last_tile_pass].kind == Pass::SPAN) &&
                 out.passes[last_tile_pass].m == op.m && fuse_fast(out.passes[last_tile_pass], *wd, false)) {
                 last_tile_pass = -1;
             } else if (last_tile_pass >= 0 && out.passes[last_tile_pass].kind == Pass::GROW &&
@@ -1578,6 +1659,17 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
         if (ps.kind == Pass::ROW) {
             ps.row.off_gates = put_vec(out.blob, ps.fgates);
             ps.off = put(out.blob, ps.row);
+            continue;
+        }
+        if (ps.kind == Pass::SPAN) {
+            ps.real = 0;  // the kernel form for its windows
+            for (const uint64_t ow : {ps.span.off_pre, ps.span.off_post}) {
+                if (!ow) continue;
+                const DiagDev *d = reinterpret_cast<const DiagDev *>(out.blob.data() + ow);
+                const bool lin = d->n_in_quad == 0 && d->n_cross == 0 && d->n_out_quad == 0 && d->n_gen == 0;
+                ps.real = std::max(ps.real, lin ? 1 : 2);
+            }
+            ps.off = put(out.blob, ps.span);
             continue;
         }
         if (ps.kind == Pass::FAST) {

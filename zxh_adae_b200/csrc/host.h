@@ -71,6 +71,11 @@ struct PlanParams {
                                 // instead of general terms evaluated per amplitude (split every 32 terms)
     int walsh_min_general = 2;  // general (multi-bit selector) terms from which a standalone window takes the
                                 // Walsh pass; 0: every standalone window does
+    int span = 1;               // complex64 U3 batches (real split) run as span passes: 13 gates on bits 0..12,
+                                // then up to 10 high-bit gates per pass (span.cu); 0: the register-row passes
+    int span_min_run = 3;       // log2 of the shortest run of contiguous amplitudes a strided span pass
+                                // reads (3..8: 64 B .. 2 KiB): its gates number at most 13 - span_min_run
+                                // (3: a 32-qubit layer in 3 passes, 54.7 ms on B200, vs 4 passes, 57.2 ms)
 };
 
 // General strided pass shape (grow.cu): fixed low bits and register coordinates.
@@ -99,7 +104,7 @@ struct GrowBuild {
 };
 
 struct Pass {
-    enum Kind { PRODUCT, EXPAND, TILE, PAIR, DIAG, FAST, ROW, GROW, INIT, WALSH } kind;  // INIT: |0...0> (grow_only)
+    enum Kind { PRODUCT, EXPAND, TILE, PAIR, DIAG, FAST, ROW, GROW, INIT, WALSH, SPAN } kind;  // INIT: |0...0> (grow_only)
     int m = 0;
     uint64_t off = 0;    // blob offset of the pass descriptor
     uint64_t off2 = 0;   // PRODUCT: lookup table; DIAG: exp table
@@ -107,9 +112,12 @@ struct Pass {
     std::vector<StepDev> steps;
     FastDev fast;                        // FAST
     RowPassDev row;                      // ROW
+    SpanDev span;                        // SPAN
     int wide = 0;                        // ROW: kernel shape
-    int low = 0;                         // ROW: the low pass (lane bits 0..3 swapped into registers)
-    int real = 0;                        // ROW: every gate matrix is real
+    int low = 0;                         // ROW: the low pass (lane bits 0..3 swapped into registers);
+                                         // SPAN: the tile is real bits 0..12
+    int real = 0;                        // ROW: every gate matrix is real; SPAN: its windows (0 none,
+                                         // 1 linear terms only, 2 quadratic terms), set when the plan is done
     int chunk_bits = -1;                 // DIAG: tiles per Gray-code chunk (log2, -1 = automatic)
     int row_bits = 0;                    // DIAG: log2 rows of a warp tile; WALSH: the window's term count
     int prefetch = 0;                    // DIAG: tiles staged one ahead by TMA bulk copies; GROW: the
@@ -129,6 +137,10 @@ struct Plan {
 // one fast-pass round.
 int diag_tile_bits(int elem_bytes, int row_bits);
 int walsh_tile_bits(int elem_bytes);
+// Span pass (span.cu): tile coordinates, and whether the gates of `gates` (bit k =
+// coordinate k) sit on coordinates the pass's layouts hold in registers.
+int span_tile_bits();
+bool span_coverable(uint32_t gates, bool low);
 int fast_tile_bits(int elem_bytes);
 int fast_reg_bits(int elem_bytes);
 int row_reg_bits(int elem_bytes, int wide);
