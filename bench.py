@@ -96,6 +96,8 @@ def parse():
                     choices=["diag", "cxwindow", "u3", "adjoint", "batch", "sample", "config2", "config3"])
     ap.add_argument("--dtype", default="complex64", choices=["complex64", "complex128"],
                     help="diag / cxwindow / u3 workloads: the state's type")
+    ap.add_argument("--set-param", action="append", default=[], metavar="NAME=VALUE",
+                    help="planner knob (zxh_set_param) on the headline workload's simulators, e.g. span=0")
     ap.add_argument("--no-tune", action="store_true", help="batch workload: skip the autotuner")
     ap.add_argument("--batch-count", type=int, default=512, help="batch workload: circuits")
     ap.add_argument("--no-extras", action="store_true", help="skip the U3-layer and adjoint legs of the diag line")
@@ -663,7 +665,7 @@ def timed_applies(sim, batches, warmup, steps, pg, local):
     return dev_ms, launches, passes, wall, clk.summary()
 
 
-def timed_async(n, dtype, local, batches, warmup, steps, pg, prefix=None) -> float:
+def timed_async(n, dtype, local, batches, warmup, steps, pg, prefix=None, knobs=()) -> float:
     """End-to-end wall time of K zxh_apply_async calls and the closing zxh_sync on a
     fresh H-prepared simulator: every step plans on the host, uploads its program
     from pinned memory and reads its status word back; step k + 1 is planned while
@@ -672,6 +674,8 @@ def timed_async(n, dtype, local, batches, warmup, steps, pg, prefix=None) -> flo
     from zxh_adae_b200 import workloads as wl
 
     sim = zx.ZXH(n, dtype=dtype, device=local)
+    for k, v in knobs:
+        sim.set_param(k, v)
     sim.push_gates(wl.h_all(n))
     sim.execute()
     if prefix is not None:
@@ -865,7 +869,10 @@ def run_ours(args):
                             checks=not args.no_adjoint_checks)
             print(json.dumps({"metric": METRIC, "workload": "adjoint", **d}))
         return
+    knobs = [(kv.split("=")[0], int(kv.split("=")[1])) for kv in args.set_param]
     sim = zx.ZXH(n, dtype=dtype, device=local)
+    for k, v in knobs:
+        sim.set_param(k, v)
     sim.push_gates(wl.h_all(n))
     sim.execute()
     tag = "c64" if dtype == "complex64" else "c128"
@@ -873,7 +880,9 @@ def run_ours(args):
     if args.workload == "u3":
         batches = [wl.u3_layer(n, seed=rank * 100000 + k) for k in range(args.warmup + args.steps)]
         desc = f"U3 layer on all {n} qubits, {dtype}, H-prepared, random angles per step"
-        dominant, traffic_file = "row_pass_kernel", f"row_pass_{n}q_{tag}.md"
+        span = dtype == "complex64" and dict(knobs).get("span", 1) != 0
+        dominant = "span_kernel" if span else "row_pass_kernel"
+        traffic_file = f"span_pass_{n}q_{tag}.md" if span else f"row_pass_{n}q_{tag}.md"
     elif args.workload == "cxwindow":
         # a CX chain first (map updates only): every selector of the windows is then
         # a parity of several real bits, and each window is one Walsh-sum pass
@@ -896,7 +905,7 @@ def run_ours(args):
         fid = fidelity_err(sim, ref)
         ref.close()
     sim.close()
-    wall_async = timed_async(n, dtype, local, batches, args.warmup, args.steps, pg, prefix)
+    wall_async = timed_async(n, dtype, local, batches, args.warmup, args.steps, pg, prefix, knobs)
     bytes_step = (passes / args.steps) * 2 * state
     dev_total_ms = max_over_ranks(pg, sum(dev_ms), local)
     wall = max_over_ranks(pg, wall, local)
@@ -951,6 +960,7 @@ def run_ours(args):
             "state_bytes": state,
             "l2": "state larger than L2, no flush" if state > 126 * 2**20 else "state fits in L2",
             "fidelity_err_vs_complex128": fid,
+            "planner_knobs": dict(knobs),
             "parallelism": f"replicas x{world}",
         },
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(len(batches[0]) * 40),
