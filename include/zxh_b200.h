@@ -80,6 +80,11 @@ typedef struct zxh_sim zxh_sim;
 /* Library version string. */
 const char *zxh_version(void);
 
+/* Name (NUL-terminated, at most capacity - 1 characters) and SM count of CUDA
+ * device `device`; either pointer may be NULL. Used to key tuned settings. No
+ * counterpart in the reference. */
+int zxh_device_info(int device, char *name, size_t capacity, int *sms);
+
 /* Message of the last failing call on this handle, or of the last failing
  * zxh_create in this thread when sim is NULL. Never NULL. */
 const char *zxh_last_error(const zxh_sim *sim);
@@ -270,17 +275,20 @@ int zxh_batch_gradient_offsets(const zxh_batch *batch, size_t *offsets);
  * that launch from a CUDA graph captured on first use. */
 int zxh_batch_run(zxh_batch *batch, int mode, double *energies, double *grads, size_t ngrads);
 /* Knobs: grow_regs (1..4, gates with high deltas per general strided pass),
- * task_items (pass items per task), task_elems (amplitudes per task of the
- * element-wise passes); setting one of these recompiles the batch.
+ * adj_regs (1..3, the same for the reverse passes), task_items (pass items per
+ * task), task_elems (amplitudes per task of the element-wise passes); setting
+ * one of these recompiles the batch. threads (64, 128 or 256): threads per CTA
+ * of the persistent kernel, i.e. the warps that work on one task.
  * wait_limit_log2 (0..31, default 31): a persistent task waits at most
  * 2^wait_limit_log2 SM clocks for the previous pass of its circuit, then the run
  * ends early and zxh_batch_run returns ZXH_ERR_TIMEOUT; the handle stays usable
  * (the next run starts from scratch). Small values exist to test that path. */
 int zxh_batch_set(zxh_batch *batch, const char *name, int value);
 int zxh_batch_get(const zxh_batch *batch, const char *name, int *value);
-/* Times the persistent launch over grow_regs in {2, 3, 4} x task_items in {32,
- * 128, 512, 2048} (task_elems = 1024 x task_items; reps timed runs each after one
- * warm-up) and keeps the fastest. */
+/* Times the persistent launch (reps timed runs per setting after one warm-up)
+ * and keeps the fastest: grow_regs in {2, 3, 4} x task_items in {32, 128, 512,
+ * 2048} (task_elems = 1024 x task_items), then threads in {64, 128, 256}, then
+ * adj_regs in {1, 2, 3}, each at the best setting so far. */
 int zxh_batch_tune(zxh_batch *batch, int reps);
 /* ops and tasks of the compiled batch, device ms of the last run, and the
  * algorithmic state bytes of one run (each pass reads and writes its states once:

@@ -103,18 +103,32 @@ def test_batch_complex64_against_complex128():
         assert np.max(np.abs(gi - gr)) < 1e-5
 
 
-def test_batch_tune_and_knobs():
+def test_batch_tune_and_knobs(tmp_path):
     circ = wl.batch_tfim(24, 6, nmin=6, nmax=13, layers=2)
     b = Batch([(c[0], c[1], c[2]) for c in circ], dtype="complex64")
     e0, g0 = b.run("persistent")
-    best = b.tune(reps=1)
+    best = b.tune(reps=1, cache=tmp_path / "tune.json")
+    assert not best["cached"]
     assert best["grow_regs"] in (2, 3, 4) and best["task_items"] in (32, 128, 512, 2048)
+    assert best["threads"] in (64, 128, 256) and best["adj_regs"] in (1, 2, 3)
     e1, g1 = b.run("graph")
     assert np.max(np.abs(e1 - e0)) < 1e-5 and np.max(np.abs(g1 - g0)) < 1e-5
-    b.set("grow_regs", 1)
-    b.set("task_items", 3)
-    e2, g2 = b.run("persistent")
-    assert np.max(np.abs(e2 - e0)) < 1e-5 and np.max(np.abs(g2 - g0)) < 1e-5
+    # a second batch of the same shape takes the stored settings without timing
+    b2 = Batch([(c[0], c[1], c[2]) for c in circ], dtype="complex64")
+    again = b2.tune(reps=1, cache=tmp_path / "tune.json")
+    assert again["cached"] and {k: again[k] for k in b2.settings()} == b.settings() == b2.settings()
+    e3, g3 = b2.run("persistent")
+    assert np.max(np.abs(e3 - e0)) < 1e-5 and np.max(np.abs(g3 - g0)) < 1e-5
+    # every knob value runs and agrees
+    for knobs in ({"grow_regs": 1, "task_items": 3}, {"threads": 64}, {"threads": 128, "adj_regs": 1},
+                  {"threads": 256, "adj_regs": 2}):
+        for k, v in knobs.items():
+            b.set(k, v)
+        for mode in ("persistent", "graph"):
+            e2, g2 = b.run(mode)
+            assert np.max(np.abs(e2 - e0)) < 1e-5 and np.max(np.abs(g2 - g0)) < 1e-5, (knobs, mode)
+    with pytest.raises(ValueError):
+        b.set("threads", 96)
     ops, tasks, ms = b.stats()
     assert ops > 0 and tasks >= ops and ms > 0
 

@@ -91,6 +91,7 @@ _sig("zxh_state_view", [_P, ctypes.POINTER(_P), ctypes.POINTER(_SZ), ctypes.POIN
 _sig("zxh_stream", [_P, ctypes.POINTER(_P)])
 _sig("zxh_set_param", [_P, ctypes.c_char_p, ctypes.c_int])
 _sig("zxh_plan_stats", [_SZ, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _SZ, _P])
+_sig("zxh_device_info", [ctypes.c_int, ctypes.c_char_p, _SZ, ctypes.POINTER(ctypes.c_int)])
 _sig("zxh_optimize_gates", [_SZ, ctypes.c_int, _P, _SZ, _P, _SZ, ctypes.POINTER(_SZ)])
 _sig("zxh_last_stats", [_P, ctypes.POINTER(_U64), ctypes.POINTER(_U64), ctypes.POINTER(_D)])
 _sig("zxh_expectation", [_P, _P, _SZ, ctypes.POINTER(_D)])
@@ -123,6 +124,16 @@ def _raise(rc: int, handle) -> None:
 
 
 PASS_KINDS = ("product", "expand", "tile", "pair", "diagonal", "fast", "row", "grow")  # out[2..9]
+
+
+def device_info(device: int = 0) -> tuple:
+    """(name, SM count) of a CUDA device (zxh_device_info)."""
+    buf = ctypes.create_string_buffer(256)
+    sms = ctypes.c_int(0)
+    rc = _lib.zxh_device_info(int(device), buf, 256, ctypes.byref(sms))
+    if rc != 0:
+        _raise(rc, None)
+    return buf.value.decode(errors="replace"), int(sms.value)
 
 
 def plan_stats(n: int, gates, dtype: str = "complex64", disable_x: bool = False,

@@ -7,7 +7,9 @@ terms; the library compiles every circuit once into a chain of passes and runs
 all chains either one launch at a time (``"sequential"``), in one persistent
 kernel that takes tasks from a queue (``"persistent"``), or by replaying that
 launch from a captured CUDA graph (``"graph"``). ``tune()`` times the persistent
-launch over the pass shape and the task size and keeps the fastest.
+launch over the gate-fusion depth, the task size (the tile of work one CTA
+takes), the threads per CTA and the reverse passes' depth, keeps the fastest,
+and can persist the choice (tuning.py).
 """
 from __future__ import annotations
 
@@ -16,7 +18,8 @@ import ctypes
 import numpy as np
 
 from . import _core
-from ._core import _D, _P, _SZ, _U64, C64, C128, _lib, as_records, as_terms
+from ._core import _D, _P, _SZ, _U64, C64, C128, _lib, as_records, as_terms, device_info
+from .tuning import KNOBS, TuneCache, batch_key
 
 MODES = {"sequential": 0, "persistent": 1, "graph": 2}
 _ERRORS = _core._ERRORS
@@ -53,6 +56,8 @@ class Batch:
         self._h = h
         self.count = len(circuits)
         self.nqubits = nq
+        self.dtype = dtype
+        self.device = int(device)
         off = np.zeros(self.count + 1, np.uint64)
         self._ck(_lib.zxh_batch_gradient_offsets(self._h, off.ctypes.data))
         self.grad_offsets = off.astype(np.int64)
@@ -89,9 +94,26 @@ class Batch:
         self._ck(_lib.zxh_batch_get(self._h, name.encode(), ctypes.byref(v)))
         return int(v.value)
 
-    def tune(self, reps: int = 1) -> dict:
+    def settings(self) -> dict:
+        """The knob settings in use (tuning.KNOBS)."""
+        return {k: self.get(k) for k in KNOBS}
+
+    def tune(self, reps: int = 1, cache=None) -> dict:
+        """Times the persistent launch over its knobs (zxh_batch_tune) and keeps
+        the fastest. cache: a path (or TuneCache); settings found there for this
+        batch's shape and GPU are applied without timing, and new ones are stored."""
+        tc = cache if isinstance(cache, TuneCache) or cache is None else TuneCache(cache)
+        key = batch_key(self.nqubits, self.dtype, *device_info(self.device)) if tc else None
+        hit = tc.get(key) if tc else None
+        if hit:
+            for k in KNOBS:
+                self.set(k, hit[k])
+            return {**hit, "cached": True}
         self._ck(_lib.zxh_batch_tune(self._h, int(reps)))
-        return {k: self.get(k) for k in ("grow_regs", "task_items", "task_elems")}
+        out = self.settings()
+        if tc:
+            tc.put(key, out)
+        return {**out, "cached": False}
 
     def stats(self) -> tuple:
         """(ops, tasks, device ms of the last run)."""

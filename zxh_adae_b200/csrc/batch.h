@@ -42,12 +42,13 @@ struct BatchTask {
 
 // Runs every task of the queue; counters: `next` (queue head, zeroed) and
 // `remaining[op]` (tasks of each op, preset). grid = resident CTAs. real: every
-// strided op of the queue has real gates (the kernel's real-gate form). A task
-// waits at most 2^wait_limit_log2 SM clocks for its op's predecessor; then it
-// records a timeout in the status word and its CTA ends.
+// strided op of the queue has real gates (the kernel's real-gate form). threads:
+// 64, 128 or 256 per CTA (the warps that work on one task). A task waits at most
+// 2^wait_limit_log2 SM clocks for its op's predecessor; then it records a timeout
+// in the status word and its CTA ends.
 cudaError_t run_batch_persistent(const uint8_t *blob, const BatchOp *ops, const BatchTask *tasks, uint32_t ntasks,
                                  uint32_t *next, uint32_t *remaining, void *arena, double *grads, double *energies,
-                                 DevStatus *status, int elem_bytes, bool real, int wait_limit_log2, int sms,
-                                 cudaStream_t st);
+                                 DevStatus *status, int elem_bytes, bool real, int threads, int wait_limit_log2,
+                                 int sms, cudaStream_t st);
 
 }  // namespace zxh

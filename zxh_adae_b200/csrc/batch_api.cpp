@@ -61,6 +61,8 @@ struct zxh_batch {
     cudaGraphExec_t gexec = nullptr;
 
     int grow_regs = 4, task_items = 128, task_elems = 1 << 17;
+    int threads = 256;         // threads per CTA of the persistent kernel (the warps working on one task)
+    int adj_regs = 3;          // register coordinates (gates with high deltas) per reverse pass
     int wait_limit_log2 = 31;  // a task's wait for its predecessor: 2^31 SM clocks (about a second)
     uint64_t bytes = 0;  // algorithmic state bytes of one run
     bool real = false;   // every strided op has real gates: the persistent kernel's real-gate form
@@ -131,7 +133,7 @@ int compile(zxh_batch *b)
     zxh::PlanParams pp;
     pp.grow_only = 1;
     pp.grow_regs = b->grow_regs;
-    pp.adj_regs = 3;  // the persistent kernel runs reverse passes of at most 3 register coordinates
+    pp.adj_regs = b->adj_regs;  // the persistent kernel runs reverse passes of at most 3 register coordinates
     std::vector<uint8_t> etab;
     zxh::exp_table(b->eb, etab);
     const uint64_t exp_off = append(b->blob, etab.data(), etab.size());
@@ -316,7 +318,7 @@ int enqueue_persistent(zxh_batch *b)
         "reset counters");
     BCK(b, zxh::run_batch_persistent(b->d_blob, b->d_ops, b->d_tasks, uint32_t(b->tasks.size()), b->d_next, b->d_rem,
                                      b->d_arena, b->d_grads, b->d_energy, b->d_status, b->eb, b->real,
-                                     b->wait_limit_log2, b->sms, b->stream),
+                                     b->threads, b->wait_limit_log2, b->sms, b->stream),
         "batch launch");
     return ZXH_OK;
 }
@@ -519,18 +521,22 @@ int zxh_batch_set(zxh_batch *b, const char *name, int value)
     else if (!std::strcmp(name, "task_items")) field = &b->task_items, lo = 1, hi = 1 << 20;
     else if (!std::strcmp(name, "task_elems")) field = &b->task_elems, lo = 256, hi = 1 << 26;
     else if (!std::strcmp(name, "wait_limit_log2")) field = &b->wait_limit_log2, lo = 0, hi = 31;
+    else if (!std::strcmp(name, "threads")) field = &b->threads, lo = 64, hi = 256;
+    else if (!std::strcmp(name, "adj_regs")) field = &b->adj_regs, lo = 1, hi = 3;
     else return bfail(b, ZXH_ERR_ARG, std::string("unknown batch parameter ") + name);
-    if (value < lo || value > hi)
+    if (value < lo || value > hi || (field == &b->threads && value != 64 && value != 128 && value != 256))
         return bfail(b, ZXH_ERR_ARG, std::string(name) + " must be in [" + std::to_string(lo) + ", " +
-                                         std::to_string(hi) + "]");
+                                         std::to_string(hi) + "]" +
+                                         (field == &b->threads ? " and one of 64, 128, 256" : ""));
     *field = value;
     BCK(b, cudaSetDevice(b->device), "cudaSetDevice");
-    if (field == &b->wait_limit_log2) {  // a launch argument: only the captured graph holds the old value
+    if (field == &b->wait_limit_log2 || field == &b->threads) {
+        // launch parameters: only the captured graph holds the old value
         BCK(b, cudaStreamSynchronize(b->stream), "sync");
         drop_graph(b);
         return ZXH_OK;
     }
-    return field == &b->grow_regs ? build(b) : retask(b);
+    return (field == &b->grow_regs || field == &b->adj_regs) ? build(b) : retask(b);
 }
 
 int zxh_batch_get(const zxh_batch *b, const char *name, int *value)
@@ -540,6 +546,8 @@ int zxh_batch_get(const zxh_batch *b, const char *name, int *value)
     else if (!std::strcmp(name, "task_items")) *value = b->task_items;
     else if (!std::strcmp(name, "task_elems")) *value = b->task_elems;
     else if (!std::strcmp(name, "wait_limit_log2")) *value = b->wait_limit_log2;
+    else if (!std::strcmp(name, "threads")) *value = b->threads;
+    else if (!std::strcmp(name, "adj_regs")) *value = b->adj_regs;
     else return ZXH_ERR_ARG;
     return ZXH_OK;
 }
@@ -561,6 +569,16 @@ int zxh_batch_tune(zxh_batch *b, int reps)
     BCK(b, cudaSetDevice(b->device), "cudaSetDevice");
     const size_t ngr = b->grad_off.back();
     std::vector<double> e(b->n.size()), g(std::max<size_t>(ngr, 1));
+    // best of reps timed persistent runs (the first run of a setting warms up)
+    auto timed = [&](double &t) -> int {
+        t = 1e300;
+        for (int k = 0; k <= reps; k++) {
+            if (int rc = zxh_batch_run(b, ZXH_BATCH_PERSISTENT, e.data(), g.data(), g.size())) return rc;
+            if (k) t = std::min(t, double(b->last_ms));
+        }
+        return ZXH_OK;
+    };
+    // 1. gate-fusion depth x task size at the current threads and reverse depth
     const int regs_c[] = {2, 3, 4};
     const int items_c[] = {32, 128, 512, 2048};
     double best = 1e300;
@@ -572,17 +590,42 @@ int zxh_batch_tune(zxh_batch *b, int reps)
             b->task_items = it;
             b->task_elems = it * 1024;
             if (int rc = retask(b)) return rc;
-            double t = 1e300;
-            for (int k = 0; k <= reps; k++) {  // first run warms up
-                if (int rc = zxh_batch_run(b, ZXH_BATCH_PERSISTENT, e.data(), g.data(), g.size())) return rc;
-                if (k) t = std::min(t, double(b->last_ms));
-            }
+            double t;
+            if (int rc = timed(t)) return rc;
             if (t < best) best = t, best_r = r, best_i = it;
         }
     }
     b->grow_regs = best_r;
     b->task_items = best_i;
     b->task_elems = best_i * 1024;
+    if (int rc = build(b)) return rc;
+    // 2. threads per CTA (the warps that share a task) at that setting
+    const int threads_c[] = {64, 128, 256};
+    int best_n = b->threads;
+    for (int nt : threads_c) {
+        if (nt == best_n) continue;
+        const int keep = b->threads;
+        b->threads = nt;
+        double t;
+        if (int rc = timed(t)) return rc;
+        if (t < best) best = t, best_n = nt;
+        b->threads = keep;
+    }
+    b->threads = best_n;
+    // 3. register coordinates per reverse pass (fewer: more passes, less register pressure)
+    int best_a = b->adj_regs;
+    for (int a = 1; a <= 3; a++) {
+        if (a == best_a) continue;
+        const int keep = b->adj_regs;
+        b->adj_regs = a;
+        if (int rc = build(b)) return rc;
+        double t;
+        if (int rc = timed(t)) return rc;
+        if (t < best) best = t, best_a = a;
+        b->adj_regs = keep;
+    }
+    b->adj_regs = best_a;
+    drop_graph(b);
     return build(b);
 }
 

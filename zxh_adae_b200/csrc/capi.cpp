@@ -174,6 +174,20 @@ extern "C" {
 
 const char *zxh_version(void) { return "zxh_b200 0.1.0 (sm_100a)"; }
 
+int zxh_device_info(int device, char *name, size_t capacity, int *sms)
+{
+    if (device < 0) return ZXH_ERR_ARG;
+    cudaDeviceProp prop;
+    const cudaError_t e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess) return ZXH_ERR_CUDA;
+    if (name && capacity) {
+        std::strncpy(name, prop.name, capacity - 1);
+        name[capacity - 1] = '\0';
+    }
+    if (sms) *sms = prop.multiProcessorCount;
+    return ZXH_OK;
+}
+
 const char *zxh_last_error(const zxh_sim *sim)
 {
     if (!sim) return g_create_error.c_str();

@@ -282,7 +282,7 @@ __device__ __forceinline__ void apply_poly(VT (&x)[1 << R], const WinPoly<R> (&P
     }
 }
 
-template <typename E>
+template <typename E, int NT = kThreads>
 struct GrowShared {
     using RT = typename ET<E>::R;
     E s_exp[1 << kExpTableBits];
@@ -292,11 +292,11 @@ struct GrowShared {
     uint64_t s_alpha[kGrowMaxSel];
     int8_t s_kb[kGrowMaxSel];
     GrowTermDev s_t[2][kGrowMaxTerms];
-    double s_red[kThreads / 32];
+    double s_red[NT / 32];
     uint8_t s_mu[kGrowMaxSel];                     // selector bits inside the lane / vector bits
     uint64_t s_bmask;                              // selector betas
-    double s_tacc[kThreads / 32][kGrowMaxTerms];   // adjoint windows: per-warp term gradients
-    double s_gacc[kThreads / 32][kGrowAdjGates][32];  // adjoint gates: per-lane gradient sums (off the registers)
+    double s_tacc[NT / 32][kGrowMaxTerms];         // adjoint windows: per-warp term gradients
+    double s_gacc[NT / 32][kGrowAdjGates][32];     // adjoint gates: per-lane gradient sums (off the registers)
 };
 
 // Adjoint window gradients of one item, before the inverse phases are applied.
@@ -459,10 +459,11 @@ __host__ __device__ constexpr size_t grow_stage_bytes()
 // psi_src (optional): psi is read from there and written to psi (the adjoint
 // sweep's first pass after a checkpoint reads the checkpoint instead of copying
 // it back first); every amplitude is read before it is written, by its own warp.
-template <typename E, int R, bool ADJ, bool REAL = false, bool PF = false>
+// NT: threads of the CTA (a multiple of 32).
+template <typename E, int R, bool ADJ, bool REAL = false, bool PF = false, int NT = kThreads>
 __device__ __forceinline__ void grow_body(const uint8_t *__restrict__ blob, uint64_t poff, uint64_t toff,
                                           E *__restrict__ psi, E *__restrict__ lam, double *grads, uint64_t first,
-                                          uint64_t step, uint64_t end, GrowShared<E> &sm, uint8_t *stage = nullptr,
+                                          uint64_t step, uint64_t end, GrowShared<E, NT> &sm, uint8_t *stage = nullptr,
                                           DevStatus *status = nullptr, const E *psi_src = nullptr)
 {
     const E *ps = psi_src ? psi_src : psi;
@@ -472,7 +473,7 @@ __device__ __forceinline__ void grow_body(const uint8_t *__restrict__ blob, uint
     constexpr int LV = (V == 2) ? 1 : 0;
     constexpr int F = 5 + LV;
     constexpr int NR = 1 << R;
-    constexpr int WARPS = kThreads / 32;
+    constexpr int WARPS = NT / 32;
 
     const GrowDev &p = *reinterpret_cast<const GrowDev *>(blob + poff);
     const GrowGateDev *gates = reinterpret_cast<const GrowGateDev *>(blob + p.off_gates);
@@ -493,11 +494,11 @@ __device__ __forceinline__ void grow_body(const uint8_t *__restrict__ blob, uint
 
     if (win0 || win1) {
         const E *tab = reinterpret_cast<const E *>(blob + toff);
-        for (int i = tid; i < (1 << kExpTableBits); i += kThreads) s_exp[i] = tab[i];
+        for (int i = tid; i < (1 << kExpTableBits); i += NT) s_exp[i] = tab[i];
     }
     for (int w = 0; w < 2; w++) {
         const GrowTermDev *tt = reinterpret_cast<const GrowTermDev *>(blob + p.off_terms[w]);
-        for (uint32_t i = uint32_t(tid); i < p.ncls[w][2]; i += kThreads) s_t[w][i] = tt[i];
+        for (uint32_t i = uint32_t(tid); i < p.ncls[w][2]; i += NT) s_t[w][i] = tt[i];
     }
     if (tid < int(ngates)) {
         const GrowGateDev &gg = gates[tid];
@@ -523,8 +524,8 @@ __device__ __forceinline__ void grow_body(const uint8_t *__restrict__ blob, uint
         sm.s_bmask = bm;
     }
     if constexpr (ADJ) {
-        for (uint32_t i = uint32_t(tid); i < uint32_t(WARPS) * kGrowMaxTerms; i += kThreads) (&sm.s_tacc[0][0])[i] = 0.0;
-        for (uint32_t i = uint32_t(tid); i < uint32_t(WARPS) * kGrowAdjGates * 32; i += kThreads)
+        for (uint32_t i = uint32_t(tid); i < uint32_t(WARPS) * kGrowMaxTerms; i += NT) (&sm.s_tacc[0][0])[i] = 0.0;
+        for (uint32_t i = uint32_t(tid); i < uint32_t(WARPS) * kGrowAdjGates * 32; i += NT)
             (&sm.s_gacc[0][0][0])[i] = 0.0;
     }
     // lane part of every selector (with beta), per vector slot
@@ -744,7 +745,7 @@ __device__ __forceinline__ void grow_body(const uint8_t *__restrict__ blob, uint
     if constexpr (ADJ) {
         if (win1) {
             __syncthreads();
-            for (uint32_t q = uint32_t(tid); q < p.ncls[1][2]; q += kThreads) {
+            for (uint32_t q = uint32_t(tid); q < p.ncls[1][2]; q += NT) {
                 if (!s_t[1][q].gk) continue;
                 double t = 0.0;
                 for (int w = 0; w < WARPS; w++) t += sm.s_tacc[w][q];
