@@ -497,33 +497,50 @@ def _span_case(n, kind, seed):
     return zx.as_records(recs)
 
 
+_SPAN_ORACLE = {}
+
+
+def _span_oracle_state(n, kind):
+    # one oracle run per circuit, shared by the dtype and plan variants
+    if (n, kind) not in _SPAN_ORACLE:
+        o = Oracle(n)
+        o.push(_span_case(n, kind, 500 + n))
+        o.execute()
+        _SPAN_ORACLE[(n, kind)] = o.get_state(0)
+    return _SPAN_ORACLE[(n, kind)]
+
+
 @pytest.mark.parametrize("kind", ["plain", "flips", "cp", "mixed"])
-@pytest.mark.parametrize("n", [13, 14, 17, 23])
+@pytest.mark.parametrize("n", [12, 13, 14, 17, 21, 23])
 @pytest.mark.parametrize("span", [1, 0])
-def test_span_passes(kind, n, span):
-    # complex64 U3 batches as span passes (13 gates on bits 0..12, up to 10 high-bit
-    # gates per strided pass), against the oracle; span = 0 is the row-pass plan
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_span_passes(kind, n, span, dtype):
+    # U3 batches as span passes against the oracle: complex64 tiles of 2^13 (13
+    # gates on bits 0..12, up to 10 high-bit gates per strided pass), complex128
+    # tiles of 2^12 (12 gates on bits 0..11, up to 9 per strided pass; at 21 qubits
+    # one strided pass of 9 gates, whose runs of 8 amplitudes need the third layout);
+    # span = 0 is the row-pass plan
     gates = _span_case(n, kind, 500 + n)
-    o = Oracle(n)
-    o.push(gates)
-    o.execute()
-    s = zx.ZXH(n, dtype="complex64")
+    want = _span_oracle_state(n, kind)
+    s = zx.ZXH(n, dtype=dtype)
     s.set_param("span", span)
     s.push_gates(gates)
     s.execute()
-    assert max_err(s, o) <= TOL["complex64"]
+    assert float(np.max(np.abs(s.get_state(0).astype(np.complex128) - want))) <= TOL[dtype]
 
 
-def test_span_pass_through_apply_round_trip():
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_span_pass_through_apply_round_trip(dtype):
     # a 26-qubit U3 layer and its inverse through apply(): back to |+...+> (the
-    # layer runs as three span passes each way: 7 + 6 high-bit gates, 13 low)
+    # layer runs as three span passes each way: complex64 7 + 6 high-bit gates and
+    # 13 low, complex128 7 + 7 and 12 low)
     n = 26
     rng = np.random.default_rng(9)
     ang = rng.uniform(0, 2 * np.pi, (n, 3))
     fwd = zx.as_records([(zx._core.U3, 0, q, *ang[q]) for q in range(n)])
     # U3(t, l, p)^-1 = U3(-t, -p, -l) (records carry theta, lambda, phi)
     inv = zx.as_records([(zx._core.U3, 0, q, -ang[q][0], -ang[q][2], -ang[q][1]) for q in range(n)])
-    s = zx.ZXH(n, dtype="complex64")
+    s = zx.ZXH(n, dtype=dtype)
     s.push_gates(wl.h_all(n))
     s.execute()
     s.apply(fwd)
@@ -533,7 +550,8 @@ def test_span_pass_through_apply_round_trip():
     import torch
 
     class _CAI:
-        __cuda_array_interface__ = {"shape": (1 << m,), "typestr": "<c8", "data": (ptr, False), "version": 3}
+        __cuda_array_interface__ = {"shape": (1 << m,), "typestr": "<c8" if dtype == "complex64" else "<c16",
+                                    "data": (ptr, False), "version": 3}
     st = torch.as_tensor(_CAI(), device="cuda").to(torch.complex128) * complex(g)
     want = 2.0 ** (-n / 2)
-    assert float((st - want).abs().max()) < 1e-6
+    assert float((st - want).abs().max()) < TOL[dtype]

@@ -41,12 +41,12 @@ def test_u3_layer_splits_into_low_and_strided_passes():
     rng = np.random.default_rng(0)
     lay = zx.as_records([(zx._core.U3, 0, q, *rng.uniform(0, 6.28, 3)) for q in range(30)])
     # complex64: span passes, 13 gates on bits 0..12 and the 17 high-bit gates in
-    # two strided passes (9 + 8, runs of 16 and 32 amplitudes); complex128: the
-    # register-row passes (one low pass of the 5 lane bits + 4, then passes of 4)
+    # two strided passes (9 + 8, runs of 16 and 32 amplitudes); complex128: 12 gates
+    # on bits 0..11 and two strided passes of 9 (runs of 8 amplitudes, 128 B)
     st = plan_stats(30, np.concatenate([wl.h_all(30), lay]), dtype="complex64")
     assert st["span"] == 3 and st["row"] == 0 and st["passes"] == 3
     st = plan_stats(30, np.concatenate([wl.h_all(30), lay]), dtype="complex128")
-    assert st["fast"] == 0 and st["row"] == 7 and st["passes"] == 7
+    assert st["span"] == 3 and st["row"] == 0 and st["passes"] == 3
     # 32 qubits: 13 + 10 + 9 (at most 10 high-bit gates per pass: runs of at
     # least 8 amplitudes)
     st = plan_stats(32, np.concatenate([wl.h_all(32), wl.u3_layer(32, 3)]))
@@ -57,7 +57,7 @@ def test_small_windows_fuse_into_u3_passes():
     st = plan_stats(20, wl.plain_layers(20, 10, 1))
     assert st["diagonal"] == 0 and st["passes"] == 20  # 10 layers x (1 strided + 1 low span pass), cp chains fused
     st = plan_stats(20, wl.plain_layers(20, 10, 1), dtype="complex128")
-    assert st["diagonal"] == 0 and st["passes"] == 40  # 10 layers x (1 low + 3 strided)
+    assert st["diagonal"] == 0 and st["passes"] == 20  # 10 layers x (1 strided + 1 low span pass)
     st = plan_stats(32, wl.u3_matching_layers(32, 4, 33))
     assert st["diagonal"] == 0 and st["passes"] == 12  # 3 span passes per layer, cz matchings fused
 

@@ -250,12 +250,12 @@ struct RowPassDev {
     uint64_t off_pre, off_post;
 };
 
-// Span pass (span.cu, complex64): a CTA holds a tile of 2^13 amplitudes whose
-// coordinates k = 0..12 are the real bits pos[k] (ascending: bits 0..c-1, then the
-// gates' bits); every other real bit enumerates tiles. The amplitudes move between
-// register layouts through shared memory, so a gate on any coordinate is a
-// register update: one pass applies up to 13 gates (the low pass, c = 13) or up to
-// 10 on high bits (c >= 3). Coordinate k's real rotation [[c, -s], [s, c]]
+// Span pass (span.cu): a CTA holds a tile of 2^T amplitudes (T = 13 complex64, 12
+// complex128) whose coordinates k = 0..T-1 are the real bits pos[k] (ascending: bits
+// 0..c-1, then the gates' bits); every other real bit enumerates tiles. The
+// amplitudes move between register layouts through shared memory, so a gate on any
+// coordinate is a register update: one pass applies up to T gates (the low pass,
+// c = T) or up to T - 3 on high bits (c >= 3). Coordinate k's real rotation [[c, -s], [s, c]]
 // (already oriented by its selector's beta) is stored with one coefficient
 // factored out: rot[k] = (tau, 0) with tau = s / c when |c| >= |s| (x' = x - tau y,
 // y' = y + tau x, factor c), else (mu, 1) with mu = c / s (x' = mu x - y,
@@ -266,8 +266,8 @@ struct SpanDev {
     uint32_t m, c, low, gates;  // low: the tile is real bits 0..12; gates: bit k = coordinate k has one
     uint8_t pos[16];
     uint64_t tile_mask, ntiles;
-    float rot[kSpanBits][2];
-    float scale, pad;
+    double rot[kSpanBits][2];  // complex64 passes round both to float
+    double scale;
     uint64_t off_pre, off_post;  // DiagDev windows (tile coordinates = pos), 0 if none
 };
 

@@ -1307,12 +1307,12 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
             std::vector<const U3Op *> gs;
             for (const U3Op &u : (split ? rot : op.u3)) gs.push_back(&u);
             std::sort(gs.begin(), gs.end(), [](const U3Op *a, const U3Op *b) { return a->delta < b->delta; });
-            if (split && elem_bytes == 8 && pp.span && mm >= span_tile_bits()) {
+            if (split && pp.span && mm >= span_tile_bits(elem_bytes)) {
                 // span passes (span.cu): the gates on bits 0..T-1 in one low pass, the rest
                 // in as few strided passes as take T - 3 each, spread evenly (fewer gates
                 // per pass = longer contiguous runs, c = T - gates); the low pass runs
                 // last, like the row passes' (the windows then land on the strided passes)
-                const int T = span_tile_bits();
+                const int T = span_tile_bits(elem_bytes);
                 std::vector<const U3Op *> lowg, highg;
                 for (const U3Op *u : gs) (__builtin_ctzll(u->delta) < T ? lowg : highg).push_back(u);
                 const int first_pass = int(out.passes.size());
@@ -1332,8 +1332,8 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
                     ps.span.low = low ? 1u : 0u;
                     for (int k2 = 0; k2 < T; k2++) {
                         ps.span.pos[k2] = ps.geom.pos[k2];
-                        ps.span.rot[k2][0] = 0.0f;
-                        ps.span.rot[k2][1] = 0.0f;
+                        ps.span.rot[k2][0] = 0.0;
+                        ps.span.rot[k2][1] = 0.0;
                     }
                     ps.span.tile_mask = ps.geom.tile_mask;
                     ps.span.ntiles = ps.geom.ntiles;
@@ -1347,16 +1347,16 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
                         // (the larger of |c|, |s|), the factors multiply into scale.
                         const double cc = u->u[0].real(), ss = u->sel.beta ? -u->u[2].real() : u->u[2].real();
                         if (std::fabs(cc) >= std::fabs(ss)) {
-                            ps.span.rot[coord][0] = float(ss / cc);
-                            ps.span.rot[coord][1] = 0.0f;
+                            ps.span.rot[coord][0] = ss / cc;
+                            ps.span.rot[coord][1] = 0.0;
                             scale *= cc;
                         } else {
-                            ps.span.rot[coord][0] = float(cc / ss);
-                            ps.span.rot[coord][1] = 1.0f;
+                            ps.span.rot[coord][0] = cc / ss;
+                            ps.span.rot[coord][1] = 1.0;
                             scale *= ss;
                         }
                     }
-                    ps.span.scale = float(scale);
+                    ps.span.scale = scale;
                     out.passes.push_back(ps);
                     last_tile_pass = int(out.passes.size()) - 1;
                 };

@@ -71,10 +71,11 @@ struct PlanParams {
                                 // instead of general terms evaluated per amplitude (split every 32 terms)
     int walsh_min_general = 2;  // general (multi-bit selector) terms from which a standalone window takes the
                                 // Walsh pass; 0: every standalone window does
-    int span = 1;               // complex64 U3 batches (real split) run as span passes: 13 gates on bits 0..12,
-                                // then up to 10 high-bit gates per pass (span.cu); 0: the register-row passes
+    int span = 1;               // U3 batches (real split) run as span passes (span.cu): the gates on bits
+                                // 0..T-1 in one pass, then up to T - span_min_run high-bit gates per pass
+                                // (T = 13 complex64, 12 complex128); 0: the register-row passes
     int span_min_run = 3;       // log2 of the shortest run of contiguous amplitudes a strided span pass
-                                // reads (3..8: 64 B .. 2 KiB): its gates number at most 13 - span_min_run
+                                // reads (3..8: 64 B .. 2 KiB complex64, 128 B .. 4 KiB complex128)
                                 // (3: a 32-qubit layer in 3 passes, 54.7 ms on B200, vs 4 passes, 57.2 ms)
 };
 
@@ -137,10 +138,11 @@ struct Plan {
 // one fast-pass round.
 int diag_tile_bits(int elem_bytes, int row_bits);
 int walsh_tile_bits(int elem_bytes);
-// Span pass (span.cu): tile coordinates, and whether the gates of `gates` (bit k =
-// coordinate k) sit on coordinates the pass's layouts hold in registers.
-int span_tile_bits();
-bool span_coverable(uint32_t gates, bool low);
+// Span pass (span.cu): tile coordinates (13 for complex64, 12 for complex128), and
+// the register layouts a pass with the gates of `gates` (bit k = coordinate k) runs
+// through: 2 or 3, 0 if some gate sits on a coordinate no layout holds in registers.
+int span_tile_bits(int elem_bytes);
+int span_layouts(int elem_bytes, uint32_t gates, bool low);
 int fast_tile_bits(int elem_bytes);
 int fast_reg_bits(int elem_bytes);
 int row_reg_bits(int elem_bytes, int wide);

@@ -66,11 +66,12 @@ cudaError_t run_fast_tile(const uint8_t *dblob, uint64_t foff, uint64_t toff, ui
 // pass has a real matrix (both need row_low_ok); win: the pass has a window.
 cudaError_t run_row_pass(const uint8_t *dblob, uint64_t poff, uint64_t toff, uint64_t nitems, int elem_bytes,
                          int wide, bool low, bool real, bool win, void *state, int sms, cudaStream_t st);
-// Span pass (span.cu, complex64): up to 13 real-rotation gates on a 2^13-amplitude
-// tile per read-modify-write; low: the tile is real bits 0..12; win: 0 no window,
-// 1 windows with linear terms only, 2 windows with quadratic terms.
-cudaError_t run_span(const uint8_t *dblob, uint64_t soff, uint64_t toff, uint64_t ntiles, bool low, int win,
-                     void *state, DevStatus *status, int sms, cudaStream_t st);
+// Span pass (span.cu): up to T real-rotation gates on a 2^T-amplitude tile per
+// read-modify-write (T = 13 complex64, 12 complex128); low: the tile is real bits
+// 0..T-1; layouts: 2 or 3 (span_layouts); win: 0 no window, 1 windows with linear
+// terms only, 2 windows with quadratic terms.
+cudaError_t run_span(const uint8_t *dblob, uint64_t soff, uint64_t toff, uint64_t ntiles, int elem_bytes, bool low,
+                     int layouts, int win, void *state, int sms, cudaStream_t st);
 // amplitude 0 := 1 (the rest of an INIT pass is a memset)
 cudaError_t run_set_one(void *state, int elem_bytes, cudaStream_t st);
 // General strided pass (grow.cu): lam == nullptr applies the pass to psi; otherwise
