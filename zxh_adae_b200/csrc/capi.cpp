@@ -761,6 +761,7 @@ int zxh_set_param(zxh_sim *s, const char *name, int value)
         {"walsh_min_general", &s->pp.walsh_min_general, 0, 1 << 20},
         {"span", &s->pp.span, 0, 1},
         {"span_min_run", &s->pp.span_min_run, 3, 8},
+        {"span_land", &s->pp.span_land, 0, 1},
         {"diag_chunk_bits", &s->pp.diag_chunk_bits, -1, 8},
         {"grow", &s->pp.grow, 0, 1},
         {"grow_regs", &s->pp.grow_regs, 1, 4},

@@ -74,6 +74,8 @@ struct PlanParams {
     int span = 1;               // U3 batches (real split) run as span passes (span.cu): the gates on bits
                                 // 0..T-1 in one pass, then up to T - span_min_run high-bit gates per pass
                                 // (T = 13 complex64, 12 complex128); 0: the register-row passes
+    int span_land = 1;          // complex64 span passes in the landing form (the next tile lands in shared
+                                // memory during the current one); 0: the register form
     int span_min_run = 3;       // log2 of the shortest run of contiguous amplitudes a strided span pass
                                 // reads (3..8: 64 B .. 2 KiB complex64, 128 B .. 4 KiB complex128)
                                 // (3: a 32-qubit layer in 3 passes, 54.7 ms on B200, vs 4 passes, 57.2 ms)
@@ -122,7 +124,7 @@ struct Pass {
     int chunk_bits = -1;                 // DIAG: tiles per Gray-code chunk (log2, -1 = automatic)
     int row_bits = 0;                    // DIAG: log2 rows of a warp tile; WALSH: the window's term count
     int prefetch = 0;                    // DIAG: tiles staged one ahead by TMA bulk copies; GROW: the
-                                         // staged form (next item in shared memory)
+                                         // staged form (next item in shared memory); SPAN: the landing form
     std::vector<FastGateDev> fgates;     // FAST
     GrowBuild gb;                        // GROW
 };
@@ -140,9 +142,10 @@ int diag_tile_bits(int elem_bytes, int row_bits);
 int walsh_tile_bits(int elem_bytes);
 // Span pass (span.cu): tile coordinates (13 for complex64, 12 for complex128), and
 // the register layouts a pass with the gates of `gates` (bit k = coordinate k) runs
-// through: 2 or 3, 0 if some gate sits on a coordinate no layout holds in registers.
+// through (land: the complex64 landing form): 2 or 3, 0 if some gate sits on a
+// coordinate no layout holds in registers.
 int span_tile_bits(int elem_bytes);
-int span_layouts(int elem_bytes, uint32_t gates, bool low);
+int span_layouts(int elem_bytes, uint32_t gates, bool low, bool land);
 int fast_tile_bits(int elem_bytes);
 int fast_reg_bits(int elem_bytes);
 int row_reg_bits(int elem_bytes, int wide);
