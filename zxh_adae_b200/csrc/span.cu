@@ -204,6 +204,7 @@ __device__ __forceinline__ uint64_t real_of(uint32_t t, const uint8_t *pos)
 template <class G, int LA, int LB>
 __device__ __forceinline__ void exchange(typename G::E (&x)[span_nr<G>()], typename G::E *slab, int lane, int warp)
 {
+    asm volatile("" : "+r"(lane), "+r"(warp));  // slot bases rebuilt here, not kept live across the tile loop
     const uint32_t sa = G::slot(fixed_index<G, LA>(lane, warp)), sb = G::slot(fixed_index<G, LB>(lane, warp));
     __syncthreads();  // the slab's previous reads are done
 #pragma unroll
@@ -222,6 +223,9 @@ __device__ __forceinline__ void exchange_half(typename G::E (&x)[span_nr<G>()], 
     using H = HalfX<X>;
     constexpr int RS = reg_bit_of<G, LA>(H::split);
     static_assert(RS >= 0 && RS == reg_bit_of<G, LB>(H::split), "the split coordinate sits at one register bit");
+    // the slot bases are rebuilt here from lane and warp (a few logic ops) rather
+    // than kept live across the tile loop, where registers are short
+    asm volatile("" : "+r"(lane), "+r"(warp));
     const uint32_t sa = H::slot(fixed_index<G, LA>(lane, warp)), sb = H::slot(fixed_index<G, LB>(lane, warp));
 #pragma unroll
     for (int h = 0; h < 2; h++) {
