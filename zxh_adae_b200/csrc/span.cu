@@ -299,8 +299,9 @@ __device__ __forceinline__ void rotate(typename G::E (&x)[span_nr<G>()], const t
 // A window's phase at a thread's amplitudes in layout L for one tile, in a form
 // that needs few registers while the amplitudes are live: linear windows give
 // one factor per thread (times rowf[j] per register pattern); others give the
-// thread's constant and its R register coefficients in turns (register x register
-// terms come from qreg[j]): 32-bit turns for complex64, 64-bit for complex128.
+// thread's constant and its R register coefficients in turns (32-bit turns for
+// complex64, 64-bit for complex128), the register x register terms a factor
+// rowf[j] per register pattern.
 template <typename E>
 struct SpanWin;
 template <>
@@ -370,7 +371,7 @@ __device__ __forceinline__ SpanWin<typename G::E> span_window_setup(const uint8_
     for (uint32_t q = 0; q < dd.n_in_quad; q++) {
         const QuadTerm t = iq[q];
         const bool ri = (RM >> t.i) & 1, rj = (RM >> t.j) & 1;
-        if (ri && rj) continue;  // register x register: in qreg
+        if (ri && rj) continue;  // register x register: in rowf
         if (!ri && !rj) {
             if (((fix >> t.i) & 1) && ((fix >> t.j) & 1)) acc += t.coef;
             continue;
@@ -389,23 +390,35 @@ __device__ __forceinline__ SpanWin<typename G::E> span_window_setup(const uint8_
 
 template <class G, bool LINEAR>
 __device__ __forceinline__ void span_window_apply(typename G::E (&x)[span_nr<G>()], const SpanWin<typename G::E> &sw,
-                                                  const typename G::E *rowf, const int64_t *qreg,
+                                                  const typename G::E *rowf, bool quad_regs,
                                                   const typename G::E *s_exp)
 {
+    using E = typename G::E;
     if constexpr (LINEAR) {
 #pragma unroll
         for (int j = 0; j < span_nr<G>(); j++) x[j] = cmul(x[j], cmul(sw.f, rowf[j]));
     } else {
-        auto a = sw.a;
+        // the phase of pattern j = jl + 4 jh is a + w0 jl0 + w1 jl1 + sum_r>=2 w_r jh_r-2
+        // (+ the register x register terms): four factors for jl, one per jh, and
+        // their product per amplitude (each factor evaluated from turns, so no
+        // product chains more than three factors)
+        E lo[4];
 #pragma unroll
-        for (int jj = 0; jj < span_nr<G>(); jj++) {
-            const int gj = jj ^ (jj >> 1);
-            if (jj > 0) {
-                const int fb = ctz_const(jj);
-                if ((gj >> fb) & 1) a += sw.w[fb];
-                else a -= sw.w[fb];
+        for (int jl = 0; jl < 4; jl++) lo[jl] = span_phase(s_exp, sw.a + ((jl & 1) ? sw.w[0] : 0) + ((jl & 2) ? sw.w[1] : 0));
+#pragma unroll
+        for (int jh = 0; jh < span_nr<G>() / 4; jh++) {
+            decltype(sw.a) t = 0;
+#pragma unroll
+            for (int r = 2; r < G::R; r++)
+                if ((jh >> (r - 2)) & 1) t += sw.w[r];
+            const E hf = span_phase(s_exp, t);
+#pragma unroll
+            for (int jl = 0; jl < 4; jl++) {
+                const int j = jl | (jh << 2);
+                E f = cmul(lo[jl], hf);
+                if (quad_regs) f = cmul(f, rowf[j]);
+                x[j] = cmul(x[j], f);
             }
-            x[gj] = cmul(x[gj], span_phase(s_exp, a + span_turns(qreg[gj], s_exp)));
         }
     }
 }
@@ -418,8 +431,9 @@ struct SpanShared {
     E exp[WIN ? (1 << kExpTableBits) : 1];  // WIN != 0
     E rot[kSpanBits];                       // (coefficient, form) per coordinate
     uint64_t roff[2][span_nr<G>()];         // real offsets of the register patterns: layout A (loads), LS (stores)
-    int64_t qreg[2][span_nr<G>()];          // window 0 in layout A, window 1 in layout LS
-    E rowf[2][span_nr<G>()];
+    E rowf[2][span_nr<G>()];                // window 0 in layout A, 1 in LS: linear windows the
+                                            // pattern's factor, others its register x register factor
+    int quad_regs[2];                       // window d has register x register terms
     uint64_t grp[16];                       // landing form: real offset of tile index k << 9
     int64_t fixl[2][32], fixw[2][8];        // linear windows: lin_in summed over a thread's lane / warp coordinates
     uint8_t pos[16];
@@ -432,6 +446,7 @@ __device__ __forceinline__ void span_setup(SpanShared<G, WIN> &sh, const SpanDev
     using E = typename G::E;
     constexpr int NR = span_nr<G>();
     if (tid < 16) sh.pos[tid] = p.pos[tid];
+    if (tid < 2) sh.quad_regs[tid] = 0;
     if (tid < G::T) {
         sh.rot[tid].x = decltype(E{}.x)(p.rot[tid][0]);
         sh.rot[tid].y = decltype(E{}.x)(p.rot[tid][1]);
@@ -446,8 +461,8 @@ __device__ __forceinline__ void span_setup(SpanShared<G, WIN> &sh, const SpanDev
         sh.roff[L][j] = real_of<G>(L ? reg_index<G, LS>(j) : reg_index<G, 0>(j), sh.pos);
     }
     if (WIN && tid >= 2 * NR && tid < 4 * NR) {
-        // tile-independent window parts: the register x register quadratic terms and,
-        // for linear windows, the per-pattern factors
+        // tile-independent window parts: the per-pattern factors of linear windows,
+        // the register x register quadratic terms of the others
         const int d = (tid - 2 * NR) / NR, j = tid % NR;
         const uint64_t ow = d ? p.off_post : p.off_pre;
         int64_t qa = 0, lb = 0;
@@ -460,8 +475,8 @@ __device__ __forceinline__ void span_setup(SpanShared<G, WIN> &sh, const SpanDev
             for (int k = 0; k < G::T; k++)
                 if ((t >> k) & 1) lb += dd.lin_in[k];
         }
-        sh.qreg[d][j] = qa;
-        sh.rowf[d][j] = phase_factor(sh.exp, lb);
+        sh.rowf[d][j] = phase_factor(sh.exp, WIN == 1 ? lb : qa);
+        if (qa != 0) sh.quad_regs[d] = 1;
     }
     if (tid >= 4 * NR && tid < 4 * NR + 16) sh.grp[tid - 4 * NR] = real_of<G>(uint32_t(tid - 4 * NR) << 9, sh.pos);
     if (WIN == 1 && tid >= 160 && tid < 240) {
@@ -582,7 +597,7 @@ __global__ void __launch_bounds__(kSpanThreads, 2) span_kernel(const uint8_t *__
 #pragma unroll
         for (int j = 0; j < NR; j++) x[j] = __ldcs(src + sh.roff[0][j]);
         if constexpr (WIN != 0) {
-            if (p.off_pre) span_window_apply<G, WIN == 1>(x, wpre, sh.rowf[0], sh.qreg[0], sh.exp);
+            if (p.off_pre) span_window_apply<G, WIN == 1>(x, wpre, sh.rowf[0], sh.quad_regs[0] != 0, sh.exp);
         }
         rotate<G, 0>(x, sh.rot, g.gA);
         if constexpr (THREE) {
@@ -594,7 +609,7 @@ __global__ void __launch_bounds__(kSpanThreads, 2) span_kernel(const uint8_t *__
         }
         rotate<G, 2>(x, sh.rot, g.gB);
         if constexpr (WIN != 0) {
-            if (p.off_post) span_window_apply<G, WIN == 1>(x, wpost, sh.rowf[1], sh.qreg[1], sh.exp);
+            if (p.off_post) span_window_apply<G, WIN == 1>(x, wpost, sh.rowf[1], sh.quad_regs[1] != 0, sh.exp);
         }
         if (g.scale_end) {
 #pragma unroll
@@ -658,7 +673,7 @@ __global__ void __launch_bounds__(kSpanThreads, 2) span_land_kernel(const uint8_
         __syncthreads();  // every thread has read the landing slab
         issue(tile + gridDim.x);
         if constexpr (WIN != 0) {
-            if (p.off_pre) span_window_apply<G, WIN == 1>(x, wpre, sh.rowf[0], sh.qreg[0], sh.exp);
+            if (p.off_pre) span_window_apply<G, WIN == 1>(x, wpre, sh.rowf[0], sh.quad_regs[0] != 0, sh.exp);
         }
         rotate<G, 0>(x, sh.rot, g.gA);
         if constexpr (THREE) {
@@ -670,7 +685,7 @@ __global__ void __launch_bounds__(kSpanThreads, 2) span_land_kernel(const uint8_
         }
         rotate<G, LS>(x, sh.rot, g.gB);
         if constexpr (WIN != 0) {
-            if (p.off_post) span_window_apply<G, WIN == 1>(x, wpost, sh.rowf[1], sh.qreg[1], sh.exp);
+            if (p.off_post) span_window_apply<G, WIN == 1>(x, wpost, sh.rowf[1], sh.quad_regs[1] != 0, sh.exp);
         }
         if (g.scale_end) {
 #pragma unroll
