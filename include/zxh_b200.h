@@ -197,8 +197,8 @@ int zxh_last_stats(const zxh_sim *sim, uint64_t *kernels, uint64_t *passes, doub
 /* Multinomial sampler that allocates nothing, for callers that cannot call
  * cudaMalloc (a process whose device memory is reserved once up front, a
  * framework whose own allocator owns the device, or a latency path that must not
- * take the CUDA allocator's locks). No counterpart in the reference: it has no
- * counterpart to replace. It draws shots outcomes
+ * take the CUDA allocator's locks). It has no counterpart in the reference. It
+ * draws shots outcomes
  * from the 2^m_bits-amplitude device state `state` (dtype ZXH_C64 or ZXH_C128,
  * interleaved re/im, real-address order) with the same uniform stream and the
  * same output order as zxh_measure after zxh_set_seed(seed), and writes the
