@@ -515,14 +515,13 @@ def _span_oracle_state(n, kind):
 @pytest.mark.parametrize("plan", ["span", "span_register_form", "rows"])
 @pytest.mark.parametrize("dtype", DTYPES)
 def test_span_passes(kind, n, plan, dtype):
-    # U3 batches as span passes against the oracle: complex64 tiles of 2^13 (13
-    # gates on bits 0..12, up to 10 high-bit gates per strided pass; at 23 qubits
-    # one strided pass of 10 gates, c = 3, which needs the third layout), in the
-    # landing form and the register form; complex128 tiles of 2^12 (12 gates on bits
-    # 0..11, up to 9 per strided pass; at 21 qubits one strided pass of 9 gates,
-    # whose runs of 8 amplitudes need the third layout); "rows" is the row-pass plan
-    if dtype == "complex128" and plan == "span_register_form":
-        pytest.skip("complex128 span passes have the register form only")
+    # U3 batches as span passes against the oracle, in the landing form and the
+    # register form: complex64 tiles of 2^13 (13 gates on bits 0..12, up to 10
+    # high-bit gates per strided pass; at 23 qubits one strided pass of 10 gates,
+    # c = 3, which needs the third layout); complex128 tiles of 2^12 (12 gates on
+    # bits 0..11, up to 9 per strided pass; at 21 qubits one strided pass of 9
+    # gates, whose runs of 8 amplitudes need the third layout in the register
+    # form); "rows" is the row-pass plan
     gates = _span_case(n, kind, 500 + n)
     want = _span_oracle_state(n, kind)
     s = zx.ZXH(n, dtype=dtype)

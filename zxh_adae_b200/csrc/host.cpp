@@ -1357,7 +1357,7 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
                         }
                     }
                     ps.span.scale = scale;
-                    ps.prefetch = elem_bytes == 8 ? pp.span_land : 0;
+                    ps.prefetch = pp.span_land;
                     out.passes.push_back(ps);
                     last_tile_pass = int(out.passes.size()) - 1;
                 };

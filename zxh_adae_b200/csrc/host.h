@@ -74,8 +74,8 @@ struct PlanParams {
     int span = 1;               // U3 batches (real split) run as span passes (span.cu): the gates on bits
                                 // 0..T-1 in one pass, then up to T - span_min_run high-bit gates per pass
                                 // (T = 13 complex64, 12 complex128); 0: the register-row passes
-    int span_land = 1;          // complex64 span passes in the landing form (the next tile lands in shared
-                                // memory during the current one); 0: the register form
+    int span_land = 1;          // span passes in the landing form (the next tile lands in shared memory
+                                // during the current one); 0: the register form
     int span_min_run = 3;       // log2 of the shortest run of contiguous amplitudes a strided span pass
                                 // reads (3..8: 64 B .. 2 KiB complex64, 128 B .. 4 KiB complex128)
                                 // (3: a 32-qubit layer in 3 passes, 54.7 ms on B200, vs 4 passes, 57.2 ms)

@@ -94,10 +94,14 @@ struct GeoReg128 {
     __host__ __device__ static constexpr uint32_t slot(uint32_t t) { return t ^ ((t >> 4) & 7u); }
 };
 
-// Landing form, complex64: layouts 0 A, 1 A', 2 B, 3 B2 (the table at the top).
+// Landing form, complex64: layouts 0 A, 1 A', 2 B, 3 B2 (the table at the top);
+// layout changes split on a shared register coordinate (HalfX).
 struct GeoLand64 {
     using E = float2;
     static constexpr int T = 13, R = 5, W = 3;
+    static constexpr int ACP = 2;  // amplitudes per 16-byte copy
+    static constexpr bool EXP_SHARED = true;
+    __host__ __device__ static constexpr int store_layout(bool three) { return three ? 2 : 3; }
     __host__ __device__ static constexpr int reg(int L, int r)
     {
         return L == 0 ? 5 + r
@@ -110,6 +114,25 @@ struct GeoLand64 {
         return L == 0 ? b : L == 1 ? 4 + b : L == 2 ? (b < 3 ? b : 2 + b) : (b < 4 ? b : 5);
     }
     __host__ __device__ static constexpr int warp(int L, int w) { return L < 2 ? 10 + w : L == 2 ? 7 + w : 6 + w; }
+};
+
+// Landing form, complex128: layouts 0 A, 1 A', 2 B (the table at the top); every
+// pass runs A -> A' -> B. Four register coordinates per layout leave none to share,
+// so a layout change splits on a warp coordinate both layouts have at the same
+// warp bit (HalfW): coordinate 9 for A -> A', 7 for A' -> B. The exp table stays
+// in global memory (read through L1) so that two CTAs fit an SM.
+struct GeoLand128 {
+    using E = double2;
+    static constexpr int T = 12, R = 4, W = 3;
+    static constexpr int ACP = 1;
+    static constexpr bool EXP_SHARED = false;
+    __host__ __device__ static constexpr int store_layout(bool) { return 2; }
+    __host__ __device__ static constexpr int reg(int L, int r) { return L == 0 ? 5 + r : L == 1 ? r : (r == 0 ? 4 : 8 + r); }
+    __host__ __device__ static constexpr int lane(int L, int b)
+    {
+        return L == 0 ? b : L == 1 ? (b < 3 ? 4 + b : 7 + b) : (b < 3 ? b : 2 + b);
+    }
+    __host__ __device__ static constexpr int warp(int L, int w) { return L == 0 ? 9 + w : w == 0 ? (L == 1 ? 9 : 3) : 6 + w; }
 };
 
 // The half-slab exchanges of the landing form: X = 1 A -> B2, 2 A -> A', 3 A' -> B.
@@ -151,6 +174,20 @@ struct HalfX {
         for (int k = 0; k < 13; k++)
             if ((t >> k) & 1) s ^= col(k);
         return s;
+    }
+};
+
+// The half-slab exchanges of the complex128 landing form (16-byte slots): the slot
+// of a tile index is the index with the split coordinate taken out, its bits 0..2
+// XOR bits 4..6. A 16-byte access is served per 8 consecutive lanes, whose lane
+// bits 0..2 are coordinates 0..2 (A, B) or 4..6 (A'): one to one on slot bits 0..2.
+template <int SPLIT, int WB>
+struct HalfW {
+    static constexpr int split = SPLIT, warp_bit = WB;
+    __host__ __device__ static constexpr uint32_t slot(uint32_t t)
+    {
+        const uint32_t u = (t & ((1u << SPLIT) - 1u)) | ((t >> (SPLIT + 1)) << SPLIT);
+        return u ^ ((u >> 4) & 7u);
     }
 };
 
@@ -237,6 +274,32 @@ __device__ __forceinline__ void exchange_half(typename G::E (&x)[span_nr<G>()], 
 #pragma unroll
         for (int j = 0; j < span_nr<G>(); j++)
             if (((j >> RS) & 1) == h) x[j] = slab[sb ^ H::slot(reg_index<G, LB>(j))];
+    }
+}
+
+// Landing form, complex128: one exchange through the half slab, in two rounds on
+// the shared warp coordinate: round h moves the tile entries of the warps whose
+// warp bit WB is h (the others wait at the barriers).
+template <class G, int LA, int LB, class H>
+__device__ __forceinline__ void exchange_warps(typename G::E (&x)[span_nr<G>()], typename G::E *slab, int lane, int warp)
+{
+    static_assert(G::warp(LA, H::warp_bit) == H::split && G::warp(LB, H::warp_bit) == H::split,
+                  "the split coordinate is the same warp bit in both layouts");
+    asm volatile("" : "+r"(lane), "+r"(warp));  // slot bases rebuilt here, not kept live across the tile loop
+    const uint32_t sa = H::slot(fixed_index<G, LA>(lane, warp)), sb = H::slot(fixed_index<G, LB>(lane, warp));
+    const bool mine = (warp >> H::warp_bit) & 1;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        __syncthreads();  // the half slab's previous reads are done
+        if (int(mine) == h) {
+#pragma unroll
+            for (int j = 0; j < span_nr<G>(); j++) slab[sa ^ H::slot(reg_index<G, LA>(j))] = x[j];
+        }
+        __syncthreads();
+        if (int(mine) == h) {
+#pragma unroll
+            for (int j = 0; j < span_nr<G>(); j++) x[j] = slab[sb ^ H::slot(reg_index<G, LB>(j))];
+        }
     }
 }
 
@@ -425,10 +488,17 @@ __device__ __forceinline__ void span_window_apply(typename G::E (&x)[span_nr<G>(
 
 // Per-CTA tables of a span pass, filled once per launch by span_setup; LS is the
 // store layout.
-template <class G, int WIN>
+template <class G, int WIN, bool EXPS = true>
 struct SpanShared {
     using E = typename G::E;
-    E exp[WIN ? (1 << kExpTableBits) : 1];  // WIN != 0
+    E exp[(WIN && EXPS) ? (1 << kExpTableBits) : 1];  // WIN != 0 and the table in shared memory
+    const E *gtab;                                    // else the blob's copy (read through L1)
+    // the exp table: a shared-memory address the compiler can see, or the global copy
+    __device__ __forceinline__ const E *table() const
+    {
+        if constexpr (EXPS) return exp;
+        else return gtab;
+    }
     E rot[kSpanBits];                       // (coefficient, form) per coordinate
     uint64_t roff[2][span_nr<G>()];         // real offsets of the register patterns: layout A (loads), LS (stores)
     E rowf[2][span_nr<G>()];                // window 0 in layout A, 1 in LS: linear windows the
@@ -439,9 +509,9 @@ struct SpanShared {
     uint8_t pos[16];
 };
 
-template <class G, int LS, int WIN>
-__device__ __forceinline__ void span_setup(SpanShared<G, WIN> &sh, const SpanDev &p, const uint8_t *blob, uint64_t toff,
-                                           int tid)
+template <class G, int LS, int WIN, bool EXPS>
+__device__ __forceinline__ void span_setup(SpanShared<G, WIN, EXPS> &sh, const SpanDev &p, const uint8_t *blob,
+                                           uint64_t toff, int tid)
 {
     using E = typename G::E;
     constexpr int NR = span_nr<G>();
@@ -453,7 +523,11 @@ __device__ __forceinline__ void span_setup(SpanShared<G, WIN> &sh, const SpanDev
     }
     if constexpr (WIN != 0) {
         const E *tab = reinterpret_cast<const E *>(blob + toff);
-        for (int i = tid; i < (1 << kExpTableBits); i += kSpanThreads) sh.exp[i] = tab[i];
+        if constexpr (EXPS) {
+            for (int i = tid; i < (1 << kExpTableBits); i += kSpanThreads) sh.exp[i] = tab[i];
+        } else {
+            if (tid == 0) sh.gtab = tab;
+        }
     }
     __syncthreads();
     if (tid < 2 * NR) {
@@ -475,10 +549,14 @@ __device__ __forceinline__ void span_setup(SpanShared<G, WIN> &sh, const SpanDev
             for (int k = 0; k < G::T; k++)
                 if ((t >> k) & 1) lb += dd.lin_in[k];
         }
-        sh.rowf[d][j] = phase_factor(sh.exp, WIN == 1 ? lb : qa);
+        sh.rowf[d][j] = phase_factor(sh.table(), WIN == 1 ? lb : qa);
         if (qa != 0) sh.quad_regs[d] = 1;
     }
-    if (tid >= 4 * NR && tid < 4 * NR + 16) sh.grp[tid - 4 * NR] = real_of<G>(uint32_t(tid - 4 * NR) << 9, sh.pos);
+    // landing form: tile index of a thread's k-th 16-byte copy = (tid + 256 k) x amplitudes per copy
+    if (tid >= 4 * NR && tid < 4 * NR + 16) {
+        constexpr uint32_t acp = 16 / sizeof(E);
+        sh.grp[tid - 4 * NR] = real_of<G>(uint32_t(tid - 4 * NR) * 256u * acp, sh.pos);
+    }
     if (WIN == 1 && tid >= 160 && tid < 240) {
         // window d's coefficients summed over lane bits (fixl) and warp bits (fixw)
         const int i = tid - 160, d = i / 40, v = i % 40;
@@ -543,20 +621,21 @@ __device__ __forceinline__ SpanGates<typename G::E> span_gates(const SpanDev &p)
 __device__ __forceinline__ void span_scale(float2 &x, float s) { x = __fmul2_rn(make_float2(s, s), x); }
 __device__ __forceinline__ void span_scale(double2 &x, double s) { x = make_double2(x.x * s, x.y * s); }
 
-template <class G, int LS, int WIN>
+template <class G, int LS, int WIN, bool EXPS>
 __device__ __forceinline__ void span_windows_setup(SpanWin<typename G::E> &wpre, SpanWin<typename G::E> &wpost,
-                                                   const SpanDev &p, const uint8_t *blob, const SpanShared<G, WIN> &sh,
+                                                   const SpanDev &p, const uint8_t *blob,
+                                                   const SpanShared<G, WIN, EXPS> &sh,
                                                    const SpanGates<typename G::E> &g, uint64_t base, int lane, int warp)
 {
     if constexpr (WIN != 0) {
         if (p.off_pre) {
-            wpre = span_window_setup<G, 0, WIN == 1>(blob, *reinterpret_cast<const DiagDev *>(blob + p.off_pre), sh.exp,
+            wpre = span_window_setup<G, 0, WIN == 1>(blob, *reinterpret_cast<const DiagDev *>(blob + p.off_pre), sh.table(),
                                                      base, lane, warp, sh.fixl[0][lane] + sh.fixw[0][warp]);
             if (g.scale_pre) span_scale(wpre.f, g.scale);
         }
         if (p.off_post) {
             wpost = span_window_setup<G, LS, WIN == 1>(blob, *reinterpret_cast<const DiagDev *>(blob + p.off_post),
-                                                       sh.exp, base, lane, warp, sh.fixl[1][lane] + sh.fixw[1][warp]);
+                                                       sh.table(), base, lane, warp, sh.fixl[1][lane] + sh.fixw[1][warp]);
             if (g.scale_post) span_scale(wpost.f, g.scale);
         }
     }
@@ -575,7 +654,7 @@ __global__ void __launch_bounds__(kSpanThreads, 2) span_kernel(const uint8_t *__
 {
     using E = typename G::E;
     constexpr int NR = span_nr<G>();
-    extern __shared__ __align__(16) unsigned char s_raw[];
+    extern __shared__ __align__(128) unsigned char s_raw[];
     E *slab = reinterpret_cast<E *>(s_raw);  // 2^T slots
     __shared__ SpanShared<G, WIN> sh;
 
@@ -591,13 +670,13 @@ __global__ void __launch_bounds__(kSpanThreads, 2) span_kernel(const uint8_t *__
     for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const uint64_t base = span_tile_base<G, LOW>(tile, sh.pos);
         [[maybe_unused]] SpanWin<E> wpre, wpost;
-        span_windows_setup<G, 2>(wpre, wpost, p, blob, sh, g, base, lane, warp);
+        span_windows_setup<G, 2, WIN, true>(wpre, wpost, p, blob, sh, g, base, lane, warp);
         E x[NR];
         const E *src = state + base + offA;
 #pragma unroll
         for (int j = 0; j < NR; j++) x[j] = __ldcs(src + sh.roff[0][j]);
         if constexpr (WIN != 0) {
-            if (p.off_pre) span_window_apply<G, WIN == 1>(x, wpre, sh.rowf[0], sh.quad_regs[0] != 0, sh.exp);
+            if (p.off_pre) span_window_apply<G, WIN == 1>(x, wpre, sh.rowf[0], sh.quad_regs[0] != 0, sh.table());
         }
         rotate<G, 0>(x, sh.rot, g.gA);
         if constexpr (THREE) {
@@ -609,7 +688,7 @@ __global__ void __launch_bounds__(kSpanThreads, 2) span_kernel(const uint8_t *__
         }
         rotate<G, 2>(x, sh.rot, g.gB);
         if constexpr (WIN != 0) {
-            if (p.off_post) span_window_apply<G, WIN == 1>(x, wpost, sh.rowf[1], sh.quad_regs[1] != 0, sh.exp);
+            if (p.off_post) span_window_apply<G, WIN == 1>(x, wpost, sh.rowf[1], sh.quad_regs[1] != 0, sh.table());
         }
         if (g.scale_end) {
 #pragma unroll
@@ -621,41 +700,44 @@ __global__ void __launch_bounds__(kSpanThreads, 2) span_kernel(const uint8_t *__
     }
 }
 
-// Landing form (complex64): the dynamic shared memory holds the landing slab (2^13
-// slots) and the half slab (2^12 slots). A tile's turn: wait for its copies, read
-// it from the landing slab in layout A, then (once every thread has read it) start
-// the copies of the CTA's next tile into the landing slab, and work on this one.
-template <bool LOW, bool THREE, int WIN>
+// Landing form: the dynamic shared memory holds the landing slab (2^T slots) and
+// the half slab (2^(T-1) slots). A tile's turn: wait for its copies, read it from
+// the landing slab in layout A, then (once every thread has read it) start the
+// copies of the CTA's next tile into the landing slab, and work on this one.
+template <class G, bool LOW, bool THREE, int WIN>
 __global__ void __launch_bounds__(kSpanThreads, 2) span_land_kernel(const uint8_t *__restrict__ blob, uint64_t soff,
-                                                                   uint64_t toff, float2 *__restrict__ state)
+                                                                   uint64_t toff, typename G::E *__restrict__ state)
 {
-    using G = GeoLand64;
+    using E = typename G::E;
     constexpr int NR = span_nr<G>();
-    constexpr int LS = THREE ? 2 : 3;  // store layout: B or B2
-    extern __shared__ __align__(16) float2 s_land[];
-    float2 *half = s_land + (1 << G::T);
-    __shared__ SpanShared<G, WIN> sh;
+    constexpr int LS = G::store_layout(THREE);  // B, or B2 for two-layout complex64 passes
+    constexpr bool EXPS = G::EXP_SHARED;
+    static_assert(THREE || std::is_same_v<G, GeoLand64>, "complex128 landing passes run A -> A' -> B");
+    extern __shared__ __align__(128) unsigned char s_raw[];
+    E *s_land = reinterpret_cast<E *>(s_raw);
+    E *half = s_land + (1 << G::T);
+    __shared__ SpanShared<G, WIN, EXPS> sh;
 
     const SpanDev &p = *reinterpret_cast<const SpanDev *>(blob + soff);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     span_setup<G, LS>(sh, p, blob, toff, tid);
 
     // per-thread offsets kept in shared memory (registers are the scarce resource):
-    // this thread's amplitude pair in each group of 512 tile indices, and its store
-    // pattern's base
+    // this thread's first 16-byte copy in each group of 256 x ACP tile indices, and
+    // its store pattern's base
     __shared__ uint64_t s_cpo[kSpanThreads], s_offS[kSpanThreads];
-    s_cpo[tid] = real_of<G>(uint32_t(tid) << 1, sh.pos);
+    s_cpo[tid] = real_of<G>(uint32_t(tid) * G::ACP, sh.pos);
     s_offS[tid] = real_of<G>(fixed_index<G, LS>(lane, warp), sh.pos);
     const uint32_t fa = fixed_index<G, 0>(lane, warp);
-    const SpanGates<float2> g = span_gates<G, THREE, LS, WIN>(p);
+    const SpanGates<E> g = span_gates<G, THREE, LS, WIN>(p);
     const uint64_t ntiles = p.ntiles;
 
     // the copies of a tile into the landing slab; a group is committed either way
     auto issue = [&](uint64_t tile) {
         if (tile < ntiles) {
-            const float2 *src = state + span_tile_base<G, LOW>(tile, sh.pos) + s_cpo[tid];
+            const E *src = state + span_tile_base<G, LOW>(tile, sh.pos) + s_cpo[tid];
 #pragma unroll
-            for (int k = 0; k < 16; k++) cp_async16(s_land + 2 * tid + (k << 9), src + sh.grp[k]);
+            for (int k = 0; k < 16; k++) cp_async16(s_land + (tid + 256 * k) * G::ACP, src + sh.grp[k]);
         }
         cp_async_commit();
     };
@@ -663,35 +745,41 @@ __global__ void __launch_bounds__(kSpanThreads, 2) span_land_kernel(const uint8_
 
     for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const uint64_t base = span_tile_base<G, LOW>(tile, sh.pos);
-        [[maybe_unused]] SpanWin<float2> wpre, wpost;
+        [[maybe_unused]] SpanWin<E> wpre, wpost;
         span_windows_setup<G, LS>(wpre, wpost, p, blob, sh, g, base, lane, warp);
         cp_async_wait<0>();  // this thread's copies of the tile have landed
         __syncthreads();     // and everyone's
-        float2 x[NR];
+        E x[NR];
 #pragma unroll
         for (int j = 0; j < NR; j++) x[j] = s_land[fa | reg_index<G, 0>(j)];
         __syncthreads();  // every thread has read the landing slab
         issue(tile + gridDim.x);
         if constexpr (WIN != 0) {
-            if (p.off_pre) span_window_apply<G, WIN == 1>(x, wpre, sh.rowf[0], sh.quad_regs[0] != 0, sh.exp);
+            if (p.off_pre) span_window_apply<G, WIN == 1>(x, wpre, sh.rowf[0], sh.quad_regs[0] != 0, sh.table());
         }
         rotate<G, 0>(x, sh.rot, g.gA);
-        if constexpr (THREE) {
-            exchange_half<G, 0, 1, 2>(x, half, lane, warp);
-            rotate<G, 1>(x, sh.rot, g.gAp);
-            exchange_half<G, 1, 2, 3>(x, half, lane, warp);
+        if constexpr (std::is_same_v<G, GeoLand64>) {
+            if constexpr (THREE) {
+                exchange_half<G, 0, 1, 2>(x, half, lane, warp);
+                rotate<G, 1>(x, sh.rot, g.gAp);
+                exchange_half<G, 1, 2, 3>(x, half, lane, warp);
+            } else {
+                exchange_half<G, 0, 3, 1>(x, half, lane, warp);
+            }
         } else {
-            exchange_half<G, 0, 3, 1>(x, half, lane, warp);
+            exchange_warps<G, 0, 1, HalfW<9, 0>>(x, half, lane, warp);
+            rotate<G, 1>(x, sh.rot, g.gAp);
+            exchange_warps<G, 1, 2, HalfW<7, 1>>(x, half, lane, warp);
         }
         rotate<G, LS>(x, sh.rot, g.gB);
         if constexpr (WIN != 0) {
-            if (p.off_post) span_window_apply<G, WIN == 1>(x, wpost, sh.rowf[1], sh.quad_regs[1] != 0, sh.exp);
+            if (p.off_post) span_window_apply<G, WIN == 1>(x, wpost, sh.rowf[1], sh.quad_regs[1] != 0, sh.table());
         }
         if (g.scale_end) {
 #pragma unroll
             for (int j = 0; j < NR; j++) span_scale(x[j], g.scale);
         }
-        float2 *dst = state + base + s_offS[tid];
+        E *dst = state + base + s_offS[tid];
 #pragma unroll
         for (int j = 0; j < NR; j++) __stcs(dst + sh.roff[1][j], x[j]);
     }
@@ -721,16 +809,16 @@ cudaError_t launch_span(const uint8_t *dblob, uint64_t soff, uint64_t toff, uint
     return cudaGetLastError();
 }
 
-template <bool LOW, bool THREE, int WIN>
+template <class G, bool LOW, bool THREE, int WIN>
 cudaError_t launch_span_land(const uint8_t *dblob, uint64_t soff, uint64_t toff, uint64_t ntiles, void *state, int sms,
                              cudaStream_t st)
 {
-    auto kern = span_land_kernel<LOW, THREE, WIN>;
-    const size_t smem = (sizeof(float2) << GeoLand64::T) + (sizeof(float2) << (GeoLand64::T - 1));  // 64 + 32 KiB
+    using E = typename G::E;
+    auto kern = span_land_kernel<G, LOW, THREE, WIN>;
+    const size_t smem = (sizeof(E) << G::T) + (sizeof(E) << (G::T - 1));  // 64 + 32 KiB
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
-    kern<<<span_grid(kern, smem, ntiles, sms), kSpanThreads, smem, st>>>(dblob, soff, toff,
-                                                                         static_cast<float2 *>(state));
+    kern<<<span_grid(kern, smem, ntiles, sms), kSpanThreads, smem, st>>>(dblob, soff, toff, static_cast<E *>(state));
     return cudaGetLastError();
 }
 
@@ -738,13 +826,16 @@ template <int FORM, bool LOW, bool THREE>
 cudaError_t launch_span_win(const uint8_t *dblob, uint64_t soff, uint64_t toff, uint64_t ntiles, int win, void *state,
                             int sms, cudaStream_t st)
 {
-    // FORM: 0 register form complex64, 1 register form complex128, 2 landing form complex64
+    // FORM: 0 register form complex64, 1 register form complex128, 2 landing form
+    // complex64, 3 landing form complex128
     auto go = [&](auto w) -> cudaError_t {
         constexpr int W = decltype(w)::value;
         if constexpr (FORM == 0) return launch_span<GeoReg64, LOW, THREE, W>(dblob, soff, toff, ntiles, state, sms, st);
         else if constexpr (FORM == 1)
             return launch_span<GeoReg128, LOW, THREE, W>(dblob, soff, toff, ntiles, state, sms, st);
-        else return launch_span_land<LOW, THREE, W>(dblob, soff, toff, ntiles, state, sms, st);
+        else if constexpr (FORM == 2)
+            return launch_span_land<GeoLand64, LOW, THREE, W>(dblob, soff, toff, ntiles, state, sms, st);
+        else return launch_span_land<GeoLand128, LOW, THREE, W>(dblob, soff, toff, ntiles, state, sms, st);
     };
     switch (win) {
     case 0: return go(std::integral_constant<int, 0>{});
@@ -771,7 +862,10 @@ int span_tile_bits(int elem_bytes) { return elem_bytes == 8 ? GeoReg64::T : GeoR
 
 int span_layouts(int elem_bytes, uint32_t gates, bool low, bool land)
 {
-    if (elem_bytes != 8) return layouts_of<GeoReg128, 2>(gates, low);
+    if (elem_bytes != 8) {
+        const int n = layouts_of<GeoReg128, 2>(gates, low);
+        return (land && n) ? 3 : n;  // the complex128 landing form always runs A -> A' -> B
+    }
     if (land) return layouts_of<GeoLand64, 3>(gates, low);
     // complex64 register form: the low pass runs A -> A' -> B, a strided pass A -> B
     const int n = layouts_of<GeoReg64, 2>(gates, low);
@@ -784,6 +878,11 @@ cudaError_t run_span(const uint8_t *dblob, uint64_t soff, uint64_t toff, uint64_
     if (layouts != 2 && layouts != 3) return cudaErrorInvalidValue;
     const bool three = layouts == 3;
     if (elem_bytes == 16) {
+        if (land) {
+            if (!three) return cudaErrorInvalidValue;
+            return low ? launch_span_win<3, true, true>(dblob, soff, toff, ntiles, win, state, sms, st)
+                       : launch_span_win<3, false, true>(dblob, soff, toff, ntiles, win, state, sms, st);
+        }
         if (low) return launch_span_win<1, true, true>(dblob, soff, toff, ntiles, win, state, sms, st);
         return three ? launch_span_win<1, false, true>(dblob, soff, toff, ntiles, win, state, sms, st)
                      : launch_span_win<1, false, false>(dblob, soff, toff, ntiles, win, state, sms, st);

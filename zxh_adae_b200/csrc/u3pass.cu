@@ -693,7 +693,7 @@ __global__ void __launch_bounds__(kThreads, 2) row_pass_kernel(const uint8_t *__
     constexpr int WARPS = kThreads / 32;
     static_assert(!XP || (R == 4 && sizeof(VT) == 16) || (R == 5 && sizeof(VT) == 8),
                   "the low pass swaps lane bits with 16 rows of 16 bytes or 32 rows of 8 bytes");
-    extern __shared__ __align__(16) float4 s_xp[];  // XP: NR x 32 row slots per warp
+    extern __shared__ __align__(128) float4 s_xp[];  // XP: NR x 32 row slots per warp
 
     const RowPassDev &p = *reinterpret_cast<const RowPassDev *>(blob + poff);
     const FastGateDev *gates = reinterpret_cast<const FastGateDev *>(blob + p.off_gates);

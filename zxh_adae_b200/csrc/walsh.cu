@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(kThreads, 2) walsh_kernel(const uint8_t *__res
 
     __shared__ E s_exp[1 << kExpTableBits];
     __shared__ __align__(16) PT s_u[WARPS][1 << T];
-    extern __shared__ __align__(16) WalshTermDev s_terms[];  // min(n_terms, kWalshSmemTerms) staged terms
+    extern __shared__ __align__(128) WalshTermDev s_terms[];  // min(n_terms, kWalshSmemTerms) staged terms
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const WalshDev &d = *reinterpret_cast<const WalshDev *>(blob + woff);
