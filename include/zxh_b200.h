@@ -344,9 +344,13 @@ int zxh_optimize_gates(size_t n, int level, const zxh_gate *gates, size_t count,
  * cost per amplitude independent of the window's size; 0: general terms
  * evaluated per amplitude, 32 per pass), walsh_min_general (general terms from
  * which a standalone window takes the Walsh pass; 0 = every one), span (1:
- * complex64 U3 batches run as span passes, 13 gates on the low bits and up to 10
- * high-bit gates per pass; 0: the register-row passes). Takes effect at the next
- * zxh_execute / zxh_apply. No counterpart in the reference. */
+ * U3 batches run as span passes, the gates on the low 13 (complex64) or 12
+ * (complex128) bits in one pass and up to 10 / 9 high-bit gates per pass; 0: the
+ * register-row passes), span_min_run (3..8: log2 of the shortest contiguous run
+ * a strided span pass reads), span_land (1: the span pass's next tile lands in
+ * shared memory while the current one is worked on; 0: tiles loaded straight
+ * into registers). Takes effect at the next zxh_execute / zxh_apply. No
+ * counterpart in the reference. */
 int zxh_set_param(zxh_sim *sim, const char *name, int value);
 
 #ifdef __cplusplus
