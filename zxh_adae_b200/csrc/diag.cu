@@ -10,8 +10,8 @@
 // general terms evaluated with parity bit tests on packed masks.
 //
 // Work split: each WARP owns tiles of 2^T contiguous amplitudes: 2^ROWB rows of 64
-// amplitudes (complex64) or 32 (complex128); ROWB is a planner knob, 3 and 2 by
-// default (T = 9 and 7), the fastest on B200 at 30 qubits. A lane holds one 16-byte
+// amplitudes (complex64) or 32 (complex128); ROWB is a planner knob, 2 and 3 by
+// default (T = 8: 2 KiB and 4 KiB tiles), the fastest on B200 at 26-32 qubits. A lane holds one 16-byte
 // vector per row, all rows loaded before any is used, with no block-level barrier
 // in the loop.
 // A warp takes chunks of 2^cb consecutive tiles and walks each chunk in Gray-code
@@ -402,12 +402,15 @@ cudaError_t launch_diag(const uint8_t *dblob, uint64_t doff, uint64_t toff, int 
     int per_sm = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem);
     if (per_sm < 1) per_sm = 1;
-    // chunks of 2^cb tiles: at least 16 chunks per warp of a full grid (tail balance),
-    // at most 256 tiles per chunk
-    const uint64_t warps_full = uint64_t(sms) * uint64_t(per_sm) * (kThreads / 32);
-    int lw = 0;
-    while ((1ULL << lw) < 16 * warps_full) lw++;
-    const int cb = chunk_bits >= 0 ? std::min(chunk_bits, nout) : std::max(0, std::min(8, nout - lw));
+    // chunks of 2^cb tiles: a chunk spans 32 KiB (16 complex64 tiles of 2 KiB, 8
+    // complex128 tiles of 4 KiB at the default row counts), the fastest on B200 at
+    // 26-32 qubits
+    int cb = chunk_bits;
+    if (cb < 0) {
+        cb = 0;
+        while ((size_t(sizeof(E)) << (T + cb)) < (size_t(32) << 10)) cb++;
+    }
+    cb = std::min(cb, nout);
     const uint64_t nchunks = 1ULL << (nout - cb);
     const uint64_t ctas_needed = (nchunks + kThreads / 32 - 1) / (kThreads / 32);
     const unsigned grid = unsigned(std::max<uint64_t>(1, std::min<uint64_t>(ctas_needed, uint64_t(sms) * uint64_t(per_sm))));
