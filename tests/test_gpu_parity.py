@@ -97,6 +97,24 @@ def test_diag_pass_gray_code_chunks(dtype, chunk_bits, prefetch):
 
 
 @pytest.mark.parametrize("dtype", DTYPES)
+@pytest.mark.parametrize("row_bits", [2, 3, 4])
+@pytest.mark.parametrize("n", [7, 19])
+def test_diag_pass_row_counts(dtype, row_bits, n):
+    # warp tiles of 4, 8 or 16 rows (the default is 4 rows for complex64, 8 for
+    # complex128), chunks chosen per launch; at n = 7 the state is one tile smaller
+    # than a full one
+    gates = np.concatenate([wl.h_all(n), wl.diag_batch(n, 700, 9 + n), wl.cp_cascade(n)])
+    o = Oracle(n)
+    o.push(gates)
+    o.execute()
+    s = zx.ZXH(n, dtype=dtype)
+    s.set_param("diag_row_bits_c64" if dtype == "complex64" else "diag_row_bits_c128", row_bits)
+    s.push_gates(gates)
+    s.execute()
+    assert max_err(s, o) <= TOL[dtype]
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
 @pytest.mark.parametrize("n,seed", [(6, 1), (9, 2), (12, 3), (16, 4)])
 def test_general_strided_pass_after_cx_transport(dtype, n, seed):
     # CX gates make the pair deltas span several real bits; those U3 batches run as
