@@ -285,8 +285,10 @@ def run_reference(args):
     world, rank, local, pg = dist_setup(args)
     if rank != 0:
         return
-    steps = min(args.steps, 10)
-    cb = ref_cpu_sample(steps, min(args.warmup, 1), args.batch)
+    # a step is about 0.3 s on 16 host cores: the requested warm-up (at most 10) and
+    # up to 30 timed steps keep the run within a minute
+    steps, warmup = min(args.steps, 30), min(args.warmup, 10)
+    cb = ref_cpu_sample(steps, warmup, args.batch)
     if cb is None:
         print(json.dumps({"impl": "reference", "unavailable": "reference OpenMP backend not built (oracle/_ref)"}))
         return
@@ -297,7 +299,7 @@ def run_reference(args):
         "unit": UNIT,
         "n_gpus": args.gpus,
         "steps": steps,
-        "warmup": min(args.warmup, 1),
+        "warmup": warmup,
         "ms_per_step": cb["ms_per_step"],
         "higher_is_better": True,
         "scaling": "weak",
