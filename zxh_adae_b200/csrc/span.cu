@@ -501,6 +501,7 @@ struct SpanShared {
     }
     E rot[kSpanBits];                       // (coefficient, form) per coordinate
     uint64_t roff[2][span_nr<G>()];         // real offsets of the register patterns: layout A (loads), LS (stores)
+    uint64_t soff[G::R];                    // real offset of each register coordinate of LS
     E rowf[2][span_nr<G>()];                // window 0 in layout A, 1 in LS: linear windows the
                                             // pattern's factor, others its register x register factor
     int quad_regs[2];                       // window d has register x register terms
@@ -533,6 +534,7 @@ __device__ __forceinline__ void span_setup(SpanShared<G, WIN, EXPS> &sh, const S
     if (tid < 2 * NR) {
         const int L = tid / NR, j = tid % NR;
         sh.roff[L][j] = real_of<G>(L ? reg_index<G, LS>(j) : reg_index<G, 0>(j), sh.pos);
+        if (L && j < G::R) sh.soff[j] = 1ULL << sh.pos[G::reg(LS, j)];
     }
     if (WIN && tid >= 2 * NR && tid < 4 * NR) {
         // tile-independent window parts: the per-pattern factors of linear windows,
@@ -779,9 +781,22 @@ __global__ void __launch_bounds__(kSpanThreads, 2) span_land_kernel(const uint8_
 #pragma unroll
             for (int j = 0; j < NR; j++) span_scale(x[j], g.scale);
         }
+        // the store patterns walked in Gray-code order: one 64-bit add per amplitude
+        // from the register coordinates' offsets, instead of a table load each
         E *dst = state + base + s_offS[tid];
+        uint64_t so[G::R];
 #pragma unroll
-        for (int j = 0; j < NR; j++) __stcs(dst + sh.roff[1][j], x[j]);
+        for (int r = 0; r < G::R; r++) so[r] = sh.soff[r];
+#pragma unroll
+        for (int jj = 0; jj < NR; jj++) {
+            const int gj = jj ^ (jj >> 1);
+            if (jj > 0) {
+                const int fb = ctz_const(jj);
+                if ((gj >> fb) & 1) dst += so[fb];
+                else dst -= so[fb];
+            }
+            __stcs(dst, x[gj]);
+        }
     }
     cp_async_wait<0>();  // the last committed group is empty; nothing lands after exit
 }
