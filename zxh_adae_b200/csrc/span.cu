@@ -458,8 +458,20 @@ __device__ __forceinline__ void span_window_apply(typename G::E (&x)[span_nr<G>(
 {
     using E = typename G::E;
     if constexpr (LINEAR) {
+        // a linear phase factors over the register bits: rowf[jl + 4 jh] = rowf[jl]
+        // rowf[4 jh], so four per-thread factors and one table load per four patterns
+        E lo[4];
 #pragma unroll
-        for (int j = 0; j < span_nr<G>(); j++) x[j] = cmul(x[j], cmul(sw.f, rowf[j]));
+        for (int jl = 0; jl < 4; jl++) lo[jl] = cmul(sw.f, rowf[jl]);
+#pragma unroll
+        for (int jh = 0; jh < span_nr<G>() / 4; jh++) {
+            const E hf = rowf[jh << 2];
+#pragma unroll
+            for (int jl = 0; jl < 4; jl++) {
+                const int j = jl | (jh << 2);
+                x[j] = cmul(x[j], jh ? cmul(lo[jl], hf) : lo[jl]);
+            }
+        }
     } else {
         // the phase of pattern j = jl + 4 jh is a + w0 jl0 + w1 jl1 + sum_r>=2 w_r jh_r-2
         // (+ the register x register terms): four factors for jl, one per jh, and
