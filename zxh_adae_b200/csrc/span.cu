@@ -749,9 +749,19 @@ __global__ void __launch_bounds__(kSpanThreads, 2) span_land_kernel(const uint8_
     // the copies of a tile into the landing slab; a group is committed either way
     auto issue = [&](uint64_t tile) {
         if (tile < ntiles) {
+            // copy k's source by a Gray-code walk over k from the offsets of its four bits
             const E *src = state + span_tile_base<G, LOW>(tile, sh.pos) + s_cpo[tid];
+            const uint64_t go[4] = {sh.grp[1], sh.grp[2], sh.grp[4], sh.grp[8]};
 #pragma unroll
-            for (int k = 0; k < 16; k++) cp_async16(s_land + (tid + 256 * k) * G::ACP, src + sh.grp[k]);
+            for (int kk = 0; kk < 16; kk++) {
+                const int k = kk ^ (kk >> 1);
+                if (kk > 0) {
+                    const int fb = ctz_const(kk);
+                    if ((k >> fb) & 1) src += go[fb];
+                    else src -= go[fb];
+                }
+                cp_async16(s_land + (tid + 256 * k) * G::ACP, src);
+            }
         }
         cp_async_commit();
     };
