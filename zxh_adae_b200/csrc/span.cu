@@ -714,13 +714,21 @@ __global__ void __launch_bounds__(kSpanThreads, 2) span_kernel(const uint8_t *__
     }
 }
 
+// A pass's rotation coefficients as a kernel parameter: read from the constant bank
+// where a gate is applied, with no shared-memory load.
+template <typename E>
+struct SpanRot {
+    E r[kSpanBits];
+};
+
 // Landing form: the dynamic shared memory holds the landing slab (2^T slots) and
 // the half slab (2^(T-1) slots). A tile's turn: wait for its copies, read it from
 // the landing slab in layout A, then (once every thread has read it) start the
 // copies of the CTA's next tile into the landing slab, and work on this one.
 template <class G, bool LOW, bool THREE, int WIN>
-__global__ void __launch_bounds__(kSpanThreads, 2) span_land_kernel(const uint8_t *__restrict__ blob, uint64_t soff,
-                                                                   uint64_t toff, typename G::E *__restrict__ state)
+__global__ void __launch_bounds__(kSpanThreads, 2)
+    span_land_kernel(const uint8_t *__restrict__ blob, uint64_t soff, uint64_t toff, typename G::E *__restrict__ state,
+                     const __grid_constant__ SpanRot<typename G::E> rotp)
 {
     using E = typename G::E;
     constexpr int NR = span_nr<G>();
@@ -781,21 +789,21 @@ __global__ void __launch_bounds__(kSpanThreads, 2) span_land_kernel(const uint8_
         if constexpr (WIN != 0) {
             if (p.off_pre) span_window_apply<G, WIN == 1>(x, wpre, sh.rowf[0], sh.quad_regs[0] != 0, sh.table());
         }
-        rotate<G, 0>(x, sh.rot, g.gA);
+        rotate<G, 0>(x, rotp.r, g.gA);
         if constexpr (std::is_same_v<G, GeoLand64>) {
             if constexpr (THREE) {
                 exchange_half<G, 0, 1, 2>(x, half, lane, warp);
-                rotate<G, 1>(x, sh.rot, g.gAp);
+                rotate<G, 1>(x, rotp.r, g.gAp);
                 exchange_half<G, 1, 2, 3>(x, half, lane, warp);
             } else {
                 exchange_half<G, 0, 3, 1>(x, half, lane, warp);
             }
         } else {
             exchange_warps<G, 0, 1, HalfW<9, 0>>(x, half, lane, warp);
-            rotate<G, 1>(x, sh.rot, g.gAp);
+            rotate<G, 1>(x, rotp.r, g.gAp);
             exchange_warps<G, 1, 2, HalfW<7, 1>>(x, half, lane, warp);
         }
-        rotate<G, LS>(x, sh.rot, g.gB);
+        rotate<G, LS>(x, rotp.r, g.gB);
         if constexpr (WIN != 0) {
             if (p.off_post) span_window_apply<G, WIN == 1>(x, wpost, sh.rowf[1], sh.quad_regs[1] != 0, sh.table());
         }
@@ -847,21 +855,27 @@ cudaError_t launch_span(const uint8_t *dblob, uint64_t soff, uint64_t toff, uint
 }
 
 template <class G, bool LOW, bool THREE, int WIN>
-cudaError_t launch_span_land(const uint8_t *dblob, uint64_t soff, uint64_t toff, uint64_t ntiles, void *state, int sms,
-                             cudaStream_t st)
+cudaError_t launch_span_land(const uint8_t *dblob, uint64_t soff, uint64_t toff, uint64_t ntiles, void *state,
+                             const double (*rot)[2], int sms, cudaStream_t st)
 {
     using E = typename G::E;
+    SpanRot<E> rp;
+    for (int k = 0; k < kSpanBits; k++) {
+        rp.r[k].x = decltype(E{}.x)(rot[k][0]);
+        rp.r[k].y = decltype(E{}.x)(rot[k][1]);
+    }
     auto kern = span_land_kernel<G, LOW, THREE, WIN>;
     const size_t smem = (sizeof(E) << G::T) + (sizeof(E) << (G::T - 1));  // 64 + 32 KiB
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
-    kern<<<span_grid(kern, smem, ntiles, sms), kSpanThreads, smem, st>>>(dblob, soff, toff, static_cast<E *>(state));
+    kern<<<span_grid(kern, smem, ntiles, sms), kSpanThreads, smem, st>>>(dblob, soff, toff, static_cast<E *>(state),
+                                                                         rp);
     return cudaGetLastError();
 }
 
 template <int FORM, bool LOW, bool THREE>
 cudaError_t launch_span_win(const uint8_t *dblob, uint64_t soff, uint64_t toff, uint64_t ntiles, int win, void *state,
-                            int sms, cudaStream_t st)
+                            const double (*rot)[2], int sms, cudaStream_t st)
 {
     // FORM: 0 register form complex64, 1 register form complex128, 2 landing form
     // complex64, 3 landing form complex128
@@ -871,8 +885,8 @@ cudaError_t launch_span_win(const uint8_t *dblob, uint64_t soff, uint64_t toff, 
         else if constexpr (FORM == 1)
             return launch_span<GeoReg128, LOW, THREE, W>(dblob, soff, toff, ntiles, state, sms, st);
         else if constexpr (FORM == 2)
-            return launch_span_land<GeoLand64, LOW, THREE, W>(dblob, soff, toff, ntiles, state, sms, st);
-        else return launch_span_land<GeoLand128, LOW, THREE, W>(dblob, soff, toff, ntiles, state, sms, st);
+            return launch_span_land<GeoLand64, LOW, THREE, W>(dblob, soff, toff, ntiles, state, rot, sms, st);
+        else return launch_span_land<GeoLand128, LOW, THREE, W>(dblob, soff, toff, ntiles, state, rot, sms, st);
     };
     switch (win) {
     case 0: return go(std::integral_constant<int, 0>{});
@@ -910,28 +924,28 @@ int span_layouts(int elem_bytes, uint32_t gates, bool low, bool land)
 }
 
 cudaError_t run_span(const uint8_t *dblob, uint64_t soff, uint64_t toff, uint64_t ntiles, int elem_bytes, bool low,
-                     int layouts, bool land, int win, void *state, int sms, cudaStream_t st)
+                     int layouts, bool land, int win, void *state, const double (*rot)[2], int sms, cudaStream_t st)
 {
     if (layouts != 2 && layouts != 3) return cudaErrorInvalidValue;
     const bool three = layouts == 3;
     if (elem_bytes == 16) {
         if (land) {
             if (!three) return cudaErrorInvalidValue;
-            return low ? launch_span_win<3, true, true>(dblob, soff, toff, ntiles, win, state, sms, st)
-                       : launch_span_win<3, false, true>(dblob, soff, toff, ntiles, win, state, sms, st);
+            return low ? launch_span_win<3, true, true>(dblob, soff, toff, ntiles, win, state, rot, sms, st)
+                       : launch_span_win<3, false, true>(dblob, soff, toff, ntiles, win, state, rot, sms, st);
         }
-        if (low) return launch_span_win<1, true, true>(dblob, soff, toff, ntiles, win, state, sms, st);
-        return three ? launch_span_win<1, false, true>(dblob, soff, toff, ntiles, win, state, sms, st)
-                     : launch_span_win<1, false, false>(dblob, soff, toff, ntiles, win, state, sms, st);
+        if (low) return launch_span_win<1, true, true>(dblob, soff, toff, ntiles, win, state, rot, sms, st);
+        return three ? launch_span_win<1, false, true>(dblob, soff, toff, ntiles, win, state, rot, sms, st)
+                     : launch_span_win<1, false, false>(dblob, soff, toff, ntiles, win, state, rot, sms, st);
     }
     if (land) {
-        if (low) return launch_span_win<2, true, true>(dblob, soff, toff, ntiles, win, state, sms, st);
-        return three ? launch_span_win<2, false, true>(dblob, soff, toff, ntiles, win, state, sms, st)
-                     : launch_span_win<2, false, false>(dblob, soff, toff, ntiles, win, state, sms, st);
+        if (low) return launch_span_win<2, true, true>(dblob, soff, toff, ntiles, win, state, rot, sms, st);
+        return three ? launch_span_win<2, false, true>(dblob, soff, toff, ntiles, win, state, rot, sms, st)
+                     : launch_span_win<2, false, false>(dblob, soff, toff, ntiles, win, state, rot, sms, st);
     }
-    if (low) return launch_span_win<0, true, true>(dblob, soff, toff, ntiles, win, state, sms, st);
+    if (low) return launch_span_win<0, true, true>(dblob, soff, toff, ntiles, win, state, rot, sms, st);
     if (three) return cudaErrorInvalidValue;
-    return launch_span_win<0, false, false>(dblob, soff, toff, ntiles, win, state, sms, st);
+    return launch_span_win<0, false, false>(dblob, soff, toff, ntiles, win, state, rot, sms, st);
 }
 
 }  // namespace zxh
