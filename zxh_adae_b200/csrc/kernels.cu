@@ -566,7 +566,7 @@ cudaError_t run_passes(const std::vector<Pass> &passes, const uint8_t *dblob, vo
         } else if (ps.kind == Pass::SPAN) {
             e = run_span(dblob, ps.off, ps.off2, ps.span.ntiles, elem_bytes, ps.low != 0,
                          span_layouts(elem_bytes, ps.span.gates, ps.low != 0, ps.prefetch != 0), ps.prefetch != 0,
-                         ps.real, state, ps.span.rot, sms, st);
+                         ps.real, state, ps.span.rot, ps.span.pos, sms, st);
         } else if (ps.kind == Pass::WALSH) {
             e = run_walsh(dblob, ps.off, ps.off2, ps.m, uint32_t(ps.row_bits), elem_bytes, state, sms, st);
         } else if (ps.kind == Pass::PAIR) {

@@ -69,11 +69,12 @@ cudaError_t run_row_pass(const uint8_t *dblob, uint64_t poff, uint64_t toff, uin
 // Span pass (span.cu): up to T real-rotation gates on a 2^T-amplitude tile per
 // read-modify-write (T = 13 complex64, 12 complex128); low: the tile is real bits
 // 0..T-1; layouts: 2 or 3 (span_layouts); land: the landing form; win: 0 no window,
-// 1 windows with linear terms only, 2 windows with quadratic terms; rot: the pass's
-// rotation coefficients (host copy of SpanDev::rot, passed to the landing form as a
-// kernel parameter).
+// 1 windows with linear terms only, 2 windows with quadratic terms; rot, pos: the
+// pass's rotation coefficients and tile coordinates (host copies of SpanDev::rot and
+// SpanDev::pos, passed to the landing form as a kernel parameter).
 cudaError_t run_span(const uint8_t *dblob, uint64_t soff, uint64_t toff, uint64_t ntiles, int elem_bytes, bool low,
-                     int layouts, bool land, int win, void *state, const double (*rot)[2], int sms, cudaStream_t st);
+                     int layouts, bool land, int win, void *state, const double (*rot)[2], const uint8_t *pos, int sms,
+                     cudaStream_t st);
 // amplitude 0 := 1 (the rest of an INIT pass is a memset)
 cudaError_t run_set_one(void *state, int elem_bytes, cudaStream_t st);
 // General strided pass (grow.cu): lam == nullptr applies the pass to psi; otherwise

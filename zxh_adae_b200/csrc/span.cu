@@ -393,10 +393,19 @@ __device__ __forceinline__ SpanWin<typename G::E> span_window_setup(const uint8_
         // only linear terms: the tile's out-of-tile bits give one sum shared by all
         // threads, the thread's lane and warp coordinates a constant (fixc)
         const LinTerm *ol = reinterpret_cast<const LinTerm *>(blob + dd.off_out_lin);
-        int64_t K = 0;
-        for (uint32_t q = uint32_t(lane); q < dd.n_out_lin; q += 32)
-            if ((base >> ol[q].bit) & 1) K += ol[q].coef;
-        sw.f = phase_factor(s_exp, warp_sum_i64(K) + dd.c0 + fixc);
+        if constexpr (std::is_same_v<typename G::E, float2>) {
+            // complex64: the sum in 32-bit turns (each term rounded once), one warp
+            // reduction instruction instead of a shuffle tree of 64-bit values
+            uint32_t K = 0;
+            for (uint32_t q = uint32_t(lane); q < dd.n_out_lin; q += 32)
+                if ((base >> ol[q].bit) & 1) K += turns32(ol[q].coef);
+            sw.f = phase_factor32(s_exp, __reduce_add_sync(0xffffffffu, K) + turns32(dd.c0 + fixc));
+        } else {
+            int64_t K = 0;
+            for (uint32_t q = uint32_t(lane); q < dd.n_out_lin; q += 32)
+                if ((base >> ol[q].bit) & 1) K += ol[q].coef;
+            sw.f = phase_factor(s_exp, warp_sum_i64(K) + dd.c0 + fixc);
+        }
         return sw;
     }
     constexpr uint32_t RM = reg_mask<G, L>();
@@ -714,11 +723,13 @@ __global__ void __launch_bounds__(kSpanThreads, 2) span_kernel(const uint8_t *__
     }
 }
 
-// A pass's rotation coefficients as a kernel parameter: read from the constant bank
-// where a gate is applied, with no shared-memory load.
+// A pass's rotation coefficients and tile coordinates as a kernel parameter: read
+// from the constant bank where a gate is applied or a tile's base address is formed,
+// with no shared-memory load.
 template <typename E>
-struct SpanRot {
+struct SpanConst {
     E r[kSpanBits];
+    uint8_t pos[16];
 };
 
 // Landing form: the dynamic shared memory holds the landing slab (2^T slots) and
@@ -728,7 +739,7 @@ struct SpanRot {
 template <class G, bool LOW, bool THREE, int WIN>
 __global__ void __launch_bounds__(kSpanThreads, 2)
     span_land_kernel(const uint8_t *__restrict__ blob, uint64_t soff, uint64_t toff, typename G::E *__restrict__ state,
-                     const __grid_constant__ SpanRot<typename G::E> rotp)
+                     const __grid_constant__ SpanConst<typename G::E> kc)
 {
     using E = typename G::E;
     constexpr int NR = span_nr<G>();
@@ -758,7 +769,7 @@ __global__ void __launch_bounds__(kSpanThreads, 2)
     auto issue = [&](uint64_t tile) {
         if (tile < ntiles) {
             // copy k's source by a Gray-code walk over k from the offsets of its four bits
-            const E *src = state + span_tile_base<G, LOW>(tile, sh.pos) + s_cpo[tid];
+            const E *src = state + span_tile_base<G, LOW>(tile, kc.pos) + s_cpo[tid];
             const uint64_t go[4] = {sh.grp[1], sh.grp[2], sh.grp[4], sh.grp[8]};
 #pragma unroll
             for (int kk = 0; kk < 16; kk++) {
@@ -776,7 +787,7 @@ __global__ void __launch_bounds__(kSpanThreads, 2)
     issue(blockIdx.x);
 
     for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const uint64_t base = span_tile_base<G, LOW>(tile, sh.pos);
+        const uint64_t base = span_tile_base<G, LOW>(tile, kc.pos);
         [[maybe_unused]] SpanWin<E> wpre, wpost;
         span_windows_setup<G, LS>(wpre, wpost, p, blob, sh, g, base, lane, warp);
         cp_async_wait<0>();  // this thread's copies of the tile have landed
@@ -789,21 +800,21 @@ __global__ void __launch_bounds__(kSpanThreads, 2)
         if constexpr (WIN != 0) {
             if (p.off_pre) span_window_apply<G, WIN == 1>(x, wpre, sh.rowf[0], sh.quad_regs[0] != 0, sh.table());
         }
-        rotate<G, 0>(x, rotp.r, g.gA);
+        rotate<G, 0>(x, kc.r, g.gA);
         if constexpr (std::is_same_v<G, GeoLand64>) {
             if constexpr (THREE) {
                 exchange_half<G, 0, 1, 2>(x, half, lane, warp);
-                rotate<G, 1>(x, rotp.r, g.gAp);
+                rotate<G, 1>(x, kc.r, g.gAp);
                 exchange_half<G, 1, 2, 3>(x, half, lane, warp);
             } else {
                 exchange_half<G, 0, 3, 1>(x, half, lane, warp);
             }
         } else {
             exchange_warps<G, 0, 1, HalfW<9, 0>>(x, half, lane, warp);
-            rotate<G, 1>(x, rotp.r, g.gAp);
+            rotate<G, 1>(x, kc.r, g.gAp);
             exchange_warps<G, 1, 2, HalfW<7, 1>>(x, half, lane, warp);
         }
-        rotate<G, LS>(x, rotp.r, g.gB);
+        rotate<G, LS>(x, kc.r, g.gB);
         if constexpr (WIN != 0) {
             if (p.off_post) span_window_apply<G, WIN == 1>(x, wpost, sh.rowf[1], sh.quad_regs[1] != 0, sh.table());
         }
@@ -856,26 +867,27 @@ cudaError_t launch_span(const uint8_t *dblob, uint64_t soff, uint64_t toff, uint
 
 template <class G, bool LOW, bool THREE, int WIN>
 cudaError_t launch_span_land(const uint8_t *dblob, uint64_t soff, uint64_t toff, uint64_t ntiles, void *state,
-                             const double (*rot)[2], int sms, cudaStream_t st)
+                             const double (*rot)[2], const uint8_t *pos, int sms, cudaStream_t st)
 {
     using E = typename G::E;
-    SpanRot<E> rp;
+    SpanConst<E> kc;
     for (int k = 0; k < kSpanBits; k++) {
-        rp.r[k].x = decltype(E{}.x)(rot[k][0]);
-        rp.r[k].y = decltype(E{}.x)(rot[k][1]);
+        kc.r[k].x = decltype(E{}.x)(rot[k][0]);
+        kc.r[k].y = decltype(E{}.x)(rot[k][1]);
     }
+    for (int k = 0; k < 16; k++) kc.pos[k] = pos[k];
     auto kern = span_land_kernel<G, LOW, THREE, WIN>;
     const size_t smem = (sizeof(E) << G::T) + (sizeof(E) << (G::T - 1));  // 64 + 32 KiB
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     kern<<<span_grid(kern, smem, ntiles, sms), kSpanThreads, smem, st>>>(dblob, soff, toff, static_cast<E *>(state),
-                                                                         rp);
+                                                                         kc);
     return cudaGetLastError();
 }
 
 template <int FORM, bool LOW, bool THREE>
 cudaError_t launch_span_win(const uint8_t *dblob, uint64_t soff, uint64_t toff, uint64_t ntiles, int win, void *state,
-                            const double (*rot)[2], int sms, cudaStream_t st)
+                            const double (*rot)[2], const uint8_t *pos, int sms, cudaStream_t st)
 {
     // FORM: 0 register form complex64, 1 register form complex128, 2 landing form
     // complex64, 3 landing form complex128
@@ -885,8 +897,8 @@ cudaError_t launch_span_win(const uint8_t *dblob, uint64_t soff, uint64_t toff, 
         else if constexpr (FORM == 1)
             return launch_span<GeoReg128, LOW, THREE, W>(dblob, soff, toff, ntiles, state, sms, st);
         else if constexpr (FORM == 2)
-            return launch_span_land<GeoLand64, LOW, THREE, W>(dblob, soff, toff, ntiles, state, rot, sms, st);
-        else return launch_span_land<GeoLand128, LOW, THREE, W>(dblob, soff, toff, ntiles, state, rot, sms, st);
+            return launch_span_land<GeoLand64, LOW, THREE, W>(dblob, soff, toff, ntiles, state, rot, pos, sms, st);
+        else return launch_span_land<GeoLand128, LOW, THREE, W>(dblob, soff, toff, ntiles, state, rot, pos, sms, st);
     };
     switch (win) {
     case 0: return go(std::integral_constant<int, 0>{});
@@ -924,28 +936,29 @@ int span_layouts(int elem_bytes, uint32_t gates, bool low, bool land)
 }
 
 cudaError_t run_span(const uint8_t *dblob, uint64_t soff, uint64_t toff, uint64_t ntiles, int elem_bytes, bool low,
-                     int layouts, bool land, int win, void *state, const double (*rot)[2], int sms, cudaStream_t st)
+                     int layouts, bool land, int win, void *state, const double (*rot)[2], const uint8_t *pos, int sms,
+                     cudaStream_t st)
 {
     if (layouts != 2 && layouts != 3) return cudaErrorInvalidValue;
     const bool three = layouts == 3;
     if (elem_bytes == 16) {
         if (land) {
             if (!three) return cudaErrorInvalidValue;
-            return low ? launch_span_win<3, true, true>(dblob, soff, toff, ntiles, win, state, rot, sms, st)
-                       : launch_span_win<3, false, true>(dblob, soff, toff, ntiles, win, state, rot, sms, st);
+            return low ? launch_span_win<3, true, true>(dblob, soff, toff, ntiles, win, state, rot, pos, sms, st)
+                       : launch_span_win<3, false, true>(dblob, soff, toff, ntiles, win, state, rot, pos, sms, st);
         }
-        if (low) return launch_span_win<1, true, true>(dblob, soff, toff, ntiles, win, state, rot, sms, st);
-        return three ? launch_span_win<1, false, true>(dblob, soff, toff, ntiles, win, state, rot, sms, st)
-                     : launch_span_win<1, false, false>(dblob, soff, toff, ntiles, win, state, rot, sms, st);
+        if (low) return launch_span_win<1, true, true>(dblob, soff, toff, ntiles, win, state, rot, pos, sms, st);
+        return three ? launch_span_win<1, false, true>(dblob, soff, toff, ntiles, win, state, rot, pos, sms, st)
+                     : launch_span_win<1, false, false>(dblob, soff, toff, ntiles, win, state, rot, pos, sms, st);
     }
     if (land) {
-        if (low) return launch_span_win<2, true, true>(dblob, soff, toff, ntiles, win, state, rot, sms, st);
-        return three ? launch_span_win<2, false, true>(dblob, soff, toff, ntiles, win, state, rot, sms, st)
-                     : launch_span_win<2, false, false>(dblob, soff, toff, ntiles, win, state, rot, sms, st);
+        if (low) return launch_span_win<2, true, true>(dblob, soff, toff, ntiles, win, state, rot, pos, sms, st);
+        return three ? launch_span_win<2, false, true>(dblob, soff, toff, ntiles, win, state, rot, pos, sms, st)
+                     : launch_span_win<2, false, false>(dblob, soff, toff, ntiles, win, state, rot, pos, sms, st);
     }
-    if (low) return launch_span_win<0, true, true>(dblob, soff, toff, ntiles, win, state, rot, sms, st);
+    if (low) return launch_span_win<0, true, true>(dblob, soff, toff, ntiles, win, state, rot, pos, sms, st);
     if (three) return cudaErrorInvalidValue;
-    return launch_span_win<0, false, false>(dblob, soff, toff, ntiles, win, state, rot, sms, st);
+    return launch_span_win<0, false, false>(dblob, soff, toff, ntiles, win, state, rot, pos, sms, st);
 }
 
 }  // namespace zxh
