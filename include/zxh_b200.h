@@ -349,7 +349,12 @@ int zxh_optimize_gates(size_t n, int level, const zxh_gate *gates, size_t count,
  * register-row passes), span_min_run (3..8: log2 of the shortest contiguous run
  * a strided span pass reads), span_land (1: the span pass's next tile lands in
  * shared memory while the current one is worked on; 0: tiles loaded straight
- * into registers). Takes effect at the next zxh_execute / zxh_apply. No
+ * into registers), span_split (0: the high-bit gates dealt to the strided span
+ * passes in blocks of neighbouring bits, the larger blocks on the lower bits; 1:
+ * round robin; 2: blocks, the larger on the higher bits), span_order (0: the
+ * strided span passes from the lowest bits up, but the first one that runs two
+ * layouts moved to the front, so the window before the batch rides on it; 1:
+ * from the lowest bits up; 2: from the highest down). Takes effect at the next zxh_execute / zxh_apply. No
  * counterpart in the reference. */
 int zxh_set_param(zxh_sim *sim, const char *name, int value);
 

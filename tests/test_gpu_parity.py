@@ -550,6 +550,28 @@ def test_span_passes(kind, n, plan, dtype):
     assert float(np.max(np.abs(s.get_state(0).astype(np.complex128) - want))) <= TOL[dtype]
 
 
+@pytest.mark.parametrize("kind", ["plain", "mixed"])
+@pytest.mark.parametrize("n,min_run", [(21, 6), (23, 6), (23, 8)])
+@pytest.mark.parametrize("split,order", [(1, 0), (2, 0), (0, 1), (0, 2), (2, 2)])
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_span_passes_split_and_order(kind, n, min_run, split, order, dtype):
+    # other deals of the high-bit gates to the strided span passes (knob span_split:
+    # 1 round robin, every strided pass holding bits from the whole high range, none
+    # of them neighbours; 2 the larger blocks on the higher bits) and other orders of
+    # the strided passes (knob span_order: 1 from the lowest bits up, 2 from the
+    # highest down; the window before the batch rides on the first); complex64 at 23
+    # qubits and run 2^8: two passes of 5 gates; complex128: three passes of 4, 4, 3
+    gates = _span_case(n, kind, 500 + n)
+    want = _span_oracle_state(n, kind)
+    s = zx.ZXH(n, dtype=dtype)
+    s.set_param("span_min_run", min_run)
+    s.set_param("span_split", split)
+    s.set_param("span_order", order)
+    s.push_gates(gates)
+    s.execute()
+    assert float(np.max(np.abs(s.get_state(0).astype(np.complex128) - want))) <= TOL[dtype]
+
+
 @pytest.mark.parametrize("dtype", DTYPES)
 def test_span_pass_through_apply_round_trip(dtype):
     # a 26-qubit U3 layer and its inverse through apply(): back to |+...+> (the

@@ -762,6 +762,8 @@ int zxh_set_param(zxh_sim *s, const char *name, int value)
         {"span", &s->pp.span, 0, 1},
         {"span_min_run", &s->pp.span_min_run, 3, 8},
         {"span_land", &s->pp.span_land, 0, 1},
+        {"span_split", &s->pp.span_split, 0, 2},
+        {"span_order", &s->pp.span_order, 0, 2},
         {"diag_chunk_bits", &s->pp.diag_chunk_bits, -1, 8},
         {"grow", &s->pp.grow, 0, 1},
         {"grow_regs", &s->pp.grow_regs, 1, 4},

@@ -80,6 +80,12 @@ struct PlanParams {
     int span_min_run = 3;       // log2 of the shortest run of contiguous amplitudes a strided span pass
                                 // reads (3..8: 64 B .. 2 KiB complex64, 128 B .. 4 KiB complex128)
                                 // (3: a 32-qubit layer in 3 passes, 54.7 ms on B200, vs 4 passes, 57.2 ms)
+    int span_split = 0;         // how the high-bit gates are dealt to the strided span passes: 0 in blocks of
+                                // neighbouring bits, the larger blocks on the lower bits; 1 round robin (every
+                                // pass gets bits from the whole range); 2 blocks, the larger on the higher bits
+    int span_order = 0;         // order of the strided span passes (the first one carries the window before the
+                                // batch): 0 from the lowest bits up, but the first pass that runs two layouts
+                                // (not three) moved to the front; 1 from the lowest bits up; 2 from the highest down
 };
 
 // General strided pass shape (grow.cu): fixed low bits and register coordinates.
