@@ -124,9 +124,20 @@ int zxh_execute(zxh_sim *sim);
 /* Applies count more gates to the current state, continuing from where the last
  * zxh_execute / zxh_apply left the state and the affine map, without recording
  * them. Gates that would enlarge the state beyond the size chosen at the last
- * zxh_execute return ZXH_ERR_LIMIT. No counterpart in the reference (its
- * execute() always restarts from |0...0>, zxh.cpp:329-338). */
+ * zxh_execute return ZXH_ERR_LIMIT. The phases that U3 gates leave after their
+ * rotations (the real split's P(b) and global phase of the batch's last U3 gates)
+ * are carried to the next zxh_apply, which takes them into the window before its
+ * own first pass, so a circuit applied layer by layer costs what it costs in one
+ * zxh_execute; every call that reads the state (zxh_measure, zxh_get_state*,
+ * zxh_state_view, zxh_expectation) and zxh_flush apply them first. No counterpart
+ * in the reference (its execute() always restarts from |0...0>,
+ * zxh.cpp:329-338). */
 int zxh_apply(zxh_sim *sim, const zxh_gate *gates, size_t count);
+
+/* Applies the phases the last zxh_apply / zxh_apply_async carried over (one
+ * diagonal pass; nothing when there are none) and returns once the device is
+ * done; zxh_last_stats reports that pass. No counterpart in the reference. */
+int zxh_flush(zxh_sim *sim);
 
 /* zxh_apply without waiting: plans the batch on the host, queues its upload
  * (from one of two pinned program slots), its passes and the read-back of its
@@ -181,7 +192,9 @@ int zxh_required_M(const zxh_sim *sim, size_t *out);
 int zxh_num_qubits(const zxh_sim *sim, size_t *out);
 
 /* Device view of the real-address state after zxh_execute: data pointer, number
- * of real address bits m (2^m elements), bytes per element, global phase. */
+ * of real address bits m (2^m elements), bytes per element, global phase. Applies
+ * the phases carried over by the last zxh_apply first (see zxh_apply); after a
+ * later zxh_apply, call it again before reading the state. */
 int zxh_state_view(zxh_sim *sim, void **data, size_t *m_bits, size_t *elem_bytes, double *global_phase_re,
                    double *global_phase_im);
 

@@ -78,6 +78,7 @@ _sig("zxh_execute", [_P])
 _sig("zxh_apply", [_P, _P, _SZ])
 _sig("zxh_apply_async", [_P, _P, _SZ])
 _sig("zxh_sync", [_P])
+_sig("zxh_flush", [_P])
 _sig("zxh_measure", [_P, _SZ])
 _sig("zxh_get_results", [_P, _P, _SZ])
 _sig("zxh_measured_count", [_P, ctypes.POINTER(_SZ)])
@@ -304,6 +305,11 @@ class ZXH:
     def sync(self) -> None:
         """Waits for the apply_async work in flight."""
         self._ck(_lib.zxh_sync(self._h))
+
+    def flush(self) -> None:
+        """Applies the phases the last apply carried over (every call that reads the
+        state does so itself); last_stats() then reports that pass."""
+        self._ck(_lib.zxh_flush(self._h))
 
     def measure(self, shots: int) -> None:
         self._ck(_lib.zxh_measure(self._h, int(shots)))

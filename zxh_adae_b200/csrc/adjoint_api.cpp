@@ -448,6 +448,7 @@ int zxh_expectation(zxh_sim *s, const zxh_term *terms, size_t nterms, double *va
     if (!value) return fail(s, ZXH_ERR_ARG, "value is null");
     if (!s->executed) return fail(s, ZXH_ERR_STATE, "expectation requires execute() first");
     if (int rc = use_device(s)) return rc;
+    if (int rc = flush_pending(s)) return rc;
     std::vector<TermDev> dt;
     if (int rc = compile_terms(s, terms, nterms, s->ws.map, s->ws.m, true, dt)) return rc;
     const AdjLayout L(0, dt.size());
@@ -487,6 +488,7 @@ int zxh_adjoint_gradient(zxh_sim *s, const zxh_term *terms, size_t nterms, size_
     if (nterms > zxh::kMaxTerms)
         return fail(s, ZXH_ERR_LIMIT, "at most " + std::to_string(zxh::kMaxTerms) + " observable terms");
     if (int rc = use_device(s)) return rc;
+    s->pending.clear();  // the forward segments rebuild the state from |0...0>
     const int N = int(s->n);
 
     // forward segments

@@ -148,6 +148,18 @@ int run_plan(zxh_sim *s, const zxh::Plan &pl)
     return ZXH_OK;
 }
 
+int flush_pending(zxh_sim *s)
+{
+    if (s->pending.empty()) return ZXH_OK;
+    zxh::Plan pl;
+    std::string err;
+    if (int rc = zxh::plan(std::vector<zxh::Op>(), s->elem_bytes, s->pp, s->ws, pl, err, &s->pending, nullptr))
+        return fail(s, rc, err);
+    if (int rc = run_plan(s, pl)) return rc;
+    s->pending.clear();
+    return ZXH_OK;
+}
+
 void column_tables(const zxh::AffineMap &A, uint64_t tab[8][256])
 {
     uint64_t col[64] = {0};
@@ -375,6 +387,7 @@ int zxh_execute(zxh_sim *s)
     s->M = M;
     s->executed = false;
     s->measured = 0;
+    s->pending.clear();  // the state restarts from |0...0>
     zxh::WalkState &ws = s->ws;
     ws.map.reset(int(s->n));
     ws.m = 0;
@@ -398,9 +411,11 @@ int zxh_execute(zxh_sim *s)
     return ZXH_OK;
 }
 
-// Host planning of one batch (zxh_apply and zxh_apply_async): the plan and the
-// walk state after it.
-static int plan_batch(zxh_sim *s, const zxh_gate *gates, size_t count, zxh::Plan &pl, zxh::WalkState &ws)
+// Host planning of one batch (zxh_apply and zxh_apply_async): the plan, the walk
+// state after it and the phases it leaves over. The phases the previous batch left
+// over ride in this batch's first window (or run first, on their own).
+static int plan_batch(zxh_sim *s, const zxh_gate *gates, size_t count, zxh::Plan &pl, zxh::WalkState &ws,
+                      std::vector<zxh::DiagTerm> &left)
 {
     std::vector<Gate> tmp;
     for (size_t i = 0; i < count; i++)
@@ -410,7 +425,7 @@ static int plan_batch(zxh_sim *s, const zxh_gate *gates, size_t count, zxh::Plan
     std::vector<zxh::Op> ops;
     std::string err;
     if (int rc = zxh::walk(tmp.data(), tmp.size(), s->disable_x, s->M, ws, ops, err)) return fail(s, rc, err);
-    if (int rc = zxh::plan(ops, s->elem_bytes, s->pp, start, pl, err)) return fail(s, rc, err);
+    if (int rc = zxh::plan(ops, s->elem_bytes, s->pp, start, pl, err, &s->pending, &left)) return fail(s, rc, err);
     return ZXH_OK;
 }
 
@@ -422,9 +437,11 @@ int zxh_apply(zxh_sim *s, const zxh_gate *gates, size_t count)
     if (int rc = use_device(s)) return rc;
     zxh::Plan pl;
     zxh::WalkState ws;
-    if (int rc = plan_batch(s, gates, count, pl, ws)) return rc;
+    std::vector<zxh::DiagTerm> left;
+    if (int rc = plan_batch(s, gates, count, pl, ws, left)) return rc;
     if (int rc = run_plan(s, pl)) return rc;
     s->ws = ws;
+    s->pending = std::move(left);
     s->measured = 0;
     return ZXH_OK;
 }
@@ -437,7 +454,8 @@ int zxh_apply_async(zxh_sim *s, const zxh_gate *gates, size_t count)
     CK(s, cudaSetDevice(s->device), "cudaSetDevice");
     zxh::Plan pl;
     zxh::WalkState ws;
-    if (int rc = plan_batch(s, gates, count, pl, ws)) return rc;  // overlaps the steps in flight
+    std::vector<zxh::DiagTerm> left;
+    if (int rc = plan_batch(s, gates, count, pl, ws, left)) return rc;  // overlaps the steps in flight
     const size_t bytes = std::max<size_t>(pl.blob.size(), 16);
     if (bytes > s->async_cap || bytes > s->blob_cap) {
         // growing a buffer that queued work may still read: settle first
@@ -478,8 +496,20 @@ int zxh_apply_async(zxh_sim *s, const zxh_gate *gates, size_t count)
         if (p.kind != zxh::Pass::PRODUCT) s->stat_passes++;
     s->last_ms = 0.0f;
     s->ws = ws;
+    s->pending = std::move(left);
     s->measured = 0;
     return ZXH_OK;
+}
+
+int zxh_flush(zxh_sim *s)
+{
+    if (!s) return ZXH_ERR_ARG;
+    if (!s->executed) return fail(s, ZXH_ERR_STATE, "zxh_flush requires zxh_execute first");
+    if (int rc = use_device(s)) return rc;
+    s->stat_kernels = 0;
+    s->stat_passes = 0;
+    s->last_ms = 0.0f;
+    return flush_pending(s);
 }
 
 int zxh_sync(zxh_sim *s)
@@ -504,6 +534,7 @@ int zxh_measure(zxh_sim *s, size_t shots)
     if (!s->executed) return fail(s, ZXH_ERR_STATE, "measure requires execute() to be called first");
     if (shots > (size_t(1) << 40)) return fail(s, ZXH_ERR_LIMIT, "too many shots");
     if (int rc = use_device(s)) return rc;
+    if (int rc = flush_pending(s)) return rc;
     const uint64_t base = s->use_seed ? s->seed : uint64_t(std::random_device{}());  // measure_cuda.cu:111-116
     const uint64_t stream_seed = zxh::mix_seed_host(base, 0);                        // measure_cuda.cu:1033
     const int m = s->ws.m;
@@ -638,6 +669,7 @@ int zxh_get_state(zxh_sim *s, void *out, size_t out_elems, int order)
     const uint64_t nv = 1ULL << s->n;
     if (out_elems < nv) return fail(s, ZXH_ERR_ARG, "output buffer holds fewer than 2^n amplitudes");
     if (int rc = use_device(s)) return rc;
+    if (int rc = flush_pending(s)) return rc;
     const size_t bytes = size_t(nv) * size_t(s->elem_bytes);
     if (int rc = ensure_dev(s, &s->d_out, s->out_cap, bytes, "cudaMalloc(get_state)")) return rc;
     if (int rc = state_to_device(s, s->d_out, order)) return rc;
@@ -654,6 +686,7 @@ int zxh_get_state_device(zxh_sim *s, void *out_device, size_t out_elems, int ord
     if (s->n > 40) return fail(s, ZXH_ERR_LIMIT, "get_state export needs fewer than 41 qubits");
     if (out_elems < (1ULL << s->n)) return fail(s, ZXH_ERR_ARG, "output buffer holds fewer than 2^n amplitudes");
     if (int rc = use_device(s)) return rc;
+    if (int rc = flush_pending(s)) return rc;
     if (int rc = state_to_device(s, out_device, order)) return rc;
     CK(s, cudaStreamSynchronize(s->stream), "get_state");
     return ZXH_OK;
@@ -677,6 +710,10 @@ int zxh_state_view(zxh_sim *s, void **data, size_t *m_bits, size_t *elem_bytes, 
 {
     if (!s) return ZXH_ERR_ARG;
     if (!s->executed) return fail(s, ZXH_ERR_STATE, "state_view requires execute() first");
+    if (!s->pending.empty()) {  // the state as it stands, with the phases the last apply left over
+        if (int rc = use_device(s)) return rc;
+        if (int rc = flush_pending(s)) return rc;
+    }
     if (data) *data = s->d_state;
     if (m_bits) *m_bits = size_t(s->ws.m);
     if (elem_bytes) *elem_bytes = size_t(s->elem_bytes);

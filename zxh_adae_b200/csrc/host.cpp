@@ -887,7 +887,7 @@ std::vector<Op> split_windows(const std::vector<Op> &ops, size_t max_general)
 }
 
 int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, const WalkState &start, Plan &out,
-         std::string &err)
+         std::string &err, const std::vector<DiagTerm> *carry_in, std::vector<DiagTerm> *carry_out)
 {
     out.clear();
     // windows with more than 32 general terms are split; otherwise the ops are used as given
@@ -1016,6 +1016,7 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
     const std::vector<DiagTerm> *held = nullptr;  // window waiting for the next tile pass
     std::deque<std::vector<DiagTerm>> owned;       // windows the planner builds (stable addresses)
     std::vector<DiagTerm> carry;                   // phases split off the last U3 batch, due after it
+    if (carry_in) carry = *carry_in;               // (or left over by the previous plan)
 
     auto emit_tile = [&](int mm, int c, const std::vector<int> &dirs, const std::vector<const U3Op *> &u3s,
                          const std::vector<DiagTerm> *pro) {
@@ -1264,6 +1265,12 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
                 carry.clear();
             } else if (op.kind == Op::U3BATCH && fast_ok(op) && !held && op.m == m) {
                 owned.push_back(carry);  // the next batch's prologue
+                held = &owned.back();
+                carry.clear();
+            } else if (op.kind == Op::U3BATCH && !held && last_tile_pass < 0) {
+                // phases left over by the previous plan and no pass of this one yet to
+                // take them as an epilogue: a window before the batch's first pass
+                owned.push_back(carry);
                 held = &owned.back();
                 carry.clear();
             } else {
@@ -1661,6 +1668,10 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
         }
         held = nullptr;
         m = mm;
+    }
+    if (carry_out) {
+        *carry_out = carry;
+        carry.clear();
     }
     flush_carry();
     if (held) standalone_diag(m, *held);

@@ -159,7 +159,13 @@ int row_reg_bits(int elem_bytes, int wide);
 int row_fixed_bits(int elem_bytes, int wide);
 bool row_low_ok(int elem_bytes, int wide);  // the shape's lane bits can swap with its rows (the low pass)
 
+// carry_in: phases due on the state before the ops (left over by the previous
+// plan; real-bit selectors, so the affine map's changes since do not touch them);
+// carry_out: if given, the phases split off the last U3 batch are returned there
+// instead of being applied (the caller applies them later, or hands them to the
+// next plan, whose first U3 batch takes them into its own window).
 int plan(const std::vector<Op> &ops, int elem_bytes, const PlanParams &pp, const WalkState &start, Plan &out,
-         std::string &err);
+         std::string &err, const std::vector<DiagTerm> *carry_in = nullptr,
+         std::vector<DiagTerm> *carry_out = nullptr);
 
 }  // namespace zxh

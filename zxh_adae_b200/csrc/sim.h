@@ -28,6 +28,11 @@ struct zxh_sim {
     int M = 0;
     zxh::WalkState ws;
     bool executed = false;
+    // phases due on the state that the last zxh_apply / zxh_apply_async left over
+    // (the real split's P(b) and global phase after its last U3 batch): the next
+    // apply takes them into its first window; every call that reads the state
+    // applies them first (flush_pending)
+    std::vector<zxh::DiagTerm> pending;
 
     uint8_t *d_blob = nullptr;
     size_t blob_cap = 0;
@@ -91,6 +96,9 @@ int ensure_dev(zxh_sim *s, void **p, size_t &cap, size_t need, const char *what)
 int lower(zxh_sim *s, const zxh_gate &g, std::vector<Gate> &out);
 // Uploads the plan, runs it on the handle's stream and waits for the device.
 int run_plan(zxh_sim *s, const zxh::Plan &pl);
+// Applies the phases a previous apply left over (sim.pending), if any: one
+// diagonal pass, run like a plan (its device time in the handle's stats).
+int flush_pending(zxh_sim *s);
 
 }  // namespace api
 }  // namespace zxh
