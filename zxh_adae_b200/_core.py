@@ -292,7 +292,10 @@ class ZXH:
         self._ck(_lib.zxh_execute(self._h))
 
     def apply(self, gates) -> None:
-        """Applies more gates to the current state without recording them."""
+        """Applies more gates to the current state without recording them. The
+        phases left after the batch's last U3 rotations ride in the next apply's
+        first window; reads of the state (get_state, state_view, measure,
+        expectation) and flush() apply them first."""
         rec = as_records(gates)
         self._ck(_lib.zxh_apply(self._h, rec.ctypes.data, len(rec)))
 
