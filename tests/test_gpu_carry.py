@@ -143,3 +143,31 @@ def test_flush_runs_one_pass_then_nothing(dtype):
     assert s.last_stats()[:2] == (0, 0)
     o = oracle_state(n, [wl.h_all(n), wl.u3_layer(n, seed=8)])
     assert err(s, o) <= TOL[dtype]
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_carried_phases_across_plan_knobs(dtype):
+    # the phases one apply leaves are taken by the next whatever pass kind it plans:
+    # span passes, register-row passes (span = 0), passes without the real split
+    # (nothing carried further), the register form of the span pass, general
+    # strided passes after a CX chain
+    n = 16
+    head = wl.h_all(n)
+    layers = [wl.u3_layer(n, seed=60 + k) for k in range(6)]
+    chain = zx.as_records([(zx._core.CX, i, i + 1) for i in range(n - 1)])
+    s = zx.ZXH(n, dtype=dtype)
+    s.push_gates(head)
+    s.execute()
+    s.apply(layers[0])
+    s.set_param("span", 0)
+    s.apply(layers[1])
+    s.set_param("real_split", 0)
+    s.apply(layers[2])
+    s.set_param("real_split", 1)
+    s.set_param("span", 1)
+    s.set_param("span_land", 0)
+    s.apply(layers[3])
+    s.set_param("span_land", 1)
+    s.apply(layers[4])
+    s.apply(np.concatenate([chain, layers[5]]))
+    assert err(s, oracle_state(n, [head] + layers[:5] + [chain, layers[5]])) <= TOL[dtype]
