@@ -367,7 +367,11 @@ int zxh_optimize_gates(size_t n, int level, const zxh_gate *gates, size_t count,
  * round robin; 2: blocks, the larger on the higher bits), span_order (0: the
  * strided span passes from the lowest bits up, but the first one that runs two
  * layouts moved to the front, so the window before the batch rides on it; 1:
- * from the lowest bits up; 2: from the highest down). Takes effect at the next zxh_execute / zxh_apply. No
+ * from the lowest bits up; 2: from the highest down), span_mixed (1: a U3 batch
+ * mixing gates with single-bit pair deltas (at least 8) and gates whose deltas
+ * span several bits runs the single-bit ones as span passes first and the rest
+ * as general strided passes; 0: all as general strided passes). Takes effect at
+ * the next zxh_execute / zxh_apply. No
  * counterpart in the reference. */
 int zxh_set_param(zxh_sim *sim, const char *name, int value);
 

@@ -572,6 +572,38 @@ def test_span_passes_split_and_order(kind, n, min_run, split, order, dtype):
     assert float(np.max(np.abs(s.get_state(0).astype(np.complex128) - want))) <= TOL[dtype]
 
 
+def _mixed_case(n, seed):
+    # CX gates from a few qubits first: those qubits' U3 gates then have pair
+    # deltas over two real bits, the rest single-bit deltas, in the same batch
+    rng = np.random.default_rng(seed)
+    recs = [(zx._core.H, 0, q) for q in range(n)]
+    recs += [(zx._core.CX, int(c), int(c) + 1) for c in rng.choice(n - 1, 3, replace=False)]
+    for layer in range(2):
+        recs += [(zx._core.U3, 0, q, *rng.uniform(0, 2 * np.pi, 3)) for q in range(n)]
+        recs += [(zx._core.CP, i, i + 1, float(rng.uniform(0, 2 * np.pi))) for i in range(n - 1)]
+    return zx.as_records(recs)
+
+
+@pytest.mark.parametrize("n", [14, 16, 19])
+@pytest.mark.parametrize("mixed", [0, 1])
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_u3_batches_mixing_single_and_multi_bit_deltas(n, mixed, dtype):
+    # knob span_mixed: the single-bit gates of a mixed batch run as span passes
+    # first, the others as general strided passes after them (1), or the whole
+    # batch as general strided passes (0)
+    gates = _mixed_case(n, 900 + n)
+    st = plan_stats(n, gates, dtype=dtype)
+    assert st["span"] > 0 and st["grow"] > 0
+    o = Oracle(n)
+    o.push(gates)
+    o.execute()
+    s = zx.ZXH(n, dtype=dtype)
+    s.set_param("span_mixed", mixed)
+    s.push_gates(gates)
+    s.execute()
+    assert max_err(s, o) <= TOL[dtype]
+
+
 @pytest.mark.parametrize("dtype", DTYPES)
 def test_span_pass_through_apply_round_trip(dtype):
     # a 26-qubit U3 layer and its inverse through apply(): back to |+...+> (the

@@ -801,6 +801,7 @@ int zxh_set_param(zxh_sim *s, const char *name, int value)
         {"span_land", &s->pp.span_land, 0, 1},
         {"span_split", &s->pp.span_split, 0, 2},
         {"span_order", &s->pp.span_order, 0, 2},
+        {"span_mixed", &s->pp.span_mixed, 0, 1},
         {"diag_chunk_bits", &s->pp.diag_chunk_bits, -1, 8},
         {"grow", &s->pp.grow, 0, 1},
         {"grow_regs", &s->pp.grow_regs, 1, 4},

@@ -905,7 +905,42 @@ int plan(const std::vector<Op> &ops_in, int elem_bytes, const PlanParams &pp, co
     need_split = need_split && !pp.walsh;
     std::vector<Op> split_ops;
     if (need_split) split_ops = split_windows(ops_in, 32);
-    const std::vector<Op> &ops = need_split ? split_ops : ops_in;
+    const std::vector<Op> *opsp = need_split ? &split_ops : &ops_in;
+    // A U3 batch that mixes gates whose pair delta is their own selector bit with
+    // gates whose deltas span several bits (after CX transport) is split in two:
+    // its gates act on distinct qubits and commute, so the single-bit ones run
+    // first as span passes and the rest as general strided passes, instead of all
+    // of them filling general strided passes.
+    std::vector<Op> mixed_ops;
+    if (pp.span && pp.real_split && !pp.grow_only && pp.span_mixed) {
+        auto single = [](const U3Op &u) {
+            return !u.has_ctrl && u.delta && !(u.delta & (u.delta - 1)) && u.sel.alpha == u.delta;
+        };
+        auto mixed = [&](const Op &op) {
+            if (op.kind != Op::U3BATCH || op.m < span_tile_bits(elem_bytes)) return false;
+            size_t nf = 0;
+            for (const U3Op &u : op.u3) nf += single(u) ? 1 : 0;
+            return nf >= 8 && nf < op.u3.size();
+        };
+        bool any = false;
+        for (const Op &op : *opsp) any = any || mixed(op);
+        if (any) {
+            for (const Op &op : *opsp) {
+                if (!mixed(op)) {
+                    mixed_ops.push_back(op);
+                    continue;
+                }
+                Op a = op, b = op;
+                a.u3.clear();
+                b.u3.clear();
+                for (const U3Op &u : op.u3) (single(u) ? a : b).u3.push_back(u);
+                mixed_ops.push_back(std::move(a));
+                mixed_ops.push_back(std::move(b));
+            }
+            opsp = &mixed_ops;
+        }
+    }
+    const std::vector<Op> &ops = *opsp;
     size_t i = 0;
     int m = start.m;
 

@@ -83,6 +83,8 @@ struct PlanParams {
     int span_split = 0;         // how the high-bit gates are dealt to the strided span passes: 0 in blocks of
                                 // neighbouring bits, the larger blocks on the lower bits; 1 round robin (every
                                 // pass gets bits from the whole range); 2 blocks, the larger on the higher bits
+    int span_mixed = 1;         // 1: a U3 batch mixing single-bit and multi-bit pair deltas (at least 8
+                                // single-bit gates) runs the single-bit gates as span passes first
     int span_order = 0;         // order of the strided span passes (the first one carries the window before the
                                 // batch): 0 from the lowest bits up, but the first pass that runs two layouts
                                 // (not three) moved to the front; 1 from the lowest bits up; 2 from the highest down
